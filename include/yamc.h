@@ -1,0 +1,177 @@
+/*
+ * yamc.h -- C ABI of the B200 engine for YAMC's per-trial-move energy path.
+ *
+ * The engine replaces the body of the reference's MC module (MC.f90): initmc,
+ * movemc and mc_total_energy, and the run_mc loop that calls movemc
+ * (runmc.f90:178-334).  A Fortran host binds these entry points through
+ * ISO_C_BINDING (the interface module is given in INTEGRATION.md); the
+ * Python package yamc_b200 binds them through ctypes.
+ *
+ * Conventions (as in the reference): coordinates in box units (-0.5..0.5),
+ * energies in kT, molecule numbers 1-based, atoms stored molecule by molecule.
+ * Every function returns an int status: 0 = OK, negative = error (below).
+ * A hard-core overlap is not an error; it is reported through *overlap or the
+ * per-move flags, exactly like EwaldSumRealSpace_calc's logical overlap.
+ * No function aborts the process or throws across the ABI.
+ */
+#ifndef YAMC_H
+#define YAMC_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes; -1..-5 mirror ERROR_IO, ERROR_LIMITS, ERROR_PARAMETER,
+   ERROR_INITIALIZATION, ERROR_WRONG_FUNCTION of error.f90:47-51 */
+#define YAMC_OK 0
+#define YAMC_EIO (-1)
+#define YAMC_ELIMITS (-2)
+#define YAMC_EPARAMETER (-3)
+#define YAMC_EINIT (-4)
+#define YAMC_EWRONG_FUNCTION (-5)
+#define YAMC_ECUDA (-10)
+#define YAMC_ETIMEOUT (-11)
+#define YAMC_ERNG_EXHAUSTED (-12)
+#define YAMC_ENAN (-13)
+#define YAMC_EOVERLAP_INIT (-14)
+
+/* precision of the device arithmetic */
+#define YAMC_FP64 0   /* plain method: every operation in FP64 */
+#define YAMC_MIXED 1  /* FP32 pair/erfc/phase arithmetic, FP64 rho(k), sums and Metropolis */
+
+/* Simulation parameters: the module variables of parameters.f90:11-86.
+   The primary block is what parameters.prm sets; yamc_params_recalc fills
+   the derived block exactly as Parameters_recalc (parameters.f90:355-413). */
+typedef struct {
+    /* primary */
+    double sr, sk, alphaL, temp, external_permutivity, BoxLength, density;
+    double dr_a, d_angle_degree, xlambda_c, xlambda_f, pressure;
+    double pressure_step_multiplier, max_volume_scaling;
+    double n_store_traj_interval, n_store_energy_interval;
+    int32_t max_cycle, random_seed;
+    int32_t input_nbytes_xyz, input_nbytes_ang, output_nbytes_xyz, output_nbytes_ang;
+    /* derived (Parameters_recalc) */
+    double alpha; /* alpha*L in box units (alphaL, defaulted to 2*sr) */
+    double rmax, rmax2, kT_kcal_mol, dbjr_a, dbjr, xclb;
+    double alpha_over_sqrt_pi, two_alpha_over_sqrt_pi, kext, minus_two_kext;
+    double dr, d_angle, log_max_volume_scaling, pressure_angstr_kT;
+    int32_t kmax;
+    int32_t precision; /* YAMC_FP64 or YAMC_MIXED (not a reference parameter) */
+} yamc_params;
+
+/* The system as the reference host holds it after MoleculeTable_fillAtomicData
+   (MoleculeTable.f90:584-705): per-atom arrays of length natom in molecule order. */
+typedef struct {
+    int32_t natom, nmol;
+    const double *x, *y, *z;        /* box units */
+    const double *charge;           /* e */
+    const double *sigma;            /* sigma / BoxLength */
+    const double *epsilon;          /* epsilon / kT */
+    const double *hard_core_angstr; /* hard-core diameter, Angstrom */
+    const double *mass;             /* atomic masses (centre of mass of a molecule) */
+    const int32_t *first_atom;      /* per molecule, 1-based, inclusive */
+    const int32_t *last_atom;       /* per molecule, 1-based, inclusive */
+    /* composition: molecule counts per species in composition order; the LJ
+       tails read them by LJ type (EwaldSumTails.f90:88) */
+    int32_t n_species;
+    const int32_t *mol_numbers;
+    /* molecule-choice weights of run_mc (init_freq, runmc.f90:25-67);
+       NULL = flat weights (no frequencies file) */
+    const double *move_weights;
+} yamc_system;
+
+typedef struct yamc_ctx yamc_ctx;
+
+/* One movemc record (optional output of yamc_run_chain). */
+typedef struct {
+    int32_t imol;    /* 1-based molecule tried */
+    int32_t flags;   /* bit0 accepted, bit1 hard-core overlap (rejected, no acceptance draw) */
+    int64_t cursor;  /* RNG cursor after the move */
+    double du_real, du_k_coul, du_k_lj, du_ext; /* movemc Steps 7, 10, 11, 11A */
+} yamc_move_record;
+
+/* ---- parameters (parameters.f90) ---- */
+/* Parameters_read (parameters.f90:266-305) on top of the defaults (:18-72). */
+int yamc_params_read(const char *path, const char *extra, yamc_params *p);
+/* Parameters_init (:323-352): BoxLength from density when zero, then recalc. */
+int yamc_params_init(yamc_params *p, int32_t nmol);
+/* Parameters_recalc (:355-413). */
+int yamc_params_recalc(yamc_params *p, double box_length);
+
+/* ---- host-side inputs: the reference readers, for hosts without their own ----
+   Composition_read_from_file + Molecule_read_from_file/centrate (composition.f90:84-142,
+   Molecule.f90:142-209), MoleculeTable_load_binary (MoleculeTable.f90:240-319) and
+   MoleculeTable_fillAtomicData (:584-705).  The returned yamc_system's arrays are
+   owned by the handle and freed by yamc_inputs_free. */
+typedef struct yamc_inputs yamc_inputs;
+int yamc_inputs_load(const char *parameters_path, const char *composition_path,
+                     const char *moltab_path, const char *extra, yamc_inputs **out);
+int yamc_inputs_get(const yamc_inputs *in, yamc_system *sys, yamc_params *p);
+int yamc_inputs_free(yamc_inputs *in);
+
+/* ---- engine lifecycle: initmc (MC.f90:587-602) ---- */
+/* Copies the system to the device, builds LJ types (LJTypes_fill), the k-grid
+   (FourierGrid_init), beta/beta6/beta12/beta_LJ (EwaldSumKSpace_initBeta[LJ]),
+   the tails (EwaldSumTails) and runs the full sums (mc_calc_total_sums). */
+int yamc_create(const yamc_system *sys, const yamc_params *p, int32_t device, yamc_ctx **out);
+int yamc_destroy(yamc_ctx *ctx);
+
+/* energy.dat columns 2..9 (runmc.f90:349-351): U_total, U_total_ew, U_total_lj,
+   uu_ew, uu_lj6, uu_lj12, E_k_coulomb, E_k_lj -- the incremental values
+   (mc_total_energy, MC.f90:681-698). */
+int yamc_energies(yamc_ctx *ctx, double e[8]);
+/* mc_calc_total_sums (MC.f90:477-585): recompute rho(k), the real-space sums and
+   mu from the current positions and return the same 8 numbers. */
+int yamc_full_sums(yamc_ctx *ctx, double e[8]);
+int yamc_get_positions(yamc_ctx *ctx, double *x, double *y, double *z);
+/* sizes: natom, nmol, nk (half-space k), nsigned (signed k entries), ntype */
+int yamc_sizes(yamc_ctx *ctx, int32_t out[5]);
+
+/* ---- per-move drop-in for the body of movemc (MC.f90:831-1322) ---- */
+/* Steps 0-4: old molecular force and torque of molecule imol (1-based). */
+int yamc_move_old(yamc_ctx *ctx, int32_t imol, double f[3], double tau[3]);
+/* Steps 6-12 for the proposed atom positions (box units, natom of the molecule):
+   du = {dU_real, dU_k_coulomb, dU_k_LJ, dU_ext}; *overlap as Step 6; new
+   molecular force and torque.  Must follow yamc_move_old for the same imol. */
+int yamc_move_eval(yamc_ctx *ctx, int32_t imol, const double *xn, const double *yn,
+                   const double *zn, double du[4], int32_t *overlap, double f[3], double tau[3]);
+/* Step 14: commit (accepted != 0) or drop the evaluated move. */
+int yamc_move_commit(yamc_ctx *ctx, int32_t accepted);
+
+/* ---- device-resident run_mc (runmc.f90:178-334, NVT single-molecule moves) ----
+   Runs n_moves movemc calls with the proposal, Metropolis test and commit on
+   the device, consuming the raw gfortran random_number stream rng[0..n_rng)
+   from *cursor (rand() redraw rule of random.f90:65-93 applied on the device).
+   Cycle structure, the per-cycle pressure draw and the energy.dat rows
+   (frame + 8 columns, at cycles where mod(n_mv_steps/nmol + n_vol_steps,
+   n_store_energy_interval) < 1e-10) follow run_mc.  rng is a HOST pointer; it
+   is copied to the device inside the call.  log (n_moves records) and rows
+   (9 doubles each, max_rows) are optional host outputs.  Returns
+   YAMC_ERNG_EXHAUSTED with *moves_done < n_moves when the buffer runs out; the
+   interrupted move is not committed and resumes exactly from *cursor. */
+int yamc_run_chain(yamc_ctx *ctx, const float *rng, int64_t n_rng, int64_t *cursor,
+                   int64_t n_moves, int64_t *moves_done, yamc_move_record *log,
+                   double *rows, int32_t max_rows, int32_t *n_rows);
+/* Same loop with the random stream and outputs already on the device (device
+   pointers); used by the benchmark to time the device-resident path. */
+int yamc_run_chain_device(yamc_ctx *ctx, const float *d_rng, int64_t n_rng, int64_t *cursor,
+                          int64_t n_moves, int64_t *moves_done, yamc_move_record *d_log,
+                          double *d_rows, int32_t max_rows, int32_t *n_rows);
+
+/* ---- launch configuration and diagnostics ---- */
+/* Threads per block and blocks per cluster of the persistent chain kernel
+   (0 = autotuned); takes effect on the next yamc_run_chain. */
+int yamc_set_launch(yamc_ctx *ctx, int32_t cluster_blocks, int32_t threads);
+int yamc_get_launch(yamc_ctx *ctx, int32_t out[4]);
+/* device time (ms) of the last run_chain kernel, measured with CUDA events on its stream */
+int yamc_last_kernel_ms(yamc_ctx *ctx, double *ms);
+const char *yamc_error_string(int status);
+const char *yamc_last_error_detail(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,170 @@
+"""GPU engine against the CPU oracle, through the C ABI, on the same inputs and the
+same gfortran random stream.
+
+Tolerances (the contract of the plain FP64 method): per-move dE components
+|dE_gpu - dE_ref| <= 1e-10 * max(|dE_ref|, 1 kT); identical molecule choices,
+overlap flags, accept/reject decisions and random-stream cursors; energy.dat
+totals within 1e-9 relative."""
+import numpy as np
+import pytest
+
+import pyoracle
+from yamc_b200 import api, rng as grng
+
+pytestmark = pytest.mark.gpu
+
+DU = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
+
+
+def close_du(a, b, tol=1e-10):
+    return np.abs(a - b) <= tol * np.maximum(np.abs(b), 1.0)
+
+
+def rel_close(a, b, tol):
+    return np.all(np.abs(a - b) <= tol * np.maximum(np.abs(b), 1.0))
+
+
+def compare_logs(glog, olog):
+    assert len(glog) == len(olog)
+    assert np.array_equal(glog["imol"], olog["imol"])
+    bad = np.nonzero(glog["flags"] != olog["flags"])[0]
+    assert bad.size == 0, f"first decision mismatch at move {bad[:1]}"
+    assert np.array_equal(glog["cursor"], olog["cursor"])
+    for k in DU:
+        ok = close_du(glog[k], olog[k])
+        assert ok.all(), (k, int(np.argmin(ok)), glog[k][~ok][:3], olog[k][~ok][:3])
+
+
+@pytest.mark.parametrize("which", ["tiny_files", "spce_files", "nacl_files"])
+def test_initial_full_sums(which, request):
+    files = request.getfixturevalue(which)
+    o = pyoracle.Oracle(files)
+    eng = api.Engine.from_files(files)
+    assert rel_close(eng.energies(), o.energies(), 1e-10)
+    assert (eng.nk, eng.ntype) == (o.nk, o.ntype)
+
+
+def _run_pair(files, n_moves, seed=12345, cluster=0, threads=0):
+    buf = grng.gfortran_stream(seed, 40 * n_moves + 10000)
+    o = pyoracle.Oracle(files)
+    olog, orows, ocur = o.run_mc(buf, n_moves)
+    eng = api.Engine.from_files(files)
+    if cluster or threads:
+        eng.set_launch(cluster, threads)
+    glog, grows, gcur, done, st = eng.run_chain(buf, n_moves)
+    assert st == 0 and done == n_moves
+    return o, olog, ocur, eng, glog, gcur
+
+
+
+
+@pytest.mark.parametrize("cluster", [1, 2, 4])
+def test_chain_matches_oracle_tiny(tiny_files, cluster):
+    o, olog, ocur, eng, glog, gcur = _run_pair(tiny_files, 3000, cluster=cluster)
+    compare_logs(glog, olog)
+    assert gcur == ocur
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+
+
+def test_chain_matches_oracle_spce256_1e5(spce_files):
+    """256 SPC/E: the identical accept/reject sequence over 1e5 moves."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(spce_files, 100096)
+    compare_logs(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+    # the incremental state still equals a full recompute on the device
+    assert rel_close(eng.full_sums(), o.full_sums(), 1e-9)
+
+
+def test_chain_matches_oracle_nacl(nacl_files):
+    o, olog, ocur, eng, glog, gcur = _run_pair(nacl_files, 6000)
+    compare_logs(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+
+
+def test_chain_force_biased(tiny_biased_files):
+    o, olog, ocur, eng, glog, gcur = _run_pair(tiny_biased_files, 2000, seed=77)
+    compare_logs(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+
+
+def test_energy_rows(tiny_files, tmp_path):
+    from yamc_b200 import formats, systems
+    spec = systems.small_spec()
+    spec.n_store_energy_interval = 2.0
+    files = systems.write_system(spec, str(tmp_path / "rows"))
+    buf = grng.gfortran_stream(5, 200000)
+    o = pyoracle.Oracle(files)
+    n = 10 * (spec.nmol)
+    _, orows, _ = o.run_mc(buf, n, max_rows=20)
+    eng = api.Engine.from_files(files)
+    _, grows, _, _, _ = eng.run_chain(buf, n, log=False, max_rows=20)
+    assert len(orows) == len(grows) == 5
+    assert np.array_equal(orows[:, 0], grows[:, 0])
+    assert rel_close(grows[:, 1:], orows[:, 1:], 1e-9)
+    path = str(tmp_path / "energy.dat")
+    formats.write_energy_rows(path, grows, append=False)
+    assert np.allclose(formats.read_energy_dat(path), grows, rtol=1e-15, atol=0)
+
+
+def test_rng_exhausted_resume_is_exact(tiny_files):
+    buf = grng.gfortran_stream(9, 200000)
+    ref = api.Engine.from_files(tiny_files)
+    rlog, _, rcur, rdone, rst = ref.run_chain(buf, 1500)
+    assert rst == 0
+    eng = api.Engine.from_files(tiny_files)
+    cut = int(rlog["cursor"][700]) + 5  # the buffer ends inside move 702
+    log1, _, cur1, done1, st1 = eng.run_chain(buf[:cut], 1500)
+    assert st1 == -12 and done1 == 701 and cur1 == rlog["cursor"][700]
+    log2, _, cur2, done2, st2 = eng.run_chain(buf, 1500 - done1, cursor=cur1)
+    assert st2 == 0 and cur2 == rcur
+    both = np.concatenate([log1, log2])
+    assert np.array_equal(both, rlog)
+    assert np.array_equal(eng.energies(), ref.energies())
+
+
+def test_chain_is_deterministic(spce_files):
+    buf = grng.gfortran_stream(4, 200000)
+    a = api.Engine.from_files(spce_files)
+    b = api.Engine.from_files(spce_files)
+    la = a.run_chain(buf, 3000)[0]
+    lb = b.run_chain(buf, 3000)[0]
+    assert np.array_equal(la, lb)
+    assert np.array_equal(a.energies(), b.energies())
+
+
+@pytest.mark.parametrize("which", ["tiny_files", "tiny_biased_files"])
+def test_per_move_api_matches_oracle(which, request):
+    """movemc driven from the host through yamc_move_old / _eval / _commit."""
+    files = request.getfixturevalue(which)
+    o = pyoracle.Oracle(files)
+    eng = api.Engine.from_files(files)
+    rng = np.random.default_rng(3)
+    f, l = o.mols()
+    L = o.params.BoxLength
+    for it in range(60):
+        imol = int(rng.integers(1, o.nmol + 1))
+        fo_g, to_g = eng.move_old(imol)
+        fo_o, to_o = o.move_old(imol)
+        assert rel_close(fo_g, fo_o, 1e-9) and rel_close(to_g, to_o, 1e-9)
+        x, y, z, *_ = o.atoms()
+        a, b = f[imol - 1] - 1, l[imol - 1]
+        ang = rng.uniform(-0.2, 0.2)
+        c, s = np.cos(ang), np.sin(ang)
+        cx, cy, cz = x[a], y[a], z[a]
+        d = rng.uniform(-0.2, 0.2, 3) / L
+        xn = cx + c * (x[a:b] - cx) - s * (y[a:b] - cy) + d[0]
+        yn = cy + s * (x[a:b] - cx) + c * (y[a:b] - cy) + d[1]
+        zn = z[a:b] + d[2]
+        du_g, ov_g, fn_g, tn_g = eng.move_eval(imol, xn, yn, zn)
+        du_o, ov_o, fn_o, tn_o = o.move_eval(xn, yn, zn)
+        assert ov_g == ov_o
+        if ov_o:
+            eng.move_commit(False)
+            continue
+        assert close_du(du_g, du_o).all(), (du_g, du_o)
+        assert rel_close(fn_g, fn_o, 1e-9) and rel_close(tn_g, tn_o, 1e-9)
+        acc = (du_o.sum() < 0.5)
+        eng.move_commit(acc)
+        if acc:
+            o.move_commit()
+    assert rel_close(eng.energies(), o.energies(), 1e-9)

@@ -1,0 +1,211 @@
+"""Host-side mirror of the reference's MC interface over the C ABI.
+
+``Engine`` stands where the reference's MC module is: ``initmc`` (construction),
+``mc_total_energy`` / ``mc_calc_total_sums`` (``energies`` / ``full_sums``), the
+body of ``movemc`` split like the C ABI (``move_old`` / ``move_eval`` /
+``move_commit``) and the device-resident ``run_mc`` loop (``run_chain``).
+All arithmetic happens in libyamc_b200.so on the GPU.
+"""
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+from typing import Optional
+
+import numpy as np
+
+from . import _lib
+from ._lib import MOVE_RECORD_DTYPE, YamcParams, YamcSystem, check
+
+ENERGY_COLUMNS = ("U_total", "U_total_ew", "U_total_lj", "uu_ew", "uu_lj6", "uu_lj12", "E_k_coulomb", "E_k_lj")
+
+
+def _dptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+
+
+def _iptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_int32))
+
+
+def read_parameters(path: str, extra: str = "") -> YamcParams:
+    """Parameters_read (defaults + parameters.prm + "k=v,..." overrides)."""
+    lib = _lib.load()
+    p = YamcParams()
+    check(lib.yamc_params_read(path.encode(), extra.encode(), ctypes.byref(p)), "yamc_params_read")
+    return p
+
+
+def params_init(p: YamcParams, nmol: int) -> YamcParams:
+    lib = _lib.load()
+    check(lib.yamc_params_init(ctypes.byref(p), int(nmol)), "yamc_params_init")
+    return p
+
+
+@dataclass
+class Inputs:
+    """A system as the reference host holds it after MoleculeTable_fillAtomicData."""
+    params: YamcParams
+    x: np.ndarray
+    y: np.ndarray
+    z: np.ndarray
+    charge: np.ndarray
+    sigma: np.ndarray
+    epsilon: np.ndarray
+    hard_core: np.ndarray
+    mass: np.ndarray
+    first_atom: np.ndarray
+    last_atom: np.ndarray
+    mol_numbers: np.ndarray
+    move_weights: Optional[np.ndarray] = None
+
+    @property
+    def natom(self) -> int:
+        return int(self.x.size)
+
+    @property
+    def nmol(self) -> int:
+        return int(self.first_atom.size)
+
+    def as_struct(self) -> YamcSystem:
+        s = YamcSystem()
+        s.natom = self.natom
+        s.nmol = self.nmol
+        s.x, s.y, s.z = _dptr(self.x), _dptr(self.y), _dptr(self.z)
+        s.charge, s.sigma, s.epsilon = _dptr(self.charge), _dptr(self.sigma), _dptr(self.epsilon)
+        s.hard_core_angstr, s.mass = _dptr(self.hard_core), _dptr(self.mass)
+        s.first_atom, s.last_atom = _iptr(self.first_atom), _iptr(self.last_atom)
+        s.n_species = int(self.mol_numbers.size)
+        s.mol_numbers = _iptr(self.mol_numbers)
+        s.move_weights = _dptr(self.move_weights) if self.move_weights is not None else None
+        return s
+
+
+def load_inputs(parameters: str, composition: str, moltab: str, extra: str = "") -> Inputs:
+    """The reference readers (composition, .mol, moltab, fillAtomicData) in the library."""
+    lib = _lib.load()
+    h = ctypes.c_void_p()
+    check(lib.yamc_inputs_load(parameters.encode(), composition.encode(), moltab.encode(), extra.encode(),
+                               ctypes.byref(h)), "yamc_inputs_load")
+    try:
+        s = YamcSystem()
+        p = YamcParams()
+        check(lib.yamc_inputs_get(h, ctypes.byref(s), ctypes.byref(p)), "yamc_inputs_get")
+        n, m = s.natom, s.nmol
+        cp = lambda ptr, k: np.ctypeslib.as_array(ptr, shape=(k,)).copy()
+        return Inputs(p, cp(s.x, n), cp(s.y, n), cp(s.z, n), cp(s.charge, n), cp(s.sigma, n), cp(s.epsilon, n),
+                      cp(s.hard_core_angstr, n), cp(s.mass, n), cp(s.first_atom, m).astype(np.int32),
+                      cp(s.last_atom, m).astype(np.int32), cp(s.mol_numbers, s.n_species).astype(np.int32))
+    finally:
+        lib.yamc_inputs_free(h)
+
+
+class Engine:
+    """initmc + movemc + run_mc of one system on one GPU."""
+
+    def __init__(self, inputs: Inputs, device: int = 0, precision: int = _lib.YAMC_FP64):
+        self.lib = _lib.load()
+        self.inputs = inputs
+        p = YamcParams()
+        ctypes.memmove(ctypes.byref(p), ctypes.byref(inputs.params), ctypes.sizeof(YamcParams))
+        p.precision = precision
+        self.params = p
+        self._sys = inputs.as_struct()
+        h = ctypes.c_void_p()
+        check(self.lib.yamc_create(ctypes.byref(self._sys), ctypes.byref(p), int(device), ctypes.byref(h)), "yamc_create")
+        self.h = h
+        sz = np.zeros(5, dtype=np.int32)
+        check(self.lib.yamc_sizes(self.h, _iptr(sz)), "yamc_sizes")
+        self.natom, self.nmol, self.nk, self.nsigned, self.ntype = (int(v) for v in sz)
+
+    @classmethod
+    def from_files(cls, files: dict, extra: str = "", device: int = 0, precision: int = _lib.YAMC_FP64) -> "Engine":
+        return cls(load_inputs(files["parameters"], files["composition"], files["moltab"], extra), device, precision)
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.yamc_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # -- energies ---------------------------------------------------------------------------
+    def energies(self) -> np.ndarray:
+        e = np.zeros(8)
+        check(self.lib.yamc_energies(self.h, _dptr(e)), "yamc_energies")
+        return e
+
+    def full_sums(self) -> np.ndarray:
+        e = np.zeros(8)
+        check(self.lib.yamc_full_sums(self.h, _dptr(e)), "yamc_full_sums")
+        return e
+
+    def positions(self):
+        x, y, z = (np.zeros(self.natom) for _ in range(3))
+        check(self.lib.yamc_get_positions(self.h, _dptr(x), _dptr(y), _dptr(z)), "yamc_get_positions")
+        return x, y, z
+
+    # -- per-move drop-in -------------------------------------------------------------------
+    def move_old(self, imol: int):
+        f, t = np.zeros(3), np.zeros(3)
+        check(self.lib.yamc_move_old(self.h, int(imol), _dptr(f), _dptr(t)), "yamc_move_old")
+        return f, t
+
+    def move_eval(self, imol: int, xn, yn, zn):
+        xn, yn, zn = (np.ascontiguousarray(v, dtype=np.float64) for v in (xn, yn, zn))
+        du, f, t = np.zeros(4), np.zeros(3), np.zeros(3)
+        ov = ctypes.c_int32(0)
+        check(self.lib.yamc_move_eval(self.h, int(imol), _dptr(xn), _dptr(yn), _dptr(zn), _dptr(du), ctypes.byref(ov),
+                                      _dptr(f), _dptr(t)), "yamc_move_eval")
+        return du, bool(ov.value), f, t
+
+    def move_commit(self, accepted: bool) -> None:
+        check(self.lib.yamc_move_commit(self.h, 1 if accepted else 0), "yamc_move_commit")
+
+    # -- device-resident run_mc -------------------------------------------------------------
+    def run_chain(self, rng: np.ndarray, n_moves: int, cursor: int = 0, log: bool = True, max_rows: int = 0):
+        """Runs n_moves movemc calls on the device.  Returns (log, rows, cursor, moves_done, status)."""
+        rng = np.ascontiguousarray(rng, dtype=np.float32)
+        cur = ctypes.c_int64(int(cursor))
+        done = ctypes.c_int64(0)
+        nrow = ctypes.c_int32(0)
+        rec = np.zeros(n_moves if log else 0, dtype=MOVE_RECORD_DTYPE)
+        rows = np.zeros((max(max_rows, 0), 9))
+        st = self.lib.yamc_run_chain(self.h, rng.ctypes.data, rng.size, ctypes.byref(cur), int(n_moves), ctypes.byref(done),
+                                     rec.ctypes.data if log else None, rows.ctypes.data if max_rows else None,
+                                     int(max_rows), ctypes.byref(nrow))
+        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+            check(st, "yamc_run_chain")
+        return rec[: done.value], rows[: nrow.value], cur.value, done.value, st
+
+    def run_chain_device(self, d_rng_ptr: int, n_rng: int, n_moves: int, cursor: int = 0, d_log_ptr: int = 0):
+        cur = ctypes.c_int64(int(cursor))
+        done = ctypes.c_int64(0)
+        nrow = ctypes.c_int32(0)
+        st = self.lib.yamc_run_chain_device(self.h, ctypes.c_void_p(d_rng_ptr), int(n_rng), ctypes.byref(cur), int(n_moves),
+                                            ctypes.byref(done), ctypes.c_void_p(d_log_ptr) if d_log_ptr else None, None, 0,
+                                            ctypes.byref(nrow))
+        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+            check(st, "yamc_run_chain_device")
+        return cur.value, done.value, st
+
+    # -- launch control ---------------------------------------------------------------------
+    def set_launch(self, cluster_blocks: int = 0, threads: int = 0) -> None:
+        check(self.lib.yamc_set_launch(self.h, int(cluster_blocks), int(threads)), "yamc_set_launch")
+
+    @property
+    def launch(self):
+        out = np.zeros(4, dtype=np.int32)
+        check(self.lib.yamc_get_launch(self.h, _iptr(out)), "yamc_get_launch")
+        return {"cluster_blocks": int(out[0]), "threads": int(out[1]), "entries_per_thread": int(out[2]),
+                "smem_bytes": int(out[3])}
+
+    @property
+    def last_kernel_ms(self) -> float:
+        v = ctypes.c_double(0)
+        check(self.lib.yamc_last_kernel_ms(self.h, ctypes.byref(v)), "yamc_last_kernel_ms")
+        return v.value

@@ -1,0 +1,433 @@
+// Device-side building blocks of the engine: the pair kernel of the real-space
+// Ewald sum, the k-space phase factors, the random stream consumer and the
+// move proposal / Metropolis test.  The proposal and acceptance code is
+// __host__ __device__ so the host-driven per-move API and the device-resident
+// chain draw identical proposals from the same stream.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace yamc {
+
+constexpr int kMaxA = 4;  // atoms per molecule handled on the device
+
+// ------------------------------------------------------------------ system view
+struct DevSys {
+    int N, M, S, nt, kmax, npair, freq_monotone, n_species;
+    double rmax2, alpha, xclb, taosp, kext, m2k, dr, d_angle, xlf, xlc, psm, n_store_energy_interval;
+    double4 *atom;         // x, y, z (box units), q
+    const int2 *meta;      // 0-based molecule, LJ type (0 = none)
+    const double *dhs;     // hard-core diameter / BoxLength
+    const double *mass;    // per atom
+    const int2 *mol;       // first atom (0-based), atoms in molecule
+    const int4 *kvec;      // kx, signed ky, signed kz, half-space index
+    const double *ebeta;   // Coulomb beta per signed entry (2x for kx>0 folded in)
+    const double *ebetalj; // npair x S
+    const int *pair_index; // nt*nt -> pair row
+    const double *lj_sig6, *lj_feps;  // nt*nt tables (offset (t1-1)*nt + t2-1)
+    double2 *rho;          // (1+nt) x S: Coulomb then one row per LJ type
+    const double *freq_beg, *freq_end;
+    double *scal;          // engine scalars, see Scal
+    long long *cnt;        // run_mc counters, see Cnt
+};
+
+// engine scalars (double)
+enum Scal {
+    SC_UU_EW = 0, SC_UU_LJ6, SC_UU_LJ12, SC_EK_C, SC_EK_LJ, SC_MU_X, SC_MU_Y, SC_MU_Z,
+    SC_TAIL_C, SC_TAIL_LJ6, SC_TAIL_LJ12, SC_UU_EW_INTRA, SC_UU_LJ6_INTRA, SC_UU_LJ12_INTRA,
+    SC_N_MV_STEPS, SC_N_MV_ACC, SC_N_VOL_STEPS, SC_COUNT
+};
+// run_mc counters (int64)
+enum Cnt { CN_ICYCLE = 0, CN_MOVE_IN_CYCLE, CN_COUNT };
+
+// ------------------------------------------------------------------ Functions.f90
+// erfc_Luc / erf_Luc (Functions.f90:116-171): Taylor series below 0.455,
+// Abramowitz & Stegun 7.1.26 up to 3, asymptotic series above.
+template <class R>
+__host__ __device__ inline R d_erfc_luc(R x, R x2, R ee2) {
+    const R P = R(0.3275911), A1 = R(0.254829592), A2 = R(-0.284496736), A3 = R(1.421413741),
+            A4 = R(-1.453152027), A5 = R(1.061405429), pi05 = R(1.7724538509055);
+    if (x < R(0.455)) return R(1) - R(2) / pi05 * x * (R(1) - x2 * (R(1) / R(3) - x2 * (R(0.1) - x2 * (R(1) / R(42) - x2 / R(216)))));
+    if (x > R(3)) return (R(1) - R(0.5) * (R(1) - R(1.5) / x2) / x2) / (pi05 * x) * ee2;
+    const R t = R(1) / (R(1) + P * x);
+    return t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ee2;
+}
+template <class R>
+__host__ __device__ inline R d_erf_luc(R x, R x2, R ee2) {
+    const R P = R(0.3275911), A1 = R(0.254829592), A2 = R(-0.284496736), A3 = R(1.421413741),
+            A4 = R(-1.453152027), A5 = R(1.061405429), pi05 = R(1.7724538509055);
+    if (x < R(0.455)) return R(2) / pi05 * x * (R(1) - x2 * (R(1) / R(3) - x2 * (R(0.1) - x2 * (R(1) / R(42) - x2 / R(216)))));
+    if (x > R(3)) return R(1) - (R(1) - R(0.5) * (R(1) - R(1.5) / x2) / x2) / (pi05 * x) * ee2;
+    const R t = R(1) / (R(1) + P * x);
+    return R(1) - t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ee2;
+}
+
+// shi_sans_exp_f (Functions.f90:225-289): Shi(x) exp(-x), force-bias acceptance
+__host__ __device__ inline double d_shi_sans_exp(double x) {
+    const double dx0 = 0.2;
+    double shi_f, x1;
+    if (x <= 1.0) {
+        const double x2 = x * x;
+        double fac = 1.0, xn = x;
+        shi_f = x;
+        for (int i = 1; i <= 4; ++i) {
+            const double di = 2.0 * i;
+            xn = xn * x2;
+            fac = fac * di * (di + 1.0);
+            shi_f = shi_f + xn / (di + 1.0) / fac;
+        }
+        return exp(-x) * shi_f;
+    }
+    if (x > 20.0) {
+        double som = 1.0, term = 1.0;
+        for (int i = 1; i <= 6; ++i) { term = term * i / x; som = som + term; }
+        return 1.0 / 2.0 / x * som;
+    }
+    if (x < 5.0) { x1 = 1.0; shi_f = 1.057250875; }
+    else if (x < 10.0) { x1 = 5.0; shi_f = 20.093211826; }
+    else if (x < 15.0) { x1 = 10.0; shi_f = 1246.11449; }
+    else { x1 = 15.0; shi_f = 117477.926; }
+    const int n = (int)((x - x1) / dx0 + 2);
+    const double dx = (x - x1) / (n - 1);
+    shi_f = shi_f + dx * sinh(x1) / x1 / 2.0 + dx * dx / 12.0 * (cosh(x1) / x1 - sinh(x1) / (x1 * x1));
+    double t = x1, s = 0.0;
+    for (int i = 2; i <= n; ++i) {
+        t = x1 + (double)(i - 1) * dx;
+        s = sinh(t);
+        shi_f = shi_f + dx * s / t;
+    }
+    shi_f = shi_f - dx * s / t / 2.0 - dx * dx / 12.0 * (cosh(t) / t - s / (t * t));
+    return exp(-x) * shi_f;
+}
+
+// ------------------------------------------------------------------ pair term
+// RealSumLocal (RealSumLocal.f90:63-168): one pair of the real-space sum.
+// ew = xclb qi qj erfc_Luc(a)/r (or -erf_Luc for an intra-molecular pair),
+// lj6/lj12 the dispersion-Ewald LJ terms, FR the radial force factor
+// (F_i += FR * (r_i - r_j)).
+template <class R>
+struct PairTerm { R ew, lj6, lj12, FR; };
+
+template <class R, bool WANT_FR>
+__host__ __device__ inline PairTerm<R> pair_term(R r2, R qq_xclb, bool lj, R sigma6, R four_eps, R alpha,
+                                                 R taosp, bool same_mol) {
+    PairTerm<R> t;
+    const R r = sqrt(r2);
+    const R a = alpha * r;
+    const R a2 = a * a;
+    const R e2 = exp(-a2);
+    const R erfc_a = same_mol ? -d_erf_luc<R>(a, a2, e2) : d_erfc_luc<R>(a, a2, e2);
+    t.ew = qq_xclb * erfc_a / r;
+    if (WANT_FR) t.FR = qq_xclb * (erfc_a / r + taosp * e2) / r2;
+    else t.FR = R(0);
+    t.lj6 = R(0); t.lj12 = R(0);
+    if (lj) {
+        const R r6 = r2 * r2 * r2;
+        const R so6 = sigma6 / r6;
+        const R C6 = R(1) + a2 * (R(1) + a2 / R(2));
+        const R a6 = a2 * a2 * a2;
+        const R C12 = C6 + a6 * (R(1) + a2 * (R(1) + a2 / R(5)) / R(4)) / R(6);
+        t.lj6 = four_eps * so6 * e2 * C6;
+        t.lj12 = four_eps * (so6 * so6) * e2 * C12;
+        if (WANT_FR)
+            t.FR = t.FR + four_eps * R(6) * so6 * e2 * (R(2) * so6 * (C12 + a6 * a6 / R(720)) - (C6 + a6 / R(6))) / r2;
+    }
+    return t;
+}
+
+// minimum image by one conditional wrap per axis (EwaldSumRealSpace.f90:394-401)
+template <class R>
+__host__ __device__ inline R min_image(R d) {
+    if (d > R(0.5)) d = d - R(1);
+    if (d < R(-0.5)) d = d + R(1);
+    return d;
+}
+
+// ------------------------------------------------------------------ k-space phase
+// q * (cos, sin)(2 pi (x kx + y ky + z kz)) for a signed entry from per-axis
+// tables T[m] = (cos 2 pi m u, sin 2 pi m u), with SinCosKR_fill's arithmetic
+// (SumSinCosKR.f90:362-448): q cos(X)cos(Y) -/+ q sin(X)sin(Y), then the z factor.
+template <class R, class T2>
+__host__ __device__ inline void entry_phase(const T2 *tx, const T2 *ty, const T2 *tz, int kx, int ky, int kz, R q,
+                                            R &c, R &s) {
+    const R cx = tx[kx].x, sx = tx[kx].y;
+    const int aky = ky < 0 ? -ky : ky, akz = kz < 0 ? -kz : kz;
+    const R cy = ty[aky].x, sy = ky < 0 ? -ty[aky].y : ty[aky].y;
+    const R cz = tz[akz].x, sz = kz < 0 ? -tz[akz].y : tz[akz].y;
+    const R qcc = q * cx * cy, qss = q * sx * sy, qsc = q * sx * cy, qcs = q * cx * sy;
+    const R qc = qcc - qss, qs = qsc + qcs;
+    const R c1 = qc * cz, s1 = qs * sz, s2 = qs * cz, c2 = qc * sz;
+    c = c1 - s1;
+    s = s2 + c2;
+}
+
+// ------------------------------------------------------------------ random stream
+// rand() of random.f90:65-93: successive REAL(4) random_number values, values
+// outside [1e-14, 1-1e-14] are drawn again.  The buffer holds the raw stream.
+struct RngReader {
+    const float *buf;  // holds stream positions [off, n)
+    long long off;
+    long long n;       // end of the stream available
+    long long cur;     // next position to read
+    int out;           // set once the stream ran out
+    __host__ __device__ inline float raw() {
+        if (cur >= n) { out = 1; return 0.5f; }
+        return buf[(cur++) - off];
+    }
+    __host__ __device__ inline double next() {
+        const double eps = 1e-14;
+        float v = 0.0f;
+        while ((double)v < eps || (double)v > 1.0 - eps) {
+            v = raw();
+            if (out) return 0.5;
+        }
+        return (double)v;
+    }
+};
+
+// BiasedRandom_choose (BiasedRandom.f90:81-109): first i with beg(i) < r < end(i),
+// else 1.  The intervals are contiguous (beg(i) = end(i-1)) and increasing when
+// every weight is positive, so a binary search gives the same answer.
+__host__ __device__ inline int choose_molecule(double r, const double *beg, const double *end, int M, int monotone) {
+    if (!monotone) {
+        for (int i = 0; i < M; ++i)
+            if (r > beg[i] && r < end[i]) return i + 1;
+        return 1;
+    }
+    int lo = 0, hi = M - 1;  // smallest i with end[i] > r
+    if (!(end[hi] > r)) return 1;
+    while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (end[mid] > r) hi = mid; else lo = mid + 1;
+    }
+    return (r > beg[lo]) ? lo + 1 : 1;
+}
+
+// ------------------------------------------------------------------ MonteCarloMove.f90
+struct MoveState {
+    double fxo, fyo, fzo, fo, cxo, cyo, czo, co, umaxold, vmaxold, cold, qold;
+    double vx, vy, vz, deltx, delty, deltz, angle;
+    double fxn, fyn, fzn, fn, cxn, cyn, czn, cn, umaxnew, vmaxnew, cnew, qnew;
+    double cphi, sphi, ct, st, ca, sa;  // rotation (TRotation)
+};
+
+__host__ __device__ inline void cross(double x1, double y1, double z1, double x2, double y2, double z2, double &xp,
+                                      double &yp, double &zp) {
+    xp = y1 * z2 - z1 * y2;   // prod_vect (geometry.f90:65-101)
+    yp = z1 * x2 - x1 * z2;
+    zp = x1 * y2 - y1 * x2;
+}
+
+// MonteCarloMove_init_old (MonteCarloMove.f90:34-54)
+__host__ __device__ inline void mcm_init_old(MoveState &m, const double f[3], const double t[3]) {
+    m.fxo = f[0]; m.fyo = f[1]; m.fzo = f[2]; m.fo = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    m.cxo = t[0]; m.cyo = t[1]; m.czo = t[2]; m.co = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+}
+
+// MonteCarloMove_init_new (MonteCarloMove.f90:56-106)
+__host__ __device__ inline void mcm_init_new(MoveState &m, const double f[3], const double t[3], double xlf, double xlc,
+                                             double dr, double d_angle) {
+    m.fxn = f[0]; m.fyn = f[1]; m.fzn = f[2]; m.fn = sqrt(f[0] * f[0] + f[1] * f[1] + f[2] * f[2]);
+    m.cxn = t[0]; m.cyn = t[1]; m.czn = t[2]; m.cn = sqrt(t[0] * t[0] + t[1] * t[1] + t[2] * t[2]);
+    double umax = xlf * m.fn * dr;
+    if (umax > 1e-2) {
+        const double e = exp(-2.0 * umax);
+        const double t2 = (umax * (1.0 + e) - (1.0 - e)) / 2.0;
+        m.cnew = 3.0 * t2 / (umax * umax * umax);
+    } else { umax = 0.0; m.cnew = 1.0; }
+    m.umaxnew = umax;
+    double vmax = xlc * m.cn * d_angle;
+    if (vmax > 1e-2) m.qnew = d_shi_sans_exp(vmax) / vmax;
+    else { vmax = 0.0; m.qnew = 1.0; }
+    m.vmaxnew = vmax;
+}
+
+// MonteCarloMove_chooseDisplacement (MonteCarloMove.f90:109-266): a ball of
+// radius dr, or the force-biased distribution exp(lambda F.dr) when biased.
+__host__ __device__ inline void mcm_choose_displacement(MoveState &m, RngReader &rng, double xlf, double dr) {
+    double umax = xlf * m.fo * dr;
+    if (umax > 1e-2) {
+        double e = exp(-2.0 * umax);
+        const double t = (umax * (1.0 + e) - (1.0 - e)) / 2.0;
+        m.cold = 3.0 * t / (umax * umax * umax);
+        double xksi = 0.0;
+        while (xksi < 1e-10) { xksi = rng.next(); if (rng.out) return; }
+        const double z = umax + log(xksi * t);
+        double u;
+        if (z <= log(4.0)) { const double s = exp(z); u = pow(3.0 * s, 1.0 / 3.0) - s / 10.0; }
+        else u = z - log(z / 2.0);
+        for (int k = 1; k <= 10; ++k) {   // Newton on h(u) = u + ln(u ch u - sh u) = z
+            e = exp(-2.0 * u);
+            const double ch = (1.0 + e) / 2.0;
+            double sh = (1.0 - e) / 2.0;
+            if (u < 1e-5) sh = u - u * u;
+            double g = u * ch - sh;
+            if (u < 1e-3) g = u * u * u / 3.0;
+            const double h = u + log(g);
+            const double h1 = u * sh / g;
+            if (k < 10) u = u + (z - h) / h1;
+        }
+        const double deltar = u / (xlf * m.fo);
+        xksi = 1.0;
+        while (xksi > (1.0 - 1e-10) || xksi < 1e-10) { xksi = rng.next(); if (rng.out) return; }
+        double xc = 1.0 + log(xksi + (1.0 - xksi) * e) / u;
+        if (u < 1e-7) xc = 1.0 - 2.0 * (1.0 - xksi);
+        if (xc > 1.0 - 1e-14) xc = 1.0 - 1e-14;
+        if (xc < -1.0 + 1e-14) xc = -1.0 + 1e-14;
+        const double xs = sqrt(1.0 - xc * xc);
+        double w = -1.0, wx = 0, wy = 0, wz = 0;
+        while (w <= 1e-10) {
+            double v2 = 2.0, vx = 0, vy = 0, vz = 0;
+            while (v2 > 1.0) {
+                vx = 2.0 * rng.next() - 1.0; vy = 2.0 * rng.next() - 1.0; vz = 2.0 * rng.next() - 1.0;
+                if (rng.out) return;
+                v2 = vx * vx + vy * vy + vz * vz;
+            }
+            cross(vx, vy, vz, m.fxo, m.fyo, m.fzo, wx, wy, wz);
+            w = sqrt(wx * wx + wy * wy + wz * wz);
+        }
+        m.deltx = deltar * (xc * m.fxo / m.fo + xs * wx / w);
+        m.delty = deltar * (xc * m.fyo / m.fo + xs * wy / w);
+        m.deltz = deltar * (xc * m.fzo / m.fo + xs * wz / w);
+    } else {
+        double v2 = 2.0, vx = 0, vy = 0, vz = 0;
+        while (v2 > 1.0) {
+            vx = 2.0 * rng.next() - 1.0; vy = 2.0 * rng.next() - 1.0; vz = 2.0 * rng.next() - 1.0;
+            if (rng.out) return;
+            v2 = vx * vx + vy * vy + vz * vz;
+        }
+        m.deltx = dr * vx; m.delty = dr * vy; m.deltz = dr * vz;
+        umax = 0.0; m.cold = 1.0;
+    }
+    m.umaxold = umax;
+}
+
+// MonteCarloMove_chooseRotation (MonteCarloMove.f90:269-444)
+__host__ __device__ inline void mcm_choose_rotation(MoveState &m, RngReader &rng, double xlc, double d_angle) {
+    double vmax = xlc * m.co * d_angle, vx, vy, vz, angle;
+    if (vmax > 1e-2) {
+        const double emax = exp(-2.0 * vmax);
+        const double shmax = (1.0 - emax) / 2.0;
+        double xksi = 1.0, proba = 0.0, v = 0.0, e = 0.0;
+        while (xksi >= proba) {
+            v = 0.0;
+            while (fabs(v) < 1e-10) {
+                xksi = rng.next();
+                if (rng.out) return;
+                const double xs = xksi * shmax;
+                v = vmax + log(xs + sqrt(xs * xs + emax));
+                if (xs * xs < 1e-14 * emax) v = xs / sqrt(emax);
+            }
+            e = exp(-2.0 * v);
+            proba = (1.0 - e) / v / (1.0 + e);
+            if (v < 1e-5) proba = (2.0 * v - 2.0 * v * v) / v / (1.0 + e);
+            xksi = rng.next();
+            if (rng.out) return;
+        }
+        const double cosx = v / vmax;
+        m.qold = d_shi_sans_exp(vmax) / vmax;
+        xksi = 1.0;
+        while (xksi > (1.0 - 1e-10)) { xksi = rng.next(); if (rng.out) return; }
+        angle = d_angle * (1.0 + log(xksi + (1.0 - xksi) * e) / v);
+        if (v < 1e-7) angle = d_angle * (1.0 - 2.0 * (1.0 - xksi));
+        double w = -1.0, wx = 0, wy = 0, wz = 0;
+        vx = vy = vz = 0;
+        while (w <= 1e-10) {
+            double v2 = 2.0;
+            while (v2 > 1.0 || v2 < 1e-10) {
+                vx = 2.0 * rng.next() - 1.0; vy = 2.0 * rng.next() - 1.0; vz = 2.0 * rng.next() - 1.0;
+                if (rng.out) return;
+                v2 = vx * vx + vy * vy + vz * vz;
+            }
+            cross(vx, vy, vz, m.cxo, m.cyo, m.czo, wx, wy, wz);
+            w = sqrt(wx * wx + wy * wy + wz * wz);
+        }
+        const double sinx = sqrt(1.0 - cosx * cosx);
+        vx = m.cxo / m.co * cosx + wx / w * sinx;
+        vy = m.cyo / m.co * cosx + wy / w * sinx;
+        vz = m.czo / m.co * cosx + wz / w * sinx;
+    } else {
+        double v2 = 2.0;
+        vx = vy = vz = 0;
+        while (v2 > 1.0 || v2 < 1e-10) {
+            vx = 2.0 * rng.next() - 1.0; vy = 2.0 * rng.next() - 1.0; vz = 2.0 * rng.next() - 1.0;
+            if (rng.out) return;
+            v2 = vx * vx + vy * vy + vz * vz;
+        }
+        const double v = sqrt(v2);
+        vx = vx / v; vy = vy / v; vz = vz / v;
+        angle = d_angle * (2.0 * rng.next() - 1.0);
+        if (rng.out) return;
+        vmax = 0.0; m.qold = 1.0;
+    }
+    m.ca = cos(angle); m.sa = sin(angle);
+    m.ct = vz; m.st = sqrt(1.0 - m.ct * m.ct);
+    m.cphi = 0.0; m.sphi = 0.0;
+    if (m.st > 0.0) { m.cphi = vx / m.st; m.sphi = vy / m.st; }
+    m.vx = vx; m.vy = vy; m.vz = vz; m.vmaxold = vmax; m.angle = angle;
+}
+
+// MonteCarloMove_accept_or_decline (MonteCarloMove.f90:447-570); one draw
+__host__ __device__ inline int mcm_accept(const MoveState &m, double dutot, double xlf, double xlc, RngReader &rng) {
+    const double exposu = -dutot;
+    const double exposf = -xlf * ((m.fxo + m.fxn) * m.deltx + (m.fyo + m.fyn) * m.delty + (m.fzo + m.fzn) * m.deltz);
+    const double exposfcorr = m.umaxold - m.umaxnew;
+    const double exposc = -xlc * m.angle * ((m.cxo + m.cxn) * m.vx + (m.cyo + m.cyn) * m.vy + (m.czo + m.czn) * m.vz);
+    const double exposccorr = m.vmaxold - m.vmaxnew;
+    const double factor = m.cold * m.qold / (m.cnew * m.qnew) * exp(exposu + exposf + exposfcorr + exposc + exposccorr);
+    const double xksi = rng.next();
+    return xksi > factor ? 0 : 1;
+}
+
+// movemc Step 5 (MC.f90:1031-1067): new atom positions from the proposal.
+// Centre of mass of the old atoms, wrapped new centre (ANINT), rotation of the
+// atoms about the centre with fill_rot_matrix/rotate_vect (geometry.f90:103-168).
+__host__ __device__ inline void place_molecule(const MoveState &m, int na, const double *xo, const double *yo,
+                                               const double *zo, const double *mass, double *xn, double *yn,
+                                               double *zn) {
+    double sx = 0, sy = 0, sz = 0, tm = 0;
+    for (int i = 0; i < na; ++i) { sx = sx + mass[i] * xo[i]; sy = sy + mass[i] * yo[i]; sz = sz + mass[i] * zo[i]; tm = tm + mass[i]; }
+    const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
+    const double xcn = xc + m.deltx - round(xc + m.deltx);
+    const double ycn = yc + m.delty - round(yc + m.delty);
+    const double zcn = zc + m.deltz - round(zc + m.deltz);
+    if (na > 1) {
+        const double cphi = m.cphi, sphi = m.sphi, st = m.st, ct = m.ct, ca = m.ca, sa = m.sa, ca1 = 1 - ca;
+        const double rxx = (cphi * cphi * (st * st) * ca1 + ca);
+        const double rxy = (sphi * cphi * (st * st) * ca1 - ct * sa);
+        const double rxz = st * (ct * ca1 * cphi + sa * sphi);
+        const double ryx = (cphi * sphi * (st * st) * ca1 + ct * sa);
+        const double ryy = (sphi * sphi * (st * st) * ca1 + ca);
+        const double ryz = st * (ct * ca1 * sphi - sa * cphi);
+        const double rzx = st * (ct * ca1 * cphi - sa * sphi);
+        const double rzy = st * (ct * ca1 * sphi + sa * cphi);
+        const double rzz = (st * st * ca + ct * ct);
+        for (int i = 0; i < na; ++i) {
+            const double xr = xo[i] - xc, yr = yo[i] - yc, zr = zo[i] - zc;
+            xn[i] = (rxx * xr + rxy * yr + rxz * zr) + xcn;
+            yn[i] = (ryx * xr + ryy * yr + ryz * zr) + ycn;
+            zn[i] = (rzx * xr + rzy * yr + rzz * zr) + zcn;
+        }
+    } else {
+        xn[0] = xcn; yn[0] = ycn; zn[0] = zcn;
+    }
+}
+
+// molecular force and torque about the centre of mass (MC.f90:1002-1025)
+__host__ __device__ inline void mol_force_torque(int na, const double *x, const double *y, const double *z,
+                                                 const double *mass, const double *fx, const double *fy,
+                                                 const double *fz, double F[3], double T[3]) {
+    double sx = 0, sy = 0, sz = 0, tm = 0;
+    for (int i = 0; i < na; ++i) { sx = sx + mass[i] * x[i]; sy = sy + mass[i] * y[i]; sz = sz + mass[i] * z[i]; tm = tm + mass[i]; }
+    const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
+    F[0] = F[1] = F[2] = 0; T[0] = T[1] = T[2] = 0;
+    for (int i = 0; i < na; ++i) { F[0] = F[0] + fx[i]; F[1] = F[1] + fy[i]; F[2] = F[2] + fz[i]; }
+    for (int i = 0; i < na; ++i) {
+        double tx, ty, tz;
+        cross(x[i] - xc, y[i] - yc, z[i] - zc, fx[i], fy[i], fz[i], tx, ty, tz);
+        T[0] = T[0] + tx; T[1] = T[1] + ty; T[2] = T[2] + tz;
+    }
+}
+
+}  // namespace yamc
