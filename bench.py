@@ -1,0 +1,324 @@
+"""Benchmark: MC trial moves/s of YAMC's movemc path on B200.
+
+Workload (default): 2048 SPC/E + 38 Na+ + 38 Cl- (6,220 atoms), L = 39.6 A,
+alpha = 0.30/A, rc = 12 A, kmax = 12 (1,068 half-space / 3,796 signed k),
+dispersion-Ewald LJ, plain FP64 method, unbiased moves (0.15 A ball, 0.15 rad),
+synthetic jittered-lattice start, gfortran random stream.  One step = one
+device-resident run_mc segment of --moves moves on one independent chain per GPU
+(replicas only: the Markov chain does not shard).
+
+  value  moves/s with the random stream already in HBM, CUDA events around each
+         persistent-kernel launch, L2 flushed (256 MB write) between steps
+  e2e    the same through yamc_run_chain with the stream in pinned host memory,
+         host->device copy of each step's stream window and device->host read of
+         the step result inside the timed region
+  --impl reference  the CPU restatement of the reference (oracle/, -O3) timed on
+         the host cores: independent chains, one per core
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC trial moves/s (SPC/E+NaCl Ewald); mixed vs FP64 GPU at |ΔE err|≤1e-4 kT"
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+def algorithmic_bytes_per_move(spec, nk, nsigned, ntype, p_acc):
+    """Bytes a move must move at least (the per-move accounting of the design notes):
+    real-space neighbours (old + new positions, 3 sites share most neighbours: 1.3x),
+    40 B per neighbour atom; rho(k) read; beta tables; k indices; accepted rho write."""
+    L = spec.box
+    natom = spec.natom
+    nnb = natom / L ** 3 * 4.0 / 3.0 * math.pi * spec.rc ** 3
+    real = 2 * 1.3 * nnb * 40
+    rho = (1 + ntype) * 2 * nsigned * 8
+    beta = (1 + ntype * (ntype + 1) / 2) * nk * 8
+    kidx = 12 * nk
+    commit = p_acc * (1 + ntype) * 2 * nsigned * 8
+    return real + rho + beta + kidx + commit
+
+
+class Clocks:
+    """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.out = None
+
+    def __enter__(self):
+        try:
+            self.out = open(f"/tmp/yamc_clocks_{os.getpid()}.csv", "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        if self.out:
+            self.out.close()
+
+    def summary(self):
+        path = f"/tmp/yamc_clocks_{os.getpid()}.csv"
+        try:
+            rows = [l.strip().split(",") for l in open(path) if l.strip()]
+        except Exception:
+            return None
+        if not rows:
+            return None
+        sm = [float(r[1]) for r in rows if r[1].strip().replace(".", "").isdigit()]
+        smax = [float(r[2]) for r in rows if r[2].strip().replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = set()
+        for r in rows:
+            for n, v in zip(names, r[5:9]):
+                if "Active" in v and "Not" not in v:
+                    reasons.add(n)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(rows)}
+
+
+def cpu_baseline(files, seconds=12.0):
+    """The oracle's -O3 build on one host core: a bounded sample of the same workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from yamc_b200 import rng as grng
+    o = pyoracle.Oracle(files, fast=True)
+    buf = grng.gfortran_stream(12345, 2_000_000)
+    cur = 0
+    done = 0
+    t0 = time.perf_counter()
+    while time.perf_counter() - t0 < seconds:
+        _, _, cur = o.run_mc(buf, 500, cursor=cur)
+        done += 500
+    dt = time.perf_counter() - t0
+    return {"value": done / dt, "unit": "moves/s", "cores": 1, "kind": "port",
+            "sample": f"{done} moves of the same workload from its initial configuration, one chain, "
+                      f"C restatement of the reference built -O3 (oracle/liboracle_fast.so)"}
+
+
+def _ref_worker(args):
+    files, seed, moves = args
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle
+    from yamc_b200 import rng as grng
+    o = pyoracle.Oracle(files, fast=True)
+    buf = grng.gfortran_stream(seed, 40 * moves + 10000)
+    t0 = time.perf_counter()
+    o.run_mc(buf, moves)
+    return moves, time.perf_counter() - t0
+
+
+def run_reference(args, files, spec_name):
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    import multiprocessing as mp
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    moves = args.ref_moves
+    ctx = mp.get_context("spawn")
+    vals = []
+    with ctx.Pool(cores) as pool:
+        for w in range(args.warmup + args.steps):
+            t0 = time.perf_counter()
+            res = pool.map(_ref_worker, [(files, 1000 + 97 * c + w, moves) for c in range(cores)])
+            dt = time.perf_counter() - t0
+            if w >= args.warmup:
+                vals.append(sum(m for m, _ in res) / dt)
+    value = float(np.median(vals))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * moves * cores / value,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": spec_name, "moves_per_chain_per_step": moves, "chains": cores},
+            "cpu_baseline": {"value": value, "unit": "moves/s", "cores": cores, "kind": "port",
+                             "sample": f"{cores} independent chains x {moves} moves per step, C restatement of "
+                                       f"the reference (-O3), no Fortran compiler on this image"},
+            "e2e": {"value": value, "unit": "moves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--moves", type=int, default=20000, help="moves per step")
+    ap.add_argument("--workload", default="nacl1m")
+    ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
+    ap.add_argument("--ref-moves", type=int, default=1500)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+
+    from yamc_b200 import systems
+    ws, rank, local = dist_env()
+    spec = systems.WORKLOADS[args.workload]
+    wdir = f"/tmp/yamc_bench_{args.workload}_r{rank}_{os.getpid()}"
+    files = systems.write_system(spec, wdir, seed=3 + rank, rng_seed=12345 + rank)
+
+    if args.impl == "reference":
+        if ws > 1:
+            import torch.distributed as dist
+            dist.init_process_group("gloo", timeout=__import__("datetime").timedelta(seconds=600))
+        run_reference(args, files, args.workload)
+        if ws > 1:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    import torch
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+    from yamc_b200 import api, rng as grng
+
+    eng = api.Engine.from_files(files, device=local)
+    n_steps = args.warmup + args.steps
+    per_move = 24  # generous upper bound of random numbers per unbiased move
+    stream = grng.gfortran_stream(12345 + rank, per_move * args.moves * (2 * n_steps + 2) + 100000)
+    d_stream = torch.from_numpy(stream).to(f"cuda:{local}")
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+
+    def l2_flush():
+        flush.fill_(1.0)
+        torch.cuda.synchronize()
+
+    # ---------------- device-resident value
+    cur = 0
+    acc_before = eng.energies()  # initial state read
+    kernel_ms = []
+    for w in range(args.warmup):
+        cur, done, st = eng.run_chain_device(d_stream.data_ptr(), d_stream.numel(), args.moves, cursor=cur)
+        l2_flush()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with Clocks(local) as clk:
+        for s in range(args.steps):
+            cur, done, st = eng.run_chain_device(d_stream.data_ptr(), d_stream.numel(), args.moves, cursor=cur)
+            assert st == 0 and done == args.moves, (st, done)
+            kernel_ms.append(eng.last_kernel_ms)
+            l2_flush()
+    torch.cuda.synchronize()
+    t_dev = sum(kernel_ms) / 1e3
+    if ws > 1:
+        t = torch.tensor([t_dev], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_dev = float(t.item())
+    value = ws * args.steps * args.moves / t_dev
+
+    # ---------------- end to end through the C ABI with host buffers
+    pinned = torch.from_numpy(stream).pin_memory()
+    host = pinned.numpy()
+    import ctypes
+    lib = eng.lib
+    window = per_move * args.moves
+    h2d = 0
+    ecur = cur
+    e_moves = 0
+    energies = np.zeros(8)
+    nrow = ctypes.c_int32(0)
+    for w in range(args.warmup):
+        c = ctypes.c_int64(ecur); dn = ctypes.c_int64(0)
+        lib.yamc_run_chain(eng.h, host.ctypes.data, min(host.size, ecur + window), ctypes.byref(c), args.moves,
+                           ctypes.byref(dn), None, None, 0, ctypes.byref(nrow))
+        ecur = c.value
+        l2_flush()
+    if ws > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    e_times = []
+    for s in range(args.steps):
+        c = ctypes.c_int64(ecur); dn = ctypes.c_int64(0)
+        n_rng = min(host.size, ecur + window)
+        h2d = (n_rng - ecur) * 4
+        t0 = time.perf_counter()
+        st = lib.yamc_run_chain(eng.h, host.ctypes.data, n_rng, ctypes.byref(c), args.moves, ctypes.byref(dn),
+                                None, None, 0, ctypes.byref(nrow))
+        lib.yamc_energies(eng.h, energies.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        e_times.append(time.perf_counter() - t0)
+        assert st == 0 and dn.value == args.moves, (st, dn.value)
+        ecur = c.value
+        e_moves += dn.value
+        l2_flush()
+    t_e2e = sum(e_times)
+    if ws > 1:
+        t = torch.tensor([t_e2e], device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        t_e2e = float(t.item())
+    e2e = ws * e_moves / t_e2e
+    d2h = 80 + 8 * 17 + 8 * 2  # run slot + engine scalars + counters read back per step
+
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+
+    # ---------------- roofline of the chain kernel
+    log, _, _, _, _ = eng.run_chain(stream, 2000, cursor=ecur)
+    p_acc = float(np.mean(log["flags"] & 1))
+    bpm = algorithmic_bytes_per_move(spec, eng.nk, eng.nsigned, eng.ntype, p_acc)
+    ms_launch = float(np.mean(kernel_ms))
+    achieved = bpm * args.moves / (ms_launch / 1e3) / 1e9
+    peak, which = peaks()
+    line = {
+        "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": f"{args.workload}: {spec.n_water} SPC/E + {spec.n_na} Na + {spec.n_cl} Cl, "
+                               f"{spec.natom} atoms, L={spec.box} A, alpha={spec.alpha}/A, rc={spec.rc} A, "
+                               f"kmax={spec.kmax}", "method": "plain FP64, unbiased moves",
+                   "moves_per_step": args.moves, "chains_per_gpu": 1, "parallelism": "replicas",
+                   "launch": eng.launch, "l2": "256 MB write between steps", "accept_fraction": p_acc},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_source": which, "algorithmic_bytes_per_move": bpm},
+        "e2e": {"value": e2e, "unit": "moves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(files)
+    print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

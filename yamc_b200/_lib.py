@@ -86,6 +86,7 @@ SIGNATURES = {
     "yamc_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
     "yamc_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
+    "yamc_phase_cycles": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
     "yamc_error_string": (ctypes.c_char_p, [ctypes.c_int]),
     "yamc_last_error_detail": (ctypes.c_char_p, []),
 }

@@ -204,6 +204,15 @@ class Engine:
         return {"cluster_blocks": int(out[0]), "threads": int(out[1]), "entries_per_thread": int(out[2]),
                 "smem_bytes": int(out[3])}
 
+    PHASES = ("choose", "old_pass", "propose", "tables", "kspace", "pair_filter", "pairs", "cta_reduce",
+              "cluster_exchange", "metropolis", "commit")
+
+    def phase_cycles(self, mode: int = 2) -> dict:
+        out = np.zeros(len(self.PHASES), dtype=np.int64)
+        check(self.lib.yamc_phase_cycles(self.h, int(mode), out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64)),
+                                         out.size), "yamc_phase_cycles")
+        return dict(zip(self.PHASES, (int(v) for v in out)))
+
     @property
     def last_kernel_ms(self) -> float:
         v = ctypes.c_double(0)

@@ -1,0 +1,1653 @@
+// B200 engine for YAMC's per-trial-move energy evaluation (movemc, MC.f90:831-1322).
+//
+// Kernels (sm_100a):
+//   k_realspace_full  all-pairs real-space sum (EwaldSumRealSpace_calc, full)      -- init / full recompute
+//   k_rho_full        structure factors rho(k) of all atoms (RhoSquared_addAtoms)  -- init / full recompute
+//   k_kspace_energy   k-space Coulomb + dispersion energy of rho(k)               -- init / full recompute
+//   k_chain<NT,EPT>   persistent Markov chain: one thread-block cluster per chain; every move runs
+//                     proposal -> fused real-space + k-space pass -> cluster reduction -> Metropolis
+//                     -> commit on the device, consuming the host-made random stream by cursor.
+//                     The same kernel serves the per-move C ABI (one pass per launch).
+//
+// Layout in HBM (per system): atoms as double4 (x, y, z, q) + int2 (molecule, LJ type) + double
+// hard-core diameter; the k-set as a compact list of S signed entries (+kx, +-ky, +-kz) with their
+// beta and beta_LJ rows; rho(k) as double2 (C, S) per structure (Coulomb, then each LJ type) and
+// entry, coalesced along the entry index.  During a chain every thread keeps its own entries' rho
+// in registers and every CTA stages its share of the atoms in shared memory; HBM is touched only
+// for the random stream, the moved molecule and the logs.
+#include <cooperative_groups.h>
+#include <cuda_pipeline.h>
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "yamc_device.cuh"
+#include "yamc_internal.h"
+
+namespace cg = cooperative_groups;
+
+namespace yamc {
+
+// ------------------------------------------------------------------------------------------
+// full sums
+// ------------------------------------------------------------------------------------------
+constexpr int kFullTile = 256;
+constexpr int kFullParts = 8;  // ew, lj6, lj12, ew_intra, lj6_intra, lj12_intra, overlap, spare
+
+template <int BS>
+__device__ inline void block_sum(double *vals, int nv, double *sh) {
+    // deterministic block reduction of nv values: warp xor tree, then warps in order
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    for (int v = 0; v < nv; ++v) {
+        double x = vals[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        if (lane == 0) sh[warp * nv + v] = x;
+    }
+    __syncthreads();
+    if (threadIdx.x < nv) {
+        double s = 0;
+        for (int w = 0; w < BS / 32; ++w) s += sh[w * nv + threadIdx.x];
+        sh[(BS / 32) * nv + threadIdx.x] = s;
+    }
+    __syncthreads();
+    for (int v = 0; v < nv; ++v) vals[v] = sh[(BS / 32) * nv + v];
+    __syncthreads();
+}
+
+// EwaldSumRealSpace_calc on the full sum (EwaldSumRealSpace.f90:233-500, j0 = i+1):
+// one thread per atom i runs over all j (tiles staged in shared memory), so per-atom
+// uu(i) and F(i) accumulate in increasing j order like the reference; the energy
+// totals count each pair once (j > i), intra-molecular pairs with -erf_Luc.
+__global__ void __launch_bounds__(kFullTile) k_realspace_full(DevSys D, double *uu, double *fx, double *fy, double *fz,
+                                                             double *part) {
+    __shared__ double4 tp[kFullTile];
+    __shared__ int2 tm[kFullTile];
+    __shared__ double td[kFullTile];
+    __shared__ double red[(kFullTile / 32 + 1) * kFullParts];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < D.N;
+    double4 pi = make_double4(0, 0, 0, 0);
+    int2 mi = make_int2(-1, 0);
+    double di = 0;
+    if (valid) { pi = D.atom[i]; mi = D.meta[i]; di = D.dhs[i]; }
+    double u = 0, gx = 0, gy = 0, gz = 0;
+    double acc[kFullParts] = {0, 0, 0, 0, 0, 0, 0, 0};
+    const int nt = D.nt;
+    for (int t0 = 0; t0 < D.N; t0 += kFullTile) {
+        const int j = t0 + threadIdx.x;
+        if (j < D.N) { tp[threadIdx.x] = D.atom[j]; tm[threadIdx.x] = D.meta[j]; td[threadIdx.x] = D.dhs[j]; }
+        __syncthreads();
+        const int nj = min(kFullTile, D.N - t0);
+        if (valid) {
+            for (int jj = 0; jj < nj; ++jj) {
+                const int jg = t0 + jj;
+                if (jg == i) continue;
+                const double4 pj = tp[jj];
+                const int2 mj = tm[jj];
+                const bool same = mi.x == mj.x;
+                const double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (!same && mi.y > 0 && mj.y > 0) {
+                    const double d12 = (di + td[jj]) / 2;
+                    if (r2 < d12 * d12) acc[6] = 1.0;
+                }
+                if (r2 >= D.rmax2) continue;
+                const bool lj = mi.y > 0 && mj.y > 0;
+                const int off = lj ? (mi.y - 1) * nt + (mj.y - 1) : 0;
+                const PairTerm<double> t = pair_term<double, true>(r2, D.xclb * pi.w * pj.w, lj, lj ? D.lj_sig6[off] : 0.0,
+                                                                    lj ? D.lj_feps[off] : 0.0, D.alpha, D.taosp, same);
+                if (jg > i) {
+                    acc[0] += t.ew; acc[1] += t.lj6; acc[2] += t.lj12;
+                    if (same) { acc[3] += t.ew; acc[4] += t.lj6; acc[5] += t.lj12; }
+                }
+                if (!same) {
+                    u = u + (t.ew + t.lj12 - t.lj6);
+                    gx = gx + dx * t.FR; gy = gy + dy * t.FR; gz = gz + dz * t.FR;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (valid) { uu[i] = u; fx[i] = gx; fy[i] = gy; fz[i] = gz; }
+    block_sum<kFullTile>(acc, kFullParts, red);
+    if (threadIdx.x < kFullParts) part[blockIdx.x * kFullParts + threadIdx.x] = acc[threadIdx.x];
+}
+
+// RhoSquared_addAtoms (RhoSquared.f90:188-243): for each signed entry the sum over all atoms,
+// in atom order, of the charge-weighted phase (Coulomb) and of the unit phase per LJ type,
+// the LJ phase being the Coulomb one times 1/q like RhoSquared_addAtom (RhoSquared.f90:173-176).
+constexpr int kRhoBlock = 128;
+constexpr int kRhoChunk = 32;
+
+template <int NT>
+__global__ void __launch_bounds__(kRhoBlock) k_rho_full(DevSys D, double2 *rho) {
+    extern __shared__ double2 stab[];  // [kRhoChunk][3][kmax+1]
+    __shared__ double sq[kRhoChunk];
+    __shared__ int st[kRhoChunk];
+    const int KM = D.kmax + 1;
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = e < D.S;
+    int4 kv = make_int4(0, 0, 0, 0);
+    if (valid) kv = D.kvec[e];
+    double cC = 0, sC = 0;
+    double cL[NT > 0 ? NT : 1], sL[NT > 0 ? NT : 1];
+#pragma unroll
+    for (int t = 0; t < NT; ++t) { cL[t] = 0; sL[t] = 0; }
+    for (int a0 = 0; a0 < D.N; a0 += kRhoChunk) {
+        const int na = min(kRhoChunk, D.N - a0);
+        for (int idx = threadIdx.x; idx < na * 3 * KM; idx += blockDim.x) {
+            const int a = idx / (3 * KM), r = idx % (3 * KM), d = r / KM, m = r % KM;
+            const double4 p = D.atom[a0 + a];
+            const double u = d == 0 ? p.x : (d == 1 ? p.y : p.z);
+            double s, c;
+            sincospi(2.0 * (double)m * u, &s, &c);
+            if (m == 0) { s = 0.0; c = 1.0; }
+            stab[(a * 3 + d) * KM + m] = make_double2(c, s);
+        }
+        if (threadIdx.x < na) { sq[threadIdx.x] = D.atom[a0 + threadIdx.x].w; st[threadIdx.x] = D.meta[a0 + threadIdx.x].y; }
+        __syncthreads();
+        if (valid) {
+            for (int a = 0; a < na; ++a) {
+                const double2 *T = stab + (size_t)a * 3 * KM;
+                const double q = sq[a];
+                const int t = st[a];
+                double c = 0, s = 0;
+                if (q != 0.0) {
+                    entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, q, c, s);
+                    cC = cC + c; sC = sC + s;
+                }
+                if (t > 0) {
+                    double cl, sl;
+                    if (q != 0.0) { const double iq = 1.0 / q; cl = c * iq; sl = s * iq; }
+                    else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, 1.0, cl, sl);
+#pragma unroll
+                    for (int tt = 0; tt < NT; ++tt)
+                        if (tt == t - 1) { cL[tt] = cL[tt] + cl; sL[tt] = sL[tt] + sl; }
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (valid) {
+        rho[e] = make_double2(cC, sC);
+#pragma unroll
+        for (int t = 0; t < NT; ++t) rho[(size_t)(1 + t) * D.S + e] = make_double2(cL[t], sL[t]);
+    }
+}
+
+// EwaldSumKSpace_calc_coulomb_energy / _calc_LJ_energy (EwaldSumKSpace.f90:389-526) per entry,
+// reduced per block (host adds the blocks in order).
+template <int NT>
+__global__ void __launch_bounds__(256) k_kspace_energy(DevSys D, const double2 *rho, double *part) {
+    __shared__ double red[(256 / 32 + 1) * 2];
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[2] = {0, 0};
+    if (e < D.S) {
+        const double2 c = rho[e];
+        acc[0] = D.ebeta[e] * (c.x * c.x + c.y * c.y);
+        double2 r[NT > 0 ? NT : 1];
+#pragma unroll
+        for (int t = 0; t < NT; ++t) r[t] = rho[(size_t)(1 + t) * D.S + e];
+#pragma unroll
+        for (int t1 = 0; t1 < NT; ++t1)
+#pragma unroll
+            for (int t2 = t1; t2 < NT; ++t2) {
+                const int p = D.pair_index[t1 * NT + t2];
+                double l = D.ebetalj[(size_t)p * D.S + e] * (r[t1].x * r[t2].x + r[t1].y * r[t2].y);
+                if (t1 != t2) l = l + l;
+                acc[1] += l;
+            }
+    }
+    block_sum<256>(acc, 2, red);
+    if (threadIdx.x < 2) part[blockIdx.x * 2 + threadIdx.x] = acc[threadIdx.x];
+}
+
+// ------------------------------------------------------------------------------------------
+// the chain kernel
+// ------------------------------------------------------------------------------------------
+enum ChainMode { MODE_RUN = 0, MODE_OLD = 1, MODE_EVAL = 2 };
+
+// per-replica run control, in device memory
+struct RunSlot {
+    const float *rng;       // stream positions [rng_off, n_rng)
+    long long rng_off;
+    long long n_rng;
+    long long cursor;       // in: start cursor; out: cursor after the last completed move
+    long long n_moves;      // moves requested
+    long long moves_done;   // out
+    yamc_move_record *log;  // optional, n_moves records
+    double *rows;           // optional energy rows (9 doubles)
+    int max_rows, n_rows;
+    int status, accepted;
+};
+
+struct ChainArgs {
+    const DevSys *sys;  // [R]
+    RunSlot *run;       // [R]
+    int G;              // CTAs per chain (cluster size)
+    int mode;
+    int nown_max;       // atoms staged per CTA (interleaved ownership: atom j lives in CTA j % G)
+    int qcap;           // pair queue capacity per CTA
+    // per-move API (R == 1): imol (1-based) and proposed positions in, results out
+    const double *api_in;  // [0] imol, [1 + 3a + c] coordinate c of atom a
+    double *api_out;       // the reduction vector of the pass (RV_* layout)
+    double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas
+    long long *prof;       // optional per-phase cycle counters (PH_* layout), written by CTA 0 thread 0
+};
+
+// phases timed when ChainArgs::prof is set
+enum Phase { PH_CHOOSE = 0, PH_PASS_OLD, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE, PH_CLUSTER,
+             PH_DECIDE, PH_COMMIT, PH_COUNT };
+
+// reduction vector of one pass
+constexpr int RV_EW = 0, RV_LJ6 = 1, RV_LJ12 = 2, RV_DUC = 3, RV_DUL = 4, RV_OVL = 5, RV_F = 6;
+constexpr int kNV = 6 + 3 * kMaxA;
+
+enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
+
+struct Slot { double x, y, z, q, iq, dhs; int type, pad; };
+constexpr int kMaxSpecies = 8;
+constexpr int kCPT = 4;  // atoms each thread tests per filter round
+constexpr int kWin = 256;
+
+struct ChainShared {
+    int imol, first, na, abort, accepted, kind, forces, last_mol;
+    long long cursor, cursor_start, icycle, mic;
+    Slot slot[2 * kMaxA];  // [0, na): new positions, [na, 2na): old positions
+    double mass[kMaxA];
+    double eold[3], fold[3 * kMaxA];
+    double mu_old[3];
+    MoveState mv;
+    double sc[SC_COUNT];
+    double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (global positions may lag for other CTAs)
+    int qcount;
+    int wcount[64];  // per-warp pair counts and their exclusive prefix
+    double tot[kNV];
+    // molecule species (runs of identical consecutive molecules): first molecule, count, atoms, first atom
+    int nspec;
+    int sp_m0[kMaxSpecies], sp_cnt[kMaxSpecies], sp_na[kMaxSpecies], sp_a0[kMaxSpecies];
+    Slot sp_atom[kMaxSpecies][kMaxA];
+    double sp_mass[kMaxSpecies][kMaxA];
+    // two windows of the random stream, refilled asynchronously one move ahead
+    long long wbase[2];
+    int wn[2];
+};
+
+__device__ inline unsigned lane_lt_mask() {
+    unsigned m;
+    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
+    return m;
+}
+
+// Phase tables for slots [s0, s1): T[slot][axis][m] = (cos, sin)(2 pi m u)
+__device__ inline void build_tables(double2 *tab, const ChainShared &sh, int s0, int s1, int KM) {
+    const int n = (s1 - s0) * 3 * KM;
+    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
+        const int sl = s0 + idx / (3 * KM), r = idx % (3 * KM), d = r / KM, m = r % KM;
+        const double u = d == 0 ? sh.slot[sl].x : (d == 1 ? sh.slot[sl].y : sh.slot[sl].z);
+        double s, c;
+        sincospi(2.0 * (double)m * u, &s, &c);
+        if (m == 0) { s = 0.0; c = 1.0; }
+        tab[(sl * 3 + d) * KM + m] = make_double2(c, s);
+    }
+}
+
+// Molecule phase sums of one entry over slots [s0, s0+na) -- RhoSquared_addAtom per atom:
+// Coulomb phase q (cos, sin), LJ phase = Coulomb phase * (1/q) (the unit phase when q == 0),
+// accumulated per LJ type in atom order.  ph/phl keep the per-atom phases for the forces.
+template <int NT>
+__device__ __forceinline__ void mol_phase_sum(const double2 *tab, const ChainShared &sh, int s0, int na, int KM, int kx, int ky,
+                                     int kz, double2 (&out)[1 + NT], double2 (&ph)[kMaxA], double2 (&phl)[kMaxA]) {
+#pragma unroll
+    for (int t = 0; t <= NT; ++t) out[t] = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        ph[a] = make_double2(0.0, 0.0);
+        phl[a] = make_double2(0.0, 0.0);
+        if (a < na) {
+            const Slot &sl = sh.slot[s0 + a];
+            const double2 *T = tab + (size_t)(s0 + a) * 3 * KM;
+            double c = 0, s = 0;
+            if (sl.q != 0.0) {
+                entry_phase<double, double2>(T, T + KM, T + 2 * KM, kx, ky, kz, sl.q, c, s);
+                out[0].x = out[0].x + c; out[0].y = out[0].y + s;
+            }
+            ph[a] = make_double2(c, s);
+            if (sl.type > 0) {
+                double cl, sl2;
+                if (sl.q != 0.0) { cl = c * sl.iq; sl2 = s * sl.iq; }
+                else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kx, ky, kz, 1.0, cl, sl2);
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                    if (t == sl.type - 1) { out[1 + t].x = out[1 + t].x + cl; out[1 + t].y = out[1 + t].y + sl2; }
+                phl[a] = make_double2(cl, sl2);
+            }
+        }
+    }
+}
+
+template <int NT>
+struct NPair { static constexpr int value = NT * (NT + 1) / 2; };
+
+template <int I>
+struct IntC { static constexpr int value = I; };
+
+// calls f(IntC<I>) for I in [B, E): loop indices known at compile time
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (B < E) {
+        f(IntC<B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
+// row of the packed upper triangle t1 <= t2 (the host's pair_index enumeration)
+template <int NT>
+__host__ __device__ constexpr int pair_idx(int a, int b) {
+    return a <= b ? a * NT - a * (a - 1) / 2 + (b - a) : b * NT - b * (b - 1) / 2 + (a - b);
+}
+
+template <int NT, int EPT>
+struct EntryRegs {
+    int e[EPT];
+    int kx[EPT], ky[EPT], kz[EPT];
+    double beta[EPT];
+    double bl[EPT][NPair<NT>::value];  // beta_LJ of every type pair for this entry
+    double2 rho[EPT][1 + NT];
+    double2 mold[EPT][1 + NT];
+    double2 dl[EPT][1 + NT];
+};
+
+// k-space force on the molecule's atoms from one entry: 4 pi beta (C sin - S cos) k per atom,
+// Coulomb with the q-weighted phase and the current (or new) Coulomb rho, plus the dispersion
+// terms of the atom's LJ type against every type's rho (ForceKSpace.f90:59-302).
+template <int NT>
+__device__ __forceinline__ void entry_forces(const ChainShared &sh, int s0, int na, int kx, int ky, int kz, double beta,
+                                    const double (&bl)[NPair<NT>::value], const double2 (&C)[1 + NT],
+                                    const double2 (&ph)[kMaxA], const double2 (&phl)[kMaxA], double (&acc)[kNV]) {
+    const double fourpi = kFourPi;
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        if (a >= na) break;
+        const int ta = sh.slot[s0 + a].type;
+        double w = fourpi * ((C[0].x * ph[a].y - C[0].y * ph[a].x) * beta);
+        if (ta > 0) {
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                double b = 0.0;
+#pragma unroll
+                for (int u = 0; u < NT; ++u)
+                    if (u == ta - 1) b = bl[pair_idx<NT>(u, t)];
+                w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * b);
+            }
+        }
+        acc[RV_F + 3 * a] += w * kx;
+        acc[RV_F + 3 * a + 1] += w * ky;
+        acc[RV_F + 3 * a + 2] += w * kz;
+    }
+}
+
+// One pass over the moved molecule's slots: k-space over the thread's entries, real space over
+// the CTA's atoms (pairs within the cutoff are compacted into a queue, then evaluated densely),
+// reduced over the CTA and then over the cluster in rank order.  Result: sh.tot, identical in
+// every CTA of the cluster.
+template <int NT, int EPT, int KIND, bool FORCES>
+__device__ __forceinline__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh, EntryRegs<NT, EPT> &R, double2 *tab,
+                           const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue, double *red,
+                           double *xch, const double *lj_s, int nown, int G, int rank, int xpar,
+                           cg::cluster_group &cluster) {
+    constexpr int kind = KIND;
+    constexpr bool forces = FORCES;
+    constexpr int NVMAX = FORCES ? kNV : RV_F;  // accumulators this pass needs
+    const int na = sh.na;
+    const int KM = D.kmax + 1;
+    const int nt = D.nt;
+    const int imol0 = sh.imol - 1;
+    const int s_lo = (kind == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
+    const int s_hi = (kind == PASS_NEW) ? na : 2 * na;
+    const bool prof = A.prof && threadIdx.x == 0 && rank == 0;
+    long long t_mark = prof ? clock64() : 0;
+#define YAMC_PH(ph) do { if (prof) { const long long t_now = clock64(); A.prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+    build_tables(tab, sh, s_lo, s_hi, KM);
+    __syncthreads();
+    YAMC_PH(PH_TABLES);
+
+    double acc[NVMAX];
+#pragma unroll
+    for (int v = 0; v < NVMAX; ++v) acc[v] = 0.0;
+
+    // ---- k-space: every entry of the thread, with compile-time entry indices so the entry
+    //      state stays in registers
+    static_for<0, EPT>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        if (R.e[k] < 0) return;
+        double2 ph[kMaxA], phl[kMaxA];
+        if constexpr (KIND != PASS_NEW) mol_phase_sum<NT>(tab, sh, na, na, KM, R.kx[k], R.ky[k], R.kz[k], R.mold[k], ph, phl);
+        if constexpr (KIND == PASS_OLD) {
+            if constexpr (FORCES) entry_forces<NT>(sh, na, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k], ph, phl, acc);
+        } else {
+            double2 mnew[1 + NT];
+            mol_phase_sum<NT>(tab, sh, 0, na, KM, R.kx[k], R.ky[k], R.kz[k], mnew, ph, phl);
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) R.dl[k][t] = make_double2(mnew[t].x - R.mold[k][t].x, mnew[t].y - R.mold[k][t].y);
+            {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
+                const double2 C = R.rho[k][0], d = R.dl[k][0];
+                acc[RV_DUC] += (((C.x + C.x) + d.x) * d.x + ((C.y + C.y) + d.y) * d.y) * R.beta[k];
+            }
+            // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
+            // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
+#pragma unroll
+            for (int t1 = 0; t1 < NT; ++t1) {
+                const double2 C1 = R.rho[k][1 + t1], D1 = R.dl[k][1 + t1];
+                const double tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
+#pragma unroll
+                for (int t2 = 0; t2 < NT; ++t2) {
+                    const double2 D2 = R.dl[k][1 + t2];
+                    if (D2.x == 0.0 && D2.y == 0.0) continue;
+                    acc[RV_DUL] += (tc * D2.x + ts * D2.y) * R.bl[k][pair_idx<NT>(t1, t2)];
+                }
+            }
+            if constexpr (KIND == PASS_NEW && FORCES) {  // against total_new = rho + delta (MC.f90:1136-1163)
+                double2 Cn[1 + NT];
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) Cn[t] = make_double2(R.rho[k][t].x + R.dl[k][t].x, R.rho[k][t].y + R.dl[k][t].y);
+                entry_forces<NT>(sh, 0, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], Cn, ph, phl, acc);
+            }
+        }
+    });
+
+    YAMC_PH(PH_KSPACE);
+    // ---- real space: each thread tests CPT of the CTA's atoms against the active slots, the
+    //      (atom, slot) pairs inside the cutoff are laid out in the queue by a prefix sum over
+    //      threads (deterministic order), then evaluated by all threads, item i by thread i % B.
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
+    const int B = blockDim.x;
+    const int round_atoms = B * kCPT;
+    for (int c0 = 0; c0 < nown; c0 += round_atoms) {
+        unsigned masks = 0;  // kCPT slot masks of 8 bits
+        int count = 0;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            const int jl = c0 + c * B + threadIdx.x;
+            if (jl < nown && meta_s[jl].x != imol0) {
+                const double4 pj = atom_s[jl];
+                const int tj = meta_s[jl].y;
+                const double dj = dhs_s[jl];
+                unsigned m = 0;
+                for (int s = s_lo; s < s_hi; ++s) {
+                    const Slot &sl = sh.slot[s];
+                    const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (s < na && kind != PASS_OLD && sl.type > 0 && tj > 0) {  // hard core (EwaldSumRealSpace.f90:409)
+                        const double d12 = (sl.dhs + dj) / 2;
+                        if (r2 < d12 * d12) acc[RV_OVL] = 1.0;
+                    }
+                    if (r2 < D.rmax2) m |= 1u << s;
+                }
+                masks |= m << (8 * c);
+                count += __popc(m);
+            }
+        }
+        // exclusive prefix of the counts: within the warp, then over the warps
+        int incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) sh.wcount[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int v = lane < nwarp ? sh.wcount[lane] : 0;
+            int x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane < nwarp) sh.wcount[32 + lane] = x - v;
+            if (lane == 31) sh.qcount = x;
+        }
+        __syncthreads();
+        int pos = sh.wcount[32 + warp] + incl - count;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            unsigned m = (masks >> (8 * c)) & 0xffu;
+            const int jl = c0 + c * B + threadIdx.x;
+            while (m) {
+                const int s = __ffs(m) - 1;
+                m &= m - 1;
+                queue[pos++] = (jl << 3) | s;
+            }
+        }
+        __syncthreads();
+        YAMC_PH(PH_FILTER);
+        const int nq = sh.qcount;
+        for (int qi = threadIdx.x; qi < nq; qi += B) {
+            const int item = queue[qi];
+            const int jl = item >> 3, s = item & 7;
+            const Slot &sl = sh.slot[s];
+            const double4 pj = atom_s[jl];
+            const int tj = meta_s[jl].y;
+            const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const bool lj = sl.type > 0 && tj > 0;
+            const int off = lj ? (sl.type - 1) * nt + (tj - 1) : 0;
+            const double qq = D.xclb * sl.q * pj.w;
+            const double s6 = lj ? lj_s[off] : 0.0, fe = lj ? lj_s[nt * nt + off] : 0.0;
+            const bool isnew = s < na;
+            const double sign = (kind == PASS_BOTH && !isnew) ? -1.0 : 1.0;
+            if constexpr (FORCES) {
+                const PairTerm<double> t = pair_term<double, true>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
+                acc[RV_EW] += sign * t.ew; acc[RV_LJ6] += sign * t.lj6; acc[RV_LJ12] += sign * t.lj12;
+                const int a = isnew ? s : s - na;
+#pragma unroll
+                for (int aa = 0; aa < kMaxA; ++aa)
+                    if (aa == a) { acc[RV_F + 3 * aa] += dx * t.FR; acc[RV_F + 3 * aa + 1] += dy * t.FR; acc[RV_F + 3 * aa + 2] += dz * t.FR; }
+            } else {
+                const PairTerm<double> t = pair_term<double, false>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
+                acc[RV_EW] += sign * t.ew; acc[RV_LJ6] += sign * t.lj6; acc[RV_LJ12] += sign * t.lj12;
+            }
+        }
+        __syncthreads();
+        YAMC_PH(PH_PAIRS);
+    }
+
+    // ---- reduction: xor trees within each warp, across the warps (one warp per value) and
+    //      across the cluster's CTAs; fixed trees, so every CTA gets bit-identical totals
+    if (A.mode == MODE_RUN && threadIdx.x >= 32 && threadIdx.x < 64) __pipeline_wait_prior(0);  // random window
+    const int nv = forces ? (RV_F + 3 * na) : RV_F;
+#pragma unroll
+    for (int v = 0; v < kNV; ++v) {
+        if (v >= nv) break;
+        double x = acc[v];
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = (v == RV_OVL) ? fmax(x, y) : x + y;
+        }
+        if (lane == 0) red[warp * kNV + v] = x;
+    }
+    __syncthreads();
+    for (int v = warp; v < nv; v += nwarp) {
+        double x = lane < nwarp ? red[lane * kNV + v] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = (v == RV_OVL) ? fmax(x, y) : x + y;
+        }
+        if (G > 1) {
+            if (lane < G) {
+                double *dst = cluster.map_shared_rank(xch, lane);
+                dst[(xpar * G + rank) * kNV + v] = x;
+            }
+        } else if (lane == 0) {
+            sh.tot[v] = x;
+        }
+    }
+    YAMC_PH(PH_REDUCE);
+    if (G > 1) {
+        cluster.sync();
+        for (int v = warp; v < nv; v += nwarp) {
+            double x = lane < G ? xch[(xpar * G + lane) * kNV + v] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = (v == RV_OVL) ? fmax(x, y) : x + y;
+            }
+            if (lane == 0) sh.tot[v] = x;
+        }
+    }
+    __syncthreads();
+    YAMC_PH(PH_CLUSTER);
+#undef YAMC_PH
+}
+
+template <int NT, int EPT>
+__global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ChainShared sh;
+    __shared__ float rwin[2][kWin];
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const int G = A.G;
+    const int rank = G > 1 ? (int)cluster.block_rank() : 0;
+    const int rep = blockIdx.x / G;
+    const DevSys D = A.sys[rep];
+    RunSlot *run = A.run + rep;
+    const int B = blockDim.x;
+    const int tid = threadIdx.x;
+    const int KM = D.kmax + 1;
+    const int S = D.S;
+    const int nt = D.nt;
+
+    // shared memory carve-up (chain_smem_bytes on the host computes the same sizes)
+    double2 *tab = reinterpret_cast<double2 *>(smem_raw);                     // [2 kMaxA][3][KM]
+    double4 *atom_s = reinterpret_cast<double4 *>(tab + 2 * kMaxA * 3 * KM);  // [nown_max]
+    double *dhs_s = reinterpret_cast<double *>(atom_s + A.nown_max);          // [nown_max]
+    int2 *meta_s = reinterpret_cast<int2 *>(dhs_s + A.nown_max);              // [nown_max]
+    int *queue = reinterpret_cast<int *>(meta_s + A.nown_max);                // [qcap]
+    double *red = reinterpret_cast<double *>(queue + ((A.qcap + 1) & ~1));    // [B/32][kNV]
+    double *xch = red + (B / 32) * kNV;                                       // [2][G][kNV]
+    double *lj_s = xch + 2 * G * kNV;                                         // [2][nt*nt]
+
+    // atoms of this CTA: j = rank + G * local (interleaved, so every CTA holds a spatial mix)
+    const int nown = (D.N - rank + G - 1) / G;
+    for (int i = tid; i < nown; i += B) {
+        const int j = rank + G * i;
+        atom_s[i] = D.atom[j]; dhs_s[i] = D.dhs[j]; meta_s[i] = D.meta[j];
+    }
+    for (int i = tid; i < nt * nt; i += B) { lj_s[i] = D.lj_sig6[i]; lj_s[nt * nt + i] = D.lj_feps[i]; }
+
+    // entries of this thread; rho stays in registers for the whole launch
+    EntryRegs<NT, EPT> R;
+    const int gthreads = G * B;
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+        const int e = rank * B + tid + k * gthreads;
+        R.e[k] = e < S ? e : -1;
+        R.kx[k] = R.ky[k] = R.kz[k] = 0;
+        R.beta[k] = 0;
+        if (e < S) {
+            const int4 kv = D.kvec[e];
+            R.kx[k] = kv.x; R.ky[k] = kv.y; R.kz[k] = kv.z;
+            R.beta[k] = D.ebeta[e];
+        }
+#pragma unroll
+        for (int p = 0; p < NPair<NT>::value; ++p) R.bl[k][p] = e < S ? D.ebetalj[(size_t)p * S + e] : 0.0;
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) {
+            R.rho[k][t] = e < S ? D.rho[(size_t)t * S + e] : make_double2(0, 0);
+            R.mold[k][t] = (A.mode == MODE_EVAL && e < S) ? A.scratch[(size_t)t * S + e] : make_double2(0, 0);
+            R.dl[k][t] = make_double2(0, 0);
+        }
+    }
+    if (tid == 0) {
+        for (int c = 0; c < SC_COUNT; ++c) sh.sc[c] = D.scal[c];
+        sh.icycle = D.cnt[CN_ICYCLE];
+        sh.mic = D.cnt[CN_MOVE_IN_CYCLE];
+        sh.cursor = run->cursor;
+        sh.last_mol = -1;
+        sh.abort = 0;
+        sh.qcount = 0;
+        sh.wbase[0] = sh.wbase[1] = -1;
+        sh.wn[0] = sh.wn[1] = 0;
+        // static atom data of each molecule species, taken from its first molecule
+        sh.nspec = D.nspec <= kMaxSpecies ? D.nspec : 0;
+        for (int sp = 0; sp < sh.nspec; ++sp) {
+            const int4 c = D.spec[sp];
+            sh.sp_m0[sp] = c.x; sh.sp_cnt[sp] = c.y; sh.sp_na[sp] = c.z; sh.sp_a0[sp] = c.w;
+            for (int a = 0; a < c.z; ++a) {
+                const int j = c.w + a;
+                Slot t;
+                t.x = t.y = t.z = 0.0;
+                t.q = D.atom[j].w; t.iq = t.q != 0.0 ? 1.0 / t.q : 0.0;
+                t.dhs = D.dhs[j]; t.type = D.meta[j].y; t.pad = 0;
+                sh.sp_atom[sp][a] = t;
+                sh.sp_mass[sp][a] = D.mass[j];
+            }
+        }
+    }
+    __syncthreads();
+    const bool biased = (D.xlf > 0.0 || D.xlc > 0.0);
+
+    long long moves_done = 0;
+    int n_acc = 0, rows = 0;
+    int xpar = 0;  // parity of the cluster exchange buffer, flipped after every pass
+    const long long n_moves = (A.mode == MODE_RUN) ? run->n_moves : 1;
+
+    const bool prof = A.prof && tid == 0 && rank == 0;
+    long long t_mark = 0;
+#define YAMC_PH(ph) do { if (prof) { const long long t_now = clock64(); A.prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+    for (long long it = 0; it < n_moves; ++it) {
+        if (prof) t_mark = clock64();
+        // ------------------------------------------------ choose the molecule, stage its atoms
+        if (tid == 0) {
+            sh.cursor_start = sh.cursor;
+            sh.abort = 0;
+            int imol = 1;
+            if (A.mode == MODE_RUN) {
+                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
+                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
+                if (sh.mic == 0) (void)rng.next();  // per-cycle pressure-step draw (runmc.f90:206)
+                (void)rng.next();                   // move-or-exchange draw (runmc.f90:232), never an exchange
+                const double r = rng.next();        // BiasedRandom_choose (runmc.f90:258)
+                imol = choose_molecule_guess(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
+                if (rng.out) sh.abort = 1;
+                else sh.cursor = rng.cur;
+            } else {
+                imol = (int)A.api_in[0];
+            }
+            // molecule -> species -> first atom; static atom data from the species table
+            int sp = -1;
+            for (int q = 0; q < sh.nspec; ++q)
+                if (imol - 1 >= sh.sp_m0[q] && imol - 1 < sh.sp_m0[q] + sh.sp_cnt[q]) { sp = q; break; }
+            int first, nam;
+            if (sp >= 0) { nam = sh.sp_na[sp]; first = sh.sp_a0[sp] + (imol - 1 - sh.sp_m0[sp]) * nam; }
+            else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
+            sh.imol = imol; sh.first = first; sh.na = nam;
+            double mx = 0, my = 0, mz = 0;
+            for (int a = 0; a < nam; ++a) {
+                const int j = first + a;
+                Slot s;
+                if (sp >= 0) { s = sh.sp_atom[sp][a]; sh.mass[a] = sh.sp_mass[sp][a]; }
+                else {
+                    const double q = D.atom[j].w;
+                    s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y; s.pad = 0;
+                    sh.mass[a] = D.mass[j];
+                }
+                // positions: the last accepted move's cache, else the owning CTA's staged copy
+                if (imol - 1 == sh.last_mol) { s.x = sh.lx[a]; s.y = sh.ly[a]; s.z = sh.lz[a]; }
+                else {
+                    const double4 *src = (G > 1) ? cluster.map_shared_rank(atom_s, j % G) : atom_s;
+                    const double4 p = src[j / G];
+                    s.x = p.x; s.y = p.y; s.z = p.z;
+                }
+                sh.slot[nam + a] = s;  // old positions
+                sh.slot[a] = s;        // new positions, replaced after the proposal
+                // dipole of the molecule at the old positions (EwaldSumExternal_calc_mu)
+                mx = mx + s.q * s.x; my = my + s.q * s.y; mz = mz + s.q * s.z;
+            }
+            sh.mu_old[0] = mx; sh.mu_old[1] = my; sh.mu_old[2] = mz;
+            sh.kind = PASS_OLD;
+            sh.forces = 1;
+        }
+        __syncthreads();
+        if (sh.abort) break;
+        const int na = sh.na;
+        YAMC_PH(PH_CHOOSE);
+
+        // ------------------------------------------------ old forces (force-biased moves, per-move API)
+        if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
+            chain_pass<NT, EPT, PASS_OLD, true>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+            xpar ^= 1;
+            if (prof) t_mark = clock64();
+            if (tid == 0) {
+                sh.eold[0] = sh.tot[RV_EW]; sh.eold[1] = sh.tot[RV_LJ6]; sh.eold[2] = sh.tot[RV_LJ12];
+                for (int a = 0; a < na; ++a) {  // external-field force -2 kext q mu (MC.f90:988-997)
+                    const double q = sh.slot[na + a].q;
+                    sh.fold[3 * a] = sh.tot[RV_F + 3 * a] + D.m2k * q * sh.sc[SC_MU_X];
+                    sh.fold[3 * a + 1] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * sh.sc[SC_MU_Y];
+                    sh.fold[3 * a + 2] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * sh.sc[SC_MU_Z];
+                }
+            }
+            if (A.mode == MODE_OLD) {
+#pragma unroll
+                for (int k = 0; k < EPT; ++k)
+                    if (R.e[k] >= 0) {
+#pragma unroll
+                        for (int t = 0; t <= NT; ++t) A.scratch[(size_t)t * S + R.e[k]] = R.mold[k][t];
+                    }
+                __syncthreads();
+                if (tid == 0 && rank == 0) {
+                    for (int c = 0; c < 3; ++c) A.api_out[c] = sh.eold[c];
+                    for (int c = 0; c < 3 * na; ++c) A.api_out[RV_F + c] = sh.fold[c];
+                }
+                moves_done = 1;
+                break;
+            }
+        }
+
+        // ------------------------------------------------ proposal (movemc Step 5)
+        if (tid == 0) {
+            double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
+            for (int a = 0; a < na; ++a) { xo[a] = sh.slot[na + a].x; yo[a] = sh.slot[na + a].y; zo[a] = sh.slot[na + a].z; }
+            if (A.mode == MODE_RUN) {
+                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
+                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
+                double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+                if (biased) {
+                    double fx[kMaxA], fy[kMaxA], fz[kMaxA];
+                    for (int a = 0; a < na; ++a) { fx[a] = sh.fold[3 * a]; fy[a] = sh.fold[3 * a + 1]; fz[a] = sh.fold[3 * a + 2]; }
+                    mol_force_torque(na, xo, yo, zo, sh.mass, fx, fy, fz, F, T);
+                }
+                MoveState &m = sh.mv;
+                mcm_init_old(m, F, T);
+                mcm_choose_displacement(m, rng, D.xlf, D.dr);
+                if (!rng.out) mcm_choose_rotation(m, rng, D.xlc, D.d_angle);
+                if (rng.out) { sh.abort = 1; sh.cursor = sh.cursor_start; }
+                else sh.cursor = rng.cur;
+                place_molecule(m, na, xo, yo, zo, sh.mass, xn, yn, zn);
+            } else {  // MODE_EVAL: positions from the host
+                for (int a = 0; a < na; ++a) { xn[a] = A.api_in[1 + 3 * a]; yn[a] = A.api_in[2 + 3 * a]; zn[a] = A.api_in[3 + 3 * a]; }
+            }
+            for (int a = 0; a < na; ++a) { sh.slot[a].x = xn[a]; sh.slot[a].y = yn[a]; sh.slot[a].z = zn[a]; }
+            const bool split = biased || A.mode == MODE_EVAL;
+            sh.kind = split ? PASS_NEW : PASS_BOTH;
+            sh.forces = split ? 1 : 0;
+        }
+        __syncthreads();
+        if (sh.abort) break;
+        YAMC_PH(PH_PROPOSE);
+        // refill the other random window from the current cursor while the pass runs; the copy
+        // is awaited by warp 1 before the pass's reduction barrier (chain_pass)
+        if (A.mode == MODE_RUN && tid >= 32 && tid < 64) {
+            const int b = (int)((it + 1) & 1);
+            const long long base = sh.cursor;
+            const long long avail = run->n_rng - base;
+            const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
+            for (int i = tid - 32; i < nw; i += 32) __pipeline_memcpy_async(&rwin[b][i], run->rng + (base + i - run->rng_off), 4);
+            __pipeline_commit();
+            if (tid == 32) { sh.wbase[b] = base; sh.wn[b] = nw; }
+        }
+
+        // ------------------------------------------------ new positions: energies, delta rho, overlap
+        if (biased || A.mode == MODE_EVAL)
+            chain_pass<NT, EPT, PASS_NEW, true>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+        else
+            chain_pass<NT, EPT, PASS_BOTH, false>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+        xpar ^= 1;
+        if (prof) t_mark = clock64();
+
+        if (A.mode == MODE_EVAL) {
+#pragma unroll
+            for (int k = 0; k < EPT; ++k)
+                if (R.e[k] >= 0) {
+#pragma unroll
+                    for (int t = 0; t <= NT; ++t) A.scratch[(size_t)(1 + nt + t) * S + R.e[k]] = R.dl[k][t];
+                }
+            if (tid == 0 && rank == 0)
+                for (int v = 0; v < RV_F + 3 * na; ++v) A.api_out[v] = sh.tot[v];
+            moves_done = 1;
+            break;
+        }
+
+        // ------------------------------------------------ Metropolis (Steps 7-13) and commit (Step 14)
+        if (tid == 0) {
+            const bool overlap = sh.tot[RV_OVL] > 0.0;
+            int flags = overlap ? 2 : 0;
+            double du_real = 0, du_kc = 0, du_kl = 0, du_ext = 0, dmx = 0, dmy = 0, dmz = 0;
+            double dew = 0, dlj6 = 0, dlj12 = 0;
+            sh.accepted = 0;
+            if (!overlap) {
+                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
+                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
+                if (biased) {
+                    dew = sh.tot[RV_EW] - sh.eold[0]; dlj6 = sh.tot[RV_LJ6] - sh.eold[1]; dlj12 = sh.tot[RV_LJ12] - sh.eold[2];
+                    du_real = (sh.tot[RV_EW] + sh.tot[RV_LJ12] - sh.tot[RV_LJ6]) - (sh.eold[0] + sh.eold[2] - sh.eold[1]);
+                } else {
+                    dew = sh.tot[RV_EW]; dlj6 = sh.tot[RV_LJ6]; dlj12 = sh.tot[RV_LJ12];
+                    du_real = dew + dlj12 - dlj6;
+                }
+                du_kc = sh.tot[RV_DUC];
+                du_kl = sh.tot[RV_DUL];
+                double mx = 0, my = 0, mz = 0;
+                for (int a = 0; a < na; ++a) { mx = mx + sh.slot[a].q * sh.slot[a].x; my = my + sh.slot[a].q * sh.slot[a].y; mz = mz + sh.slot[a].q * sh.slot[a].z; }
+                dmx = mx - sh.mu_old[0]; dmy = my - sh.mu_old[1]; dmz = mz - sh.mu_old[2];
+                const double mux = sh.sc[SC_MU_X], muy = sh.sc[SC_MU_Y], muz = sh.sc[SC_MU_Z];
+                // EwaldSumExternal_calc_dU (EwaldSumExternal.f90:68-82)
+                du_ext = D.kext * ((2 * mux + dmx) * dmx + (2 * muy + dmy) * dmy + (2 * muz + dmz) * dmz);
+                double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+                if (biased) {
+                    double fx[kMaxA], fy[kMaxA], fz[kMaxA], x[kMaxA], y[kMaxA], z[kMaxA];
+                    for (int a = 0; a < na; ++a) {
+                        const double q = sh.slot[a].q;
+                        fx[a] = sh.tot[RV_F + 3 * a] + D.m2k * q * (mux + dmx);
+                        fy[a] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * (muy + dmy);
+                        fz[a] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * (muz + dmz);
+                        x[a] = sh.slot[a].x; y[a] = sh.slot[a].y; z[a] = sh.slot[a].z;
+                    }
+                    mol_force_torque(na, x, y, z, sh.mass, fx, fy, fz, F, T);
+                }
+                const double du_total = du_real + (du_kc + du_kl) + du_ext;
+                mcm_init_new(sh.mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
+                const int acc = mcm_accept(sh.mv, du_total, D.xlf, D.xlc, rng);
+                if (rng.out) sh.abort = 1;
+                else { sh.cursor = rng.cur; sh.accepted = acc; flags |= acc; }
+            }
+            if (!sh.abort) {
+                if (sh.accepted) {
+                    sh.sc[SC_UU_EW] += dew; sh.sc[SC_UU_LJ6] += dlj6; sh.sc[SC_UU_LJ12] += dlj12;
+                    sh.sc[SC_EK_C] += du_kc; sh.sc[SC_EK_LJ] += du_kl;
+                    sh.sc[SC_MU_X] += dmx; sh.sc[SC_MU_Y] += dmy; sh.sc[SC_MU_Z] += dmz;
+                    sh.sc[SC_N_MV_ACC] += 1.0;
+                    sh.last_mol = sh.imol - 1;
+                    for (int a = 0; a < na; ++a) { sh.lx[a] = sh.slot[a].x; sh.ly[a] = sh.slot[a].y; sh.lz[a] = sh.slot[a].z; }
+                    ++n_acc;
+                }
+                sh.sc[SC_N_MV_STEPS] += 1.0;
+                if (rank == 0) {
+                    if (sh.accepted)
+                        for (int a = 0; a < na; ++a) {
+                            double4 p = D.atom[sh.first + a];
+                            p.x = sh.slot[a].x; p.y = sh.slot[a].y; p.z = sh.slot[a].z;
+                            D.atom[sh.first + a] = p;
+                        }
+                    if (run->log) {
+                        yamc_move_record rec;
+                        rec.imol = sh.imol; rec.flags = flags; rec.cursor = sh.cursor;
+                        rec.du_real = du_real; rec.du_k_coul = du_kc; rec.du_k_lj = du_kl; rec.du_ext = du_ext;
+                        run->log[it] = rec;
+                    }
+                }
+                // cycle bookkeeping and energy.dat rows (runmc.f90:230-279)
+                sh.mic += 1;
+                if (sh.mic == D.M) {
+                    sh.mic = 0;
+                    const double fr = sh.sc[SC_N_MV_STEPS] / D.M + sh.sc[SC_N_VOL_STEPS];
+                    if (fmod(fr, D.n_store_energy_interval) < 1e-10 && rank == 0 && run->rows && rows < run->max_rows) {
+                        const double *sc = sh.sc;
+                        const double uext = D.kext * (sc[SC_MU_X] * sc[SC_MU_X] + sc[SC_MU_Y] * sc[SC_MU_Y] + sc[SC_MU_Z] * sc[SC_MU_Z]);
+                        const double utew = sc[SC_UU_EW] + sc[SC_EK_C] + sc[SC_TAIL_C] + uext;
+                        const double utlj = sc[SC_UU_LJ12] - sc[SC_UU_LJ6] + sc[SC_EK_LJ] + sc[SC_TAIL_LJ12] - sc[SC_TAIL_LJ6];
+                        double *row = run->rows + 9 * (size_t)rows;
+                        row[0] = (double)sh.icycle; row[1] = utew + utlj; row[2] = utew; row[3] = utlj;
+                        row[4] = sc[SC_UU_EW]; row[5] = sc[SC_UU_LJ6]; row[6] = sc[SC_UU_LJ12];
+                        row[7] = sc[SC_EK_C]; row[8] = sc[SC_EK_LJ];
+                        ++rows;
+                    }
+                    sh.icycle += 1;
+                }
+            } else {
+                sh.cursor = sh.cursor_start;  // the interrupted move restarts from its first draw
+            }
+        }
+        __syncthreads();
+        if (sh.abort) break;
+        YAMC_PH(PH_DECIDE);
+        if (sh.accepted) {
+#pragma unroll
+            for (int k = 0; k < EPT; ++k)
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) { R.rho[k][t].x += R.dl[k][t].x; R.rho[k][t].y += R.dl[k][t].y; }
+            if (tid < na) {  // this CTA's staged copy of the moved atoms
+                const int j = sh.first + tid;
+                if (j % G == rank) {
+                    double4 p = atom_s[j / G];
+                    p.x = sh.slot[tid].x; p.y = sh.slot[tid].y; p.z = sh.slot[tid].z;
+                    atom_s[j / G] = p;
+                }
+            }
+        }
+        ++moves_done;
+        __syncthreads();
+        YAMC_PH(PH_COMMIT);
+    }
+#undef YAMC_PH
+
+    if (A.mode == MODE_RUN) {  // write back the register and shared state
+#pragma unroll
+        for (int k = 0; k < EPT; ++k)
+            if (R.e[k] >= 0) {
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) D.rho[(size_t)t * S + R.e[k]] = R.rho[k][t];
+            }
+        if (tid == 0 && rank == 0) {
+            for (int c = 0; c < SC_COUNT; ++c) D.scal[c] = sh.sc[c];
+            D.cnt[CN_ICYCLE] = sh.icycle;
+            D.cnt[CN_MOVE_IN_CYCLE] = sh.mic;
+            run->cursor = sh.cursor;
+            run->moves_done = moves_done;
+            run->n_rows = rows;
+            run->accepted = n_acc;
+            run->status = sh.abort ? YAMC_ERNG_EXHAUSTED : YAMC_OK;
+        }
+    } else if (tid == 0 && rank == 0) {
+        run->moves_done = moves_done;
+        run->status = YAMC_OK;
+    }
+    if (G > 1) cluster.sync();  // no CTA leaves while another may still address its shared memory
+}
+
+// per-move API commit: rho += delta (Step 14, MC.f90:1245)
+__global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { double2 r = rho[i]; const double2 d = delta[i]; r.x += d.x; r.y += d.y; rho[i] = r; }
+}
+
+}  // namespace yamc
+
+// ==========================================================================================
+// host side: context, launches and the C ABI
+// ==========================================================================================
+using namespace yamc;
+
+namespace {
+
+#define CUDA_TRY(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess) {                                                              \
+            set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));                    \
+            return YAMC_ECUDA;                                                                \
+        }                                                                                     \
+    } while (0)
+
+template <class T>
+int dalloc(T **p, size_t n) {
+    *p = nullptr;
+    if (n == 0) n = 1;
+    CUDA_TRY(cudaMalloc((void **)p, n * sizeof(T)));
+    return YAMC_OK;
+}
+
+template <class T>
+int upload(T *d, const T *h, size_t n, cudaStream_t s) {
+    if (n) CUDA_TRY(cudaMemcpyAsync(d, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+    return YAMC_OK;
+}
+
+struct LaunchCfg {
+    int G = 0, B = 0, EPT = 0;
+    int nown_max = 0, qcap = 0;
+    size_t smem = 0;
+};
+
+size_t chain_smem_bytes(int G, int B, int kmax, int nt, int nown_max, int qcap) {
+    const int KM = kmax + 1;
+    size_t b = sizeof(double2) * 2 * kMaxA * 3 * KM;
+    b += (sizeof(double4) + sizeof(double) + sizeof(int2)) * (size_t)nown_max;
+    b += sizeof(int) * (size_t)((qcap + 1) & ~1);
+    b += sizeof(double) * (size_t)(B / 32) * kNV;
+    b += sizeof(double) * (size_t)2 * G * kNV;
+    b += sizeof(double) * (size_t)2 * nt * nt;
+    return b;
+}
+
+}  // namespace
+
+struct yamc_ctx {
+    HostSystem H;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    float last_ms = 0.f;
+    // device state
+    double4 *atom = nullptr;
+    int2 *meta = nullptr, *mol = nullptr;
+    double *dhs = nullptr, *mass = nullptr, *ebeta = nullptr, *ebetalj = nullptr, *lj_sig6 = nullptr, *lj_feps = nullptr;
+    int4 *kvec = nullptr;
+    int *pair_index = nullptr;
+    double2 *rho = nullptr, *scratch = nullptr;
+    double *freq_beg = nullptr, *freq_end = nullptr, *scal = nullptr;
+    long long *cnt = nullptr;
+    int4 *spec = nullptr;
+    double *uu = nullptr, *fx = nullptr, *fy = nullptr, *fz = nullptr, *part = nullptr;
+    DevSys hsys{};
+    DevSys *d_sys = nullptr;
+    RunSlot *d_run = nullptr;
+    double *api_in = nullptr, *api_out = nullptr;
+    float *d_rng = nullptr;
+    size_t rng_cap = 0;
+    yamc_move_record *d_log = nullptr;
+    size_t log_cap = 0;
+    double *d_rows = nullptr;
+    int rows_cap = 0;
+    // host mirrors
+    double sc[SC_COUNT] = {};
+    long long cnt_h[CN_COUNT] = {};
+    bool pos_valid = true;  // H.x/y/z mirror the device positions
+    LaunchCfg cfg;
+    int force_G = 0, force_B = 0;
+    // per-move API state
+    int api_imol = 0, api_stage = 0;
+    double api_eold[3] = {}, api_fold[3 * kMaxA] = {};
+    double api_new[kNV] = {};
+    double api_xn[kMaxA] = {}, api_yn[kMaxA] = {}, api_zn[kMaxA] = {};
+    double api_dmu[3] = {};
+    long long *d_prof = nullptr;
+    bool prof_on = false;
+};
+
+namespace {
+
+int pick_launch(yamc_ctx *c, LaunchCfg *out) {
+    const HostSystem &H = c->H;
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, c->device));
+    const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
+    const int Bs[] = {512, 256};
+    const int Gs[] = {1, 2, 4, 8, 16};
+    for (int gi = 0; gi < 5; ++gi) {
+        const int G = Gs[gi];
+        if (c->force_G && G != c->force_G) continue;
+        for (int bi = 0; bi < 2; ++bi) {
+            const int B = Bs[bi];
+            if (c->force_B && B != c->force_B) continue;
+            if (!c->force_B && B != 512 && G * 512 < H.S) continue;
+            const int EPT = (H.S + G * B - 1) / (G * B);
+            if (EPT > 2) continue;
+            const int nown_max = (H.N + G - 1) / G;
+            const int qcap = std::min(nown_max, B * kCPT) * 2 * kMaxA;  // one filter round of pairs
+            const size_t sm = chain_smem_bytes(G, B, H.kmax, H.nt, nown_max, qcap);
+            if (sm > smem_max) continue;
+            out->G = G; out->B = B; out->EPT = EPT; out->nown_max = nown_max; out->qcap = qcap; out->smem = sm;
+            return YAMC_OK;
+        }
+    }
+    set_error("no launch configuration fits this system (k-set or atoms too large for one cluster)");
+    return YAMC_ELIMITS;
+}
+
+template <int NT, int EPT>
+int launch_chain_t(yamc_ctx *c, const ChainArgs &args) {
+    const LaunchCfg &L = c->cfg;
+    auto kfn = k_chain<NT, EPT>;
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    if (L.G > 8) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.G, 1, 1);
+    cfg.blockDim = dim3(L.B, 1, 1);
+    cfg.dynamicSmemBytes = L.smem;
+    cfg.stream = c->stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = L.G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, kfn, args));
+    return YAMC_OK;
+}
+
+int launch_chain(yamc_ctx *c, const ChainArgs &args) {
+    const int nt = c->H.nt, ept = c->cfg.EPT;
+#define YAMC_CASE(NT_, EPT_) if (nt == NT_ && ept == EPT_) return launch_chain_t<NT_, EPT_>(c, args);
+#ifdef YAMC_ONE_VARIANT  // development builds: a single instantiation compiles in seconds
+    YAMC_CASE(3, 1)
+#else
+    YAMC_CASE(1, 1) YAMC_CASE(1, 2) YAMC_CASE(2, 1) YAMC_CASE(2, 2)
+    YAMC_CASE(3, 1) YAMC_CASE(3, 2) YAMC_CASE(4, 1) YAMC_CASE(4, 2)
+#endif
+#undef YAMC_CASE
+    set_error("LJ type count outside 1..4 or k-set too large for the chain kernel");
+    return YAMC_ELIMITS;
+}
+
+template <int NT>
+int launch_rho_full(yamc_ctx *c) {
+    const int KM = c->H.kmax + 1;
+    const size_t sm = sizeof(double2) * kRhoChunk * 3 * KM;
+    CUDA_TRY(cudaFuncSetAttribute(k_rho_full<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_rho_full<NT><<<(c->H.S + kRhoBlock - 1) / kRhoBlock, kRhoBlock, sm, c->stream>>>(c->hsys, c->rho);
+    CUDA_TRY(cudaGetLastError());
+    return YAMC_OK;
+}
+
+template <int NT>
+int launch_kspace_energy(yamc_ctx *c, int nb) {
+    k_kspace_energy<NT><<<nb, 256, 0, c->stream>>>(c->hsys, c->rho, c->part);
+    CUDA_TRY(cudaGetLastError());
+    return YAMC_OK;
+}
+
+int sync_positions(yamc_ctx *c) {
+    if (c->pos_valid) return YAMC_OK;
+    std::vector<double4> a(c->H.N);
+    CUDA_TRY(cudaMemcpyAsync(a.data(), c->atom, sizeof(double4) * c->H.N, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int i = 0; i < c->H.N; ++i) { c->H.x[i] = a[i].x; c->H.y[i] = a[i].y; c->H.z[i] = a[i].z; }
+    c->pos_valid = true;
+    return YAMC_OK;
+}
+
+int pull_state(yamc_ctx *c) {
+    CUDA_TRY(cudaMemcpyAsync(c->sc, c->scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->cnt_h, c->cnt, sizeof(long long) * CN_COUNT, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return YAMC_OK;
+}
+
+int push_state(yamc_ctx *c) {
+    CUDA_TRY(cudaMemcpyAsync(c->scal, c->sc, sizeof(double) * SC_COUNT, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->cnt, c->cnt_h, sizeof(long long) * CN_COUNT, cudaMemcpyHostToDevice, c->stream));
+    return YAMC_OK;
+}
+
+// mc_calc_total_sums (MC.f90:477-585) on the device
+int full_sums(yamc_ctx *c) {
+    HostSystem &H = c->H;
+    int r = sync_positions(c);
+    if (r) return r;
+    const int nbr = (H.N + kFullTile - 1) / kFullTile;
+    k_realspace_full<<<nbr, kFullTile, 0, c->stream>>>(c->hsys, c->uu, c->fx, c->fy, c->fz, c->part);
+    CUDA_TRY(cudaGetLastError());
+    std::vector<double> pr((size_t)nbr * kFullParts);
+    CUDA_TRY(cudaMemcpyAsync(pr.data(), c->part, sizeof(double) * pr.size(), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double tot[kFullParts] = {};
+    for (int b = 0; b < nbr; ++b)
+        for (int v = 0; v < kFullParts; ++v) tot[v] = (v == 6) ? std::max(tot[v], pr[b * kFullParts + v]) : tot[v] + pr[b * kFullParts + v];
+    if (tot[6] > 0) { set_error("hard-core overlap in the configuration"); return YAMC_EOVERLAP_INIT; }
+    switch (H.nt) {
+        case 1: r = launch_rho_full<1>(c); break;
+        case 2: r = launch_rho_full<2>(c); break;
+        case 3: r = launch_rho_full<3>(c); break;
+        case 4: r = launch_rho_full<4>(c); break;
+        default: set_error("LJ type count outside 1..4"); return YAMC_ELIMITS;
+    }
+    if (r) return r;
+    const int nbk = (H.S + 255) / 256;
+    switch (H.nt) {
+        case 1: r = launch_kspace_energy<1>(c, nbk); break;
+        case 2: r = launch_kspace_energy<2>(c, nbk); break;
+        case 3: r = launch_kspace_energy<3>(c, nbk); break;
+        default: r = launch_kspace_energy<4>(c, nbk); break;
+    }
+    if (r) return r;
+    std::vector<double> pk((size_t)nbk * 2);
+    CUDA_TRY(cudaMemcpyAsync(pk.data(), c->part, sizeof(double) * pk.size(), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    double ekc = 0, ekl = 0;
+    for (int b = 0; b < nbk; ++b) { ekc += pk[2 * b]; ekl += pk[2 * b + 1]; }
+    // EwaldSumExternal_calc_mu over all atoms, in atom order (EwaldSumExternal.f90:34-52)
+    double mx = 0, my = 0, mz = 0;
+    for (int i = 0; i < H.N; ++i) { mx = mx + H.q[i] * H.x[i]; my = my + H.q[i] * H.y[i]; mz = mz + H.q[i] * H.z[i]; }
+    c->sc[SC_UU_EW] = tot[0]; c->sc[SC_UU_LJ6] = tot[1]; c->sc[SC_UU_LJ12] = tot[2];
+    c->sc[SC_UU_EW_INTRA] = tot[3]; c->sc[SC_UU_LJ6_INTRA] = tot[4]; c->sc[SC_UU_LJ12_INTRA] = tot[5];
+    c->sc[SC_EK_C] = ekc; c->sc[SC_EK_LJ] = ekl;
+    c->sc[SC_MU_X] = mx; c->sc[SC_MU_Y] = my; c->sc[SC_MU_Z] = mz;
+    c->sc[SC_TAIL_C] = H.U_tail_coul; c->sc[SC_TAIL_LJ6] = H.U_tail_lj6; c->sc[SC_TAIL_LJ12] = H.U_tail_lj12;
+    return push_state(c);
+}
+
+// mc_total_energy (MC.f90:681-698) from the engine scalars
+void energies_from(const double *sc, double kext, double e[8]) {
+    const double uext = kext * (sc[SC_MU_X] * sc[SC_MU_X] + sc[SC_MU_Y] * sc[SC_MU_Y] + sc[SC_MU_Z] * sc[SC_MU_Z]);
+    const double utew = sc[SC_UU_EW] + sc[SC_EK_C] + sc[SC_TAIL_C] + uext;
+    const double utlj = sc[SC_UU_LJ12] - sc[SC_UU_LJ6] + sc[SC_EK_LJ] + sc[SC_TAIL_LJ12] - sc[SC_TAIL_LJ6];
+    e[0] = utew + utlj; e[1] = utew; e[2] = utlj;
+    e[3] = sc[SC_UU_EW]; e[4] = sc[SC_UU_LJ6]; e[5] = sc[SC_UU_LJ12]; e[6] = sc[SC_EK_C]; e[7] = sc[SC_EK_LJ];
+}
+
+int ensure_cfg(yamc_ctx *c) {
+    if (c->cfg.G) return YAMC_OK;
+    return pick_launch(c, &c->cfg);
+}
+
+ChainArgs base_args(yamc_ctx *c, int mode) {
+    ChainArgs a{};
+    a.sys = c->d_sys; a.run = c->d_run; a.G = c->cfg.G; a.mode = mode;
+    a.nown_max = c->cfg.nown_max; a.qcap = c->cfg.qcap;
+    a.api_in = c->api_in; a.api_out = c->api_out; a.scratch = c->scratch;
+    a.prof = c->prof_on ? c->d_prof : nullptr;
+    return a;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *yamc_error_string(int s) {
+    switch (s) {
+        case YAMC_OK: return "ok";
+        case YAMC_EIO: return "I/O error";
+        case YAMC_ELIMITS: return "limits exceeded";
+        case YAMC_EPARAMETER: return "bad parameter";
+        case YAMC_EINIT: return "not initialised";
+        case YAMC_EWRONG_FUNCTION: return "wrong function for this state";
+        case YAMC_ECUDA: return "CUDA error";
+        case YAMC_ETIMEOUT: return "device wait timed out";
+        case YAMC_ERNG_EXHAUSTED: return "random stream exhausted";
+        case YAMC_ENAN: return "non-finite value";
+        case YAMC_EOVERLAP_INIT: return "hard-core overlap in the initial configuration";
+        default: return "unknown status";
+    }
+}
+
+int yamc_destroy(yamc_ctx *c);
+
+static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p, int32_t device) {
+    int r = prepare_host_system(sys, p, &c->H);
+    if (r) return r;
+    HostSystem &H = c->H;
+    if (H.nt < 1 || H.nt > 4) { set_error("the device kernels support 1..4 LJ types"); return YAMC_ELIMITS; }
+    c->device = device;
+    CUDA_TRY(cudaSetDevice(device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&c->ev0));
+    CUDA_TRY(cudaEventCreate(&c->ev1));
+    const int N = H.N, M = H.M, S = H.S, nt = H.nt;
+    if ((r = dalloc(&c->atom, N)) || (r = dalloc(&c->meta, N)) || (r = dalloc(&c->dhs, N)) || (r = dalloc(&c->mass, N)) ||
+        (r = dalloc(&c->mol, M)) || (r = dalloc(&c->kvec, S)) || (r = dalloc(&c->ebeta, S)) ||
+        (r = dalloc(&c->ebetalj, (size_t)H.npair * S)) || (r = dalloc(&c->pair_index, nt * nt)) ||
+        (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
+        (r = dalloc(&c->scratch, (size_t)2 * (1 + nt) * S)) || (r = dalloc(&c->freq_beg, M)) || (r = dalloc(&c->freq_end, M)) ||
+        (r = dalloc(&c->scal, SC_COUNT)) || (r = dalloc(&c->cnt, CN_COUNT)) || (r = dalloc(&c->uu, N)) ||
+        (r = dalloc(&c->fx, N)) || (r = dalloc(&c->fy, N)) || (r = dalloc(&c->fz, N)) ||
+        (r = dalloc(&c->part, (size_t)std::max((N + kFullTile - 1) / kFullTile * kFullParts, (S + 255) / 256 * 2))) ||
+        (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->api_in, 1 + 3 * kMaxA)) ||
+        (r = dalloc(&c->api_out, kNV)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
+        return r;
+    std::vector<double4> a(N);
+    std::vector<int2> m(N);
+    for (int i = 0; i < N; ++i) { a[i] = make_double4(H.x[i], H.y[i], H.z[i], H.q[i]); m[i] = make_int2(H.molnum[i], H.type_by_index[i]); }
+    std::vector<int2> mo(M);
+    for (int i = 0; i < M; ++i) mo[i] = make_int2(H.first[i], H.natoms[i]);
+    std::vector<int4> kv(S);
+    for (int e = 0; e < S; ++e) kv[e] = make_int4(H.ekx[e], H.eky[e], H.ekz[e], H.ekk[e]);
+    std::vector<int> pidx(nt * nt);
+    for (int i = 0; i < nt * nt; ++i) pidx[i] = H.pair_index[i];
+    if ((r = upload(c->atom, a.data(), N, c->stream)) || (r = upload(c->meta, m.data(), N, c->stream)) ||
+        (r = upload(c->dhs, H.dhs.data(), N, c->stream)) || (r = upload(c->mass, H.mass.data(), N, c->stream)) ||
+        (r = upload(c->mol, mo.data(), M, c->stream)) || (r = upload(c->kvec, kv.data(), S, c->stream)) ||
+        (r = upload(c->ebeta, H.ebeta.data(), S, c->stream)) || (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) ||
+        (r = upload(c->pair_index, pidx.data(), nt * nt, c->stream)) || (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
+        (r = upload(c->lj_feps, H.four_eps.data(), nt * nt, c->stream)) || (r = upload(c->freq_beg, H.freq_beg.data(), M, c->stream)) ||
+        (r = upload(c->freq_end, H.freq_end.data(), M, c->stream)) ||
+        (r = upload(c->spec, reinterpret_cast<const int4 *>(H.spec.data()), H.spec.size() / 4, c->stream)))
+        return r;
+    DevSys &D = c->hsys;
+    D.N = N; D.M = M; D.S = S; D.nt = nt; D.kmax = H.kmax; D.npair = H.npair; D.freq_monotone = H.freq_monotone;
+    D.n_species = (int)H.mol_numbers.size();
+    const yamc_params &P = H.p;
+    D.rmax2 = P.rmax2; D.alpha = P.alpha; D.xclb = P.xclb; D.taosp = P.two_alpha_over_sqrt_pi; D.kext = P.kext;
+    D.m2k = P.minus_two_kext; D.dr = P.dr; D.d_angle = P.d_angle; D.xlf = P.xlambda_f; D.xlc = P.xlambda_c;
+    D.psm = P.pressure_step_multiplier; D.n_store_energy_interval = P.n_store_energy_interval;
+    D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
+    D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
+    D.rho = c->rho; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
+    D.nspec = (int)(H.spec.size() / 4); D.spec = c->spec;
+    if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
+    c->cnt_h[CN_ICYCLE] = 1;
+    c->cnt_h[CN_MOVE_IN_CYCLE] = 0;
+    if ((r = full_sums(c))) return r;  // initmc
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return YAMC_OK;
+}
+
+int yamc_create(const yamc_system *sys, const yamc_params *p, int32_t device, yamc_ctx **out) {
+    if (!out) return YAMC_EPARAMETER;
+    *out = nullptr;
+    yamc_ctx *c = new yamc_ctx();
+    const int r = create_impl(c, sys, p, device);
+    if (r) { yamc_destroy(c); return r; }
+    *out = c;
+    return YAMC_OK;
+}
+
+int yamc_destroy(yamc_ctx *c) {
+    if (!c) return YAMC_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
+                    c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->uu, c->fx, c->fy,
+                    c->fz, c->part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
+                    c->d_prof, c->spec};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return YAMC_OK;
+}
+
+int yamc_sizes(yamc_ctx *c, int32_t out[5]) {
+    if (!c || !out) return YAMC_EPARAMETER;
+    out[0] = c->H.N; out[1] = c->H.M; out[2] = c->H.nk; out[3] = c->H.S; out[4] = c->H.nt;
+    return YAMC_OK;
+}
+
+int yamc_energies(yamc_ctx *c, double e[8]) {
+    if (!c || !e) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int r = pull_state(c);
+    if (r) return r;
+    energies_from(c->sc, c->H.p.kext, e);
+    return YAMC_OK;
+}
+
+int yamc_full_sums(yamc_ctx *c, double e[8]) {
+    if (!c) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int r = pull_state(c);
+    if (r) return r;
+    if ((r = full_sums(c))) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (e) energies_from(c->sc, c->H.p.kext, e);
+    return YAMC_OK;
+}
+
+int yamc_get_positions(yamc_ctx *c, double *x, double *y, double *z) {
+    if (!c) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int r = sync_positions(c);
+    if (r) return r;
+    for (int i = 0; i < c->H.N; ++i) {
+        if (x) x[i] = c->H.x[i];
+        if (y) y[i] = c->H.y[i];
+        if (z) z[i] = c->H.z[i];
+    }
+    return YAMC_OK;
+}
+
+int yamc_set_launch(yamc_ctx *c, int32_t cluster_blocks, int32_t threads) {
+    if (!c) return YAMC_EPARAMETER;
+    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > 512 || (threads % 32)) return YAMC_EPARAMETER;
+    c->force_G = cluster_blocks;
+    c->force_B = threads;
+    c->cfg = LaunchCfg();
+    return pick_launch(c, &c->cfg);
+}
+
+int yamc_get_launch(yamc_ctx *c, int32_t out[4]) {
+    if (!c || !out) return YAMC_EPARAMETER;
+    int r = ensure_cfg(c);
+    if (r) return r;
+    out[0] = c->cfg.G; out[1] = c->cfg.B; out[2] = c->cfg.EPT; out[3] = (int32_t)c->cfg.smem;
+    return YAMC_OK;
+}
+
+int yamc_last_kernel_ms(yamc_ctx *c, double *ms) {
+    if (!c || !ms) return YAMC_EPARAMETER;
+    *ms = c->last_ms;
+    return YAMC_OK;
+}
+
+static int run_chain_impl(yamc_ctx *c, const float *d_rng, long long rng_off, long long n_rng, int64_t *cursor,
+                          int64_t n_moves, int64_t *moves_done, yamc_move_record *d_log, double *d_rows, int max_rows,
+                          int32_t *n_rows) {
+    int r = ensure_cfg(c);
+    if (r) return r;
+    RunSlot rs{};
+    rs.rng = d_rng; rs.rng_off = rng_off; rs.n_rng = n_rng; rs.cursor = *cursor; rs.n_moves = n_moves;
+    rs.log = d_log; rs.rows = d_rows; rs.max_rows = max_rows;
+    if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
+    ChainArgs a = base_args(c, MODE_RUN);
+    CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
+    if ((r = launch_chain(c, a))) return r;
+    CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
+    RunSlot back{};
+    CUDA_TRY(cudaMemcpyAsync(&back, c->d_run, sizeof(RunSlot), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
+    c->pos_valid = false;
+    *cursor = back.cursor;
+    if (moves_done) *moves_done = back.moves_done;
+    if (n_rows) *n_rows = back.n_rows;
+    return back.status;
+}
+
+int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_t *cursor, int64_t n_moves,
+                          int64_t *moves_done, yamc_move_record *d_log, double *d_rows, int32_t max_rows, int32_t *n_rows) {
+    if (!c || !d_rng || !cursor || n_moves < 0) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    return run_chain_impl(c, d_rng, 0, n_rng, cursor, n_moves, moves_done, d_log, d_rows, max_rows, n_rows);
+}
+
+int yamc_run_chain(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_moves, int64_t *moves_done,
+                   yamc_move_record *log, double *rows, int32_t max_rows, int32_t *n_rows) {
+    if (!c || !rng || !cursor || n_moves < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const size_t nr = (size_t)(n_rng - *cursor);
+    if (nr > c->rng_cap) {
+        if (c->d_rng) cudaFree(c->d_rng);
+        c->d_rng = nullptr;
+        c->rng_cap = 0;
+        int r = dalloc(&c->d_rng, nr);
+        if (r) return r;
+        c->rng_cap = nr;
+    }
+    CUDA_TRY(cudaMemcpyAsync(c->d_rng, rng + *cursor, nr * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    if (log && (size_t)n_moves > c->log_cap) {
+        if (c->d_log) cudaFree(c->d_log);
+        c->d_log = nullptr;
+        c->log_cap = 0;
+        int r = dalloc(&c->d_log, (size_t)n_moves);
+        if (r) return r;
+        c->log_cap = (size_t)n_moves;
+    }
+    if (rows && max_rows > c->rows_cap) {
+        if (c->d_rows) cudaFree(c->d_rows);
+        c->d_rows = nullptr;
+        c->rows_cap = 0;
+        int r = dalloc(&c->d_rows, (size_t)9 * max_rows);
+        if (r) return r;
+        c->rows_cap = max_rows;
+    }
+    int64_t done = 0;
+    int32_t nrow = 0;
+    const int st = run_chain_impl(c, c->d_rng, *cursor, n_rng, cursor, n_moves, &done, log ? c->d_log : nullptr,
+                                  rows ? c->d_rows : nullptr, rows ? max_rows : 0, &nrow);
+    if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
+    if (log && done) CUDA_TRY(cudaMemcpy(log, c->d_log, sizeof(yamc_move_record) * done, cudaMemcpyDeviceToHost));
+    if (rows && nrow) CUDA_TRY(cudaMemcpy(rows, c->d_rows, sizeof(double) * 9 * nrow, cudaMemcpyDeviceToHost));
+    if (moves_done) *moves_done = done;
+    if (n_rows) *n_rows = nrow;
+    return st;
+}
+
+// ---------------------------------------------------------------- per-move drop-in
+
+int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
+    if (!c || imol < 1 || imol > c->H.M) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int r = ensure_cfg(c);
+    if (r) return r;
+    if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
+    double in[1 + 3 * kMaxA] = {};
+    in[0] = imol;
+    if ((r = upload(c->api_in, in, 1 + 3 * kMaxA, c->stream))) return r;
+    RunSlot rs{};
+    if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
+    if ((r = launch_chain(c, base_args(c, MODE_OLD)))) return r;
+    double out[kNV];
+    CUDA_TRY(cudaMemcpyAsync(out, c->api_out, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const HostSystem &H = c->H;
+    const int f0 = H.first[imol - 1], na = H.natoms[imol - 1];
+    for (int k = 0; k < 3; ++k) c->api_eold[k] = out[k];
+    for (int k = 0; k < 3 * na; ++k) c->api_fold[k] = out[RV_F + k];
+    double fx[kMaxA], fy[kMaxA], fz[kMaxA];
+    for (int a = 0; a < na; ++a) { fx[a] = out[RV_F + 3 * a]; fy[a] = out[RV_F + 3 * a + 1]; fz[a] = out[RV_F + 3 * a + 2]; }
+    double F[3], T[3];
+    mol_force_torque(na, &H.x[f0], &H.y[f0], &H.z[f0], &H.mass[f0], fx, fy, fz, F, T);
+    if (f) { f[0] = F[0]; f[1] = F[1]; f[2] = F[2]; }
+    if (tau) { tau[0] = T[0]; tau[1] = T[1]; tau[2] = T[2]; }
+    c->api_imol = imol;
+    c->api_stage = 1;
+    return YAMC_OK;
+}
+
+int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn, const double *zn, double du[4],
+                   int32_t *overlap, double f[3], double tau[3]) {
+    if (!c || !xn || !yn || !zn) return YAMC_EPARAMETER;
+    if (c->api_stage != 1 || imol != c->api_imol) { set_error("yamc_move_eval must follow yamc_move_old for the same molecule"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    const HostSystem &H = c->H;
+    const int f0 = H.first[imol - 1], na = H.natoms[imol - 1];
+    double in[1 + 3 * kMaxA] = {};
+    in[0] = imol;
+    for (int a = 0; a < na; ++a) { in[1 + 3 * a] = xn[a]; in[2 + 3 * a] = yn[a]; in[3 + 3 * a] = zn[a]; }
+    int r = upload(c->api_in, in, 1 + 3 * kMaxA, c->stream);
+    if (r) return r;
+    if ((r = launch_chain(c, base_args(c, MODE_EVAL)))) return r;
+    double out[kNV];
+    CUDA_TRY(cudaMemcpyAsync(out, c->api_out, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < kNV; ++v) c->api_new[v] = out[v];
+    for (int a = 0; a < na; ++a) { c->api_xn[a] = xn[a]; c->api_yn[a] = yn[a]; c->api_zn[a] = zn[a]; }
+    const int ovl = out[RV_OVL] > 0.0;
+    if (overlap) *overlap = ovl;
+    // Steps 7, 10-11, 11A
+    const double enew = out[RV_EW] + out[RV_LJ12] - out[RV_LJ6];
+    const double eold = c->api_eold[0] + c->api_eold[2] - c->api_eold[1];
+    double mo[3] = {0, 0, 0}, mn[3] = {0, 0, 0};
+    for (int a = 0; a < na; ++a) {
+        const double q = H.q[f0 + a];
+        mo[0] = mo[0] + q * H.x[f0 + a]; mo[1] = mo[1] + q * H.y[f0 + a]; mo[2] = mo[2] + q * H.z[f0 + a];
+        mn[0] = mn[0] + q * xn[a]; mn[1] = mn[1] + q * yn[a]; mn[2] = mn[2] + q * zn[a];
+    }
+    const double *mu = &c->sc[SC_MU_X];
+    for (int k = 0; k < 3; ++k) c->api_dmu[k] = mn[k] - mo[k];
+    const double *dm = c->api_dmu;
+    const double du_ext = H.p.kext * ((2 * mu[0] + dm[0]) * dm[0] + (2 * mu[1] + dm[1]) * dm[1] + (2 * mu[2] + dm[2]) * dm[2]);
+    if (du) { du[0] = ovl ? 0.0 : enew - eold; du[1] = ovl ? 0.0 : out[RV_DUC]; du[2] = ovl ? 0.0 : out[RV_DUL]; du[3] = ovl ? 0.0 : du_ext; }
+    double fx[kMaxA], fy[kMaxA], fz[kMaxA];
+    for (int a = 0; a < na; ++a) {
+        const double q = H.q[f0 + a];
+        fx[a] = out[RV_F + 3 * a] + H.p.minus_two_kext * q * (mu[0] + dm[0]);
+        fy[a] = out[RV_F + 3 * a + 1] + H.p.minus_two_kext * q * (mu[1] + dm[1]);
+        fz[a] = out[RV_F + 3 * a + 2] + H.p.minus_two_kext * q * (mu[2] + dm[2]);
+    }
+    double F[3], T[3];
+    mol_force_torque(na, xn, yn, zn, &H.mass[f0], fx, fy, fz, F, T);
+    if (f) { f[0] = F[0]; f[1] = F[1]; f[2] = F[2]; }
+    if (tau) { tau[0] = T[0]; tau[1] = T[1]; tau[2] = T[2]; }
+    c->api_stage = ovl ? 0 : 2;
+    return YAMC_OK;
+}
+
+int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
+    if (!c) return YAMC_EPARAMETER;
+    if (!accepted) { c->api_stage = 0; return YAMC_OK; }
+    if (c->api_stage != 2) { set_error("yamc_move_commit(accepted) must follow a successful yamc_move_eval"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    HostSystem &H = c->H;
+    const int imol = c->api_imol, f0 = H.first[imol - 1], na = H.natoms[imol - 1];
+    const int n = (1 + H.nt) * H.S;
+    k_commit_rho<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, c->scratch + n, n);
+    CUDA_TRY(cudaGetLastError());
+    std::vector<double4> a(na);
+    for (int i = 0; i < na; ++i) {
+        H.x[f0 + i] = c->api_xn[i]; H.y[f0 + i] = c->api_yn[i]; H.z[f0 + i] = c->api_zn[i];
+        a[i] = make_double4(H.x[f0 + i], H.y[f0 + i], H.z[f0 + i], H.q[f0 + i]);
+    }
+    int r = upload(c->atom + f0, a.data(), na, c->stream);
+    if (r) return r;
+    c->sc[SC_UU_EW] += c->api_new[RV_EW] - c->api_eold[0];
+    c->sc[SC_UU_LJ6] += c->api_new[RV_LJ6] - c->api_eold[1];
+    c->sc[SC_UU_LJ12] += c->api_new[RV_LJ12] - c->api_eold[2];
+    c->sc[SC_EK_C] += c->api_new[RV_DUC];
+    c->sc[SC_EK_LJ] += c->api_new[RV_DUL];
+    c->sc[SC_MU_X] += c->api_dmu[0]; c->sc[SC_MU_Y] += c->api_dmu[1]; c->sc[SC_MU_Z] += c->api_dmu[2];
+    if ((r = push_state(c))) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->api_stage = 0;
+    return YAMC_OK;
+}
+
+int yamc_phase_cycles(yamc_ctx *c, int32_t mode, int64_t *out, int32_t n) {
+    if (!c) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!c->d_prof) {
+        int r = dalloc(&c->d_prof, PH_COUNT);
+        if (r) return r;
+        CUDA_TRY(cudaMemset(c->d_prof, 0, sizeof(long long) * PH_COUNT));
+    }
+    if (mode == 1) { c->prof_on = true; CUDA_TRY(cudaMemset(c->d_prof, 0, sizeof(long long) * PH_COUNT)); }
+    if (mode == 0) c->prof_on = false;
+    if (out && n > 0) {
+        long long h[PH_COUNT];
+        CUDA_TRY(cudaMemcpy(h, c->d_prof, sizeof h, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n && i < PH_COUNT; ++i) out[i] = h[i];
+    }
+    return YAMC_OK;
+}
+
+const char *yamc_last_error_detail(void) {
+    static thread_local std::string copy;
+    copy = yamc::last_error();
+    return copy.c_str();
+}
+
+}  // extern "C"

@@ -30,6 +30,8 @@ struct DevSys {
     const double *freq_beg, *freq_end;
     double *scal;          // engine scalars, see Scal
     long long *cnt;        // run_mc counters, see Cnt
+    int nspec;             // runs of identical consecutive molecules (molecule species)
+    const int4 *spec;      // first molecule, count, atoms per molecule, first atom (0-based)
 };
 
 // engine scalars (double)
@@ -171,9 +173,19 @@ struct RngReader {
     long long n;       // end of the stream available
     long long cur;     // next position to read
     int out;           // set once the stream ran out
+    // optional copies of stream windows [b0, b0+n0) and [b1, b1+n1) (shared memory on the device)
+    const float *w0 = nullptr;
+    long long b0 = 0;
+    int n0 = 0;
+    const float *w1 = nullptr;
+    long long b1 = 0;
+    int n1 = 0;
     __host__ __device__ inline float raw() {
         if (cur >= n) { out = 1; return 0.5f; }
-        return buf[(cur++) - off];
+        const long long i = cur++;
+        if (w0 && i >= b0 && i < b0 + n0) return w0[i - b0];
+        if (w1 && i >= b1 && i < b1 + n1) return w1[i - b1];
+        return buf[i - off];
     }
     __host__ __device__ inline double next() {
         const double eps = 1e-14;
@@ -202,6 +214,25 @@ __host__ __device__ inline int choose_molecule(double r, const double *beg, cons
         if (end[mid] > r) hi = mid; else lo = mid + 1;
     }
     return (r > beg[lo]) ? lo + 1 : 1;
+}
+
+// Same answer with one round trip for flat weights: interval i holds (i, i+1)/M up to the
+// rounding of the running sums, so start at floor(r M) and step to the interval whose exact
+// boundaries bracket r; a value on a boundary belongs to no interval (answer 1), as in the
+// reference's strict comparisons.
+__host__ __device__ inline int choose_molecule_guess(double r, const double *beg, const double *end, int M, int monotone) {
+    if (!monotone) return choose_molecule(r, beg, end, M, 0);
+    int g = (int)(r * M);
+    if (g > M - 1) g = M - 1;
+    if (g < 0) g = 0;
+    for (int step = 0; step < 6; ++step) {
+        const double b = beg[g], e = end[g];
+        if (r > b && r < e) return g + 1;
+        if (r == b || r == e) return 1;
+        if (r > e) { if (g == M - 1) return 1; ++g; }
+        else { if (g == 0) return 1; --g; }
+    }
+    return choose_molecule(r, beg, end, M, monotone);
 }
 
 // ------------------------------------------------------------------ MonteCarloMove.f90
@@ -387,7 +418,9 @@ __host__ __device__ inline void place_molecule(const MoveState &m, int na, const
                                                const double *zo, const double *mass, double *xn, double *yn,
                                                double *zn) {
     double sx = 0, sy = 0, sz = 0, tm = 0;
-    for (int i = 0; i < na; ++i) { sx = sx + mass[i] * xo[i]; sy = sy + mass[i] * yo[i]; sz = sz + mass[i] * zo[i]; tm = tm + mass[i]; }
+#pragma unroll
+    for (int i = 0; i < kMaxA; ++i)
+        if (i < na) { sx = sx + mass[i] * xo[i]; sy = sy + mass[i] * yo[i]; sz = sz + mass[i] * zo[i]; tm = tm + mass[i]; }
     const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
     const double xcn = xc + m.deltx - round(xc + m.deltx);
     const double ycn = yc + m.delty - round(yc + m.delty);
@@ -403,12 +436,14 @@ __host__ __device__ inline void place_molecule(const MoveState &m, int na, const
         const double rzx = st * (ct * ca1 * cphi - sa * sphi);
         const double rzy = st * (ct * ca1 * sphi + sa * cphi);
         const double rzz = (st * st * ca + ct * ct);
-        for (int i = 0; i < na; ++i) {
-            const double xr = xo[i] - xc, yr = yo[i] - yc, zr = zo[i] - zc;
-            xn[i] = (rxx * xr + rxy * yr + rxz * zr) + xcn;
-            yn[i] = (ryx * xr + ryy * yr + ryz * zr) + ycn;
-            zn[i] = (rzx * xr + rzy * yr + rzz * zr) + zcn;
-        }
+#pragma unroll
+        for (int i = 0; i < kMaxA; ++i)
+            if (i < na) {
+                const double xr = xo[i] - xc, yr = yo[i] - yc, zr = zo[i] - zc;
+                xn[i] = (rxx * xr + rxy * yr + rxz * zr) + xcn;
+                yn[i] = (ryx * xr + ryy * yr + ryz * zr) + ycn;
+                zn[i] = (rzx * xr + rzy * yr + rzz * zr) + zcn;
+            }
     } else {
         xn[0] = xcn; yn[0] = ycn; zn[0] = zcn;
     }
@@ -419,15 +454,21 @@ __host__ __device__ inline void mol_force_torque(int na, const double *x, const 
                                                  const double *mass, const double *fx, const double *fy,
                                                  const double *fz, double F[3], double T[3]) {
     double sx = 0, sy = 0, sz = 0, tm = 0;
-    for (int i = 0; i < na; ++i) { sx = sx + mass[i] * x[i]; sy = sy + mass[i] * y[i]; sz = sz + mass[i] * z[i]; tm = tm + mass[i]; }
+#pragma unroll
+    for (int i = 0; i < kMaxA; ++i)
+        if (i < na) { sx = sx + mass[i] * x[i]; sy = sy + mass[i] * y[i]; sz = sz + mass[i] * z[i]; tm = tm + mass[i]; }
     const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
     F[0] = F[1] = F[2] = 0; T[0] = T[1] = T[2] = 0;
-    for (int i = 0; i < na; ++i) { F[0] = F[0] + fx[i]; F[1] = F[1] + fy[i]; F[2] = F[2] + fz[i]; }
-    for (int i = 0; i < na; ++i) {
-        double tx, ty, tz;
-        cross(x[i] - xc, y[i] - yc, z[i] - zc, fx[i], fy[i], fz[i], tx, ty, tz);
-        T[0] = T[0] + tx; T[1] = T[1] + ty; T[2] = T[2] + tz;
-    }
+#pragma unroll
+    for (int i = 0; i < kMaxA; ++i)
+        if (i < na) { F[0] = F[0] + fx[i]; F[1] = F[1] + fy[i]; F[2] = F[2] + fz[i]; }
+#pragma unroll
+    for (int i = 0; i < kMaxA; ++i)
+        if (i < na) {
+            double tx, ty, tz;
+            cross(x[i] - xc, y[i] - yc, z[i] - zc, fx[i], fy[i], fz[i], tx, ty, tz);
+            T[0] = T[0] + tx; T[1] = T[1] + ty; T[2] = T[2] + tz;
+        }
 }
 
 }  // namespace yamc

@@ -16,6 +16,7 @@
 // in registers and every CTA stages its share of the atoms in shared memory; HBM is touched only
 // for the random stream, the moved molecule and the logs.
 #include <cooperative_groups.h>
+#include <cuda_pipeline.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -238,7 +239,12 @@ struct ChainArgs {
     const double *api_in;  // [0] imol, [1 + 3a + c] coordinate c of atom a
     double *api_out;       // the reduction vector of the pass (RV_* layout)
     double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas
+    long long *prof;       // optional per-phase cycle counters (PH_* layout), written by CTA 0 thread 0
 };
+
+// phases timed when ChainArgs::prof is set
+enum Phase { PH_CHOOSE = 0, PH_PASS_OLD, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE, PH_CLUSTER,
+             PH_DECIDE, PH_COMMIT, PH_COUNT };
 
 // reduction vector of one pass
 constexpr int RV_EW = 0, RV_LJ6 = 1, RV_LJ12 = 2, RV_DUC = 3, RV_DUL = 4, RV_OVL = 5, RV_F = 6;
@@ -247,6 +253,9 @@ constexpr int kNV = 6 + 3 * kMaxA;
 enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
 
 struct Slot { double x, y, z, q, iq, dhs; int type, pad; };
+constexpr int kMaxSpecies = 8;
+constexpr int kCPT = 4;  // atoms each thread tests per filter round
+constexpr int kWin = 256;
 
 struct ChainShared {
     int imol, first, na, abort, accepted, kind, forces, last_mol;
@@ -259,7 +268,16 @@ struct ChainShared {
     double sc[SC_COUNT];
     double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (global positions may lag for other CTAs)
     int qcount;
+    int wcount[64];  // per-warp pair counts and their exclusive prefix
     double tot[kNV];
+    // molecule species (runs of identical consecutive molecules): first molecule, count, atoms, first atom
+    int nspec;
+    int sp_m0[kMaxSpecies], sp_cnt[kMaxSpecies], sp_na[kMaxSpecies], sp_a0[kMaxSpecies];
+    Slot sp_atom[kMaxSpecies][kMaxA];
+    double sp_mass[kMaxSpecies][kMaxA];
+    // two windows of the random stream, refilled asynchronously one move ahead
+    long long wbase[2];
+    int wn[2];
 };
 
 __device__ inline unsigned lane_lt_mask() {
@@ -285,7 +303,7 @@ __device__ inline void build_tables(double2 *tab, const ChainShared &sh, int s0,
 // Coulomb phase q (cos, sin), LJ phase = Coulomb phase * (1/q) (the unit phase when q == 0),
 // accumulated per LJ type in atom order.  ph/phl keep the per-atom phases for the forces.
 template <int NT>
-__device__ inline void mol_phase_sum(const double2 *tab, const ChainShared &sh, int s0, int na, int KM, int kx, int ky,
+__device__ __forceinline__ void mol_phase_sum(const double2 *tab, const ChainShared &sh, int s0, int na, int KM, int kx, int ky,
                                      int kz, double2 (&out)[1 + NT], double2 (&ph)[kMaxA], double2 (&phl)[kMaxA]) {
 #pragma unroll
     for (int t = 0; t <= NT; ++t) out[t] = make_double2(0.0, 0.0);
@@ -315,11 +333,33 @@ __device__ inline void mol_phase_sum(const double2 *tab, const ChainShared &sh, 
     }
 }
 
+template <int NT>
+struct NPair { static constexpr int value = NT * (NT + 1) / 2; };
+
+template <int I>
+struct IntC { static constexpr int value = I; };
+
+// calls f(IntC<I>) for I in [B, E): loop indices known at compile time
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (B < E) {
+        f(IntC<B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
+// row of the packed upper triangle t1 <= t2 (the host's pair_index enumeration)
+template <int NT>
+__host__ __device__ constexpr int pair_idx(int a, int b) {
+    return a <= b ? a * NT - a * (a - 1) / 2 + (b - a) : b * NT - b * (b - 1) / 2 + (a - b);
+}
+
 template <int NT, int EPT>
 struct EntryRegs {
     int e[EPT];
     int kx[EPT], ky[EPT], kz[EPT];
     double beta[EPT];
+    double bl[EPT][NPair<NT>::value];  // beta_LJ of every type pair for this entry
     double2 rho[EPT][1 + NT];
     double2 mold[EPT][1 + NT];
     double2 dl[EPT][1 + NT];
@@ -329,9 +369,9 @@ struct EntryRegs {
 // Coulomb with the q-weighted phase and the current (or new) Coulomb rho, plus the dispersion
 // terms of the atom's LJ type against every type's rho (ForceKSpace.f90:59-302).
 template <int NT>
-__device__ inline void entry_forces(const DevSys &D, const ChainShared &sh, int s0, int na, int e, int kx, int ky, int kz,
-                                    double beta, const double2 (&C)[1 + NT], const double2 (&ph)[kMaxA],
-                                    const double2 (&phl)[kMaxA], double *acc) {
+__device__ __forceinline__ void entry_forces(const ChainShared &sh, int s0, int na, int kx, int ky, int kz, double beta,
+                                    const double (&bl)[NPair<NT>::value], const double2 (&C)[1 + NT],
+                                    const double2 (&ph)[kMaxA], const double2 (&phl)[kMaxA], double (&acc)[kNV]) {
     const double fourpi = kFourPi;
 #pragma unroll
     for (int a = 0; a < kMaxA; ++a) {
@@ -341,8 +381,11 @@ __device__ inline void entry_forces(const DevSys &D, const ChainShared &sh, int 
         if (ta > 0) {
 #pragma unroll
             for (int t = 0; t < NT; ++t) {
-                const double bl = D.ebetalj[(size_t)D.pair_index[(ta - 1) * D.nt + t] * D.S + e];
-                w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * bl);
+                double b = 0.0;
+#pragma unroll
+                for (int u = 0; u < NT; ++u)
+                    if (u == ta - 1) b = bl[pair_idx<NT>(u, t)];
+                w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * b);
             }
         }
         acc[RV_F + 3 * a] += w * kx;
@@ -355,85 +398,91 @@ __device__ inline void entry_forces(const DevSys &D, const ChainShared &sh, int 
 // the CTA's atoms (pairs within the cutoff are compacted into a queue, then evaluated densely),
 // reduced over the CTA and then over the cluster in rank order.  Result: sh.tot, identical in
 // every CTA of the cluster.
-template <int NT, int EPT>
-__device__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh, EntryRegs<NT, EPT> &R, double2 *tab,
+template <int NT, int EPT, int KIND, bool FORCES>
+__device__ __forceinline__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh, EntryRegs<NT, EPT> &R, double2 *tab,
                            const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue, double *red,
                            double *xch, const double *lj_s, int nown, int G, int rank, int xpar,
                            cg::cluster_group &cluster) {
-    const int kind = sh.kind;
-    const bool forces = sh.forces != 0;
+    constexpr int kind = KIND;
+    constexpr bool forces = FORCES;
+    constexpr int NVMAX = FORCES ? kNV : RV_F;  // accumulators this pass needs
     const int na = sh.na;
     const int KM = D.kmax + 1;
     const int nt = D.nt;
     const int imol0 = sh.imol - 1;
     const int s_lo = (kind == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
     const int s_hi = (kind == PASS_NEW) ? na : 2 * na;
+    const bool prof = A.prof && threadIdx.x == 0 && rank == 0;
+    long long t_mark = prof ? clock64() : 0;
+#define YAMC_PH(ph) do { if (prof) { const long long t_now = clock64(); A.prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
     build_tables(tab, sh, s_lo, s_hi, KM);
     __syncthreads();
+    YAMC_PH(PH_TABLES);
 
-    double acc[kNV];
+    double acc[NVMAX];
 #pragma unroll
-    for (int v = 0; v < kNV; ++v) acc[v] = 0.0;
+    for (int v = 0; v < NVMAX; ++v) acc[v] = 0.0;
 
-    // ---- k-space
-#pragma unroll
-    for (int k = 0; k < EPT; ++k) {
-        if (R.e[k] < 0) continue;
-        const int e = R.e[k];
+    // ---- k-space: every entry of the thread, with compile-time entry indices so the entry
+    //      state stays in registers
+    static_for<0, EPT>([&](auto kc) {
+        constexpr int k = decltype(kc)::value;
+        if (R.e[k] < 0) return;
         double2 ph[kMaxA], phl[kMaxA];
-        if (kind != PASS_NEW) mol_phase_sum<NT>(tab, sh, na, na, KM, R.kx[k], R.ky[k], R.kz[k], R.mold[k], ph, phl);
-        if (kind == PASS_OLD) {
-            if (forces) entry_forces<NT>(D, sh, na, na, e, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.rho[k], ph, phl, acc);
-            continue;
-        }
-        double2 mnew[1 + NT];
-        mol_phase_sum<NT>(tab, sh, 0, na, KM, R.kx[k], R.ky[k], R.kz[k], mnew, ph, phl);
+        if constexpr (KIND != PASS_NEW) mol_phase_sum<NT>(tab, sh, na, na, KM, R.kx[k], R.ky[k], R.kz[k], R.mold[k], ph, phl);
+        if constexpr (KIND == PASS_OLD) {
+            if constexpr (FORCES) entry_forces<NT>(sh, na, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k], ph, phl, acc);
+        } else {
+            double2 mnew[1 + NT];
+            mol_phase_sum<NT>(tab, sh, 0, na, KM, R.kx[k], R.ky[k], R.kz[k], mnew, ph, phl);
 #pragma unroll
-        for (int t = 0; t <= NT; ++t) R.dl[k][t] = make_double2(mnew[t].x - R.mold[k][t].x, mnew[t].y - R.mold[k][t].y);
-        {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
-            const double2 C = R.rho[k][0], d = R.dl[k][0];
-            acc[RV_DUC] += (((C.x + C.x) + d.x) * d.x + ((C.y + C.y) + d.y) * d.y) * R.beta[k];
-        }
-        // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
-        // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
+            for (int t = 0; t <= NT; ++t) R.dl[k][t] = make_double2(mnew[t].x - R.mold[k][t].x, mnew[t].y - R.mold[k][t].y);
+            {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
+                const double2 C = R.rho[k][0], d = R.dl[k][0];
+                acc[RV_DUC] += (((C.x + C.x) + d.x) * d.x + ((C.y + C.y) + d.y) * d.y) * R.beta[k];
+            }
+            // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
+            // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
 #pragma unroll
-        for (int t1 = 0; t1 < NT; ++t1) {
-            const double2 C1 = R.rho[k][1 + t1], D1 = R.dl[k][1 + t1];
-            const double tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
+            for (int t1 = 0; t1 < NT; ++t1) {
+                const double2 C1 = R.rho[k][1 + t1], D1 = R.dl[k][1 + t1];
+                const double tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
 #pragma unroll
-            for (int t2 = 0; t2 < NT; ++t2) {
-                const double2 D2 = R.dl[k][1 + t2];
-                if (D2.x == 0.0 && D2.y == 0.0) continue;
-                const double bl = D.ebetalj[(size_t)D.pair_index[t1 * nt + t2] * D.S + e];
-                acc[RV_DUL] += (tc * D2.x + ts * D2.y) * bl;
+                for (int t2 = 0; t2 < NT; ++t2) {
+                    const double2 D2 = R.dl[k][1 + t2];
+                    if (D2.x == 0.0 && D2.y == 0.0) continue;
+                    acc[RV_DUL] += (tc * D2.x + ts * D2.y) * R.bl[k][pair_idx<NT>(t1, t2)];
+                }
+            }
+            if constexpr (KIND == PASS_NEW && FORCES) {  // against total_new = rho + delta (MC.f90:1136-1163)
+                double2 Cn[1 + NT];
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) Cn[t] = make_double2(R.rho[k][t].x + R.dl[k][t].x, R.rho[k][t].y + R.dl[k][t].y);
+                entry_forces<NT>(sh, 0, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], Cn, ph, phl, acc);
             }
         }
-        if (kind == PASS_NEW && forces) {  // against total_new = rho + delta (MC.f90:1136-1163)
-            double2 Cn[1 + NT];
-#pragma unroll
-            for (int t = 0; t <= NT; ++t) Cn[t] = make_double2(R.rho[k][t].x + R.dl[k][t].x, R.rho[k][t].y + R.dl[k][t].y);
-            entry_forces<NT>(D, sh, 0, na, e, R.kx[k], R.ky[k], R.kz[k], R.beta[k], Cn, ph, phl, acc);
-        }
-    }
+    });
 
-    // ---- real space
+    YAMC_PH(PH_KSPACE);
+    // ---- real space: each thread tests CPT of the CTA's atoms against the active slots, the
+    //      (atom, slot) pairs inside the cutoff are laid out in the queue by a prefix sum over
+    //      threads (deterministic order), then evaluated by all threads, item i by thread i % B.
     const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
     const int B = blockDim.x;
-    const int nslot = s_hi - s_lo;
-    int chunk = (A.qcap / nslot) / B * B;
-    if (chunk < B) chunk = B;  // qcap >= B * 2 * kMaxA is guaranteed by the host
-    for (int c0 = 0; c0 < nown; c0 += chunk) {
-        const int c1 = min(nown, c0 + chunk);
-        for (int base = c0; base < c1; base += B) {
-            const int jl = base + threadIdx.x;
-            const bool ok = jl < c1 && meta_s[jl].x != imol0;
-            double4 pj = make_double4(0, 0, 0, 0);
-            int tj = 0;
-            double dj = 0;
-            if (ok) { pj = atom_s[jl]; tj = meta_s[jl].y; dj = dhs_s[jl]; }
-            for (int s = s_lo; s < s_hi; ++s) {
-                bool pass = false;
-                if (ok) {
+    const int round_atoms = B * kCPT;
+    for (int c0 = 0; c0 < nown; c0 += round_atoms) {
+        unsigned masks = 0;  // kCPT slot masks of 8 bits
+        int count = 0;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            const int jl = c0 + c * B + threadIdx.x;
+            if (jl < nown && meta_s[jl].x != imol0) {
+                const double4 pj = atom_s[jl];
+                const int tj = meta_s[jl].y;
+                const double dj = dhs_s[jl];
+                unsigned m = 0;
+                for (int s = s_lo; s < s_hi; ++s) {
                     const Slot &sl = sh.slot[s];
                     const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
                     const double r2 = dx * dx + dy * dy + dz * dz;
@@ -441,19 +490,46 @@ __device__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh,
                         const double d12 = (sl.dhs + dj) / 2;
                         if (r2 < d12 * d12) acc[RV_OVL] = 1.0;
                     }
-                    pass = r2 < D.rmax2;
+                    if (r2 < D.rmax2) m |= 1u << s;
                 }
-                const unsigned m = __ballot_sync(0xffffffffu, pass);
-                if (m) {
-                    const int leader = __ffs(m) - 1;
-                    int basei = 0;
-                    if (lane == leader) basei = atomicAdd(&sh.qcount, __popc(m));
-                    basei = __shfl_sync(0xffffffffu, basei, leader);
-                    if (pass) queue[basei + __popc(m & lane_lt_mask())] = (jl << 3) | s;
-                }
+                masks |= m << (8 * c);
+                count += __popc(m);
+            }
+        }
+        // exclusive prefix of the counts: within the warp, then over the warps
+        int incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) sh.wcount[warp] = incl;
+        __syncthreads();
+        if (warp == 0) {
+            const int v = lane < nwarp ? sh.wcount[lane] : 0;
+            int x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane < nwarp) sh.wcount[32 + lane] = x - v;
+            if (lane == 31) sh.qcount = x;
+        }
+        __syncthreads();
+        int pos = sh.wcount[32 + warp] + incl - count;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            unsigned m = (masks >> (8 * c)) & 0xffu;
+            const int jl = c0 + c * B + threadIdx.x;
+            while (m) {
+                const int s = __ffs(m) - 1;
+                m &= m - 1;
+                queue[pos++] = (jl << 3) | s;
             }
         }
         __syncthreads();
+        YAMC_PH(PH_FILTER);
         const int nq = sh.qcount;
         for (int qi = threadIdx.x; qi < nq; qi += B) {
             const int item = queue[qi];
@@ -469,7 +545,7 @@ __device__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh,
             const double s6 = lj ? lj_s[off] : 0.0, fe = lj ? lj_s[nt * nt + off] : 0.0;
             const bool isnew = s < na;
             const double sign = (kind == PASS_BOTH && !isnew) ? -1.0 : 1.0;
-            if (forces) {
+            if constexpr (FORCES) {
                 const PairTerm<double> t = pair_term<double, true>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
                 acc[RV_EW] += sign * t.ew; acc[RV_LJ6] += sign * t.lj6; acc[RV_LJ12] += sign * t.lj12;
                 const int a = isnew ? s : s - na;
@@ -482,57 +558,64 @@ __device__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh,
             }
         }
         __syncthreads();
-        if (threadIdx.x == 0) sh.qcount = 0;
-        __syncthreads();
+        YAMC_PH(PH_PAIRS);
     }
 
-    // ---- reduction: warp xor tree, warps in order, then CTAs in rank order
+    // ---- reduction: xor trees within each warp, across the warps (one warp per value) and
+    //      across the cluster's CTAs; fixed trees, so every CTA gets bit-identical totals
+    if (A.mode == MODE_RUN && threadIdx.x >= 32 && threadIdx.x < 64) __pipeline_wait_prior(0);  // random window
     const int nv = forces ? (RV_F + 3 * na) : RV_F;
-    const int warp = threadIdx.x >> 5, nwarp = B >> 5;
 #pragma unroll
     for (int v = 0; v < kNV; ++v) {
         if (v >= nv) break;
         double x = acc[v];
-        if (v == RV_OVL) {
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x = fmax(x, __shfl_xor_sync(0xffffffffu, x, o));
-        } else {
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = (v == RV_OVL) ? fmax(x, y) : x + y;
         }
         if (lane == 0) red[warp * kNV + v] = x;
     }
     __syncthreads();
-    if (threadIdx.x < nv) {
-        const int v = threadIdx.x;
-        double s = 0;
-        for (int w = 0; w < nwarp; ++w) s = (v == RV_OVL) ? fmax(s, red[w * kNV + v]) : s + red[w * kNV + v];
+    for (int v = warp; v < nv; v += nwarp) {
+        double x = lane < nwarp ? red[lane * kNV + v] : 0.0;
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            const double y = __shfl_xor_sync(0xffffffffu, x, o);
+            x = (v == RV_OVL) ? fmax(x, y) : x + y;
+        }
         if (G > 1) {
-            for (int r = 0; r < G; ++r) {
-                double *dst = cluster.map_shared_rank(xch, r);
-                dst[(xpar * G + rank) * kNV + v] = s;
+            if (lane < G) {
+                double *dst = cluster.map_shared_rank(xch, lane);
+                dst[(xpar * G + rank) * kNV + v] = x;
             }
-        } else {
-            sh.tot[v] = s;
+        } else if (lane == 0) {
+            sh.tot[v] = x;
         }
     }
+    YAMC_PH(PH_REDUCE);
     if (G > 1) {
         cluster.sync();
-        if (threadIdx.x < nv) {
-            const int v = threadIdx.x;
-            double s = 0;
-            for (int r = 0; r < G; ++r)
-                s = (v == RV_OVL) ? fmax(s, xch[(xpar * G + r) * kNV + v]) : s + xch[(xpar * G + r) * kNV + v];
-            sh.tot[v] = s;
+        for (int v = warp; v < nv; v += nwarp) {
+            double x = lane < G ? xch[(xpar * G + lane) * kNV + v] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = (v == RV_OVL) ? fmax(x, y) : x + y;
+            }
+            if (lane == 0) sh.tot[v] = x;
         }
     }
     __syncthreads();
+    YAMC_PH(PH_CLUSTER);
+#undef YAMC_PH
 }
 
 template <int NT, int EPT>
 __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ChainShared sh;
+    __shared__ float rwin[2][kWin];
 
     cg::cluster_group cluster = cg::this_cluster();
     const int G = A.G;
@@ -579,6 +662,8 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
             R.beta[k] = D.ebeta[e];
         }
 #pragma unroll
+        for (int p = 0; p < NPair<NT>::value; ++p) R.bl[k][p] = e < S ? D.ebetalj[(size_t)p * S + e] : 0.0;
+#pragma unroll
         for (int t = 0; t <= NT; ++t) {
             R.rho[k][t] = e < S ? D.rho[(size_t)t * S + e] : make_double2(0, 0);
             R.mold[k][t] = (A.mode == MODE_EVAL && e < S) ? A.scratch[(size_t)t * S + e] : make_double2(0, 0);
@@ -593,6 +678,23 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
         sh.last_mol = -1;
         sh.abort = 0;
         sh.qcount = 0;
+        sh.wbase[0] = sh.wbase[1] = -1;
+        sh.wn[0] = sh.wn[1] = 0;
+        // static atom data of each molecule species, taken from its first molecule
+        sh.nspec = D.nspec <= kMaxSpecies ? D.nspec : 0;
+        for (int sp = 0; sp < sh.nspec; ++sp) {
+            const int4 c = D.spec[sp];
+            sh.sp_m0[sp] = c.x; sh.sp_cnt[sp] = c.y; sh.sp_na[sp] = c.z; sh.sp_a0[sp] = c.w;
+            for (int a = 0; a < c.z; ++a) {
+                const int j = c.w + a;
+                Slot t;
+                t.x = t.y = t.z = 0.0;
+                t.q = D.atom[j].w; t.iq = t.q != 0.0 ? 1.0 / t.q : 0.0;
+                t.dhs = D.dhs[j]; t.type = D.meta[j].y; t.pad = 0;
+                sh.sp_atom[sp][a] = t;
+                sh.sp_mass[sp][a] = D.mass[j];
+            }
+        }
     }
     __syncthreads();
     const bool biased = (D.xlf > 0.0 || D.xlc > 0.0);
@@ -602,36 +704,55 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
     int xpar = 0;  // parity of the cluster exchange buffer, flipped after every pass
     const long long n_moves = (A.mode == MODE_RUN) ? run->n_moves : 1;
 
+    const bool prof = A.prof && tid == 0 && rank == 0;
+    long long t_mark = 0;
+#define YAMC_PH(ph) do { if (prof) { const long long t_now = clock64(); A.prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
     for (long long it = 0; it < n_moves; ++it) {
+        if (prof) t_mark = clock64();
         // ------------------------------------------------ choose the molecule, stage its atoms
         if (tid == 0) {
             sh.cursor_start = sh.cursor;
             sh.abort = 0;
             int imol = 1;
             if (A.mode == MODE_RUN) {
-                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0};
+                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
+                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
                 if (sh.mic == 0) (void)rng.next();  // per-cycle pressure-step draw (runmc.f90:206)
                 (void)rng.next();                   // move-or-exchange draw (runmc.f90:232), never an exchange
                 const double r = rng.next();        // BiasedRandom_choose (runmc.f90:258)
-                imol = choose_molecule(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
+                imol = choose_molecule_guess(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
                 if (rng.out) sh.abort = 1;
                 else sh.cursor = rng.cur;
             } else {
                 imol = (int)A.api_in[0];
             }
-            const int2 mr = D.mol[imol - 1];
-            sh.imol = imol; sh.first = mr.x; sh.na = mr.y;
+            // molecule -> species -> first atom; static atom data from the species table
+            int sp = -1;
+            for (int q = 0; q < sh.nspec; ++q)
+                if (imol - 1 >= sh.sp_m0[q] && imol - 1 < sh.sp_m0[q] + sh.sp_cnt[q]) { sp = q; break; }
+            int first, nam;
+            if (sp >= 0) { nam = sh.sp_na[sp]; first = sh.sp_a0[sp] + (imol - 1 - sh.sp_m0[sp]) * nam; }
+            else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
+            sh.imol = imol; sh.first = first; sh.na = nam;
             double mx = 0, my = 0, mz = 0;
-            for (int a = 0; a < mr.y; ++a) {
-                const double4 pq = D.atom[mr.x + a];
+            for (int a = 0; a < nam; ++a) {
+                const int j = first + a;
                 Slot s;
-                s.x = pq.x; s.y = pq.y; s.z = pq.z;
+                if (sp >= 0) { s = sh.sp_atom[sp][a]; sh.mass[a] = sh.sp_mass[sp][a]; }
+                else {
+                    const double q = D.atom[j].w;
+                    s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y; s.pad = 0;
+                    sh.mass[a] = D.mass[j];
+                }
+                // positions: the last accepted move's cache, else the owning CTA's staged copy
                 if (imol - 1 == sh.last_mol) { s.x = sh.lx[a]; s.y = sh.ly[a]; s.z = sh.lz[a]; }
-                s.q = pq.w; s.iq = pq.w != 0.0 ? 1.0 / pq.w : 0.0;
-                s.dhs = D.dhs[mr.x + a]; s.type = D.meta[mr.x + a].y; s.pad = 0;
-                sh.slot[mr.y + a] = s;  // old positions
-                sh.slot[a] = s;         // new positions, replaced after the proposal
-                sh.mass[a] = D.mass[mr.x + a];
+                else {
+                    const double4 *src = (G > 1) ? cluster.map_shared_rank(atom_s, j % G) : atom_s;
+                    const double4 p = src[j / G];
+                    s.x = p.x; s.y = p.y; s.z = p.z;
+                }
+                sh.slot[nam + a] = s;  // old positions
+                sh.slot[a] = s;        // new positions, replaced after the proposal
                 // dipole of the molecule at the old positions (EwaldSumExternal_calc_mu)
                 mx = mx + s.q * s.x; my = my + s.q * s.y; mz = mz + s.q * s.z;
             }
@@ -642,11 +763,13 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
         __syncthreads();
         if (sh.abort) break;
         const int na = sh.na;
+        YAMC_PH(PH_CHOOSE);
 
         // ------------------------------------------------ old forces (force-biased moves, per-move API)
         if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
-            chain_pass<NT, EPT>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+            chain_pass<NT, EPT, PASS_OLD, true>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
             xpar ^= 1;
+            if (prof) t_mark = clock64();
             if (tid == 0) {
                 sh.eold[0] = sh.tot[RV_EW]; sh.eold[1] = sh.tot[RV_LJ6]; sh.eold[2] = sh.tot[RV_LJ12];
                 for (int a = 0; a < na; ++a) {  // external-field force -2 kext q mu (MC.f90:988-997)
@@ -678,7 +801,8 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
             double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
             for (int a = 0; a < na; ++a) { xo[a] = sh.slot[na + a].x; yo[a] = sh.slot[na + a].y; zo[a] = sh.slot[na + a].z; }
             if (A.mode == MODE_RUN) {
-                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0};
+                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
+                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
                 double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
                 if (biased) {
                     double fx[kMaxA], fy[kMaxA], fz[kMaxA];
@@ -702,10 +826,26 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
         }
         __syncthreads();
         if (sh.abort) break;
+        YAMC_PH(PH_PROPOSE);
+        // refill the other random window from the current cursor while the pass runs; the copy
+        // is awaited by warp 1 before the pass's reduction barrier (chain_pass)
+        if (A.mode == MODE_RUN && tid >= 32 && tid < 64) {
+            const int b = (int)((it + 1) & 1);
+            const long long base = sh.cursor;
+            const long long avail = run->n_rng - base;
+            const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
+            for (int i = tid - 32; i < nw; i += 32) __pipeline_memcpy_async(&rwin[b][i], run->rng + (base + i - run->rng_off), 4);
+            __pipeline_commit();
+            if (tid == 32) { sh.wbase[b] = base; sh.wn[b] = nw; }
+        }
 
         // ------------------------------------------------ new positions: energies, delta rho, overlap
-        chain_pass<NT, EPT>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+        if (biased || A.mode == MODE_EVAL)
+            chain_pass<NT, EPT, PASS_NEW, true>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+        else
+            chain_pass<NT, EPT, PASS_BOTH, false>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
         xpar ^= 1;
+        if (prof) t_mark = clock64();
 
         if (A.mode == MODE_EVAL) {
 #pragma unroll
@@ -728,7 +868,8 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
             double dew = 0, dlj6 = 0, dlj12 = 0;
             sh.accepted = 0;
             if (!overlap) {
-                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0};
+                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
+                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
                 if (biased) {
                     dew = sh.tot[RV_EW] - sh.eold[0]; dlj6 = sh.tot[RV_LJ6] - sh.eold[1]; dlj12 = sh.tot[RV_LJ12] - sh.eold[2];
                     du_real = (sh.tot[RV_EW] + sh.tot[RV_LJ12] - sh.tot[RV_LJ6]) - (sh.eold[0] + sh.eold[2] - sh.eold[1]);
@@ -811,6 +952,7 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
         }
         __syncthreads();
         if (sh.abort) break;
+        YAMC_PH(PH_DECIDE);
         if (sh.accepted) {
 #pragma unroll
             for (int k = 0; k < EPT; ++k)
@@ -827,7 +969,9 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
         }
         ++moves_done;
         __syncthreads();
+        YAMC_PH(PH_COMMIT);
     }
+#undef YAMC_PH
 
     if (A.mode == MODE_RUN) {  // write back the register and shared state
 #pragma unroll
@@ -925,6 +1069,7 @@ struct yamc_ctx {
     double2 *rho = nullptr, *scratch = nullptr;
     double *freq_beg = nullptr, *freq_end = nullptr, *scal = nullptr;
     long long *cnt = nullptr;
+    int4 *spec = nullptr;
     double *uu = nullptr, *fx = nullptr, *fy = nullptr, *fz = nullptr, *part = nullptr;
     DevSys hsys{};
     DevSys *d_sys = nullptr;
@@ -948,6 +1093,8 @@ struct yamc_ctx {
     double api_new[kNV] = {};
     double api_xn[kMaxA] = {}, api_yn[kMaxA] = {}, api_zn[kMaxA] = {};
     double api_dmu[3] = {};
+    long long *d_prof = nullptr;
+    bool prof_on = false;
 };
 
 namespace {
@@ -969,8 +1116,7 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
             const int EPT = (H.S + G * B - 1) / (G * B);
             if (EPT > 2) continue;
             const int nown_max = (H.N + G - 1) / G;
-            int qcap = std::min(nown_max * 2 * kMaxA, 16384);
-            qcap = std::max(qcap, B * 2 * kMaxA);
+            const int qcap = std::min(nown_max, B * kCPT) * 2 * kMaxA;  // one filter round of pairs
             const size_t sm = chain_smem_bytes(G, B, H.kmax, H.nt, nown_max, qcap);
             if (sm > smem_max) continue;
             out->G = G; out->B = B; out->EPT = EPT; out->nown_max = nown_max; out->qcap = qcap; out->smem = sm;
@@ -1006,8 +1152,12 @@ int launch_chain_t(yamc_ctx *c, const ChainArgs &args) {
 int launch_chain(yamc_ctx *c, const ChainArgs &args) {
     const int nt = c->H.nt, ept = c->cfg.EPT;
 #define YAMC_CASE(NT_, EPT_) if (nt == NT_ && ept == EPT_) return launch_chain_t<NT_, EPT_>(c, args);
+#ifdef YAMC_ONE_VARIANT  // development builds: a single instantiation compiles in seconds
+    YAMC_CASE(3, 1)
+#else
     YAMC_CASE(1, 1) YAMC_CASE(1, 2) YAMC_CASE(2, 1) YAMC_CASE(2, 2)
     YAMC_CASE(3, 1) YAMC_CASE(3, 2) YAMC_CASE(4, 1) YAMC_CASE(4, 2)
+#endif
 #undef YAMC_CASE
     set_error("LJ type count outside 1..4 or k-set too large for the chain kernel");
     return YAMC_ELIMITS;
@@ -1119,6 +1269,7 @@ ChainArgs base_args(yamc_ctx *c, int mode) {
     a.sys = c->d_sys; a.run = c->d_run; a.G = c->cfg.G; a.mode = mode;
     a.nown_max = c->cfg.nown_max; a.qcap = c->cfg.qcap;
     a.api_in = c->api_in; a.api_out = c->api_out; a.scratch = c->scratch;
+    a.prof = c->prof_on ? c->d_prof : nullptr;
     return a;
 }
 
@@ -1165,7 +1316,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->fx, N)) || (r = dalloc(&c->fy, N)) || (r = dalloc(&c->fz, N)) ||
         (r = dalloc(&c->part, (size_t)std::max((N + kFullTile - 1) / kFullTile * kFullParts, (S + 255) / 256 * 2))) ||
         (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->api_in, 1 + 3 * kMaxA)) ||
-        (r = dalloc(&c->api_out, kNV)))
+        (r = dalloc(&c->api_out, kNV)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
     std::vector<double4> a(N);
     std::vector<int2> m(N);
@@ -1182,7 +1333,8 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = upload(c->ebeta, H.ebeta.data(), S, c->stream)) || (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) ||
         (r = upload(c->pair_index, pidx.data(), nt * nt, c->stream)) || (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
         (r = upload(c->lj_feps, H.four_eps.data(), nt * nt, c->stream)) || (r = upload(c->freq_beg, H.freq_beg.data(), M, c->stream)) ||
-        (r = upload(c->freq_end, H.freq_end.data(), M, c->stream)))
+        (r = upload(c->freq_end, H.freq_end.data(), M, c->stream)) ||
+        (r = upload(c->spec, reinterpret_cast<const int4 *>(H.spec.data()), H.spec.size() / 4, c->stream)))
         return r;
     DevSys &D = c->hsys;
     D.N = N; D.M = M; D.S = S; D.nt = nt; D.kmax = H.kmax; D.npair = H.npair; D.freq_monotone = H.freq_monotone;
@@ -1194,6 +1346,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
     D.rho = c->rho; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
+    D.nspec = (int)(H.spec.size() / 4); D.spec = c->spec;
     if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
     c->cnt_h[CN_ICYCLE] = 1;
     c->cnt_h[CN_MOVE_IN_CYCLE] = 0;
@@ -1218,7 +1371,8 @@ int yamc_destroy(yamc_ctx *c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->uu, c->fx, c->fy,
-                    c->fz, c->part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows};
+                    c->fz, c->part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
+                    c->d_prof, c->spec};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1469,6 +1623,24 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     if ((r = push_state(c))) return r;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->api_stage = 0;
+    return YAMC_OK;
+}
+
+int yamc_phase_cycles(yamc_ctx *c, int32_t mode, int64_t *out, int32_t n) {
+    if (!c) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    if (!c->d_prof) {
+        int r = dalloc(&c->d_prof, PH_COUNT);
+        if (r) return r;
+        CUDA_TRY(cudaMemset(c->d_prof, 0, sizeof(long long) * PH_COUNT));
+    }
+    if (mode == 1) { c->prof_on = true; CUDA_TRY(cudaMemset(c->d_prof, 0, sizeof(long long) * PH_COUNT)); }
+    if (mode == 0) c->prof_on = false;
+    if (out && n > 0) {
+        long long h[PH_COUNT];
+        CUDA_TRY(cudaMemcpy(h, c->d_prof, sizeof h, cudaMemcpyDeviceToHost));
+        for (int i = 0; i < n && i < PH_COUNT; ++i) out[i] = h[i];
+    }
     return YAMC_OK;
 }
 

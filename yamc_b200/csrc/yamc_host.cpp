@@ -296,6 +296,24 @@ int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSyst
     for (int i = 0; i < N; ++i)
         if (H.molnum[i] < 0) { set_error("atom outside every molecule"); return YAMC_EPARAMETER; }
 
+    // runs of consecutive molecules whose atoms carry identical static data (species)
+    auto same_mol = [&](int a, int b) {
+        if (H.natoms[a] != H.natoms[b]) return false;
+        for (int k = 0; k < H.natoms[a]; ++k) {
+            const int i = H.first[a] + k, j = H.first[b] + k;
+            if (H.q[i] != H.q[j] || H.sigma[i] != H.sigma[j] || H.eps[i] != H.eps[j] || H.hc[i] != H.hc[j] ||
+                H.mass[i] != H.mass[j])
+                return false;
+        }
+        return true;
+    };
+    H.spec.clear();
+    for (int m = 0; m < M; ++m) {
+        const bool contiguous = m > 0 && H.first[m] == H.first[m - 1] + H.natoms[m - 1];
+        if (m > 0 && contiguous && same_mol(m, H.spec[H.spec.size() - 4])) { H.spec[H.spec.size() - 3] += 1; continue; }
+        H.spec.push_back(m); H.spec.push_back(1); H.spec.push_back(H.natoms[m]); H.spec.push_back(H.first[m]);
+    }
+
     // LJTypes_fill (LJTypes.f90:134-200): distinct (sigma, epsilon) pairs in order
     // of first appearance, sigma below 1e-8 (single-precision literal) has no LJ.
     std::vector<double> ts, te;

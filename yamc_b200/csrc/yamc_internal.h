@@ -43,6 +43,8 @@ struct HostSystem {
     int freq_monotone = 1;                    // intervals increasing (binary search valid)
     std::vector<int32_t> mol_numbers;
     int max_mol_atoms = 0;
+    // runs of identical consecutive molecules: first molecule, count, atoms each, first atom
+    std::vector<int> spec;  // 4 ints per run
 };
 
 int prepare_host_system(const yamc_system *sys, const yamc_params *p, HostSystem *hs);
