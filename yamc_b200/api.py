@@ -204,8 +204,8 @@ class Engine:
         return {"cluster_blocks": int(out[0]), "threads": int(out[1]), "entries_per_thread": int(out[2]),
                 "smem_bytes": int(out[3])}
 
-    PHASES = ("choose", "old_pass", "propose", "tables", "kspace", "pair_filter", "pairs", "cta_reduce",
-              "cluster_exchange", "metropolis", "commit")
+    PHASES = ("choose", "speculate", "propose", "tables", "kspace", "pair_filter", "pairs", "reduce",
+              "cluster", "metropolis", "commit")
 
     def phase_cycles(self, mode: int = 2) -> dict:
         out = np.zeros(len(self.PHASES), dtype=np.int64)

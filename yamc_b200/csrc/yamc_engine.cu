@@ -212,6 +212,15 @@ __global__ void __launch_bounds__(256) k_kspace_energy(DevSys D, const double2 *
 // ------------------------------------------------------------------------------------------
 // the chain kernel
 // ------------------------------------------------------------------------------------------
+// One thread-block cluster runs one Markov chain.  Warp 0 of every CTA is the control warp:
+// its lane 0 draws the random numbers, proposes moves and takes the Metropolis decision
+// (redundantly in every CTA, on identical data, so the CTAs agree without talking).  The
+// other warps are workers: they run the fused real-space + k-space pass of the current move
+// over the CTA's atoms and k-vector entries.  For unbiased moves the control warp prepares
+// the next move while the workers run the current pass: the next move starts either where the
+// current one ends after a hard-core overlap (no acceptance draw) or one draw later, and when
+// the next molecule is the one being moved its old positions depend on the decision, so lanes
+// 0-2 prepare the (at most) three candidates and the decision picks one.
 enum ChainMode { MODE_RUN = 0, MODE_OLD = 1, MODE_EVAL = 2 };
 
 // per-replica run control, in device memory
@@ -239,12 +248,12 @@ struct ChainArgs {
     const double *api_in;  // [0] imol, [1 + 3a + c] coordinate c of atom a
     double *api_out;       // the reduction vector of the pass (RV_* layout)
     double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas
-    long long *prof;       // optional per-phase cycle counters (PH_* layout), written by CTA 0 thread 0
+    long long *prof;       // optional per-phase cycle counters (PH_* layout), CTA 0
 };
 
-// phases timed when ChainArgs::prof is set
-enum Phase { PH_CHOOSE = 0, PH_PASS_OLD, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE, PH_CLUSTER,
-             PH_DECIDE, PH_COMMIT, PH_COUNT };
+// phases timed when ChainArgs::prof is set (control lane 0 or worker thread 32 of CTA 0)
+enum Phase { PH_CHOOSE = 0, PH_SPECULATE, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE,
+             PH_CLUSTER, PH_DECIDE, PH_COMMIT, PH_COUNT };
 
 // reduction vector of one pass
 constexpr int RV_EW = 0, RV_LJ6 = 1, RV_LJ12 = 2, RV_DUC = 3, RV_DUL = 4, RV_OVL = 5, RV_F = 6;
@@ -254,48 +263,94 @@ enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
 
 struct Slot { double x, y, z, q, iq, dhs; int type, pad; };
 constexpr int kMaxSpecies = 8;
-constexpr int kCPT = 4;  // atoms each thread tests per filter round
-constexpr int kWin = 256;
+constexpr int kCPT = 4;   // atoms each worker thread tests per filter round
+constexpr int kWin = 256; // random-stream window held in shared memory
+constexpr int kCtl = 32;  // threads of the control warp
+constexpr int kChainMaxThreads = 256;  // one CTA per SM, up to 255 registers per thread
+
+// a prepared move: the molecule, its atoms at the old and proposed positions, the proposal
+struct Cand {
+    int valid, imol, first, na;
+    long long cur_start;  // stream position at the start of the move
+    long long cur_prop;   // stream position after the proposal
+    double mu_old[3];     // dipole of the molecule at the old positions
+    Slot slot[2 * kMaxA]; // [0, na): proposed positions, [na, 2na): old positions
+    double mass[kMaxA];
+    MoveState mv;
+};
 
 struct ChainShared {
-    int imol, first, na, abort, accepted, kind, forces, last_mol;
-    long long cursor, cursor_start, icycle, mic;
-    Slot slot[2 * kMaxA];  // [0, na): new positions, [na, 2na): old positions
-    double mass[kMaxA];
+    Cand cand[4];         // the move being evaluated (cand[icur]) and up to three prepared next moves
+    int icur;             // buffer of the move being evaluated
+    int spec[3];          // buffers of the candidates: after an overlap / after a draw / accepted same molecule
+    int abort, accepted, overlap, last_mol, spec_ok;
+    long long cursor;     // stream position after the last completed move
+    long long icycle, mic;
     double eold[3], fold[3 * kMaxA];
-    double mu_old[3];
-    MoveState mv;
     double sc[SC_COUNT];
-    double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (global positions may lag for other CTAs)
+    double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (staged copies may lag in other CTAs)
     int qcount;
-    int wcount[64];  // per-warp pair counts and their exclusive prefix
+    int wcount[64];       // per-warp pair counts and their exclusive prefix
     double tot[kNV];
+    double du[4];
+    int flags;
     // molecule species (runs of identical consecutive molecules): first molecule, count, atoms, first atom
     int nspec;
     int sp_m0[kMaxSpecies], sp_cnt[kMaxSpecies], sp_na[kMaxSpecies], sp_a0[kMaxSpecies];
     Slot sp_atom[kMaxSpecies][kMaxA];
     double sp_mass[kMaxSpecies][kMaxA];
-    // two windows of the random stream, refilled asynchronously one move ahead
+    // two windows of the random stream
     long long wbase[2];
     int wn[2];
+    int wnext;
 };
 
-__device__ inline unsigned lane_lt_mask() {
-    unsigned m;
-    asm("mov.u32 %0, %%lanemask_lt;" : "=r"(m));
-    return m;
+__device__ __forceinline__ void worker_sync(int nwork) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nwork) : "memory");
 }
 
-// Phase tables for slots [s0, s1): T[slot][axis][m] = (cos, sin)(2 pi m u)
-__device__ inline void build_tables(double2 *tab, const ChainShared &sh, int s0, int s1, int KM) {
+template <int I>
+struct IntC { static constexpr int value = I; };
+
+// calls f(IntC<I>) for I in [B, E): loop indices known at compile time
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (B < E) {
+        f(IntC<B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
+template <int NT>
+struct NPair { static constexpr int value = NT * (NT + 1) / 2; };
+
+// row of the packed upper triangle t1 <= t2 (the host's pair_index enumeration)
+template <int NT>
+__host__ __device__ constexpr int pair_idx(int a, int b) {
+    return a <= b ? a * NT - a * (a - 1) / 2 + (b - a) : b * NT - b * (b - 1) / 2 + (a - b);
+}
+
+template <int NT, int EPT>
+struct EntryRegs {
+    int e[EPT];
+    int kx[EPT], ky[EPT], kz[EPT];
+    double beta[EPT];
+    double bl[EPT][NPair<NT>::value];  // beta_LJ of every type pair for this entry
+    double2 rho[EPT][1 + NT];
+    double2 mold[EPT][1 + NT];
+    double2 dl[EPT][1 + NT];
+};
+
+// Phase tables of slots [s0, s1) of move m: T[slot][axis][k] = (cos, sin)(2 pi k u), by the workers
+__device__ __forceinline__ void build_tables(double2 *tab, const Cand &m, int s0, int s1, int KM, int wtid, int nwork) {
     const int n = (s1 - s0) * 3 * KM;
-    for (int idx = threadIdx.x; idx < n; idx += blockDim.x) {
-        const int sl = s0 + idx / (3 * KM), r = idx % (3 * KM), d = r / KM, m = r % KM;
-        const double u = d == 0 ? sh.slot[sl].x : (d == 1 ? sh.slot[sl].y : sh.slot[sl].z);
+    for (int idx = wtid; idx < n; idx += nwork) {
+        const int sl = s0 + idx / (3 * KM), r = idx % (3 * KM), d = r / KM, k = r % KM;
+        const double u = d == 0 ? m.slot[sl].x : (d == 1 ? m.slot[sl].y : m.slot[sl].z);
         double s, c;
-        sincospi(2.0 * (double)m * u, &s, &c);
-        if (m == 0) { s = 0.0; c = 1.0; }
-        tab[(sl * 3 + d) * KM + m] = make_double2(c, s);
+        sincospi(2.0 * (double)k * u, &s, &c);
+        if (k == 0) { s = 0.0; c = 1.0; }
+        tab[(sl * 3 + d) * KM + k] = make_double2(c, s);
     }
 }
 
@@ -303,8 +358,8 @@ __device__ inline void build_tables(double2 *tab, const ChainShared &sh, int s0,
 // Coulomb phase q (cos, sin), LJ phase = Coulomb phase * (1/q) (the unit phase when q == 0),
 // accumulated per LJ type in atom order.  ph/phl keep the per-atom phases for the forces.
 template <int NT>
-__device__ __forceinline__ void mol_phase_sum(const double2 *tab, const ChainShared &sh, int s0, int na, int KM, int kx, int ky,
-                                     int kz, double2 (&out)[1 + NT], double2 (&ph)[kMaxA], double2 (&phl)[kMaxA]) {
+__device__ __forceinline__ void mol_phase_sum(const double2 *tab, const Cand &m, int s0, int na, int KM, int kx, int ky,
+                                              int kz, double2 (&out)[1 + NT], double2 (&ph)[kMaxA], double2 (&phl)[kMaxA]) {
 #pragma unroll
     for (int t = 0; t <= NT; ++t) out[t] = make_double2(0.0, 0.0);
 #pragma unroll
@@ -312,7 +367,7 @@ __device__ __forceinline__ void mol_phase_sum(const double2 *tab, const ChainSha
         ph[a] = make_double2(0.0, 0.0);
         phl[a] = make_double2(0.0, 0.0);
         if (a < na) {
-            const Slot &sl = sh.slot[s0 + a];
+            const Slot &sl = m.slot[s0 + a];
             const double2 *T = tab + (size_t)(s0 + a) * 3 * KM;
             double c = 0, s = 0;
             if (sl.q != 0.0) {
@@ -333,108 +388,78 @@ __device__ __forceinline__ void mol_phase_sum(const double2 *tab, const ChainSha
     }
 }
 
-template <int NT>
-struct NPair { static constexpr int value = NT * (NT + 1) / 2; };
-
-template <int I>
-struct IntC { static constexpr int value = I; };
-
-// calls f(IntC<I>) for I in [B, E): loop indices known at compile time
-template <int B, int E, class F>
-__device__ __forceinline__ void static_for(F &&f) {
-    if constexpr (B < E) {
-        f(IntC<B>{});
-        static_for<B + 1, E>(f);
-    }
-}
-
-// row of the packed upper triangle t1 <= t2 (the host's pair_index enumeration)
-template <int NT>
-__host__ __device__ constexpr int pair_idx(int a, int b) {
-    return a <= b ? a * NT - a * (a - 1) / 2 + (b - a) : b * NT - b * (b - 1) / 2 + (a - b);
-}
-
-template <int NT, int EPT>
-struct EntryRegs {
-    int e[EPT];
-    int kx[EPT], ky[EPT], kz[EPT];
-    double beta[EPT];
-    double bl[EPT][NPair<NT>::value];  // beta_LJ of every type pair for this entry
-    double2 rho[EPT][1 + NT];
-    double2 mold[EPT][1 + NT];
-    double2 dl[EPT][1 + NT];
-};
-
 // k-space force on the molecule's atoms from one entry: 4 pi beta (C sin - S cos) k per atom,
-// Coulomb with the q-weighted phase and the current (or new) Coulomb rho, plus the dispersion
-// terms of the atom's LJ type against every type's rho (ForceKSpace.f90:59-302).
+// Coulomb with the q-weighted phase, plus the dispersion terms of the atom's LJ type against
+// every type's structure factor (ForceKSpace.f90:59-302).
 template <int NT>
-__device__ __forceinline__ void entry_forces(const ChainShared &sh, int s0, int na, int kx, int ky, int kz, double beta,
-                                    const double (&bl)[NPair<NT>::value], const double2 (&C)[1 + NT],
-                                    const double2 (&ph)[kMaxA], const double2 (&phl)[kMaxA], double (&acc)[kNV]) {
+__device__ __forceinline__ void entry_forces(const Cand &m, int s0, int na, int kx, int ky, int kz, double beta,
+                                             const double (&bl)[NPair<NT>::value], const double2 (&C)[1 + NT],
+                                             const double2 (&ph)[kMaxA], const double2 (&phl)[kMaxA], double (&acc)[kNV]) {
     const double fourpi = kFourPi;
 #pragma unroll
     for (int a = 0; a < kMaxA; ++a) {
-        if (a >= na) break;
-        const int ta = sh.slot[s0 + a].type;
-        double w = fourpi * ((C[0].x * ph[a].y - C[0].y * ph[a].x) * beta);
-        if (ta > 0) {
+        if (a < na) {
+            const int ta = m.slot[s0 + a].type;
+            double w = fourpi * ((C[0].x * ph[a].y - C[0].y * ph[a].x) * beta);
+            if (ta > 0) {
 #pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                double b = 0.0;
+                for (int t = 0; t < NT; ++t) {
+                    double b = 0.0;
 #pragma unroll
-                for (int u = 0; u < NT; ++u)
-                    if (u == ta - 1) b = bl[pair_idx<NT>(u, t)];
-                w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * b);
+                    for (int u = 0; u < NT; ++u)
+                        if (u == ta - 1) b = bl[pair_idx<NT>(u, t)];
+                    w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * b);
+                }
             }
+            acc[RV_F + 3 * a] += w * kx;
+            acc[RV_F + 3 * a + 1] += w * ky;
+            acc[RV_F + 3 * a + 2] += w * kz;
         }
-        acc[RV_F + 3 * a] += w * kx;
-        acc[RV_F + 3 * a + 1] += w * ky;
-        acc[RV_F + 3 * a + 2] += w * kz;
     }
 }
 
-// One pass over the moved molecule's slots: k-space over the thread's entries, real space over
-// the CTA's atoms (pairs within the cutoff are compacted into a queue, then evaluated densely),
-// reduced over the CTA and then over the cluster in rank order.  Result: sh.tot, identical in
-// every CTA of the cluster.
+// The workers' part of one pass over the molecule's slots: k-space over their entries, real
+// space over the CTA's atoms (pairs inside the cutoff laid out in the queue by a prefix sum
+// over threads -- a deterministic order -- then evaluated item i by worker i % nwork), and a
+// per-warp reduction into red[worker warp][value].  Worker-only barriers (bar 1).
 template <int NT, int EPT, int KIND, bool FORCES>
-__device__ __forceinline__ void chain_pass(const ChainArgs &A, const DevSys &D, ChainShared &sh, EntryRegs<NT, EPT> &R, double2 *tab,
-                           const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue, double *red,
-                           double *xch, const double *lj_s, int nown, int G, int rank, int xpar,
-                           cg::cluster_group &cluster) {
-    constexpr int kind = KIND;
-    constexpr bool forces = FORCES;
-    constexpr int NVMAX = FORCES ? kNV : RV_F;  // accumulators this pass needs
-    const int na = sh.na;
+__device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, EntryRegs<NT, EPT> &R, double2 *tab,
+                                            const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue,
+                                            double *red, const double *lj_s, int nown, int qcap, long long *prof) {
+    constexpr int NVMAX = FORCES ? kNV : RV_F;
+    const Cand &m = sh.cand[sh.icur];
+    const int na = m.na;
     const int KM = D.kmax + 1;
     const int nt = D.nt;
-    const int imol0 = sh.imol - 1;
-    const int s_lo = (kind == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
-    const int s_hi = (kind == PASS_NEW) ? na : 2 * na;
-    const bool prof = A.prof && threadIdx.x == 0 && rank == 0;
-    long long t_mark = prof ? clock64() : 0;
-#define YAMC_PH(ph) do { if (prof) { const long long t_now = clock64(); A.prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
-    build_tables(tab, sh, s_lo, s_hi, KM);
-    __syncthreads();
-    YAMC_PH(PH_TABLES);
+    const int imol0 = m.imol - 1;
+    const int nwork = blockDim.x - kCtl;
+    const int wtid = threadIdx.x - kCtl;
+    const int lane = threadIdx.x & 31;
+    const int wwarp = wtid >> 5, nww = nwork >> 5;
+    const int s_lo = (KIND == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
+    const int s_hi = (KIND == PASS_NEW) ? na : 2 * na;
+    const bool pf = prof && wtid == 0;
+    long long t_mark = pf ? clock64() : 0;
+#define YAMC_WPH(ph) do { if (pf) { const long long t_now = clock64(); prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
 
-    double acc[NVMAX];
+    build_tables(tab, m, s_lo, s_hi, KM, wtid, nwork);
+    worker_sync(nwork);
+    YAMC_WPH(PH_TABLES);
+
+    double acc[FORCES ? kNV : kNV];
 #pragma unroll
-    for (int v = 0; v < NVMAX; ++v) acc[v] = 0.0;
+    for (int v = 0; v < kNV; ++v) acc[v] = 0.0;
 
-    // ---- k-space: every entry of the thread, with compile-time entry indices so the entry
-    //      state stays in registers
     static_for<0, EPT>([&](auto kc) {
         constexpr int k = decltype(kc)::value;
         if (R.e[k] < 0) return;
         double2 ph[kMaxA], phl[kMaxA];
-        if constexpr (KIND != PASS_NEW) mol_phase_sum<NT>(tab, sh, na, na, KM, R.kx[k], R.ky[k], R.kz[k], R.mold[k], ph, phl);
+        if constexpr (KIND != PASS_NEW) mol_phase_sum<NT>(tab, m, na, na, KM, R.kx[k], R.ky[k], R.kz[k], R.mold[k], ph, phl);
         if constexpr (KIND == PASS_OLD) {
-            if constexpr (FORCES) entry_forces<NT>(sh, na, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k], ph, phl, acc);
+            if constexpr (FORCES) entry_forces<NT>(m, na, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k], ph, phl, acc);
         } else {
             double2 mnew[1 + NT];
-            mol_phase_sum<NT>(tab, sh, 0, na, KM, R.kx[k], R.ky[k], R.kz[k], mnew, ph, phl);
+            mol_phase_sum<NT>(tab, m, 0, na, KM, R.kx[k], R.ky[k], R.kz[k], mnew, ph, phl);
 #pragma unroll
             for (int t = 0; t <= NT; ++t) R.dl[k][t] = make_double2(mnew[t].x - R.mold[k][t].x, mnew[t].y - R.mold[k][t].y);
             {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
@@ -458,83 +483,76 @@ __device__ __forceinline__ void chain_pass(const ChainArgs &A, const DevSys &D, 
                 double2 Cn[1 + NT];
 #pragma unroll
                 for (int t = 0; t <= NT; ++t) Cn[t] = make_double2(R.rho[k][t].x + R.dl[k][t].x, R.rho[k][t].y + R.dl[k][t].y);
-                entry_forces<NT>(sh, 0, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], Cn, ph, phl, acc);
+                entry_forces<NT>(m, 0, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], Cn, ph, phl, acc);
             }
         }
     });
+    YAMC_WPH(PH_KSPACE);
 
-    YAMC_PH(PH_KSPACE);
-    // ---- real space: each thread tests CPT of the CTA's atoms against the active slots, the
-    //      (atom, slot) pairs inside the cutoff are laid out in the queue by a prefix sum over
-    //      threads (deterministic order), then evaluated by all threads, item i by thread i % B.
-    const int lane = threadIdx.x & 31;
-    const int warp = threadIdx.x >> 5, nwarp = blockDim.x >> 5;
-    const int B = blockDim.x;
-    const int round_atoms = B * kCPT;
+    const int round_atoms = nwork * kCPT;
     for (int c0 = 0; c0 < nown; c0 += round_atoms) {
         unsigned masks = 0;  // kCPT slot masks of 8 bits
         int count = 0;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            const int jl = c0 + c * B + threadIdx.x;
+            const int jl = c0 + c * nwork + wtid;
             if (jl < nown && meta_s[jl].x != imol0) {
                 const double4 pj = atom_s[jl];
                 const int tj = meta_s[jl].y;
                 const double dj = dhs_s[jl];
-                unsigned m = 0;
+                unsigned msk = 0;
                 for (int s = s_lo; s < s_hi; ++s) {
-                    const Slot &sl = sh.slot[s];
+                    const Slot &sl = m.slot[s];
                     const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
                     const double r2 = dx * dx + dy * dy + dz * dz;
-                    if (s < na && kind != PASS_OLD && sl.type > 0 && tj > 0) {  // hard core (EwaldSumRealSpace.f90:409)
+                    if (KIND != PASS_OLD && s < na && sl.type > 0 && tj > 0) {  // hard core (EwaldSumRealSpace.f90:409)
                         const double d12 = (sl.dhs + dj) / 2;
                         if (r2 < d12 * d12) acc[RV_OVL] = 1.0;
                     }
-                    if (r2 < D.rmax2) m |= 1u << s;
+                    if (r2 < D.rmax2) msk |= 1u << s;
                 }
-                masks |= m << (8 * c);
-                count += __popc(m);
+                masks |= msk << (8 * c);
+                count += __popc(msk);
             }
         }
-        // exclusive prefix of the counts: within the warp, then over the warps
         int incl = count;
 #pragma unroll
         for (int o = 1; o < 32; o <<= 1) {
             const int y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        if (lane == 31) sh.wcount[warp] = incl;
-        __syncthreads();
-        if (warp == 0) {
-            const int v = lane < nwarp ? sh.wcount[lane] : 0;
+        if (lane == 31) sh.wcount[wwarp] = incl;
+        worker_sync(nwork);
+        if (wwarp == 0) {
+            const int v = lane < nww ? sh.wcount[lane] : 0;
             int x = v;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 const int y = __shfl_up_sync(0xffffffffu, x, o);
                 if (lane >= o) x += y;
             }
-            if (lane < nwarp) sh.wcount[32 + lane] = x - v;
+            if (lane < nww) sh.wcount[32 + lane] = x - v;
             if (lane == 31) sh.qcount = x;
         }
-        __syncthreads();
-        int pos = sh.wcount[32 + warp] + incl - count;
+        worker_sync(nwork);
+        int pos = sh.wcount[32 + wwarp] + incl - count;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            unsigned m = (masks >> (8 * c)) & 0xffu;
-            const int jl = c0 + c * B + threadIdx.x;
-            while (m) {
-                const int s = __ffs(m) - 1;
-                m &= m - 1;
+            unsigned msk = (masks >> (8 * c)) & 0xffu;
+            const int jl = c0 + c * nwork + wtid;
+            while (msk) {
+                const int s = __ffs(msk) - 1;
+                msk &= msk - 1;
                 queue[pos++] = (jl << 3) | s;
             }
         }
-        __syncthreads();
-        YAMC_PH(PH_FILTER);
+        worker_sync(nwork);
+        YAMC_WPH(PH_FILTER);
         const int nq = sh.qcount;
-        for (int qi = threadIdx.x; qi < nq; qi += B) {
+        for (int qi = wtid; qi < nq; qi += nwork) {
             const int item = queue[qi];
             const int jl = item >> 3, s = item & 7;
-            const Slot &sl = sh.slot[s];
+            const Slot &sl = m.slot[s];
             const double4 pj = atom_s[jl];
             const int tj = meta_s[jl].y;
             const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
@@ -544,7 +562,7 @@ __device__ __forceinline__ void chain_pass(const ChainArgs &A, const DevSys &D, 
             const double qq = D.xclb * sl.q * pj.w;
             const double s6 = lj ? lj_s[off] : 0.0, fe = lj ? lj_s[nt * nt + off] : 0.0;
             const bool isnew = s < na;
-            const double sign = (kind == PASS_BOTH && !isnew) ? -1.0 : 1.0;
+            const double sign = (KIND == PASS_BOTH && !isnew) ? -1.0 : 1.0;
             if constexpr (FORCES) {
                 const PairTerm<double> t = pair_term<double, true>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
                 acc[RV_EW] += sign * t.ew; acc[RV_LJ6] += sign * t.lj6; acc[RV_LJ12] += sign * t.lj12;
@@ -557,62 +575,153 @@ __device__ __forceinline__ void chain_pass(const ChainArgs &A, const DevSys &D, 
                 acc[RV_EW] += sign * t.ew; acc[RV_LJ6] += sign * t.lj6; acc[RV_LJ12] += sign * t.lj12;
             }
         }
-        __syncthreads();
-        YAMC_PH(PH_PAIRS);
+        worker_sync(nwork);
+        YAMC_WPH(PH_PAIRS);
     }
 
-    // ---- reduction: xor trees within each warp, across the warps (one warp per value) and
-    //      across the cluster's CTAs; fixed trees, so every CTA gets bit-identical totals
-    if (A.mode == MODE_RUN && threadIdx.x >= 32 && threadIdx.x < 64) __pipeline_wait_prior(0);  // random window
-    const int nv = forces ? (RV_F + 3 * na) : RV_F;
+    // per-warp reduction (xor tree) into red[worker warp][value]
+    const int nv = FORCES ? (RV_F + 3 * na) : RV_F;
 #pragma unroll
-    for (int v = 0; v < kNV; ++v) {
-        if (v >= nv) break;
-        double x = acc[v];
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double y = __shfl_xor_sync(0xffffffffu, x, o);
-            x = (v == RV_OVL) ? fmax(x, y) : x + y;
-        }
-        if (lane == 0) red[warp * kNV + v] = x;
-    }
-    __syncthreads();
-    for (int v = warp; v < nv; v += nwarp) {
-        double x = lane < nwarp ? red[lane * kNV + v] : 0.0;
-#pragma unroll
-        for (int o = 16; o > 0; o >>= 1) {
-            const double y = __shfl_xor_sync(0xffffffffu, x, o);
-            x = (v == RV_OVL) ? fmax(x, y) : x + y;
-        }
-        if (G > 1) {
-            if (lane < G) {
-                double *dst = cluster.map_shared_rank(xch, lane);
-                dst[(xpar * G + rank) * kNV + v] = x;
-            }
-        } else if (lane == 0) {
-            sh.tot[v] = x;
-        }
-    }
-    YAMC_PH(PH_REDUCE);
-    if (G > 1) {
-        cluster.sync();
-        for (int v = warp; v < nv; v += nwarp) {
-            double x = lane < G ? xch[(xpar * G + lane) * kNV + v] : 0.0;
+    for (int v = 0; v < NVMAX; ++v) {
+        if (v < nv) {
+            double x = acc[v];
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) {
                 const double y = __shfl_xor_sync(0xffffffffu, x, o);
                 x = (v == RV_OVL) ? fmax(x, y) : x + y;
             }
-            if (lane == 0) sh.tot[v] = x;
+            if (lane == 0) red[wwarp * kNV + v] = x;
         }
     }
-    __syncthreads();
-    YAMC_PH(PH_CLUSTER);
-#undef YAMC_PH
+#undef YAMC_WPH
 }
 
-template <int NT, int EPT>
-__global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
+// Control warp, after the workers' per-warp partials: trees over the worker warps, then over the
+// cluster's CTAs in a fixed order, so every CTA holds bit-identical totals in sh.tot.  Called by
+// all threads (the cluster barrier needs everyone).
+__device__ __forceinline__ void reduce_pass(ChainShared &sh, const double *red, double *xch, int nv, int G, int rank,
+                                            int xpar, cg::cluster_group &cluster) {
+    const int lane = threadIdx.x & 31;
+    const int nww = (blockDim.x - kCtl) >> 5;
+    if (threadIdx.x < kCtl) {
+        for (int v = 0; v < nv; ++v) {
+            double x = lane < nww ? red[lane * kNV + v] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = (v == RV_OVL) ? fmax(x, y) : x + y;
+            }
+            if (G > 1) {
+                if (lane < G) {
+                    double *dst = cluster.map_shared_rank(xch, lane);
+                    dst[(xpar * G + rank) * kNV + v] = x;
+                }
+            } else if (lane == 0) {
+                sh.tot[v] = x;
+            }
+        }
+    }
+    if (G > 1) {
+        cluster.sync();
+        if (threadIdx.x < kCtl) {
+            for (int v = 0; v < nv; ++v) {
+                double x = lane < G ? xch[(xpar * G + lane) * kNV + v] : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                    x = (v == RV_OVL) ? fmax(x, y) : x + y;
+                }
+                if (lane == 0) sh.tot[v] = x;
+            }
+        }
+    }
+}
+
+// Control lane work: molecule choice (run_mc draws) and the static atom data of the chosen
+// molecule at its current positions.  `moving` is the molecule of the move in flight (0-based,
+// -1 if none) whose positions come from `moving_pos` (its old or its proposed positions).
+struct ChooseCtx {
+    const DevSys *D;
+    const RunSlot *run;
+    const float *w0, *w1;
+    const double4 *atom_s;
+    int G;
+};
+
+__device__ inline RngReader make_reader(const ChooseCtx &X, const ChainShared &sh, long long cur) {
+    return RngReader{X.run->rng, X.run->rng_off, X.run->n_rng, cur, 0, X.w0, sh.wbase[0], sh.wn[0],
+                     X.w1, sh.wbase[1], sh.wn[1]};
+}
+
+__device__ inline void stage_molecule(const ChooseCtx &X, ChainShared &sh, Cand &C, int imol, int moving,
+                                      const Slot *moving_pos, cg::cluster_group &cluster) {
+    const DevSys &D = *X.D;
+    int sp = -1;
+    for (int q = 0; q < sh.nspec; ++q)
+        if (imol - 1 >= sh.sp_m0[q] && imol - 1 < sh.sp_m0[q] + sh.sp_cnt[q]) { sp = q; break; }
+    int first, nam;
+    if (sp >= 0) { nam = sh.sp_na[sp]; first = sh.sp_a0[sp] + (imol - 1 - sh.sp_m0[sp]) * nam; }
+    else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
+    C.imol = imol; C.first = first; C.na = nam;
+    double mx = 0, my = 0, mz = 0;
+    for (int a = 0; a < nam; ++a) {
+        const int j = first + a;
+        Slot s;
+        if (sp >= 0) { s = sh.sp_atom[sp][a]; C.mass[a] = sh.sp_mass[sp][a]; }
+        else {
+            const double q = D.atom[j].w;
+            s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y; s.pad = 0;
+            C.mass[a] = D.mass[j];
+        }
+        if (imol - 1 == moving) { s.x = moving_pos[a].x; s.y = moving_pos[a].y; s.z = moving_pos[a].z; }
+        else if (imol - 1 == sh.last_mol) { s.x = sh.lx[a]; s.y = sh.ly[a]; s.z = sh.lz[a]; }
+        else {
+            const double4 *src = (X.G > 1) ? cluster.map_shared_rank(X.atom_s, j % X.G) : X.atom_s;
+            const double4 p = src[j / X.G];
+            s.x = p.x; s.y = p.y; s.z = p.z;
+        }
+        C.slot[nam + a] = s;  // old positions
+        C.slot[a] = s;        // proposed positions, replaced by propose()
+        // dipole of the molecule at the old positions (EwaldSumExternal_calc_mu)
+        mx = mx + s.q * s.x; my = my + s.q * s.y; mz = mz + s.q * s.z;
+    }
+    C.mu_old[0] = mx; C.mu_old[1] = my; C.mu_old[2] = mz;
+}
+
+// run_mc's draws before movemc: the per-cycle pressure draw, the exchange draw, the molecule
+// draw (runmc.f90:206, 232, 258).  Returns the 1-based molecule, or 0 when the stream ran out.
+__device__ inline int draw_molecule(const DevSys &D, RngReader &rng, bool cycle_start) {
+    if (cycle_start) (void)rng.next();
+    (void)rng.next();
+    const double r = rng.next();
+    if (rng.out) return 0;
+    return choose_molecule_guess(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
+}
+
+// movemc Step 5 (MC.f90:1031-1067) for a staged molecule; F/T are the old molecular force and
+// torque (zero for unbiased moves)
+__device__ inline void propose(const DevSys &D, Cand &C, RngReader &rng, const double F[3], const double T[3]) {
+    const int na = C.na;
+    MoveState &m = C.mv;
+    mcm_init_old(m, F, T);
+    mcm_choose_displacement(m, rng, D.xlf, D.dr);
+    if (!rng.out) mcm_choose_rotation(m, rng, D.xlc, D.d_angle);
+    double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        const Slot &o = C.slot[a < na ? na + a : na];
+        xo[a] = o.x; yo[a] = o.y; zo[a] = o.z;
+    }
+    place_molecule(m, na, xo, yo, zo, C.mass, xn, yn, zn);
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a)
+        if (a < na) { C.slot[a].x = xn[a]; C.slot[a].y = yn[a]; C.slot[a].z = zn[a]; }
+}
+
+// SPLIT = false: unbiased device-resident chain only (one fused pass per move, speculation);
+// SPLIT = true: force-biased moves and the per-move API (old pass + new pass with forces).
+template <int NT, int EPT, bool SPLIT>
+__global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ChainShared sh;
     __shared__ float rwin[2][kWin];
@@ -628,6 +737,10 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
     const int KM = D.kmax + 1;
     const int S = D.S;
     const int nt = D.nt;
+    const int nwork = B - kCtl;
+    const int wtid = tid - kCtl;
+    const bool ctl = tid < kCtl;
+    const int lane = tid & 31;
 
     // shared memory carve-up (chain_smem_bytes on the host computes the same sizes)
     double2 *tab = reinterpret_cast<double2 *>(smem_raw);                     // [2 kMaxA][3][KM]
@@ -647,12 +760,12 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
     }
     for (int i = tid; i < nt * nt; i += B) { lj_s[i] = D.lj_sig6[i]; lj_s[nt * nt + i] = D.lj_feps[i]; }
 
-    // entries of this thread; rho stays in registers for the whole launch
+    // the workers' k-vector entries; rho stays in registers for the whole launch
     EntryRegs<NT, EPT> R;
-    const int gthreads = G * B;
+    const int gwork = G * nwork;
 #pragma unroll
     for (int k = 0; k < EPT; ++k) {
-        const int e = rank * B + tid + k * gthreads;
+        const int e = ctl ? S : rank * nwork + wtid + k * gwork;
         R.e[k] = e < S ? e : -1;
         R.kx[k] = R.ky[k] = R.kz[k] = 0;
         R.beta[k] = 0;
@@ -670,6 +783,7 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
             R.dl[k][t] = make_double2(0, 0);
         }
     }
+    const long long n_rng = run->n_rng;
     if (tid == 0) {
         for (int c = 0; c < SC_COUNT; ++c) sh.sc[c] = D.scal[c];
         sh.icycle = D.cnt[CN_ICYCLE];
@@ -678,8 +792,9 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
         sh.last_mol = -1;
         sh.abort = 0;
         sh.qcount = 0;
-        sh.wbase[0] = sh.wbase[1] = -1;
-        sh.wn[0] = sh.wn[1] = 0;
+        sh.wnext = 0;
+        sh.icur = 0;
+        sh.spec_ok = 0;
         // static atom data of each molecule species, taken from its first molecule
         sh.nspec = D.nspec <= kMaxSpecies ? D.nspec : 0;
         for (int sp = 0; sp < sh.nspec; ++sp) {
@@ -696,156 +811,166 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
             }
         }
     }
+    // first random window at the start cursor
+    if (ctl && A.mode == MODE_RUN) {
+        const long long base = run->cursor;
+        const long long avail = n_rng - base;
+        const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
+        for (int i = lane; i < nw; i += 32) rwin[0][i] = run->rng[base + i - run->rng_off];
+        if (lane == 0) { sh.wbase[0] = base; sh.wn[0] = nw; sh.wbase[1] = -1; sh.wn[1] = 0; sh.wnext = 1; }
+    }
     __syncthreads();
-    const bool biased = (D.xlf > 0.0 || D.xlc > 0.0);
+    const bool biased = SPLIT && (D.xlf > 0.0 || D.xlc > 0.0);
+    const bool speculate = !SPLIT;
+    const ChooseCtx X{&D, run, rwin[0], rwin[1], atom_s, G};
 
     long long moves_done = 0;
     int n_acc = 0, rows = 0;
     int xpar = 0;  // parity of the cluster exchange buffer, flipped after every pass
     const long long n_moves = (A.mode == MODE_RUN) ? run->n_moves : 1;
-
-    const bool prof = A.prof && tid == 0 && rank == 0;
+    long long *prof = (A.prof && rank == 0) ? A.prof : nullptr;
+    const bool pc = prof && tid == 0;
     long long t_mark = 0;
-#define YAMC_PH(ph) do { if (prof) { const long long t_now = clock64(); A.prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+#define YAMC_PH(ph) do { if (pc) { const long long t_now = clock64(); prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+
+    // ---------------------------------------------------------------- the first move of the launch
+    bool have_next = false;  // sh.cur already prepared by the previous iteration's speculation
     for (long long it = 0; it < n_moves; ++it) {
-        if (prof) t_mark = clock64();
-        // ------------------------------------------------ choose the molecule, stage its atoms
-        if (tid == 0) {
-            sh.cursor_start = sh.cursor;
-            sh.abort = 0;
-            int imol = 1;
-            if (A.mode == MODE_RUN) {
-                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
-                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
-                if (sh.mic == 0) (void)rng.next();  // per-cycle pressure-step draw (runmc.f90:206)
-                (void)rng.next();                   // move-or-exchange draw (runmc.f90:232), never an exchange
-                const double r = rng.next();        // BiasedRandom_choose (runmc.f90:258)
-                imol = choose_molecule_guess(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
-                if (rng.out) sh.abort = 1;
-                else sh.cursor = rng.cur;
-            } else {
-                imol = (int)A.api_in[0];
-            }
-            // molecule -> species -> first atom; static atom data from the species table
-            int sp = -1;
-            for (int q = 0; q < sh.nspec; ++q)
-                if (imol - 1 >= sh.sp_m0[q] && imol - 1 < sh.sp_m0[q] + sh.sp_cnt[q]) { sp = q; break; }
-            int first, nam;
-            if (sp >= 0) { nam = sh.sp_na[sp]; first = sh.sp_a0[sp] + (imol - 1 - sh.sp_m0[sp]) * nam; }
-            else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
-            sh.imol = imol; sh.first = first; sh.na = nam;
-            double mx = 0, my = 0, mz = 0;
-            for (int a = 0; a < nam; ++a) {
-                const int j = first + a;
-                Slot s;
-                if (sp >= 0) { s = sh.sp_atom[sp][a]; sh.mass[a] = sh.sp_mass[sp][a]; }
-                else {
-                    const double q = D.atom[j].w;
-                    s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y; s.pad = 0;
-                    sh.mass[a] = D.mass[j];
-                }
-                // positions: the last accepted move's cache, else the owning CTA's staged copy
-                if (imol - 1 == sh.last_mol) { s.x = sh.lx[a]; s.y = sh.ly[a]; s.z = sh.lz[a]; }
-                else {
-                    const double4 *src = (G > 1) ? cluster.map_shared_rank(atom_s, j % G) : atom_s;
-                    const double4 p = src[j / G];
-                    s.x = p.x; s.y = p.y; s.z = p.z;
-                }
-                sh.slot[nam + a] = s;  // old positions
-                sh.slot[a] = s;        // new positions, replaced after the proposal
-                // dipole of the molecule at the old positions (EwaldSumExternal_calc_mu)
-                mx = mx + s.q * s.x; my = my + s.q * s.y; mz = mz + s.q * s.z;
-            }
-            sh.mu_old[0] = mx; sh.mu_old[1] = my; sh.mu_old[2] = mz;
-            sh.kind = PASS_OLD;
-            sh.forces = 1;
-        }
-        __syncthreads();
-        if (sh.abort) break;
-        const int na = sh.na;
-        YAMC_PH(PH_CHOOSE);
-
-        // ------------------------------------------------ old forces (force-biased moves, per-move API)
-        if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
-            chain_pass<NT, EPT, PASS_OLD, true>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
-            xpar ^= 1;
-            if (prof) t_mark = clock64();
+        if (pc) t_mark = clock64();
+        if (!have_next) {
+            // choose the molecule and stage its atoms (no move in flight)
             if (tid == 0) {
-                sh.eold[0] = sh.tot[RV_EW]; sh.eold[1] = sh.tot[RV_LJ6]; sh.eold[2] = sh.tot[RV_LJ12];
-                for (int a = 0; a < na; ++a) {  // external-field force -2 kext q mu (MC.f90:988-997)
-                    const double q = sh.slot[na + a].q;
-                    sh.fold[3 * a] = sh.tot[RV_F + 3 * a] + D.m2k * q * sh.sc[SC_MU_X];
-                    sh.fold[3 * a + 1] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * sh.sc[SC_MU_Y];
-                    sh.fold[3 * a + 2] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * sh.sc[SC_MU_Z];
+                Cand &C = sh.cand[sh.icur];
+                C.cur_start = sh.cursor;
+                int imol;
+                if (A.mode == MODE_RUN) {
+                    RngReader rng = make_reader(X, sh, sh.cursor);
+                    imol = draw_molecule(D, rng, sh.mic == 0);
+                    C.valid = imol > 0;
+                    C.cur_prop = rng.cur;
+                    if (!imol) imol = 1;
+                } else {
+                    imol = (int)A.api_in[0];
+                    C.valid = 1;
+                    C.cur_prop = sh.cursor;
                 }
+                stage_molecule(X, sh, C, imol, -1, nullptr, cluster);
+                sh.abort = C.valid ? 0 : 1;
             }
-            if (A.mode == MODE_OLD) {
-#pragma unroll
-                for (int k = 0; k < EPT; ++k)
-                    if (R.e[k] >= 0) {
-#pragma unroll
-                        for (int t = 0; t <= NT; ++t) A.scratch[(size_t)t * S + R.e[k]] = R.mold[k][t];
-                    }
+            __syncthreads();
+            if (sh.abort) break;
+            YAMC_PH(PH_CHOOSE);
+            const int na0 = sh.cand[sh.icur].na;
+            // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
+            if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, prof);
                 __syncthreads();
-                if (tid == 0 && rank == 0) {
-                    for (int c = 0; c < 3; ++c) A.api_out[c] = sh.eold[c];
-                    for (int c = 0; c < 3 * na; ++c) A.api_out[RV_F + c] = sh.fold[c];
+                reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
+                xpar ^= 1;
+                __syncthreads();
+                if (tid == 0) {
+                    sh.eold[0] = sh.tot[RV_EW]; sh.eold[1] = sh.tot[RV_LJ6]; sh.eold[2] = sh.tot[RV_LJ12];
+                    for (int a = 0; a < na0; ++a) {  // external-field force -2 kext q mu (MC.f90:988-997)
+                        const double q = sh.cand[sh.icur].slot[na0 + a].q;
+                        sh.fold[3 * a] = sh.tot[RV_F + 3 * a] + D.m2k * q * sh.sc[SC_MU_X];
+                        sh.fold[3 * a + 1] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * sh.sc[SC_MU_Y];
+                        sh.fold[3 * a + 2] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * sh.sc[SC_MU_Z];
+                    }
                 }
-                moves_done = 1;
-                break;
+                if (A.mode == MODE_OLD) {
+#pragma unroll
+                    for (int k = 0; k < EPT; ++k)
+                        if (R.e[k] >= 0) {
+#pragma unroll
+                            for (int t = 0; t <= NT; ++t) A.scratch[(size_t)t * S + R.e[k]] = R.mold[k][t];
+                        }
+                    __syncthreads();
+                    if (tid == 0 && rank == 0) {
+                        for (int c = 0; c < 3; ++c) A.api_out[c] = sh.eold[c];
+                        for (int c = 0; c < 3 * na0; ++c) A.api_out[RV_F + c] = sh.fold[c];
+                    }
+                    moves_done = 1;
+                    break;
+                }
             }
+            // the proposal (movemc Step 5)
+            if (tid == 0) {
+                Cand &C = sh.cand[sh.icur];
+                if (A.mode == MODE_RUN) {
+                    RngReader rng = make_reader(X, sh, C.cur_prop);
+                    double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+                    if (biased) {
+                        double xo[kMaxA], yo[kMaxA], zo[kMaxA], fx[kMaxA], fy[kMaxA], fz[kMaxA];
+                        for (int a = 0; a < na0; ++a) {
+                            xo[a] = C.slot[na0 + a].x; yo[a] = C.slot[na0 + a].y; zo[a] = C.slot[na0 + a].z;
+                            fx[a] = sh.fold[3 * a]; fy[a] = sh.fold[3 * a + 1]; fz[a] = sh.fold[3 * a + 2];
+                        }
+                        mol_force_torque(na0, xo, yo, zo, C.mass, fx, fy, fz, F, T);
+                    }
+                    propose(D, C, rng, F, T);
+                    C.cur_prop = rng.cur;
+                    if (rng.out) { C.valid = 0; sh.abort = 1; }
+                } else {  // MODE_EVAL: positions from the host
+                    for (int a = 0; a < na0; ++a) {
+                        C.slot[a].x = A.api_in[1 + 3 * a]; C.slot[a].y = A.api_in[2 + 3 * a]; C.slot[a].z = A.api_in[3 + 3 * a];
+                    }
+                }
+            }
+            __syncthreads();
+            if (sh.abort) break;
+            YAMC_PH(PH_PROPOSE);
         }
+        const int na = sh.cand[sh.icur].na;
+        const bool split = SPLIT;
 
-        // ------------------------------------------------ proposal (movemc Step 5)
-        if (tid == 0) {
-            double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
-            for (int a = 0; a < na; ++a) { xo[a] = sh.slot[na + a].x; yo[a] = sh.slot[na + a].y; zo[a] = sh.slot[na + a].z; }
-            if (A.mode == MODE_RUN) {
-                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
-                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
-                double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-                if (biased) {
-                    double fx[kMaxA], fy[kMaxA], fz[kMaxA];
-                    for (int a = 0; a < na; ++a) { fx[a] = sh.fold[3 * a]; fy[a] = sh.fold[3 * a + 1]; fz[a] = sh.fold[3 * a + 2]; }
-                    mol_force_torque(na, xo, yo, zo, sh.mass, fx, fy, fz, F, T);
+        // ------------------------------------------------ the pass over the new positions
+        if (!ctl) {
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, prof);
+            else worker_pass<NT, EPT, PASS_BOTH, false>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, prof);
+        } else if (speculate && it + 1 < n_moves) {
+            // prepare the next move's candidates while the workers run: lane 0 after an overlap
+            // (no acceptance draw), lanes 1-2 after the acceptance draw, lane 2 with the molecule
+            // in flight at its proposed positions (used only if it is chosen again and accepted)
+            const Cand &M = sh.cand[sh.icur];
+            const long long c1 = M.cur_prop;
+            const bool next_cycle = (sh.mic + 1 == D.M);
+            // the window of the stream the candidates read: make sure it covers c1 onwards
+            {
+                const int b = sh.wnext;
+                const bool covered0 = sh.wbase[0] >= 0 && c1 >= sh.wbase[0] && c1 + kWin / 2 <= sh.wbase[0] + sh.wn[0];
+                const bool covered1 = sh.wbase[1] >= 0 && c1 >= sh.wbase[1] && c1 + kWin / 2 <= sh.wbase[1] + sh.wn[1];
+                if (!covered0 && !covered1) {
+                    const long long avail = n_rng - c1;
+                    const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
+                    __syncwarp();
+                    for (int i = lane; i < nw; i += 32) rwin[b][i] = run->rng[c1 + i - run->rng_off];
+                    __syncwarp();
+                    if (lane == 0) { sh.wbase[b] = c1; sh.wn[b] = nw; sh.wnext = b ^ 1; }
+                    __syncwarp();
                 }
-                MoveState &m = sh.mv;
-                mcm_init_old(m, F, T);
-                mcm_choose_displacement(m, rng, D.xlf, D.dr);
-                if (!rng.out) mcm_choose_rotation(m, rng, D.xlc, D.d_angle);
-                if (rng.out) { sh.abort = 1; sh.cursor = sh.cursor_start; }
-                else sh.cursor = rng.cur;
-                place_molecule(m, na, xo, yo, zo, sh.mass, xn, yn, zn);
-            } else {  // MODE_EVAL: positions from the host
-                for (int a = 0; a < na; ++a) { xn[a] = A.api_in[1 + 3 * a]; yn[a] = A.api_in[2 + 3 * a]; zn[a] = A.api_in[3 + 3 * a]; }
             }
-            for (int a = 0; a < na; ++a) { sh.slot[a].x = xn[a]; sh.slot[a].y = yn[a]; sh.slot[a].z = zn[a]; }
-            const bool split = biased || A.mode == MODE_EVAL;
-            sh.kind = split ? PASS_NEW : PASS_BOTH;
-            sh.forces = split ? 1 : 0;
+            if (lane < 3) {
+                const int buf = (sh.icur + 1 + lane) & 3;
+                if (lane == 0) { sh.spec[0] = (sh.icur + 1) & 3; sh.spec[1] = (sh.icur + 2) & 3; sh.spec[2] = (sh.icur + 3) & 3; }
+                Cand &C = sh.cand[buf];
+                RngReader rng = make_reader(X, sh, c1);
+                if (lane > 0) (void)rng.next();  // the acceptance draw (MonteCarloMove.f90:553)
+                C.cur_start = rng.cur;
+                const int imol = rng.out ? 0 : draw_molecule(D, rng, next_cycle);
+                C.valid = imol > 0;
+                const Slot *moving = (lane == 2) ? &M.slot[0] : &M.slot[M.na];
+                stage_molecule(X, sh, C, imol > 0 ? imol : 1, M.imol - 1, moving, cluster);
+                const double Z[3] = {0, 0, 0};
+                if (C.valid) propose(D, C, rng, Z, Z);
+                C.cur_prop = rng.cur;
+                if (rng.out) C.valid = 0;
+            }
+            if (pc) { const long long t_now = clock64(); prof[PH_SPECULATE] += t_now - t_mark; t_mark = t_now; }
         }
         __syncthreads();
-        if (sh.abort) break;
-        YAMC_PH(PH_PROPOSE);
-        // refill the other random window from the current cursor while the pass runs; the copy
-        // is awaited by warp 1 before the pass's reduction barrier (chain_pass)
-        if (A.mode == MODE_RUN && tid >= 32 && tid < 64) {
-            const int b = (int)((it + 1) & 1);
-            const long long base = sh.cursor;
-            const long long avail = run->n_rng - base;
-            const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
-            for (int i = tid - 32; i < nw; i += 32) __pipeline_memcpy_async(&rwin[b][i], run->rng + (base + i - run->rng_off), 4);
-            __pipeline_commit();
-            if (tid == 32) { sh.wbase[b] = base; sh.wn[b] = nw; }
-        }
-
-        // ------------------------------------------------ new positions: energies, delta rho, overlap
-        if (biased || A.mode == MODE_EVAL)
-            chain_pass<NT, EPT, PASS_NEW, true>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
-        else
-            chain_pass<NT, EPT, PASS_BOTH, false>(A, D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, xch, lj_s, nown, G, rank, xpar, cluster);
+        reduce_pass(sh, red, xch, split ? RV_F + 3 * na : RV_F, G, rank, xpar, cluster);
         xpar ^= 1;
-        if (prof) t_mark = clock64();
+        YAMC_PH(PH_REDUCE);
 
         if (A.mode == MODE_EVAL) {
 #pragma unroll
@@ -854,6 +979,7 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
 #pragma unroll
                     for (int t = 0; t <= NT; ++t) A.scratch[(size_t)(1 + nt + t) * S + R.e[k]] = R.dl[k][t];
                 }
+            __syncthreads();
             if (tid == 0 && rank == 0)
                 for (int v = 0; v < RV_F + 3 * na; ++v) A.api_out[v] = sh.tot[v];
             moves_done = 1;
@@ -862,14 +988,16 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
 
         // ------------------------------------------------ Metropolis (Steps 7-13) and commit (Step 14)
         if (tid == 0) {
+            const Cand &M = sh.cand[sh.icur];
             const bool overlap = sh.tot[RV_OVL] > 0.0;
             int flags = overlap ? 2 : 0;
             double du_real = 0, du_kc = 0, du_kl = 0, du_ext = 0, dmx = 0, dmy = 0, dmz = 0;
             double dew = 0, dlj6 = 0, dlj12 = 0;
-            sh.accepted = 0;
+            int acc = 0;
+            long long cur_after = M.cur_prop;
+            bool out = false;
             if (!overlap) {
-                RngReader rng{run->rng, run->rng_off, run->n_rng, sh.cursor, 0,
-                              rwin[0], sh.wbase[0], sh.wn[0], rwin[1], sh.wbase[1], sh.wn[1]};
+                RngReader rng = make_reader(X, sh, M.cur_prop);
                 if (biased) {
                     dew = sh.tot[RV_EW] - sh.eold[0]; dlj6 = sh.tot[RV_LJ6] - sh.eold[1]; dlj12 = sh.tot[RV_LJ12] - sh.eold[2];
                     du_real = (sh.tot[RV_EW] + sh.tot[RV_LJ12] - sh.tot[RV_LJ6]) - (sh.eold[0] + sh.eold[2] - sh.eold[1]);
@@ -880,8 +1008,8 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
                 du_kc = sh.tot[RV_DUC];
                 du_kl = sh.tot[RV_DUL];
                 double mx = 0, my = 0, mz = 0;
-                for (int a = 0; a < na; ++a) { mx = mx + sh.slot[a].q * sh.slot[a].x; my = my + sh.slot[a].q * sh.slot[a].y; mz = mz + sh.slot[a].q * sh.slot[a].z; }
-                dmx = mx - sh.mu_old[0]; dmy = my - sh.mu_old[1]; dmz = mz - sh.mu_old[2];
+                for (int a = 0; a < na; ++a) { mx = mx + M.slot[a].q * M.slot[a].x; my = my + M.slot[a].q * M.slot[a].y; mz = mz + M.slot[a].q * M.slot[a].z; }
+                dmx = mx - M.mu_old[0]; dmy = my - M.mu_old[1]; dmz = mz - M.mu_old[2];
                 const double mux = sh.sc[SC_MU_X], muy = sh.sc[SC_MU_Y], muz = sh.sc[SC_MU_Z];
                 // EwaldSumExternal_calc_dU (EwaldSumExternal.f90:68-82)
                 du_ext = D.kext * ((2 * mux + dmx) * dmx + (2 * muy + dmy) * dmy + (2 * muz + dmz) * dmz);
@@ -889,41 +1017,58 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
                 if (biased) {
                     double fx[kMaxA], fy[kMaxA], fz[kMaxA], x[kMaxA], y[kMaxA], z[kMaxA];
                     for (int a = 0; a < na; ++a) {
-                        const double q = sh.slot[a].q;
+                        const double q = M.slot[a].q;
                         fx[a] = sh.tot[RV_F + 3 * a] + D.m2k * q * (mux + dmx);
                         fy[a] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * (muy + dmy);
                         fz[a] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * (muz + dmz);
-                        x[a] = sh.slot[a].x; y[a] = sh.slot[a].y; z[a] = sh.slot[a].z;
+                        x[a] = M.slot[a].x; y[a] = M.slot[a].y; z[a] = M.slot[a].z;
                     }
-                    mol_force_torque(na, x, y, z, sh.mass, fx, fy, fz, F, T);
+                    mol_force_torque(na, x, y, z, M.mass, fx, fy, fz, F, T);
                 }
                 const double du_total = du_real + (du_kc + du_kl) + du_ext;
-                mcm_init_new(sh.mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
-                const int acc = mcm_accept(sh.mv, du_total, D.xlf, D.xlc, rng);
-                if (rng.out) sh.abort = 1;
-                else { sh.cursor = rng.cur; sh.accepted = acc; flags |= acc; }
+                MoveState mv = M.mv;
+                mcm_init_new(mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
+                acc = mcm_accept(mv, du_total, D.xlf, D.xlc, rng);
+                out = rng.out != 0;
+                cur_after = rng.cur;
+                flags |= acc;
             }
-            if (!sh.abort) {
-                if (sh.accepted) {
+            sh.accepted = 0;
+            if (out) {
+                sh.abort = 1;  // the interrupted move restarts from its first draw (sh.cursor unchanged)
+            } else {
+                sh.accepted = acc;
+                if (acc) {
                     sh.sc[SC_UU_EW] += dew; sh.sc[SC_UU_LJ6] += dlj6; sh.sc[SC_UU_LJ12] += dlj12;
                     sh.sc[SC_EK_C] += du_kc; sh.sc[SC_EK_LJ] += du_kl;
                     sh.sc[SC_MU_X] += dmx; sh.sc[SC_MU_Y] += dmy; sh.sc[SC_MU_Z] += dmz;
                     sh.sc[SC_N_MV_ACC] += 1.0;
-                    sh.last_mol = sh.imol - 1;
-                    for (int a = 0; a < na; ++a) { sh.lx[a] = sh.slot[a].x; sh.ly[a] = sh.slot[a].y; sh.lz[a] = sh.slot[a].z; }
+                    sh.last_mol = M.imol - 1;
+                    for (int a = 0; a < na; ++a) { sh.lx[a] = M.slot[a].x; sh.ly[a] = M.slot[a].y; sh.lz[a] = M.slot[a].z; }
+                    // this CTA's staged copy of the moved atoms; every reader of the old copy (this
+                    // move's pass, the candidates prepared during it, in any CTA) has passed the barriers
+                    for (int a = 0; a < na; ++a) {
+                        const int j = M.first + a;
+                        if (j % G == rank) {
+                            double4 p = atom_s[j / G];
+                            p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
+                            atom_s[j / G] = p;
+                        }
+                    }
                     ++n_acc;
                 }
                 sh.sc[SC_N_MV_STEPS] += 1.0;
+                sh.cursor = cur_after;
                 if (rank == 0) {
-                    if (sh.accepted)
+                    if (acc)
                         for (int a = 0; a < na; ++a) {
-                            double4 p = D.atom[sh.first + a];
-                            p.x = sh.slot[a].x; p.y = sh.slot[a].y; p.z = sh.slot[a].z;
-                            D.atom[sh.first + a] = p;
+                            double4 p = D.atom[M.first + a];
+                            p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
+                            D.atom[M.first + a] = p;
                         }
                     if (run->log) {
                         yamc_move_record rec;
-                        rec.imol = sh.imol; rec.flags = flags; rec.cursor = sh.cursor;
+                        rec.imol = M.imol; rec.flags = flags; rec.cursor = cur_after;
                         rec.du_real = du_real; rec.du_k_coul = du_kc; rec.du_k_lj = du_kl; rec.du_ext = du_ext;
                         run->log[it] = rec;
                     }
@@ -946,28 +1091,31 @@ __global__ void __launch_bounds__(512, 1) k_chain(ChainArgs A) {
                     }
                     sh.icycle += 1;
                 }
-            } else {
-                sh.cursor = sh.cursor_start;  // the interrupted move restarts from its first draw
+                // the next move: the prepared candidate that matches what happened
+                sh.spec_ok = 0;
+                if (speculate && it + 1 < n_moves) {
+                    const int sel = overlap ? 0 : ((acc && sh.cand[sh.spec[2]].imol == M.imol) ? 2 : 1);
+                    const int buf = sh.spec[sel];
+                    const Cand &C = sh.cand[buf];
+                    if (C.valid && C.cur_start == sh.cursor) {
+                        sh.icur = buf;
+                        sh.spec_ok = 1;
+                    }
+                }
             }
         }
         __syncthreads();
-        if (sh.abort) break;
         YAMC_PH(PH_DECIDE);
+        if (sh.abort) break;
         if (sh.accepted) {
+            // commit: rho += delta in registers (MC.f90:1245), the CTA's staged copy of the moved atoms
 #pragma unroll
             for (int k = 0; k < EPT; ++k)
 #pragma unroll
                 for (int t = 0; t <= NT; ++t) { R.rho[k][t].x += R.dl[k][t].x; R.rho[k][t].y += R.dl[k][t].y; }
-            if (tid < na) {  // this CTA's staged copy of the moved atoms
-                const int j = sh.first + tid;
-                if (j % G == rank) {
-                    double4 p = atom_s[j / G];
-                    p.x = sh.slot[tid].x; p.y = sh.slot[tid].y; p.z = sh.slot[tid].z;
-                    atom_s[j / G] = p;
-                }
-            }
         }
         ++moves_done;
+        have_next = sh.spec_ok != 0;
         __syncthreads();
         YAMC_PH(PH_COMMIT);
     }
@@ -1104,7 +1252,7 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, c->device));
     const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
-    const int Bs[] = {512, 256};
+    const int Bs[] = {kChainMaxThreads, 128};
     const int Gs[] = {1, 2, 4, 8, 16};
     for (int gi = 0; gi < 5; ++gi) {
         const int G = Gs[gi];
@@ -1112,11 +1260,12 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
         for (int bi = 0; bi < 2; ++bi) {
             const int B = Bs[bi];
             if (c->force_B && B != c->force_B) continue;
-            if (!c->force_B && B != 512 && G * 512 < H.S) continue;
-            const int EPT = (H.S + G * B - 1) / (G * B);
+            if (!c->force_B && B != kChainMaxThreads && G * (kChainMaxThreads - kCtl) < H.S) continue;
+            const int nwork = B - kCtl;  // warp 0 is the control warp
+            const int EPT = (H.S + G * nwork - 1) / (G * nwork);
             if (EPT > 2) continue;
             const int nown_max = (H.N + G - 1) / G;
-            const int qcap = std::min(nown_max, B * kCPT) * 2 * kMaxA;  // one filter round of pairs
+            const int qcap = std::min(nown_max, nwork * kCPT) * 2 * kMaxA;  // one filter round of pairs
             const size_t sm = chain_smem_bytes(G, B, H.kmax, H.nt, nown_max, qcap);
             if (sm > smem_max) continue;
             out->G = G; out->B = B; out->EPT = EPT; out->nown_max = nown_max; out->qcap = qcap; out->smem = sm;
@@ -1127,10 +1276,10 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
     return YAMC_ELIMITS;
 }
 
-template <int NT, int EPT>
+template <int NT, int EPT, bool SPLIT>
 int launch_chain_t(yamc_ctx *c, const ChainArgs &args) {
     const LaunchCfg &L = c->cfg;
-    auto kfn = k_chain<NT, EPT>;
+    auto kfn = k_chain<NT, EPT, SPLIT>;
     CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
     if (L.G > 8) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
@@ -1151,7 +1300,9 @@ int launch_chain_t(yamc_ctx *c, const ChainArgs &args) {
 
 int launch_chain(yamc_ctx *c, const ChainArgs &args) {
     const int nt = c->H.nt, ept = c->cfg.EPT;
-#define YAMC_CASE(NT_, EPT_) if (nt == NT_ && ept == EPT_) return launch_chain_t<NT_, EPT_>(c, args);
+    const bool split = args.mode != MODE_RUN || c->H.p.xlambda_f > 0.0 || c->H.p.xlambda_c > 0.0;
+#define YAMC_CASE(NT_, EPT_)                                                                                      \
+    if (nt == NT_ && ept == EPT_) return split ? launch_chain_t<NT_, EPT_, true>(c, args) : launch_chain_t<NT_, EPT_, false>(c, args);
 #ifdef YAMC_ONE_VARIANT  // development builds: a single instantiation compiles in seconds
     YAMC_CASE(3, 1)
 #else
@@ -1422,7 +1573,9 @@ int yamc_get_positions(yamc_ctx *c, double *x, double *y, double *z) {
 
 int yamc_set_launch(yamc_ctx *c, int32_t cluster_blocks, int32_t threads) {
     if (!c) return YAMC_EPARAMETER;
-    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > 512 || (threads % 32)) return YAMC_EPARAMETER;
+    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > kChainMaxThreads || (threads % 32) ||
+        (threads > 0 && threads < 64))
+        return YAMC_EPARAMETER;
     c->force_G = cluster_blocks;
     c->force_B = threads;
     c->cfg = LaunchCfg();
