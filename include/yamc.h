@@ -176,6 +176,38 @@ int yamc_phase_cycles(yamc_ctx *ctx, int32_t mode, int64_t *out, int32_t n);
 const char *yamc_error_string(int status);
 const char *yamc_last_error_detail(void);
 
+/* ---- allocation-free real-space sums ----
+   No counterpart in the reference: an extra entry point for callers that cannot
+   call cudaMalloc where they need an energy (a host whose own pool holds the
+   device memory, or one that cannot take the synchronisation that cudaMalloc and
+   cudaFree may cause).  It computes the full real-space Ewald sum of a whole
+   configuration -- the real-space half of yamc_full_sums -- from the caller's
+   DEVICE arrays into the caller's DEVICE outputs and allocates nothing: its only
+   scratch is a fixed static device array, sized for YAMC_STATIC_MAX_ATOMS atoms
+   (64 KiB, held by every GPU that loads the library until the process exits).
+   Inputs, all device pointers on the current device: x, y, z (box units), charge,
+   mol (any molecule id per atom; equal ids = same molecule, intra pairs use
+   -erf_Luc), lj_type (0 = no LJ, else 1..n_types), hard_core_angstr, and the
+   n_types x n_types tables sigma6_tab (sigma^6 in box units) and four_eps_tab
+   (4 epsilon / kT) at offset (t1-1)*n_types + t2-1, as LJTypes builds them.  From
+   p: BoxLength, alpha, rmax2, xclb, two_alpha_over_sqrt_pi.  Outputs: uu, fx, fy,
+   fz (natom doubles each, per-atom energy and force; any may be NULL) and sums[8]
+   = uu_ew, uu_lj6, uu_lj12, their intra-molecular parts, overlap (1 when two LJ
+   sites of different molecules are closer than their mean hard-core diameter)
+   and bad_type (1 when some lj_type is outside 0..n_types; those atoms get no LJ).
+   Asynchronous on `stream` (a cudaStream_t, NULL = default stream): read the
+   outputs after that stream has finished.  natom above YAMC_STATIC_MAX_ATOMS is
+   rejected with YAMC_ELIMITS.  The first call on a device looks up the static
+   array's device address (cudaGetSymbolAddress) and should come before any stream
+   capture.  Every call on a device shares the one scratch array: calls that
+   overlap on the GPU (other streams, other host threads) race on it. */
+#define YAMC_STATIC_MAX_ATOMS 262144
+int yamc_realspace_sums_static(const yamc_params *p, int32_t natom, const double *x, const double *y,
+                               const double *z, const double *charge, const int32_t *mol,
+                               const int32_t *lj_type, const double *hard_core_angstr, int32_t n_types,
+                               const double *sigma6_tab, const double *four_eps_tab, double *uu,
+                               double *fx, double *fy, double *fz, double *sums, void *stream);
+
 #ifdef __cplusplus
 }
 #endif

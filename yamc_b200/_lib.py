@@ -15,6 +15,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libyamc_b200.so")
 
 YAMC_OK = 0
+YAMC_ELIMITS = -2
 YAMC_ERNG_EXHAUSTED = -12
 YAMC_FP64 = 0
 YAMC_MIXED = 1
@@ -87,6 +88,8 @@ SIGNATURES = {
     "yamc_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_phase_cycles": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
+    "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +
+                                   [ctypes.c_int32] + [_VP] * 8),
     "yamc_error_string": (ctypes.c_char_p, [ctypes.c_int]),
     "yamc_last_error_detail": (ctypes.c_char_p, []),
 }

@@ -13,7 +13,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libyamc_b200.so")
-SOURCES = ["yamc_engine.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
+SOURCES = ["yamc_engine.cu", "yamc_static.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
 HEADERS = ["yamc_device.cuh", "yamc_internal.h", os.path.join("..", "..", "include", "yamc.h")]
 
 NVCC_FLAGS = [
