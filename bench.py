@@ -33,6 +33,11 @@ sys.path.insert(0, ROOT)
 METRIC = "MC trial moves/s (SPC/E+NaCl Ewald); mixed vs FP64 GPU at |ΔE err|≤1e-4 kT"
 
 
+# DRAM bytes per move of the chain kernel from the ncu capture of one 2,000-move launch on
+# nacl1m (dram__bytes_read.sum + dram__bytes_write.sum = 1.193 MB), used for roofline.traffic
+TRAFFIC_PER_MOVE = 597.0
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -184,6 +189,7 @@ def main():
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
     ap.add_argument("--ref-moves", type=int, default=1500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--replicas", type=int, default=0, help="chains per GPU (0 = as many clusters as are resident)")
     args = ap.parse_args()
 
     from yamc_b200 import systems
@@ -210,82 +216,100 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
     from yamc_b200 import api, rng as grng
 
-    eng = api.Engine.from_files(files, device=local)
+    dev = f"cuda:{local}"
     n_steps = args.warmup + args.steps
     per_move = 24  # generous upper bound of random numbers per unbiased move
-    stream = grng.gfortran_stream(12345 + rank, per_move * args.moves * (2 * n_steps + 2) + 100000)
-    d_stream = torch.from_numpy(stream).to(f"cuda:{local}")
-    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
+    n_stream = per_move * args.moves * (2 * n_steps + 2) + 100000
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     def l2_flush():
         flush.fill_(1.0)
         torch.cuda.synchronize()
 
+    # ---------------- one chain alone: the latency of the move (reported beside the batch)
+    eng = api.Engine.from_files(files, device=local)
+    s0 = grng.gfortran_stream(12345 + 1000 * rank, per_move * args.moves * 3 + 100000)
+    d_s0 = torch.from_numpy(s0).to(dev)
+    c0, _, _ = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves)
+    single_ms = []
+    for _ in range(2):
+        l2_flush()
+        c0, done, st = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves, cursor=c0)
+        assert st == 0 and done == args.moves
+        single_ms.append(eng.last_kernel_ms)
+    single = {"moves_per_s": args.moves / (np.mean(single_ms) / 1e3), "launch": eng.launch}
+    del d_s0
+    eng.close()
+
+    # ---------------- the batch: R independent chains of the workload, one graph launch per step
+    probe = api.Batch([api.load_inputs(files["parameters"], files["composition"], files["moltab"])], device=local)
+    R = args.replicas or max(1, probe.launch["resident_clusters"])
+    probe.close()
+    rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=3 + 101 * rank + r,
+                                                rng_seed=12345 + 1000 * rank + r) for r in range(1, R)]
+    b = api.Batch([api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files], device=local)
+    streams = [grng.gfortran_stream(12345 + 1000 * rank + 7 * r, n_stream) for r in range(R)]
+    d_streams = [torch.from_numpy(x).to(dev) for x in streams]
+    d_ptrs = [t.data_ptr() for t in d_streams]
+    n_rng = [t.numel() for t in d_streams]
+    cur = np.zeros(R, dtype=np.int64)
+    b.tune(d_ptrs, n_rng, cur, max(200, args.moves // 20))
+
     # ---------------- device-resident value
-    cur = 0
-    acc_before = eng.energies()  # initial state read
     kernel_ms = []
     for w in range(args.warmup):
-        cur, done, st = eng.run_chain_device(d_stream.data_ptr(), d_stream.numel(), args.moves, cursor=cur)
+        b.run_device(d_ptrs, n_rng, cur, args.moves)
         l2_flush()
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
     with Clocks(local) as clk:
         for s in range(args.steps):
-            cur, done, st = eng.run_chain_device(d_stream.data_ptr(), d_stream.numel(), args.moves, cursor=cur)
-            assert st == 0 and done == args.moves, (st, done)
-            kernel_ms.append(eng.last_kernel_ms)
+            done, st, s_all = b.run_device(d_ptrs, n_rng, cur, args.moves)
+            assert s_all == 0 and (done == args.moves).all(), (s_all, done)
+            kernel_ms.append(b.last_kernel_ms)
             l2_flush()
     torch.cuda.synchronize()
     t_dev = sum(kernel_ms) / 1e3
     if ws > 1:
-        t = torch.tensor([t_dev], device=f"cuda:{local}")
+        t = torch.tensor([t_dev], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_dev = float(t.item())
-    value = ws * args.steps * args.moves / t_dev
+    value = ws * R * args.steps * args.moves / t_dev
 
     # ---------------- end to end through the C ABI with host buffers
-    pinned = torch.from_numpy(stream).pin_memory()
-    host = pinned.numpy()
-    import ctypes
-    lib = eng.lib
+    pinned = [torch.from_numpy(x).pin_memory() for x in streams]
+    host = [x.numpy() for x in pinned]
+    views = [b.replica(r) for r in range(R)]
     window = per_move * args.moves
-    h2d = 0
-    ecur = cur
+    ecur = cur.copy()
     e_moves = 0
-    energies = np.zeros(8)
-    nrow = ctypes.c_int32(0)
+    h2d = 0
     for w in range(args.warmup):
-        c = ctypes.c_int64(ecur); dn = ctypes.c_int64(0)
-        lib.yamc_run_chain(eng.h, host.ctypes.data, min(host.size, ecur + window), ctypes.byref(c), args.moves,
-                           ctypes.byref(dn), None, None, 0, ctypes.byref(nrow))
-        ecur = c.value
+        _, ecur, _, _, _ = b.run(host, args.moves, cursors=ecur, limits=ecur + window)
         l2_flush()
     if ws > 1:
         dist.barrier()
     torch.cuda.synchronize()
     e_times = []
+    run_slot = 80
     for s in range(args.steps):
-        c = ctypes.c_int64(ecur); dn = ctypes.c_int64(0)
-        n_rng = min(host.size, ecur + window)
-        h2d = (n_rng - ecur) * 4
+        lim = np.minimum(ecur + window, [h.size for h in host])
+        h2d = int(4 * (lim - ecur).sum()) + R * run_slot
         t0 = time.perf_counter()
-        st = lib.yamc_run_chain(eng.h, host.ctypes.data, n_rng, ctypes.byref(c), args.moves, ctypes.byref(dn),
-                                None, None, 0, ctypes.byref(nrow))
-        lib.yamc_energies(eng.h, energies.ctypes.data_as(ctypes.POINTER(ctypes.c_double)))
+        _, ecur, done, st, s_all = b.run(host, args.moves, cursors=ecur, limits=lim)
+        energies = [v.energies() for v in views]
         e_times.append(time.perf_counter() - t0)
-        assert st == 0 and dn.value == args.moves, (st, dn.value)
-        ecur = c.value
-        e_moves += dn.value
+        assert s_all == 0 and (done == args.moves).all(), (s_all, done)
+        e_moves += int(done.sum())
         l2_flush()
     t_e2e = sum(e_times)
     if ws > 1:
-        t = torch.tensor([t_e2e], device=f"cuda:{local}")
+        t = torch.tensor([t_e2e], device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         t_e2e = float(t.item())
     e2e = ws * e_moves / t_e2e
-    d2h = 80 + 8 * 17 + 8 * 2  # run slot + engine scalars + counters read back per step
+    d2h = R * (run_slot + 8 * 17 + 8 * 2)  # run slot + engine scalars + counters per replica
 
     if ws > 1:
         dist.barrier()
@@ -294,12 +318,15 @@ def main():
         return
 
     # ---------------- roofline of the chain kernel
-    log, _, _, _, _ = eng.run_chain(stream, 2000, cursor=ecur)
+    log, _, _, _, _ = b.run(host, 2000, cursors=ecur, log=True)
     p_acc = float(np.mean(log["flags"] & 1))
-    bpm = algorithmic_bytes_per_move(spec, eng.nk, eng.nsigned, eng.ntype, p_acc)
+    v0 = views[0]
+    bpm = algorithmic_bytes_per_move(spec, v0.nk, v0.nsigned, v0.ntype, p_acc)
     ms_launch = float(np.mean(kernel_ms))
-    achieved = bpm * args.moves / (ms_launch / 1e3) / 1e9
+    moves_launch = R * args.moves
+    achieved = bpm * moves_launch / (ms_launch / 1e3) / 1e9
     peak, which = peaks()
+    launch = b.launch
     line = {
         "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
@@ -307,10 +334,13 @@ def main():
         "config": {"workload": f"{args.workload}: {spec.n_water} SPC/E + {spec.n_na} Na + {spec.n_cl} Cl, "
                                f"{spec.natom} atoms, L={spec.box} A, alpha={spec.alpha}/A, rc={spec.rc} A, "
                                f"kmax={spec.kmax}", "method": "plain FP64, unbiased moves",
-                   "moves_per_step": args.moves, "chains_per_gpu": 1, "parallelism": "replicas",
-                   "launch": eng.launch, "l2": "256 MB write between steps", "accept_fraction": p_acc},
+                   "moves_per_step_per_chain": args.moves, "chains_per_gpu": R,
+                   "parallelism": "independent replicas (one cluster per chain)",
+                   "launch": launch, "l2": "256 MB write between steps", "accept_fraction": p_acc,
+                   "single_chain": single},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_source": which, "algorithmic_bytes_per_move": bpm},
+                     "traffic": TRAFFIC_PER_MOVE * moves_launch, "peak_source": which,
+                     "algorithmic_bytes_per_move": bpm},
         "e2e": {"value": e2e, "unit": "moves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": args.steps,
         "clocks": clk.summary(),

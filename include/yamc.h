@@ -176,6 +176,46 @@ int yamc_phase_cycles(yamc_ctx *ctx, int32_t mode, int64_t *out, int32_t n);
 const char *yamc_error_string(int status);
 const char *yamc_last_error_detail(void);
 
+/* ---- batched replicas ----
+   No counterpart in the reference, which runs one chain per process (run_mc,
+   runmc.f90:178-334).  A batch holds n independent replicas -- each a full system
+   with its own size, box, temperature, composition and random stream -- and
+   advances all of them together: one persistent cluster launch per group of
+   replicas that share a kernel variant (LJ type count, force bias on or off), the
+   groups concurrently, the whole step replayed as one CUDA graph. */
+typedef struct yamc_batch yamc_batch;
+/* systems[n], params[n] as for yamc_create (initmc of every replica). */
+int yamc_batch_create(int32_t n, const yamc_system *systems, const yamc_params *params,
+                      int32_t device, yamc_batch **out);
+int yamc_batch_destroy(yamc_batch *b);
+/* Replica i as a context (owned by the batch): yamc_energies, yamc_full_sums,
+   yamc_get_positions and the other per-context calls work on it between steps. */
+int yamc_batch_replica(yamc_batch *b, int32_t i, yamc_ctx **ctx);
+/* n_moves movemc calls of every replica.  Replica i's random stream is
+   d_rng[i][0 .. n_rng[i]) (device memory); cursors[i] (in/out) indexes it.
+   moves_done[i], status[i] (optional) as for yamc_run_chain; d_log: NULL or
+   n x n_moves records, replica i from i*n_moves.  Returns the first error of any
+   replica, else YAMC_ERNG_EXHAUSTED if some stream ran out (that replica stops
+   at the move it could not complete and resumes from its cursor). */
+int yamc_batch_run_device(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng,
+                          int64_t *cursors, int64_t n_moves, int64_t *moves_done,
+                          int32_t *status, yamc_move_record *d_log);
+/* The same with the streams in host memory (each replica's unread window
+   [cursors[i], n_rng[i]) is copied to the device) and the log in host memory. */
+int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng, int64_t *cursors,
+                   int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *log);
+/* Autotuner: times every launch shape (cluster size x threads per block) that fits
+   all replicas on n_moves moves of each and keeps the one with the highest
+   aggregate moves/s.  The replicas' state is put back after every trial, so the
+   chains do not advance. */
+int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng,
+                    const int64_t *cursors, int64_t n_moves, double *best_moves_per_s);
+int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads);
+/* out: cluster blocks, threads, entries per thread, shared memory bytes, clusters
+   resident at once (of the first group) */
+int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]);
+int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms);
+
 /* ---- allocation-free real-space sums ----
    No counterpart in the reference: an extra entry point for callers that cannot
    call cudaMalloc where they need an energy (a host whose own pool holds the

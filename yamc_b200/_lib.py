@@ -88,6 +88,16 @@ SIGNATURES = {
     "yamc_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_phase_cycles": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
+    "yamc_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(YamcSystem), ctypes.POINTER(YamcParams),
+                                         ctypes.c_int32, _PPP]),
+    "yamc_batch_destroy": (ctypes.c_int, [_VP]),
+    "yamc_batch_replica": (ctypes.c_int, [_VP, ctypes.c_int32, _PPP]),
+    "yamc_batch_run_device": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP, _VP]),
+    "yamc_batch_run": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP, _VP]),
+    "yamc_batch_tune": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int64, _dp]),  # pointer arrays as void*
+    "yamc_batch_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
+    "yamc_batch_get_launch": (ctypes.c_int, [_VP, _ip]),
+    "yamc_batch_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +
                                    [ctypes.c_int32] + [_VP] * 8),
     "yamc_error_string": (ctypes.c_char_p, [ctypes.c_int]),

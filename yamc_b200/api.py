@@ -218,3 +218,122 @@ class Engine:
         v = ctypes.c_double(0)
         check(self.lib.yamc_last_kernel_ms(self.h, ctypes.byref(v)), "yamc_last_kernel_ms")
         return v.value
+
+
+class Batch:
+    """Independent replicas advanced together (yamc_batch_*): one persistent cluster launch per
+    kernel variant, the step replayed as a CUDA graph.  Each replica is its own system with its
+    own random stream; ``replica(i)`` gives it as an Engine-like view."""
+
+    def __init__(self, inputs: list, device: int = 0, precision: int = _lib.YAMC_FP64):
+        self.lib = _lib.load()
+        self.inputs = list(inputs)
+        n = len(self.inputs)
+        self._systems = (YamcSystem * n)()
+        self._params = (YamcParams * n)()
+        for i, inp in enumerate(self.inputs):
+            self._systems[i] = inp.as_struct()
+            ctypes.memmove(ctypes.byref(self._params[i]), ctypes.byref(inp.params), ctypes.sizeof(YamcParams))
+            self._params[i].precision = precision
+        h = ctypes.c_void_p()
+        check(self.lib.yamc_batch_create(n, self._systems, self._params, int(device), ctypes.byref(h)), "yamc_batch_create")
+        self.h = h
+        self.n = n
+        self._views = {}
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self._views.clear()
+            self.lib.yamc_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def replica(self, i: int) -> "_ReplicaView":
+        if i not in self._views:
+            c = ctypes.c_void_p()
+            check(self.lib.yamc_batch_replica(self.h, int(i), ctypes.byref(c)), "yamc_batch_replica")
+            self._views[i] = _ReplicaView(self, c, self.inputs[i])
+        return self._views[i]
+
+    @staticmethod
+    def _ptrs(addrs, sizes):
+        p = (ctypes.c_void_p * len(addrs))(*[int(a) for a in addrs])
+        n = np.ascontiguousarray(sizes, dtype=np.int64)
+        return p, n
+
+    def run(self, streams, n_moves: int, cursors=None, log: bool = False, limits=None):
+        """n_moves moves of every replica, replica i reading host stream streams[i] (float32)
+        from cursors[i] up to limits[i] (default: its end).  Returns (log[n, n_moves] or None,
+        cursors, moves_done, status per replica, overall status)."""
+        streams = [np.ascontiguousarray(s, dtype=np.float32) for s in streams]
+        sizes = [s.size for s in streams] if limits is None else [min(int(l), s.size) for l, s in zip(limits, streams)]
+        ptrs, n = self._ptrs([s.ctypes.data for s in streams], sizes)
+        cur = np.zeros(self.n, dtype=np.int64) if cursors is None else np.array(cursors, dtype=np.int64)
+        done = np.zeros(self.n, dtype=np.int64)
+        st = np.zeros(self.n, dtype=np.int32)
+        rec = np.zeros(self.n * n_moves if log else 0, dtype=MOVE_RECORD_DTYPE)
+        s = self.lib.yamc_batch_run(self.h, ptrs, n.ctypes.data, cur.ctypes.data, int(n_moves),
+                                    done.ctypes.data, st.ctypes.data, rec.ctypes.data if log else None)
+        if s not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+            check(s, "yamc_batch_run")
+        return (rec.reshape(self.n, n_moves) if log else None), cur, done, st, s
+
+    def run_device(self, d_ptrs, n_rng, cursors: np.ndarray, n_moves: int, d_log_ptr: int = 0):
+        """n_moves moves of every replica from device streams d_ptrs[i] of n_rng[i] floats;
+        cursors (int64 array) updated in place.  Returns (moves_done, status, overall)."""
+        ptrs, n = self._ptrs(d_ptrs, n_rng)
+        done = np.zeros(self.n, dtype=np.int64)
+        st = np.zeros(self.n, dtype=np.int32)
+        s = self.lib.yamc_batch_run_device(self.h, ptrs, n.ctypes.data, cursors.ctypes.data, int(n_moves),
+                                           done.ctypes.data, st.ctypes.data,
+                                           ctypes.c_void_p(d_log_ptr) if d_log_ptr else None)
+        if s not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+            check(s, "yamc_batch_run_device")
+        return done, st, s
+
+    def tune(self, d_ptrs, n_rng, cursors, n_moves: int) -> float:
+        """Autotune the launch shape on n_moves moves per replica (state restored)."""
+        ptrs, n = self._ptrs(d_ptrs, n_rng)
+        best = ctypes.c_double(0)
+        cur = np.ascontiguousarray(cursors, dtype=np.int64)
+        check(self.lib.yamc_batch_tune(self.h, ptrs, n.ctypes.data, cur.ctypes.data, int(n_moves),
+                                       ctypes.byref(best)), "yamc_batch_tune")
+        return best.value
+
+    def set_launch(self, cluster_blocks: int = 0, threads: int = 0) -> None:
+        check(self.lib.yamc_batch_set_launch(self.h, int(cluster_blocks), int(threads)), "yamc_batch_set_launch")
+
+    @property
+    def launch(self):
+        out = np.zeros(5, dtype=np.int32)
+        check(self.lib.yamc_batch_get_launch(self.h, _iptr(out)), "yamc_batch_get_launch")
+        return {"cluster_blocks": int(out[0]), "threads": int(out[1]), "entries_per_thread": int(out[2]),
+                "smem_bytes": int(out[3]), "resident_clusters": int(out[4])}
+
+    @property
+    def last_kernel_ms(self) -> float:
+        v = ctypes.c_double(0)
+        check(self.lib.yamc_batch_last_kernel_ms(self.h, ctypes.byref(v)), "yamc_batch_last_kernel_ms")
+        return v.value
+
+
+class _ReplicaView(Engine):
+    """A replica of a Batch seen through the per-context calls; the batch owns it."""
+
+    def __init__(self, batch: Batch, handle: ctypes.c_void_p, inputs: Inputs):
+        self.lib = batch.lib
+        self.inputs = inputs
+        self.params = inputs.params
+        self._batch = batch
+        self.h = handle
+        sz = np.zeros(5, dtype=np.int32)
+        check(self.lib.yamc_sizes(self.h, _iptr(sz)), "yamc_sizes")
+        self.natom, self.nmol, self.nk, self.nsigned, self.ntype = (int(v) for v in sz)
+
+    def close(self) -> None:  # owned by the batch
+        self.h = None

@@ -1247,26 +1247,33 @@ struct yamc_ctx {
 
 namespace {
 
-int pick_launch(yamc_ctx *c, LaunchCfg *out) {
-    const HostSystem &H = c->H;
+// The first (G, B) that fits every system of hosts: each worker thread holds at most 2 signed
+// entries, the CTA's atoms and the pair queue fit in shared memory.  G from small to large,
+// B from 256 to 128 threads; force_G / force_B pin either (0 = free).
+int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, int force_G, int force_B, LaunchCfg *out) {
     cudaDeviceProp prop;
-    CUDA_TRY(cudaGetDeviceProperties(&prop, c->device));
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
+    int Smax = 0, Nmax = 0, kmax = 0, nt = 0;
+    for (const HostSystem *h : hosts) {
+        Smax = std::max(Smax, h->S); Nmax = std::max(Nmax, h->N);
+        kmax = std::max(kmax, h->kmax); nt = std::max(nt, h->nt);
+    }
     const int Bs[] = {kChainMaxThreads, 128};
     const int Gs[] = {1, 2, 4, 8, 16};
     for (int gi = 0; gi < 5; ++gi) {
         const int G = Gs[gi];
-        if (c->force_G && G != c->force_G) continue;
+        if (force_G && G != force_G) continue;
         for (int bi = 0; bi < 2; ++bi) {
             const int B = Bs[bi];
-            if (c->force_B && B != c->force_B) continue;
-            if (!c->force_B && B != kChainMaxThreads && G * (kChainMaxThreads - kCtl) < H.S) continue;
+            if (force_B && B != force_B) continue;
+            if (!force_B && B != kChainMaxThreads && G * (kChainMaxThreads - kCtl) < Smax) continue;
             const int nwork = B - kCtl;  // warp 0 is the control warp
-            const int EPT = (H.S + G * nwork - 1) / (G * nwork);
+            const int EPT = (Smax + G * nwork - 1) / (G * nwork);
             if (EPT > 2) continue;
-            const int nown_max = (H.N + G - 1) / G;
+            const int nown_max = (Nmax + G - 1) / G;
             const int qcap = std::min(nown_max, nwork * kCPT) * 2 * kMaxA;  // one filter round of pairs
-            const size_t sm = chain_smem_bytes(G, B, H.kmax, H.nt, nown_max, qcap);
+            const size_t sm = chain_smem_bytes(G, B, kmax, nt, nown_max, qcap);
             if (sm > smem_max) continue;
             out->G = G; out->B = B; out->EPT = EPT; out->nown_max = nown_max; out->qcap = qcap; out->smem = sm;
             return YAMC_OK;
@@ -1276,17 +1283,21 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
     return YAMC_ELIMITS;
 }
 
+int pick_launch(yamc_ctx *c, LaunchCfg *out) {
+    return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, out);
+}
+
+// nrep chains of one launch shape: nrep clusters of L.G CTAs, chain r on cluster r
 template <int NT, int EPT, bool SPLIT>
-int launch_chain_t(yamc_ctx *c, const ChainArgs &args) {
-    const LaunchCfg &L = c->cfg;
+int launch_chain_t(const LaunchCfg &L, cudaStream_t stream, int nrep, const ChainArgs &args) {
     auto kfn = k_chain<NT, EPT, SPLIT>;
     CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
     if (L.G > 8) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
     cudaLaunchConfig_t cfg = {};
-    cfg.gridDim = dim3(L.G, 1, 1);
+    cfg.gridDim = dim3(L.G * nrep, 1, 1);
     cfg.blockDim = dim3(L.B, 1, 1);
     cfg.dynamicSmemBytes = L.smem;
-    cfg.stream = c->stream;
+    cfg.stream = stream;
     cudaLaunchAttribute attr[1];
     attr[0].id = cudaLaunchAttributeClusterDimension;
     attr[0].val.clusterDim.x = L.G;
@@ -1298,20 +1309,61 @@ int launch_chain_t(yamc_ctx *c, const ChainArgs &args) {
     return YAMC_OK;
 }
 
-int launch_chain(yamc_ctx *c, const ChainArgs &args) {
-    const int nt = c->H.nt, ept = c->cfg.EPT;
-    const bool split = args.mode != MODE_RUN || c->H.p.xlambda_f > 0.0 || c->H.p.xlambda_c > 0.0;
-#define YAMC_CASE(NT_, EPT_)                                                                                      \
-    if (nt == NT_ && ept == EPT_) return split ? launch_chain_t<NT_, EPT_, true>(c, args) : launch_chain_t<NT_, EPT_, false>(c, args);
+// clusters of shape L that can be resident at once (0 if the shape does not launch)
+template <int NT, int EPT, bool SPLIT>
+int max_clusters_t(const LaunchCfg &L, int *out) {
+    auto kfn = k_chain<NT, EPT, SPLIT>;
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    if (L.G > 8) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.G, 1, 1);
+    cfg.blockDim = dim3(L.B, 1, 1);
+    cfg.dynamicSmemBytes = L.smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = L.G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaOccupancyMaxActiveClusters(out, kfn, &cfg));
+    return YAMC_OK;
+}
+
+// kernel instance for (LJ types, entries per thread, split old pass); WHAT(NT, EPT, SPLIT) is
+// a call of a template above
 #ifdef YAMC_ONE_VARIANT  // development builds: a single instantiation compiles in seconds
-    YAMC_CASE(3, 1)
+#define YAMC_CHAIN_VARIANTS(X) X(3, 1)
 #else
-    YAMC_CASE(1, 1) YAMC_CASE(1, 2) YAMC_CASE(2, 1) YAMC_CASE(2, 2)
-    YAMC_CASE(3, 1) YAMC_CASE(3, 2) YAMC_CASE(4, 1) YAMC_CASE(4, 2)
+#define YAMC_CHAIN_VARIANTS(X) X(1, 1) X(1, 2) X(2, 1) X(2, 2) X(3, 1) X(3, 2) X(4, 1) X(4, 2)
 #endif
+
+int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, cudaStream_t stream, int nrep, const ChainArgs &args) {
+#define YAMC_CASE(NT_, EPT_)                                                                                  \
+    if (nt == NT_ && L.EPT == EPT_)                                                                            \
+        return split ? launch_chain_t<NT_, EPT_, true>(L, stream, nrep, args)                                  \
+                     : launch_chain_t<NT_, EPT_, false>(L, stream, nrep, args);
+    YAMC_CHAIN_VARIANTS(YAMC_CASE)
 #undef YAMC_CASE
     set_error("LJ type count outside 1..4 or k-set too large for the chain kernel");
     return YAMC_ELIMITS;
+}
+
+int max_clusters_cfg(const LaunchCfg &L, int nt, bool split, int *out) {
+#define YAMC_CASE(NT_, EPT_)                                                                                  \
+    if (nt == NT_ && L.EPT == EPT_) return split ? max_clusters_t<NT_, EPT_, true>(L, out) : max_clusters_t<NT_, EPT_, false>(L, out);
+    YAMC_CHAIN_VARIANTS(YAMC_CASE)
+#undef YAMC_CASE
+    set_error("LJ type count outside 1..4 or k-set too large for the chain kernel");
+    return YAMC_ELIMITS;
+}
+
+bool split_variant(const HostSystem &H, int mode) {
+    return mode != MODE_RUN || H.p.xlambda_f > 0.0 || H.p.xlambda_c > 0.0;
+}
+
+int launch_chain(yamc_ctx *c, const ChainArgs &args) {
+    return launch_chain_cfg(c->cfg, c->H.nt, split_variant(c->H, args.mode), c->stream, 1, args);
 }
 
 template <int NT>
@@ -1422,6 +1474,175 @@ ChainArgs base_args(yamc_ctx *c, int mode) {
     a.api_in = c->api_in; a.api_out = c->api_out; a.scratch = c->scratch;
     a.prof = c->prof_on ? c->d_prof : nullptr;
     return a;
+}
+
+}  // namespace
+
+// A batch: independent replicas (each a yamc_ctx with its own system and device state),
+// grouped by kernel variant (LJ type count, split old pass); each group is one cluster launch,
+// the groups run concurrently on their own streams, and the whole step is one CUDA graph.
+namespace {
+struct BatchGroup {
+    std::vector<int> idx;       // replicas of the group
+    int nt = 0;
+    bool split = false;
+    LaunchCfg cfg;
+    int max_clusters = 0;       // resident at once for cfg
+    DevSys *d_sys = nullptr;    // [n]
+    RunSlot *d_run = nullptr;   // [n]
+    RunSlot *h_run = nullptr;   // [n], pinned
+    cudaStream_t stream = nullptr;
+    cudaEvent_t done = nullptr;
+};
+}  // namespace
+
+struct yamc_batch {
+    int device = 0;
+    std::vector<yamc_ctx *> reps;
+    std::vector<BatchGroup> groups;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    float last_ms = 0.f;
+    int force_G = 0, force_B = 0;
+    float *d_rng = nullptr;
+    size_t rng_cap = 0;
+    yamc_move_record *d_log = nullptr;
+    size_t log_cap = 0;
+};
+
+namespace {
+
+void batch_drop_graph(yamc_batch *b) {
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+}
+
+// launch shape of every group for the current force_G / force_B
+int batch_configure(yamc_batch *b) {
+    batch_drop_graph(b);
+    for (BatchGroup &g : b->groups) {
+        std::vector<const HostSystem *> hs;
+        for (int i : g.idx) hs.push_back(&b->reps[i]->H);
+        int r = pick_launch_for(hs, b->device, b->force_G, b->force_B, &g.cfg);
+        if (r) return r;
+        if ((r = max_clusters_cfg(g.cfg, g.nt, g.split, &g.max_clusters))) return r;
+    }
+    return YAMC_OK;
+}
+
+// one batch step as a graph: run slots up, every group's launch (concurrently), run slots down
+int batch_build_graph(yamc_batch *b) {
+    if (b->graph) return YAMC_OK;
+    cudaGraph_t graph = nullptr;
+    CUDA_TRY(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeRelaxed));
+    int r = YAMC_OK;
+    for (BatchGroup &g : b->groups) {
+        if (cudaMemcpyAsync(g.d_run, g.h_run, sizeof(RunSlot) * g.idx.size(), cudaMemcpyHostToDevice, b->stream) != cudaSuccess) {
+            r = YAMC_ECUDA; break;
+        }
+    }
+    if (!r && cudaEventRecord(b->fork, b->stream) != cudaSuccess) r = YAMC_ECUDA;
+    for (size_t k = 0; !r && k < b->groups.size(); ++k) {
+        BatchGroup &g = b->groups[k];
+        if (cudaStreamWaitEvent(g.stream, b->fork, 0) != cudaSuccess) { r = YAMC_ECUDA; break; }
+        ChainArgs a{};
+        a.sys = g.d_sys; a.run = g.d_run; a.G = g.cfg.G; a.mode = MODE_RUN;
+        a.nown_max = g.cfg.nown_max; a.qcap = g.cfg.qcap;
+        if ((r = launch_chain_cfg(g.cfg, g.nt, g.split, g.stream, (int)g.idx.size(), a))) break;
+        if (cudaEventRecord(g.done, g.stream) != cudaSuccess || cudaStreamWaitEvent(b->stream, g.done, 0) != cudaSuccess)
+            r = YAMC_ECUDA;
+    }
+    for (size_t k = 0; !r && k < b->groups.size(); ++k) {
+        BatchGroup &g = b->groups[k];
+        if (cudaMemcpyAsync(g.h_run, g.d_run, sizeof(RunSlot) * g.idx.size(), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess)
+            r = YAMC_ECUDA;
+    }
+    const cudaError_t ee = cudaStreamEndCapture(b->stream, &graph);
+    if (r) {
+        if (graph) cudaGraphDestroy(graph);
+        if (r == YAMC_ECUDA) set_error("capturing the batch step failed");
+        return r;
+    }
+    CUDA_TRY(ee);
+    const cudaError_t ei = cudaGraphInstantiate(&b->graph, graph, 0);
+    cudaGraphDestroy(graph);
+    CUDA_TRY(ei);
+    return YAMC_OK;
+}
+
+// one step of every replica: replica i's stream holds positions [rng_off[i], n_rng[i]) at rng[i]
+int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, const int64_t *n_rng,
+               int64_t *cursors, int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log) {
+    int r = batch_build_graph(b);
+    if (r) return r;
+    for (BatchGroup &g : b->groups)
+        for (size_t k = 0; k < g.idx.size(); ++k) {
+            const int i = g.idx[k];
+            RunSlot &rs = g.h_run[k];
+            rs = RunSlot{};
+            rs.rng = rng[i]; rs.rng_off = rng_off[i]; rs.n_rng = n_rng[i];
+            rs.cursor = cursors[i]; rs.n_moves = n_moves;
+            rs.log = d_log ? d_log + (size_t)i * n_moves : nullptr;
+        }
+    CUDA_TRY(cudaEventRecord(b->ev0, b->stream));
+    CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
+    CUDA_TRY(cudaEventRecord(b->ev1, b->stream));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+    int worst = YAMC_OK;
+    for (BatchGroup &g : b->groups)
+        for (size_t k = 0; k < g.idx.size(); ++k) {
+            const int i = g.idx[k];
+            const RunSlot &rs = g.h_run[k];
+            cursors[i] = rs.cursor;
+            if (moves_done) moves_done[i] = rs.moves_done;
+            if (status) status[i] = rs.status;
+            b->reps[i]->pos_valid = false;
+            if (rs.status != YAMC_OK && (worst == YAMC_OK || worst == YAMC_ERNG_EXHAUSTED)) worst = rs.status;
+        }
+    return worst;
+}
+
+// device copies of the chain state of every replica (positions, rho, scalars, counters)
+struct BatchBackup {
+    std::vector<double4 *> atom;
+    std::vector<double2 *> rho;
+    std::vector<double *> scal;
+    std::vector<long long *> cnt;
+    ~BatchBackup() {
+        for (auto p : atom) if (p) cudaFree(p);
+        for (auto p : rho) if (p) cudaFree(p);
+        for (auto p : scal) if (p) cudaFree(p);
+        for (auto p : cnt) if (p) cudaFree(p);
+    }
+};
+
+int batch_copy_state(yamc_batch *b, BatchBackup &k, bool save) {
+    const size_t R = b->reps.size();
+    if (save) { k.atom.assign(R, nullptr); k.rho.assign(R, nullptr); k.scal.assign(R, nullptr); k.cnt.assign(R, nullptr); }
+    for (size_t i = 0; i < R; ++i) {
+        yamc_ctx *c = b->reps[i];
+        const size_t nr = (size_t)(1 + c->H.nt) * c->H.S;
+        int r;
+        if (save && ((r = dalloc(&k.atom[i], c->H.N)) || (r = dalloc(&k.rho[i], nr)) || (r = dalloc(&k.scal[i], SC_COUNT)) ||
+                     (r = dalloc(&k.cnt[i], CN_COUNT))))
+            return r;
+        const cudaMemcpyKind kd = cudaMemcpyDeviceToDevice;
+        if (save) {
+            CUDA_TRY(cudaMemcpyAsync(k.atom[i], c->atom, sizeof(double4) * c->H.N, kd, b->stream));
+            CUDA_TRY(cudaMemcpyAsync(k.rho[i], c->rho, sizeof(double2) * nr, kd, b->stream));
+            CUDA_TRY(cudaMemcpyAsync(k.scal[i], c->scal, sizeof(double) * SC_COUNT, kd, b->stream));
+            CUDA_TRY(cudaMemcpyAsync(k.cnt[i], c->cnt, sizeof(long long) * CN_COUNT, kd, b->stream));
+        } else {
+            CUDA_TRY(cudaMemcpyAsync(c->atom, k.atom[i], sizeof(double4) * c->H.N, kd, b->stream));
+            CUDA_TRY(cudaMemcpyAsync(c->rho, k.rho[i], sizeof(double2) * nr, kd, b->stream));
+            CUDA_TRY(cudaMemcpyAsync(c->scal, k.scal[i], sizeof(double) * SC_COUNT, kd, b->stream));
+            CUDA_TRY(cudaMemcpyAsync(c->cnt, k.cnt[i], sizeof(long long) * CN_COUNT, kd, b->stream));
+        }
+    }
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return YAMC_OK;
 }
 
 }  // namespace
@@ -1777,6 +1998,222 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->api_stage = 0;
     return YAMC_OK;
+}
+
+// ---------------------------------------------------------------- batched replicas
+
+int yamc_batch_destroy(yamc_batch *b) {
+    if (!b) return YAMC_OK;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    for (BatchGroup &g : b->groups) {
+        if (g.stream) cudaStreamSynchronize(g.stream);
+        if (g.d_sys) cudaFree(g.d_sys);
+        if (g.d_run) cudaFree(g.d_run);
+        if (g.h_run) cudaFreeHost(g.h_run);
+        if (g.done) cudaEventDestroy(g.done);
+        if (g.stream) cudaStreamDestroy(g.stream);
+    }
+    for (yamc_ctx *c : b->reps) yamc_destroy(c);
+    if (b->d_rng) cudaFree(b->d_rng);
+    if (b->d_log) cudaFree(b->d_log);
+    if (b->ev0) cudaEventDestroy(b->ev0);
+    if (b->ev1) cudaEventDestroy(b->ev1);
+    if (b->fork) cudaEventDestroy(b->fork);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return YAMC_OK;
+}
+
+static int batch_create_impl(yamc_batch *b, int32_t n, const yamc_system *systems, const yamc_params *params) {
+    CUDA_TRY(cudaSetDevice(b->device));
+    CUDA_TRY(cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking));
+    CUDA_TRY(cudaEventCreate(&b->ev0));
+    CUDA_TRY(cudaEventCreate(&b->ev1));
+    CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
+    for (int i = 0; i < n; ++i) {
+        yamc_ctx *c = nullptr;
+        const int r = yamc_create(&systems[i], &params[i], b->device, &c);
+        if (r) {
+            set_error("replica " + std::to_string(i) + ": " + last_error());
+            return r;
+        }
+        b->reps.push_back(c);
+    }
+    for (int i = 0; i < n; ++i) {
+        const HostSystem &H = b->reps[i]->H;
+        const bool split = split_variant(H, MODE_RUN);
+        size_t k = 0;
+        while (k < b->groups.size() && !(b->groups[k].nt == H.nt && b->groups[k].split == split)) ++k;
+        if (k == b->groups.size()) {
+            b->groups.emplace_back();
+            b->groups.back().nt = H.nt;
+            b->groups.back().split = split;
+        }
+        b->groups[k].idx.push_back(i);
+    }
+    for (BatchGroup &g : b->groups) {
+        const size_t m = g.idx.size();
+        int r;
+        if ((r = dalloc(&g.d_sys, m)) || (r = dalloc(&g.d_run, m))) return r;
+        CUDA_TRY(cudaMallocHost((void **)&g.h_run, sizeof(RunSlot) * m));
+        CUDA_TRY(cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking));
+        CUDA_TRY(cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming));
+        std::vector<DevSys> hs(m);
+        for (size_t k = 0; k < m; ++k) hs[k] = b->reps[g.idx[k]]->hsys;
+        if ((r = upload(g.d_sys, hs.data(), m, b->stream))) return r;
+    }
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
+    return batch_configure(b);
+}
+
+int yamc_batch_create(int32_t n, const yamc_system *systems, const yamc_params *params, int32_t device, yamc_batch **out) {
+    if (!out || n < 1 || !systems || !params) return YAMC_EPARAMETER;
+    *out = nullptr;
+    yamc_batch *b = new yamc_batch();
+    b->device = device;
+    const int r = batch_create_impl(b, n, systems, params);
+    if (r) { yamc_batch_destroy(b); return r; }
+    *out = b;
+    return YAMC_OK;
+}
+
+int yamc_batch_replica(yamc_batch *b, int32_t i, yamc_ctx **ctx) {
+    if (!b || !ctx || i < 0 || i >= (int)b->reps.size()) return YAMC_EPARAMETER;
+    *ctx = b->reps[i];
+    return YAMC_OK;
+}
+
+int yamc_batch_run_device(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng, int64_t *cursors,
+                          int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log) {
+    if (!b || !d_rng || !n_rng || !cursors || n_moves < 0) return YAMC_EPARAMETER;
+    const size_t R = b->reps.size();
+    std::vector<int64_t> off(R, 0);
+    for (size_t i = 0; i < R; ++i)
+        if (!d_rng[i] || n_rng[i] < 0 || cursors[i] < 0 || cursors[i] > n_rng[i]) {
+            set_error("replica " + std::to_string(i) + ": bad random stream or cursor");
+            return YAMC_EPARAMETER;
+        }
+    CUDA_TRY(cudaSetDevice(b->device));
+    return batch_step(b, d_rng, off.data(), n_rng, cursors, n_moves, moves_done, status, d_log);
+}
+
+int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng, int64_t *cursors, int64_t n_moves,
+                   int64_t *moves_done, int32_t *status, yamc_move_record *log) {
+    if (!b || !rng || !n_rng || !cursors || n_moves < 0) return YAMC_EPARAMETER;
+    const size_t R = b->reps.size();
+    std::vector<size_t> base(R);
+    size_t total = 0;
+    for (size_t i = 0; i < R; ++i) {
+        if (!rng[i] || n_rng[i] < 0 || cursors[i] < 0 || cursors[i] > n_rng[i]) {
+            set_error("replica " + std::to_string(i) + ": bad random stream or cursor");
+            return YAMC_EPARAMETER;
+        }
+        base[i] = total;  // the unread window [cursor, n_rng) of replica i, packed
+        total += (size_t)(n_rng[i] - cursors[i]);
+    }
+    CUDA_TRY(cudaSetDevice(b->device));
+    if (total > b->rng_cap || !b->d_rng) {
+        if (b->d_rng) cudaFree(b->d_rng);
+        b->d_rng = nullptr;
+        b->rng_cap = 0;
+        int r = dalloc(&b->d_rng, std::max<size_t>(total, 1));
+        if (r) return r;
+        b->rng_cap = std::max<size_t>(total, 1);
+    }
+    std::vector<const float *> dptr(R);
+    for (size_t i = 0; i < R; ++i) {
+        dptr[i] = b->d_rng + base[i];
+        if (n_rng[i] > cursors[i])
+            CUDA_TRY(cudaMemcpyAsync(b->d_rng + base[i], rng[i] + cursors[i], sizeof(float) * (n_rng[i] - cursors[i]),
+                                     cudaMemcpyHostToDevice, b->stream));
+    }
+    const size_t nlog = log ? R * (size_t)n_moves : 0;
+    if (nlog > b->log_cap) {
+        if (b->d_log) cudaFree(b->d_log);
+        b->d_log = nullptr;
+        b->log_cap = 0;
+        int r = dalloc(&b->d_log, nlog);
+        if (r) return r;
+        b->log_cap = nlog;
+    }
+    std::vector<int64_t> done(R, 0), off(cursors, cursors + R);
+    const int st = batch_step(b, dptr.data(), off.data(), n_rng, cursors, n_moves, done.data(), status,
+                              log ? b->d_log : nullptr);
+    if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
+    if (log) CUDA_TRY(cudaMemcpy(log, b->d_log, sizeof(yamc_move_record) * nlog, cudaMemcpyDeviceToHost));
+    if (moves_done) for (size_t i = 0; i < R; ++i) moves_done[i] = done[i];
+    return st;
+}
+
+int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads) {
+    if (!b) return YAMC_EPARAMETER;
+    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > kChainMaxThreads || (threads % 32) ||
+        (threads > 0 && threads < 64))
+        return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(b->device));
+    b->force_G = cluster_blocks;
+    b->force_B = threads;
+    return batch_configure(b);
+}
+
+int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]) {
+    if (!b || !out || b->groups.empty()) return YAMC_EPARAMETER;
+    const BatchGroup &g = b->groups[0];
+    out[0] = g.cfg.G; out[1] = g.cfg.B; out[2] = g.cfg.EPT; out[3] = (int32_t)g.cfg.smem; out[4] = g.max_clusters;
+    return YAMC_OK;
+}
+
+int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms) {
+    if (!b || !ms) return YAMC_EPARAMETER;
+    *ms = b->last_ms;
+    return YAMC_OK;
+}
+
+int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng, const int64_t *cursors,
+                    int64_t n_moves, double *best_moves_per_s) {
+    if (!b || !d_rng || !n_rng || !cursors || n_moves < 1) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(b->device));
+    const size_t R = b->reps.size();
+    BatchBackup keep;
+    int r = batch_copy_state(b, keep, true);
+    if (r) return r;
+    const int fG = b->force_G, fB = b->force_B;
+    const int Gs[] = {1, 2, 4, 8, 16};
+    const int Bs[] = {kChainMaxThreads, 128};
+    double best = -1.0;
+    int bestG = 0, bestB = 0;
+    std::vector<int64_t> cur(R), done(R);
+    for (int G : Gs) {
+        for (int B : Bs) {
+            b->force_G = G; b->force_B = B;
+            if (batch_configure(b) != YAMC_OK) continue;  // shape does not fit
+            bool ok = true;
+            for (const BatchGroup &g : b->groups) ok = ok && g.cfg.G == G && g.cfg.B == B && g.max_clusters > 0;
+            if (!ok) continue;
+            for (size_t i = 0; i < R; ++i) cur[i] = cursors[i];
+            r = yamc_batch_run_device(b, d_rng, n_rng, cur.data(), n_moves, done.data(), nullptr, nullptr);
+            const int rr = batch_copy_state(b, keep, false);
+            if (rr) return rr;
+            if (r != YAMC_OK && r != YAMC_ERNG_EXHAUSTED) return r;
+            double moves = 0;
+            for (size_t i = 0; i < R; ++i) moves += (double)done[i];
+            const double rate = b->last_ms > 0 ? moves / (1e-3 * b->last_ms) : 0.0;
+            if (rate > best) { best = rate; bestG = G; bestB = B; }
+        }
+    }
+    if (best < 0) {
+        b->force_G = fG; b->force_B = fB;
+        batch_configure(b);
+        set_error("no launch shape fits every replica of the batch");
+        return YAMC_ELIMITS;
+    }
+    b->force_G = bestG; b->force_B = bestB;
+    r = batch_configure(b);
+    for (yamc_ctx *c : b->reps) c->pos_valid = false;
+    if (best_moves_per_s) *best_moves_per_s = best;
+    return r;
 }
 
 int yamc_phase_cycles(yamc_ctx *c, int32_t mode, int64_t *out, int32_t n) {
