@@ -242,9 +242,20 @@ def main():
     eng.close()
 
     # ---------------- the batch: R independent chains of the workload, one graph launch per step
+    # R = the most chains any launch shape keeps resident at once (the tuner then picks the shape)
     probe = api.Batch([api.load_inputs(files["parameters"], files["composition"], files["moltab"])], device=local)
-    R = args.replicas or max(1, probe.launch["resident_clusters"])
+    R = args.replicas
+    resident = {}
+    for G in range(1, 17):
+        try:
+            probe.set_launch(G, 0)
+        except Exception:
+            continue
+        resident[G] = probe.launch["resident_clusters"]
+    if not R:
+        R = max(resident.values(), default=1)
     probe.close()
+    R = max(R, 1)
     rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=3 + 101 * rank + r,
                                                 rng_seed=12345 + 1000 * rank + r) for r in range(1, R)]
     b = api.Batch([api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files], device=local)
@@ -337,7 +348,7 @@ def main():
                    "moves_per_step_per_chain": args.moves, "chains_per_gpu": R,
                    "parallelism": "independent replicas (one cluster per chain)",
                    "launch": launch, "l2": "256 MB write between steps", "accept_fraction": p_acc,
-                   "single_chain": single},
+                   "single_chain": single, "resident_clusters_by_cluster_size": resident},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": TRAFFIC_PER_MOVE * moves_launch, "peak_source": which,
                      "algorithmic_bytes_per_move": bpm},

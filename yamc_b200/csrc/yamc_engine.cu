@@ -1248,22 +1248,24 @@ struct yamc_ctx {
 namespace {
 
 // The first (G, B) that fits every system of hosts: each worker thread holds at most 2 signed
-// entries, the CTA's atoms and the pair queue fit in shared memory.  G from small to large,
-// B from 256 to 128 threads; force_G / force_B pin either (0 = free).
-int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, int force_G, int force_B, LaunchCfg *out) {
+// entries, the CTA's atoms and the pair queue fit in shared memory.  G (1..16 CTAs per cluster)
+// from large to small when large_first (the shortest move for a lone chain), else from small to
+// large; B from 256 to 128 threads; force_G / force_B pin either (0 = free).
+int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, int force_G, int force_B, LaunchCfg *out,
+                    bool large_first = true) {
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
-    int Smax = 0, Nmax = 0, kmax = 0, nt = 0;
+    int Smax = 0, Nmax = 0, Nmin = 1 << 30, kmax = 0, nt = 0;
     for (const HostSystem *h : hosts) {
-        Smax = std::max(Smax, h->S); Nmax = std::max(Nmax, h->N);
+        Smax = std::max(Smax, h->S); Nmax = std::max(Nmax, h->N); Nmin = std::min(Nmin, h->N);
         kmax = std::max(kmax, h->kmax); nt = std::max(nt, h->nt);
     }
     const int Bs[] = {kChainMaxThreads, 128};
-    const int Gs[] = {1, 2, 4, 8, 16};
-    for (int gi = 0; gi < 5; ++gi) {
-        const int G = Gs[gi];
+    for (int gi = 0; gi < 16; ++gi) {
+        const int G = large_first ? 16 - gi : 1 + gi;
         if (force_G && G != force_G) continue;
+        if (G > Nmin) continue;  // every CTA owns at least one atom
         for (int bi = 0; bi < 2; ++bi) {
             const int B = Bs[bi];
             if (force_B && B != force_B) continue;
@@ -2180,12 +2182,11 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     int r = batch_copy_state(b, keep, true);
     if (r) return r;
     const int fG = b->force_G, fB = b->force_B;
-    const int Gs[] = {1, 2, 4, 8, 16};
     const int Bs[] = {kChainMaxThreads, 128};
     double best = -1.0;
     int bestG = 0, bestB = 0;
     std::vector<int64_t> cur(R), done(R);
-    for (int G : Gs) {
+    for (int G = 1; G <= 16; ++G) {
         for (int B : Bs) {
             b->force_G = G; b->force_B = B;
             if (batch_configure(b) != YAMC_OK) continue;  // shape does not fit
