@@ -165,6 +165,15 @@ int yamc_run_chain_device(yamc_ctx *ctx, const float *d_rng, int64_t n_rng, int6
 /* Threads per block and blocks per cluster of the persistent chain kernel
    (0 = autotuned); takes effect on the next yamc_run_chain. */
 int yamc_set_launch(yamc_ctx *ctx, int32_t cluster_blocks, int32_t threads);
+/* Where the chain kernel keeps the signed k entries (k, beta, beta_LJ, rho(k)):
+   in registers, at most 2 per worker thread, for the whole launch; or streamed
+   from device memory (L2-resident) by every pass, any k-set size.  AUTO takes
+   registers when they fit. */
+#define YAMC_KSPACE_AUTO 0
+#define YAMC_KSPACE_REGISTERS 1
+#define YAMC_KSPACE_STREAMED 2
+int yamc_set_kspace_layout(yamc_ctx *ctx, int32_t layout);
+/* out: cluster blocks, threads, entries per thread (0 = streamed), shared memory bytes */
 int yamc_get_launch(yamc_ctx *ctx, int32_t out[4]);
 /* device time (ms) of the last run_chain kernel, measured with CUDA events on its stream */
 int yamc_last_kernel_ms(yamc_ctx *ctx, double *ms);
@@ -204,13 +213,14 @@ int yamc_batch_run_device(yamc_batch *b, const float *const *d_rng, const int64_
    [cursors[i], n_rng[i]) is copied to the device) and the log in host memory. */
 int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng, int64_t *cursors,
                    int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *log);
-/* Autotuner: times every launch shape (cluster size x threads per block) that fits
+/* Autotuner: times every launch shape (k-space layout x cluster size x threads per block) that fits
    all replicas on n_moves moves of each and keeps the one with the highest
    aggregate moves/s.  The replicas' state is put back after every trial, so the
    chains do not advance. */
 int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng,
                     const int64_t *cursors, int64_t n_moves, double *best_moves_per_s);
 int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads);
+int yamc_batch_set_kspace_layout(yamc_batch *b, int32_t layout);
 /* out: cluster blocks, threads, entries per thread, shared memory bytes, clusters
    resident at once (of the first group) */
 int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]);

@@ -41,3 +41,15 @@ def spce_files(tmp_path_factory):
 def nacl_files(tmp_path_factory):
     from yamc_b200 import systems
     return _write(systems.WORKLOADS["nacl1m"], tmp_path_factory, "nacl1m", seed=3)
+
+
+@pytest.fixture(scope="session")
+def nacl4k_files(tmp_path_factory):
+    from yamc_b200 import systems
+    return _write(systems.WORKLOADS["nacl4k"], tmp_path_factory, "nacl4k", seed=5)
+
+
+@pytest.fixture(scope="session")
+def nacl16k_files(tmp_path_factory):
+    from yamc_b200 import systems
+    return _write(systems.WORKLOADS["nacl16k"], tmp_path_factory, "nacl16k", seed=6)

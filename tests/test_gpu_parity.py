@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 import pyoracle
-from yamc_b200 import api, rng as grng
+from yamc_b200 import _lib, api, rng as grng
 
 pytestmark = pytest.mark.gpu
 
@@ -44,11 +44,16 @@ def test_initial_full_sums(which, request):
     assert (eng.nk, eng.ntype) == (o.nk, o.ntype)
 
 
-def _run_pair(files, n_moves, seed=12345, cluster=0, threads=0):
+LAYOUTS = {"registers": _lib.YAMC_KSPACE_REGISTERS, "streamed": _lib.YAMC_KSPACE_STREAMED}
+
+
+def _run_pair(files, n_moves, seed=12345, cluster=0, threads=0, layout=_lib.YAMC_KSPACE_AUTO):
     buf = grng.gfortran_stream(seed, 40 * n_moves + 10000)
     o = pyoracle.Oracle(files)
     olog, orows, ocur = o.run_mc(buf, n_moves)
     eng = api.Engine.from_files(files)
+    if layout:
+        eng.set_kspace_layout(layout)
     if cluster or threads:
         eng.set_launch(cluster, threads)
     glog, grows, gcur, done, st = eng.run_chain(buf, n_moves)
@@ -58,9 +63,11 @@ def _run_pair(files, n_moves, seed=12345, cluster=0, threads=0):
 
 
 
+@pytest.mark.parametrize("layout", ["registers", "streamed"])
 @pytest.mark.parametrize("cluster", [1, 2, 4])
-def test_chain_matches_oracle_tiny(tiny_files, cluster):
-    o, olog, ocur, eng, glog, gcur = _run_pair(tiny_files, 3000, cluster=cluster)
+def test_chain_matches_oracle_tiny(tiny_files, cluster, layout):
+    o, olog, ocur, eng, glog, gcur = _run_pair(tiny_files, 3000, cluster=cluster, layout=LAYOUTS[layout])
+    assert eng.launch["entries_per_thread"] == (0 if layout == "streamed" else 1)
     compare_logs(glog, olog)
     assert gcur == ocur
     assert rel_close(eng.energies(), o.energies(), 1e-9)
@@ -75,23 +82,53 @@ def test_chain_matches_oracle_spce256_1e5(spce_files):
     assert rel_close(eng.full_sums(), o.full_sums(), 1e-9)
 
 
+def test_chain_streamed_spce256(spce_files):
+    """The k entries streamed from memory every pass instead of held in registers."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(spce_files, 20000, layout=_lib.YAMC_KSPACE_STREAMED)
+    compare_logs(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+    assert rel_close(eng.full_sums(), o.full_sums(), 1e-9)
+
+
 def test_chain_matches_oracle_nacl(nacl_files):
     o, olog, ocur, eng, glog, gcur = _run_pair(nacl_files, 6000)
     compare_logs(glog, olog)
     assert rel_close(eng.energies(), o.energies(), 1e-9)
 
 
-def test_chain_force_biased(tiny_biased_files):
-    """Force-biased proposals take the forces into the new positions, so ~1e-12 relative force
-    differences (summation order) move the two chains apart slowly (about 1e-10 after ~1500
-    moves of this dense 28-molecule box).  The decisions must stay identical; per-move dE meets
-    the 1e-10 bound over the first 500 moves and 1e-8 afterwards."""
-    o, olog, ocur, eng, glog, gcur = _run_pair(tiny_biased_files, 2000, seed=77)
+def compare_biased(glog, olog):
     assert np.array_equal(glog["imol"], olog["imol"]) and np.array_equal(glog["flags"], olog["flags"])
     assert np.array_equal(glog["cursor"], olog["cursor"])
     for k in DU:
         assert close_du(glog[k][:500], olog[k][:500]).all(), k
         assert close_du(glog[k], olog[k], 1e-8).all(), k
+
+
+@pytest.mark.parametrize("layout", ["registers", "streamed"])
+def test_chain_force_biased(tiny_biased_files, layout):
+    """Force-biased proposals take the forces into the new positions, so ~1e-12 relative force
+    differences (summation order) move the two chains apart slowly (about 1e-10 after ~1500
+    moves of this dense 28-molecule box).  The decisions must stay identical; per-move dE meets
+    the 1e-10 bound over the first 500 moves and 1e-8 afterwards."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(tiny_biased_files, 2000, seed=77, layout=LAYOUTS[layout])
+    compare_biased(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-8)
+
+
+def test_chain_nacl4k_force_biased(nacl4k_files):
+    """4096 SPC/E + 76 Na + 76 Cl (12,440 atoms, 7,427 signed k), force-biased moves with
+    lambda = 0.1: the k-set is too large for registers, so the entries are streamed."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(nacl4k_files, 1000, seed=41)
+    assert eng.launch["entries_per_thread"] == 0
+    compare_biased(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-8)
+
+
+def test_chain_nacl16k(nacl16k_files):
+    """16384 SPC/E + 300 Na + 300 Cl (49,752 atoms, 29,784 signed k), force-biased."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(nacl16k_files, 300, seed=43)
+    assert eng.launch["entries_per_thread"] == 0
+    compare_biased(glog, olog)
     assert rel_close(eng.energies(), o.energies(), 1e-8)
 
 
@@ -140,12 +177,14 @@ def test_chain_is_deterministic(spce_files):
     assert np.array_equal(a.energies(), b.energies())
 
 
+@pytest.mark.parametrize("layout", ["registers", "streamed"])
 @pytest.mark.parametrize("which", ["tiny_files", "tiny_biased_files"])
-def test_per_move_api_matches_oracle(which, request):
+def test_per_move_api_matches_oracle(which, layout, request):
     """movemc driven from the host through yamc_move_old / _eval / _commit."""
     files = request.getfixturevalue(which)
     o = pyoracle.Oracle(files)
     eng = api.Engine.from_files(files)
+    eng.set_kspace_layout(LAYOUTS[layout])
     rng = np.random.default_rng(3)
     f, l = o.mols()
     L = o.params.BoxLength

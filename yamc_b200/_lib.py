@@ -17,6 +17,9 @@ LIB_PATH = os.path.join(HERE, "libyamc_b200.so")
 YAMC_OK = 0
 YAMC_ELIMITS = -2
 YAMC_ERNG_EXHAUSTED = -12
+YAMC_KSPACE_AUTO = 0
+YAMC_KSPACE_REGISTERS = 1
+YAMC_KSPACE_STREAMED = 2
 YAMC_FP64 = 0
 YAMC_MIXED = 1
 
@@ -85,6 +88,7 @@ SIGNATURES = {
                                              ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_int32, _ip]),
     "yamc_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
+    "yamc_set_kspace_layout": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_phase_cycles": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
@@ -96,6 +100,7 @@ SIGNATURES = {
     "yamc_batch_run": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int64, _VP, _VP, _VP]),
     "yamc_batch_tune": (ctypes.c_int, [_VP, _VP, _VP, _VP, ctypes.c_int64, _dp]),  # pointer arrays as void*
     "yamc_batch_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
+    "yamc_batch_set_kspace_layout": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_batch_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_batch_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +

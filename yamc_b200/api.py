@@ -197,6 +197,10 @@ class Engine:
     def set_launch(self, cluster_blocks: int = 0, threads: int = 0) -> None:
         check(self.lib.yamc_set_launch(self.h, int(cluster_blocks), int(threads)), "yamc_set_launch")
 
+    def set_kspace_layout(self, layout: int) -> None:
+        """_lib.YAMC_KSPACE_AUTO / _REGISTERS / _STREAMED"""
+        check(self.lib.yamc_set_kspace_layout(self.h, int(layout)), "yamc_set_kspace_layout")
+
     @property
     def launch(self):
         out = np.zeros(4, dtype=np.int32)
@@ -307,6 +311,9 @@ class Batch:
 
     def set_launch(self, cluster_blocks: int = 0, threads: int = 0) -> None:
         check(self.lib.yamc_batch_set_launch(self.h, int(cluster_blocks), int(threads)), "yamc_batch_set_launch")
+
+    def set_kspace_layout(self, layout: int) -> None:
+        check(self.lib.yamc_batch_set_kspace_layout(self.h, int(layout)), "yamc_batch_set_kspace_layout")
 
     @property
     def launch(self):

@@ -27,6 +27,7 @@ struct DevSys {
     const int *pair_index; // nt*nt -> pair row
     const double *lj_sig6, *lj_feps;  // nt*nt tables (offset (t1-1)*nt + t2-1)
     double2 *rho;          // (1+nt) x S: Coulomb then one row per LJ type
+    double2 *scratch;      // 2 x (1+nt) x S: the moved molecule's old phase sums, then the rho deltas
     const double *freq_beg, *freq_end;
     double *scal;          // engine scalars, see Scal
     long long *cnt;        // run_mc counters, see Cnt

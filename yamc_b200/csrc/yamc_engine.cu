@@ -341,6 +341,12 @@ struct EntryRegs {
     double2 dl[EPT][1 + NT];
 };
 
+// EPT == 0: the streamed layout -- no entry lives in registers; each worker loops over its
+// entries and reads k, beta, beta_LJ and rho from memory (L2-resident) every pass.  The
+// register block of one (never touched) entry only keeps the code uniform.
+template <int NT, int EPT>
+using RegsOf = EntryRegs<NT, (EPT > 0 ? EPT : 1)>;
+
 // Phase tables of slots [s0, s1) of move m: T[slot][axis][k] = (cos, sin)(2 pi k u), by the workers
 __device__ __forceinline__ void build_tables(double2 *tab, const Cand &m, int s0, int s1, int KM, int wtid, int nwork) {
     const int n = (s1 - s0) * 3 * KM;
@@ -418,14 +424,57 @@ __device__ __forceinline__ void entry_forces(const Cand &m, int s0, int na, int 
     }
 }
 
+// One signed entry of a pass: the molecule's phase sums at the old positions (into mold) and/or
+// the new ones, the delta (into dl), dU_k Coulomb + LJ against rho, and the k-space forces.
+template <int NT, int KIND, bool FORCES>
+__device__ __forceinline__ void kspace_entry(const double2 *tab, const Cand &m, int na, int KM, int kx, int ky, int kz,
+                                             double beta, const double (&bl)[NPair<NT>::value],
+                                             const double2 (&rho)[1 + NT], double2 (&mold)[1 + NT],
+                                             double2 (&dl)[1 + NT], double (&acc)[kNV]) {
+    double2 ph[kMaxA], phl[kMaxA];
+    if constexpr (KIND != PASS_NEW) mol_phase_sum<NT>(tab, m, na, na, KM, kx, ky, kz, mold, ph, phl);
+    if constexpr (KIND == PASS_OLD) {
+        if constexpr (FORCES) entry_forces<NT>(m, na, na, kx, ky, kz, beta, bl, rho, ph, phl, acc);
+    } else {
+        double2 mnew[1 + NT];
+        mol_phase_sum<NT>(tab, m, 0, na, KM, kx, ky, kz, mnew, ph, phl);
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) dl[t] = make_double2(mnew[t].x - mold[t].x, mnew[t].y - mold[t].y);
+        {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
+            const double2 C = rho[0], d = dl[0];
+            acc[RV_DUC] += (((C.x + C.x) + d.x) * d.x + ((C.y + C.y) + d.y) * d.y) * beta;
+        }
+        // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
+        // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
+#pragma unroll
+        for (int t1 = 0; t1 < NT; ++t1) {
+            const double2 C1 = rho[1 + t1], D1 = dl[1 + t1];
+            const double tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
+#pragma unroll
+            for (int t2 = 0; t2 < NT; ++t2) {
+                const double2 D2 = dl[1 + t2];
+                if (D2.x == 0.0 && D2.y == 0.0) continue;
+                acc[RV_DUL] += (tc * D2.x + ts * D2.y) * bl[pair_idx<NT>(t1, t2)];
+            }
+        }
+        if constexpr (KIND == PASS_NEW && FORCES) {  // against total_new = rho + delta (MC.f90:1136-1163)
+            double2 Cn[1 + NT];
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) Cn[t] = make_double2(rho[t].x + dl[t].x, rho[t].y + dl[t].y);
+            entry_forces<NT>(m, 0, na, kx, ky, kz, beta, bl, Cn, ph, phl, acc);
+        }
+    }
+}
+
 // The workers' part of one pass over the molecule's slots: k-space over their entries, real
 // space over the CTA's atoms (pairs inside the cutoff laid out in the queue by a prefix sum
 // over threads -- a deterministic order -- then evaluated item i by worker i % nwork), and a
 // per-warp reduction into red[worker warp][value].  Worker-only barriers (bar 1).
 template <int NT, int EPT, int KIND, bool FORCES>
-__device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, EntryRegs<NT, EPT> &R, double2 *tab,
+__device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT> &R, double2 *tab,
                                             const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue,
-                                            double *red, const double *lj_s, int nown, int qcap, long long *prof) {
+                                            double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
+                                            long long *prof) {
     constexpr int NVMAX = FORCES ? kNV : RV_F;
     const Cand &m = sh.cand[sh.icur];
     const int na = m.na;
@@ -450,43 +499,39 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, En
 #pragma unroll
     for (int v = 0; v < kNV; ++v) acc[v] = 0.0;
 
-    static_for<0, EPT>([&](auto kc) {
-        constexpr int k = decltype(kc)::value;
-        if (R.e[k] < 0) return;
-        double2 ph[kMaxA], phl[kMaxA];
-        if constexpr (KIND != PASS_NEW) mol_phase_sum<NT>(tab, m, na, na, KM, R.kx[k], R.ky[k], R.kz[k], R.mold[k], ph, phl);
-        if constexpr (KIND == PASS_OLD) {
-            if constexpr (FORCES) entry_forces<NT>(m, na, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k], ph, phl, acc);
-        } else {
-            double2 mnew[1 + NT];
-            mol_phase_sum<NT>(tab, m, 0, na, KM, R.kx[k], R.ky[k], R.kz[k], mnew, ph, phl);
+    if constexpr (EPT > 0) {
+        static_for<0, EPT>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            if (R.e[k] < 0) return;
+            kspace_entry<NT, KIND, FORCES>(tab, m, na, KM, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k],
+                                           R.mold[k], R.dl[k], acc);
+        });
+    } else {
+        // streamed layout: entries e0, e0 + estep, ... read from memory; the old sums and the
+        // deltas go to the chain's scratch for the next pass and the commit
+        const int S = D.S;
+        double2 *mold_g = D.scratch;
+        double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
+        for (int e = e0; e < S; e += estep) {
+            const int4 kv = D.kvec[e];
+            const double beta = D.ebeta[e];
+            double bl[NPair<NT>::value];
 #pragma unroll
-            for (int t = 0; t <= NT; ++t) R.dl[k][t] = make_double2(mnew[t].x - R.mold[k][t].x, mnew[t].y - R.mold[k][t].y);
-            {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
-                const double2 C = R.rho[k][0], d = R.dl[k][0];
-                acc[RV_DUC] += (((C.x + C.x) + d.x) * d.x + ((C.y + C.y) + d.y) * d.y) * R.beta[k];
+            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = D.ebetalj[(size_t)p * S + e];
+            double2 rho[1 + NT], mold[1 + NT], dl[1 + NT];
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) {
+                rho[t] = D.rho[(size_t)t * S + e];
+                mold[t] = (KIND == PASS_NEW) ? mold_g[(size_t)t * S + e] : make_double2(0, 0);
             }
-            // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
-            // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
+            kspace_entry<NT, KIND, FORCES>(tab, m, na, KM, kv.x, kv.y, kv.z, beta, bl, rho, mold, dl, acc);
 #pragma unroll
-            for (int t1 = 0; t1 < NT; ++t1) {
-                const double2 C1 = R.rho[k][1 + t1], D1 = R.dl[k][1 + t1];
-                const double tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
-#pragma unroll
-                for (int t2 = 0; t2 < NT; ++t2) {
-                    const double2 D2 = R.dl[k][1 + t2];
-                    if (D2.x == 0.0 && D2.y == 0.0) continue;
-                    acc[RV_DUL] += (tc * D2.x + ts * D2.y) * R.bl[k][pair_idx<NT>(t1, t2)];
-                }
-            }
-            if constexpr (KIND == PASS_NEW && FORCES) {  // against total_new = rho + delta (MC.f90:1136-1163)
-                double2 Cn[1 + NT];
-#pragma unroll
-                for (int t = 0; t <= NT; ++t) Cn[t] = make_double2(R.rho[k][t].x + R.dl[k][t].x, R.rho[k][t].y + R.dl[k][t].y);
-                entry_forces<NT>(m, 0, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], Cn, ph, phl, acc);
+            for (int t = 0; t <= NT; ++t) {
+                if (KIND == PASS_OLD) mold_g[(size_t)t * S + e] = mold[t];
+                else dl_g[(size_t)t * S + e] = dl[t];
             }
         }
-    });
+    }
     YAMC_WPH(PH_KSPACE);
 
     const int round_atoms = nwork * kCPT;
@@ -761,8 +806,9 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
     for (int i = tid; i < nt * nt; i += B) { lj_s[i] = D.lj_sig6[i]; lj_s[nt * nt + i] = D.lj_feps[i]; }
 
     // the workers' k-vector entries; rho stays in registers for the whole launch
-    EntryRegs<NT, EPT> R;
+    RegsOf<NT, EPT> R;
     const int gwork = G * nwork;
+    const int e0 = rank * nwork + wtid;  // this worker's entries: e0 + k * gwork
 #pragma unroll
     for (int k = 0; k < EPT; ++k) {
         const int e = ctl ? S : rank * nwork + wtid + k * gwork;
@@ -863,7 +909,7 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
             const int na0 = sh.cand[sh.icur].na;
             // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
             if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
-                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, prof);
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, e0, gwork, prof);
                 __syncthreads();
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
                 xpar ^= 1;
@@ -925,8 +971,8 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
 
         // ------------------------------------------------ the pass over the new positions
         if (!ctl) {
-            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, prof);
-            else worker_pass<NT, EPT, PASS_BOTH, false>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, prof);
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            else worker_pass<NT, EPT, PASS_BOTH, false>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, e0, gwork, prof);
         } else if (speculate && it + 1 < n_moves) {
             // prepare the next move's candidates while the workers run: lane 0 after an overlap
             // (no acceptance draw), lanes 1-2 after the acceptance draw, lane 2 with the molecule
@@ -1108,11 +1154,24 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
         YAMC_PH(PH_DECIDE);
         if (sh.abort) break;
         if (sh.accepted) {
-            // commit: rho += delta in registers (MC.f90:1245), the CTA's staged copy of the moved atoms
+            // commit: rho += delta (MC.f90:1245), in registers or in memory by the entry's owner
 #pragma unroll
             for (int k = 0; k < EPT; ++k)
 #pragma unroll
                 for (int t = 0; t <= NT; ++t) { R.rho[k][t].x += R.dl[k][t].x; R.rho[k][t].y += R.dl[k][t].y; }
+            if constexpr (EPT == 0) {
+                if (!ctl) {
+                    const double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
+                    for (int e = e0; e < S; e += gwork)
+#pragma unroll
+                        for (int t = 0; t <= NT; ++t) {
+                            double2 r = D.rho[(size_t)t * S + e];
+                            const double2 d = dl_g[(size_t)t * S + e];
+                            r.x += d.x; r.y += d.y;
+                            D.rho[(size_t)t * S + e] = r;
+                        }
+                }
+            }
         }
         ++moves_done;
         have_next = sh.spec_ok != 0;
@@ -1234,7 +1293,7 @@ struct yamc_ctx {
     long long cnt_h[CN_COUNT] = {};
     bool pos_valid = true;  // H.x/y/z mirror the device positions
     LaunchCfg cfg;
-    int force_G = 0, force_B = 0;
+    int force_G = 0, force_B = 0, force_layout = YAMC_KSPACE_AUTO;
     // per-move API state
     int api_imol = 0, api_stage = 0;
     double api_eold[3] = {}, api_fold[3 * kMaxA] = {};
@@ -1251,8 +1310,8 @@ namespace {
 // entries, the CTA's atoms and the pair queue fit in shared memory.  G (1..16 CTAs per cluster)
 // from large to small when large_first (the shortest move for a lone chain), else from small to
 // large; B from 256 to 128 threads; force_G / force_B pin either (0 = free).
-int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, int force_G, int force_B, LaunchCfg *out,
-                    bool large_first = true) {
+int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, int force_G, int force_B, int layout,
+                    LaunchCfg *out, bool large_first = true) {
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
@@ -1271,7 +1330,9 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
             if (force_B && B != force_B) continue;
             if (!force_B && B != kChainMaxThreads && G * (kChainMaxThreads - kCtl) < Smax) continue;
             const int nwork = B - kCtl;  // warp 0 is the control warp
-            const int EPT = (Smax + G * nwork - 1) / (G * nwork);
+            int EPT = (Smax + G * nwork - 1) / (G * nwork);
+            // entries in registers (at most 2 per worker) or streamed from memory (EPT 0)
+            if (layout == YAMC_KSPACE_STREAMED || (layout == YAMC_KSPACE_AUTO && EPT > 2)) EPT = 0;
             if (EPT > 2) continue;
             const int nown_max = (Nmax + G - 1) / G;
             const int qcap = std::min(nown_max, nwork * kCPT) * 2 * kMaxA;  // one filter round of pairs
@@ -1286,7 +1347,7 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
 }
 
 int pick_launch(yamc_ctx *c, LaunchCfg *out) {
-    return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, out);
+    return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, c->force_layout, out);
 }
 
 // nrep chains of one launch shape: nrep clusters of L.G CTAs, chain r on cluster r
@@ -1335,9 +1396,10 @@ int max_clusters_t(const LaunchCfg &L, int *out) {
 // kernel instance for (LJ types, entries per thread, split old pass); WHAT(NT, EPT, SPLIT) is
 // a call of a template above
 #ifdef YAMC_ONE_VARIANT  // development builds: a single instantiation compiles in seconds
-#define YAMC_CHAIN_VARIANTS(X) X(3, 1)
+#define YAMC_CHAIN_VARIANTS(X) X(3, 0) X(3, 1)
 #else
-#define YAMC_CHAIN_VARIANTS(X) X(1, 1) X(1, 2) X(2, 1) X(2, 2) X(3, 1) X(3, 2) X(4, 1) X(4, 2)
+#define YAMC_CHAIN_VARIANTS(X) \
+    X(1, 0) X(1, 1) X(1, 2) X(2, 0) X(2, 1) X(2, 2) X(3, 0) X(3, 1) X(3, 2) X(4, 0) X(4, 1) X(4, 2)
 #endif
 
 int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, cudaStream_t stream, int nrep, const ChainArgs &args) {
@@ -1506,7 +1568,7 @@ struct yamc_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
     cudaGraphExec_t graph = nullptr;
     float last_ms = 0.f;
-    int force_G = 0, force_B = 0;
+    int force_G = 0, force_B = 0, force_layout = YAMC_KSPACE_AUTO;
     float *d_rng = nullptr;
     size_t rng_cap = 0;
     yamc_move_record *d_log = nullptr;
@@ -1526,7 +1588,7 @@ int batch_configure(yamc_batch *b) {
     for (BatchGroup &g : b->groups) {
         std::vector<const HostSystem *> hs;
         for (int i : g.idx) hs.push_back(&b->reps[i]->H);
-        int r = pick_launch_for(hs, b->device, b->force_G, b->force_B, &g.cfg);
+        int r = pick_launch_for(hs, b->device, b->force_G, b->force_B, b->force_layout, &g.cfg);
         if (r) return r;
         if ((r = max_clusters_cfg(g.cfg, g.nt, g.split, &g.max_clusters))) return r;
     }
@@ -1719,7 +1781,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.psm = P.pressure_step_multiplier; D.n_store_energy_interval = P.n_store_energy_interval;
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
-    D.rho = c->rho; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
+    D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
     D.nspec = (int)(H.spec.size() / 4); D.spec = c->spec;
     if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
     c->cnt_h[CN_ICYCLE] = 1;
@@ -1801,6 +1863,13 @@ int yamc_set_launch(yamc_ctx *c, int32_t cluster_blocks, int32_t threads) {
         return YAMC_EPARAMETER;
     c->force_G = cluster_blocks;
     c->force_B = threads;
+    c->cfg = LaunchCfg();
+    return pick_launch(c, &c->cfg);
+}
+
+int yamc_set_kspace_layout(yamc_ctx *c, int32_t layout) {
+    if (!c || layout < YAMC_KSPACE_AUTO || layout > YAMC_KSPACE_STREAMED) return YAMC_EPARAMETER;
+    c->force_layout = layout;
     c->cfg = LaunchCfg();
     return pick_launch(c, &c->cfg);
 }
@@ -2160,6 +2229,13 @@ int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads
     return batch_configure(b);
 }
 
+int yamc_batch_set_kspace_layout(yamc_batch *b, int32_t layout) {
+    if (!b || layout < YAMC_KSPACE_AUTO || layout > YAMC_KSPACE_STREAMED) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(b->device));
+    b->force_layout = layout;
+    return batch_configure(b);
+}
+
 int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]) {
     if (!b || !out || b->groups.empty()) return YAMC_EPARAMETER;
     const BatchGroup &g = b->groups[0];
@@ -2181,14 +2257,17 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     BatchBackup keep;
     int r = batch_copy_state(b, keep, true);
     if (r) return r;
-    const int fG = b->force_G, fB = b->force_B;
+    const int fG = b->force_G, fB = b->force_B, fL = b->force_layout;
     const int Bs[] = {kChainMaxThreads, 128};
+    const int Ls[] = {YAMC_KSPACE_REGISTERS, YAMC_KSPACE_STREAMED};
     double best = -1.0;
-    int bestG = 0, bestB = 0;
+    int bestG = 0, bestB = 0, bestL = 0;
     std::vector<int64_t> cur(R), done(R);
+    for (int L : Ls)
     for (int G = 1; G <= 16; ++G) {
         for (int B : Bs) {
-            b->force_G = G; b->force_B = B;
+            if (fL != YAMC_KSPACE_AUTO && L != fL) continue;
+            b->force_G = G; b->force_B = B; b->force_layout = L;
             if (batch_configure(b) != YAMC_OK) continue;  // shape does not fit
             bool ok = true;
             for (const BatchGroup &g : b->groups) ok = ok && g.cfg.G == G && g.cfg.B == B && g.max_clusters > 0;
@@ -2201,16 +2280,16 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
             double moves = 0;
             for (size_t i = 0; i < R; ++i) moves += (double)done[i];
             const double rate = b->last_ms > 0 ? moves / (1e-3 * b->last_ms) : 0.0;
-            if (rate > best) { best = rate; bestG = G; bestB = B; }
+            if (rate > best) { best = rate; bestG = G; bestB = B; bestL = L; }
         }
     }
     if (best < 0) {
-        b->force_G = fG; b->force_B = fB;
+        b->force_G = fG; b->force_B = fB; b->force_layout = fL;
         batch_configure(b);
         set_error("no launch shape fits every replica of the batch");
         return YAMC_ELIMITS;
     }
-    b->force_G = bestG; b->force_B = bestB;
+    b->force_G = bestG; b->force_B = bestB; b->force_layout = bestL;
     r = batch_configure(b);
     for (yamc_ctx *c : b->reps) c->pos_valid = false;
     if (best_moves_per_s) *best_moves_per_s = best;
