@@ -218,7 +218,7 @@ def main():
 
     dev = f"cuda:{local}"
     n_steps = args.warmup + args.steps
-    per_move = 24  # generous upper bound of random numbers per unbiased move
+    per_move = 16  # upper bound of random numbers per unbiased move (about 11 on average)
     n_stream = per_move * args.moves * (2 * n_steps + 2) + 100000
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
@@ -253,7 +253,7 @@ def main():
             continue
         resident[G] = probe.launch["resident_clusters"]
     if not R:
-        R = max(resident.values(), default=1)
+        R = min(148, max(resident.values(), default=1))
     probe.close()
     R = max(R, 1)
     rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=3 + 101 * rank + r,

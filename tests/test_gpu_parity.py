@@ -90,6 +90,16 @@ def test_chain_streamed_spce256(spce_files):
     assert rel_close(eng.full_sums(), o.full_sums(), 1e-9)
 
 
+@pytest.mark.parametrize("cluster", [1, 3])
+def test_chain_streamed_wide(spce_files, cluster):
+    """Streamed entries with 512-thread CTAs (15 worker warps)."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(spce_files, 5000, cluster=cluster, threads=512,
+                                               layout=_lib.YAMC_KSPACE_STREAMED)
+    assert eng.launch["threads"] == 512 and eng.launch["entries_per_thread"] == 0
+    compare_logs(glog, olog)
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+
+
 def test_chain_matches_oracle_nacl(nacl_files):
     o, olog, ocur, eng, glog, gcur = _run_pair(nacl_files, 6000)
     compare_logs(glog, olog)

@@ -5,6 +5,7 @@
 // chain draw identical proposals from the same stream.
 #pragma once
 
+#include <cmath>
 #include <cstdint>
 #include <cuda_runtime.h>
 
@@ -16,6 +17,7 @@ constexpr int kMaxA = 4;  // atoms per molecule handled on the device
 struct DevSys {
     int N, M, S, nt, kmax, npair, freq_monotone, n_species;
     double rmax2, alpha, xclb, taosp, kext, m2k, dr, d_angle, xlf, xlc, psm, n_store_energy_interval;
+    double rpre;           // max(cutoff, largest hard-core diameter), box units: the pair filter's reach
     double4 *atom;         // x, y, z (box units), q
     const int2 *meta;      // 0-based molecule, LJ type (0 = none)
     const double *dhs;     // hard-core diameter / BoxLength
@@ -44,25 +46,56 @@ enum Scal {
 // run_mc counters (int64)
 enum Cnt { CN_ICYCLE = 0, CN_MOVE_IN_CYCLE, CN_COUNT };
 
+// ------------------------------------------------------------------ arithmetic helpers
+// 1/y rounded to nearest (the same value as the IEEE division 1/y) and 1/sqrt(y) (within an
+// ulp).  The pair kernel multiplies by these instead of dividing: a floating-point division is a
+// long instruction sequence, and the pair term has a dozen of them.  Replacing x / c by
+// x * (1/c) changes a result by at most an ulp or two, far inside the 1e-10 parity bound.
+template <class R>
+__host__ __device__ inline R rcp(R y) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 8) return __drcp_rn(y);
+    else return __frcp_rn(y);
+#else
+    return R(1) / y;
+#endif
+}
+template <class R>
+__host__ __device__ inline R rsq(R y) {
+#ifdef __CUDA_ARCH__
+    if constexpr (sizeof(R) == 8) return rsqrt(y);
+    else return rsqrtf(y);
+#else
+    return R(1) / std::sqrt(y);
+#endif
+}
+
 // ------------------------------------------------------------------ Functions.f90
 // erfc_Luc / erf_Luc (Functions.f90:116-171): Taylor series below 0.455,
-// Abramowitz & Stegun 7.1.26 up to 3, asymptotic series above.
+// Abramowitz & Stegun 7.1.26 up to 3, asymptotic series above (divisions by
+// multiplications with reciprocals, see rcp above).
 template <class R>
 __host__ __device__ inline R d_erfc_luc(R x, R x2, R ee2) {
     const R P = R(0.3275911), A1 = R(0.254829592), A2 = R(-0.284496736), A3 = R(1.421413741),
             A4 = R(-1.453152027), A5 = R(1.061405429), pi05 = R(1.7724538509055);
-    if (x < R(0.455)) return R(1) - R(2) / pi05 * x * (R(1) - x2 * (R(1) / R(3) - x2 * (R(0.1) - x2 * (R(1) / R(42) - x2 / R(216)))));
-    if (x > R(3)) return (R(1) - R(0.5) * (R(1) - R(1.5) / x2) / x2) / (pi05 * x) * ee2;
-    const R t = R(1) / (R(1) + P * x);
+    if (x < R(0.455)) return R(1) - R(2) / pi05 * x * (R(1) - x2 * (R(1) / R(3) - x2 * (R(0.1) - x2 * (R(1) / R(42) - x2 * (R(1) / R(216))))));
+    if (x > R(3)) {
+        const R i2 = rcp(x2);
+        return (R(1) - R(0.5) * (R(1) - R(1.5) * i2) * i2) * rcp(pi05 * x) * ee2;
+    }
+    const R t = rcp(R(1) + P * x);
     return t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ee2;
 }
 template <class R>
 __host__ __device__ inline R d_erf_luc(R x, R x2, R ee2) {
     const R P = R(0.3275911), A1 = R(0.254829592), A2 = R(-0.284496736), A3 = R(1.421413741),
             A4 = R(-1.453152027), A5 = R(1.061405429), pi05 = R(1.7724538509055);
-    if (x < R(0.455)) return R(2) / pi05 * x * (R(1) - x2 * (R(1) / R(3) - x2 * (R(0.1) - x2 * (R(1) / R(42) - x2 / R(216)))));
-    if (x > R(3)) return R(1) - (R(1) - R(0.5) * (R(1) - R(1.5) / x2) / x2) / (pi05 * x) * ee2;
-    const R t = R(1) / (R(1) + P * x);
+    if (x < R(0.455)) return R(2) / pi05 * x * (R(1) - x2 * (R(1) / R(3) - x2 * (R(0.1) - x2 * (R(1) / R(42) - x2 * (R(1) / R(216))))));
+    if (x > R(3)) {
+        const R i2 = rcp(x2);
+        return R(1) - (R(1) - R(0.5) * (R(1) - R(1.5) * i2) * i2) * rcp(pi05 * x) * ee2;
+    }
+    const R t = rcp(R(1) + P * x);
     return R(1) - t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ee2;
 }
 
@@ -116,25 +149,27 @@ template <class R, bool WANT_FR>
 __host__ __device__ inline PairTerm<R> pair_term(R r2, R qq_xclb, bool lj, R sigma6, R four_eps, R alpha,
                                                  R taosp, bool same_mol) {
     PairTerm<R> t;
-    const R r = sqrt(r2);
+    const R ir = rsq(r2);       // 1/r
+    const R r = r2 * ir;
+    const R ir2 = ir * ir;      // 1/r^2
     const R a = alpha * r;
     const R a2 = a * a;
     const R e2 = exp(-a2);
     const R erfc_a = same_mol ? -d_erf_luc<R>(a, a2, e2) : d_erfc_luc<R>(a, a2, e2);
-    t.ew = qq_xclb * erfc_a / r;
-    if (WANT_FR) t.FR = qq_xclb * (erfc_a / r + taosp * e2) / r2;
+    t.ew = qq_xclb * erfc_a * ir;
+    if (WANT_FR) t.FR = qq_xclb * (erfc_a * ir + taosp * e2) * ir2;
     else t.FR = R(0);
     t.lj6 = R(0); t.lj12 = R(0);
     if (lj) {
-        const R r6 = r2 * r2 * r2;
-        const R so6 = sigma6 / r6;
-        const R C6 = R(1) + a2 * (R(1) + a2 / R(2));
+        const R so6 = sigma6 * (ir2 * ir2 * ir2);
+        const R C6 = R(1) + a2 * (R(1) + a2 * R(0.5));
         const R a6 = a2 * a2 * a2;
-        const R C12 = C6 + a6 * (R(1) + a2 * (R(1) + a2 / R(5)) / R(4)) / R(6);
+        const R C12 = C6 + a6 * (R(1) + a2 * (R(1) + a2 * (R(1) / R(5))) * R(0.25)) * (R(1) / R(6));
         t.lj6 = four_eps * so6 * e2 * C6;
         t.lj12 = four_eps * (so6 * so6) * e2 * C12;
         if (WANT_FR)
-            t.FR = t.FR + four_eps * R(6) * so6 * e2 * (R(2) * so6 * (C12 + a6 * a6 / R(720)) - (C6 + a6 / R(6))) / r2;
+            t.FR = t.FR + four_eps * R(6) * so6 * e2 *
+                              (R(2) * so6 * (C12 + a6 * a6 * (R(1) / R(720))) - (C6 + a6 * (R(1) / R(6)))) * ir2;
     }
     return t;
 }

@@ -267,6 +267,7 @@ constexpr int kCPT = 4;   // atoms each worker thread tests per filter round
 constexpr int kWin = 256; // random-stream window held in shared memory
 constexpr int kCtl = 32;  // threads of the control warp
 constexpr int kChainMaxThreads = 256;  // one CTA per SM, up to 255 registers per thread
+constexpr int kChainMaxThreadsWide = 512;  // streamed k entries, 16 warps, up to 128 registers per thread
 
 // a prepared move: the molecule, its atoms at the old and proposed positions, the proposal
 struct Cand {
@@ -341,7 +342,8 @@ struct EntryRegs {
     double2 dl[EPT][1 + NT];
 };
 
-// EPT == 0: the streamed layout -- no entry lives in registers; each worker loops over its
+// EPT <= 0: the streamed layout (EPT == -1: the same with 512-thread CTAs) -- no entry lives in
+// registers; each worker loops over its
 // entries and reads k, beta, beta_LJ and rho from memory (L2-resident) every pass.  The
 // register block of one (never touched) entry only keeps the code uniform.
 template <int NT, int EPT>
@@ -473,6 +475,7 @@ __device__ __forceinline__ void kspace_entry(const double2 *tab, const Cand &m, 
 template <int NT, int EPT, int KIND, bool FORCES>
 __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT> &R, double2 *tab,
                                             const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue,
+                                            int *nearbuf,
                                             double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
                                             long long *prof) {
     constexpr int NVMAX = FORCES ? kNV : RV_F;
@@ -507,24 +510,38 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
                                            R.mold[k], R.dl[k], acc);
         });
     } else {
-        // streamed layout: entries e0, e0 + estep, ... read from memory; the old sums and the
-        // deltas go to the chain's scratch for the next pass and the commit
+        // streamed layout: entries e0, e0 + estep, ... read from memory, the next entry's loads in
+        // flight while the current one computes; the old sums and the deltas go to the chain's
+        // scratch for the next pass and the commit
         const int S = D.S;
         double2 *mold_g = D.scratch;
         double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
-        for (int e = e0; e < S; e += estep) {
-            const int4 kv = D.kvec[e];
-            const double beta = D.ebeta[e];
-            double bl[NPair<NT>::value];
+        int4 kv_n = make_int4(0, 0, 0, 0);
+        double beta_n = 0.0, bl_n[NPair<NT>::value];
+        double2 rho_n[1 + NT], mold_n[1 + NT];
+        auto fetch = [&](int e) {
+            kv_n = D.kvec[e];
+            beta_n = D.ebeta[e];
 #pragma unroll
-            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = D.ebetalj[(size_t)p * S + e];
-            double2 rho[1 + NT], mold[1 + NT], dl[1 + NT];
+            for (int p = 0; p < NPair<NT>::value; ++p) bl_n[p] = D.ebetalj[(size_t)p * S + e];
 #pragma unroll
             for (int t = 0; t <= NT; ++t) {
-                rho[t] = D.rho[(size_t)t * S + e];
-                mold[t] = (KIND == PASS_NEW) ? mold_g[(size_t)t * S + e] : make_double2(0, 0);
+                rho_n[t] = D.rho[(size_t)t * S + e];
+                mold_n[t] = (KIND == PASS_NEW) ? mold_g[(size_t)t * S + e] : make_double2(0, 0);
             }
-            kspace_entry<NT, KIND, FORCES>(tab, m, na, KM, kv.x, kv.y, kv.z, beta, bl, rho, mold, dl, acc);
+        };
+        if (e0 < S) fetch(e0);
+        for (int e = e0; e < S; e += estep) {
+            const int kx = kv_n.x, ky = kv_n.y, kz = kv_n.z;
+            const double beta = beta_n;
+            double bl[NPair<NT>::value];
+            double2 rho[1 + NT], mold[1 + NT], dl[1 + NT];
+#pragma unroll
+            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = bl_n[p];
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) { rho[t] = rho_n[t]; mold[t] = mold_n[t]; }
+            if (e + estep < S) fetch(e + estep);
+            kspace_entry<NT, KIND, FORCES>(tab, m, na, KM, kx, ky, kz, beta, bl, rho, mold, dl, acc);
 #pragma unroll
             for (int t = 0; t <= NT; ++t) {
                 if (KIND == PASS_OLD) mold_g[(size_t)t * S + e] = mold[t];
@@ -534,14 +551,58 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
     }
     YAMC_WPH(PH_KSPACE);
 
+    // bounding spheres of the molecule at its new (slot 0) and old (slot na) positions: an atom
+    // farther than rpre + radius from a centre is outside the cutoff and every hard core of all
+    // that position's slots (triangle inequality on the periodic box), so its slot tests are skipped
+    double rp2;
+    {
+        double rad2 = 0.0;
+        for (int a = 1; a < na; ++a) {
+            const double dx = m.slot[a].x - m.slot[0].x, dy = m.slot[a].y - m.slot[0].y, dz = m.slot[a].z - m.slot[0].z;
+            rad2 = fmax(rad2, dx * dx + dy * dy + dz * dz);
+            const double ex = m.slot[na + a].x - m.slot[na].x, ey = m.slot[na + a].y - m.slot[na].y,
+                         ez = m.slot[na + a].z - m.slot[na].z;
+            rad2 = fmax(rad2, ex * ex + ey * ey + ez * ez);
+        }
+        const double rp = (D.rpre + sqrt(rad2)) * (1.0 + 1e-9);
+        rp2 = rp * rp;
+    }
+    const double cnx = m.slot[0].x, cny = m.slot[0].y, cnz = m.slot[0].z;
+    const double cox = m.slot[na].x, coy = m.slot[na].y, coz = m.slot[na].z;
+
     const int round_atoms = nwork * kCPT;
+    int *nb = nearbuf + wwarp * 32 * kCPT;  // this warp's near atoms of the round
     for (int c0 = 0; c0 < nown; c0 += round_atoms) {
+        // near atoms of the warp's 32 x kCPT candidates, compacted in (c, lane) order
+        int nnear = 0;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            const int jl = c0 + c * nwork + wtid;
+            bool near = false;
+            if (jl < nown && meta_s[jl].x != imol0) {
+                const double4 pj = atom_s[jl];
+                if (KIND != PASS_OLD) {
+                    const double dx = min_image(cnx - pj.x), dy = min_image(cny - pj.y), dz = min_image(cnz - pj.z);
+                    near = dx * dx + dy * dy + dz * dz < rp2;
+                }
+                if (KIND != PASS_NEW) {
+                    const double dx = min_image(cox - pj.x), dy = min_image(coy - pj.y), dz = min_image(coz - pj.z);
+                    near = near || dx * dx + dy * dy + dz * dz < rp2;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, near);
+            if (near) nb[nnear + __popc(bal & ((1u << lane) - 1u))] = jl;
+            nnear += __popc(bal);
+        }
+        __syncwarp();
+        // slot tests of the near atoms, densely: lane takes entries lane, lane + 32, ...
         unsigned masks = 0;  // kCPT slot masks of 8 bits
         int count = 0;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            const int jl = c0 + c * nwork + wtid;
-            if (jl < nown && meta_s[jl].x != imol0) {
+            const int k = c * 32 + lane;
+            if (k < nnear) {
+                const int jl = nb[k];
                 const double4 pj = atom_s[jl];
                 const int tj = meta_s[jl].y;
                 const double dj = dhs_s[jl];
@@ -584,7 +645,7 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
             unsigned msk = (masks >> (8 * c)) & 0xffu;
-            const int jl = c0 + c * nwork + wtid;
+            const int jl = msk ? nb[c * 32 + lane] : 0;
             while (msk) {
                 const int s = __ffs(msk) - 1;
                 msk &= msk - 1;
@@ -766,7 +827,7 @@ __device__ inline void propose(const DevSys &D, Cand &C, RngReader &rng, const d
 // SPLIT = false: unbiased device-resident chain only (one fused pass per move, speculation);
 // SPLIT = true: force-biased moves and the per-move API (old pass + new pass with forces).
 template <int NT, int EPT, bool SPLIT>
-__global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
+__global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThreads, 1) k_chain(ChainArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     __shared__ ChainShared sh;
     __shared__ float rwin[2][kWin];
@@ -793,7 +854,8 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
     double *dhs_s = reinterpret_cast<double *>(atom_s + A.nown_max);          // [nown_max]
     int2 *meta_s = reinterpret_cast<int2 *>(dhs_s + A.nown_max);              // [nown_max]
     int *queue = reinterpret_cast<int *>(meta_s + A.nown_max);                // [qcap]
-    double *red = reinterpret_cast<double *>(queue + ((A.qcap + 1) & ~1));    // [B/32][kNV]
+    int *nearbuf = queue + ((A.qcap + 1) & ~1);                               // [B/32][32 kCPT]
+    double *red = reinterpret_cast<double *>(nearbuf + B * kCPT);             // [B/32][kNV]
     double *xch = red + (B / 32) * kNV;                                       // [2][G][kNV]
     double *lj_s = xch + 2 * G * kNV;                                         // [2][nt*nt]
 
@@ -909,7 +971,7 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
             const int na0 = sh.cand[sh.icur].na;
             // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
             if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
-                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, e0, gwork, prof);
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
                 __syncthreads();
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
                 xpar ^= 1;
@@ -971,8 +1033,8 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
 
         // ------------------------------------------------ the pass over the new positions
         if (!ctl) {
-            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, e0, gwork, prof);
-            else worker_pass<NT, EPT, PASS_BOTH, false>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            else worker_pass<NT, EPT, PASS_BOTH, false>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
         } else if (speculate && it + 1 < n_moves) {
             // prepare the next move's candidates while the workers run: lane 0 after an overlap
             // (no acceptance draw), lanes 1-2 after the acceptance draw, lane 2 with the molecule
@@ -1159,7 +1221,7 @@ __global__ void __launch_bounds__(kChainMaxThreads, 1) k_chain(ChainArgs A) {
             for (int k = 0; k < EPT; ++k)
 #pragma unroll
                 for (int t = 0; t <= NT; ++t) { R.rho[k][t].x += R.dl[k][t].x; R.rho[k][t].y += R.dl[k][t].y; }
-            if constexpr (EPT == 0) {
+            if constexpr (EPT <= 0) {
                 if (!ctl) {
                     const double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
                     for (int e = e0; e < S; e += gwork)
@@ -1253,6 +1315,7 @@ size_t chain_smem_bytes(int G, int B, int kmax, int nt, int nown_max, int qcap) 
     size_t b = sizeof(double2) * 2 * kMaxA * 3 * KM;
     b += (sizeof(double4) + sizeof(double) + sizeof(int2)) * (size_t)nown_max;
     b += sizeof(int) * (size_t)((qcap + 1) & ~1);
+    b += sizeof(int) * (size_t)B * kCPT;
     b += sizeof(double) * (size_t)(B / 32) * kNV;
     b += sizeof(double) * (size_t)2 * G * kNV;
     b += sizeof(double) * (size_t)2 * nt * nt;
@@ -1320,19 +1383,23 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
         Smax = std::max(Smax, h->S); Nmax = std::max(Nmax, h->N); Nmin = std::min(Nmin, h->N);
         kmax = std::max(kmax, h->kmax); nt = std::max(nt, h->nt);
     }
-    const int Bs[] = {kChainMaxThreads, 128};
+    const int Bs[] = {kChainMaxThreads, kChainMaxThreadsWide, 128};  // unforced: 256 only
     for (int gi = 0; gi < 16; ++gi) {
         const int G = large_first ? 16 - gi : 1 + gi;
         if (force_G && G != force_G) continue;
         if (G > Nmin) continue;  // every CTA owns at least one atom
-        for (int bi = 0; bi < 2; ++bi) {
+        for (int bi = 0; bi < 3; ++bi) {
             const int B = Bs[bi];
-            if (force_B && B != force_B) continue;
-            if (!force_B && B != kChainMaxThreads && G * (kChainMaxThreads - kCtl) < Smax) continue;
+            if (force_B ? B != force_B : B != kChainMaxThreads) continue;
             const int nwork = B - kCtl;  // warp 0 is the control warp
             int EPT = (Smax + G * nwork - 1) / (G * nwork);
-            // entries in registers (at most 2 per worker) or streamed from memory (EPT 0)
+            // entries in registers (at most 2 per worker) or streamed from memory (EPT 0; EPT -1
+            // for 512-thread CTAs, which only the streamed layout runs)
             if (layout == YAMC_KSPACE_STREAMED || (layout == YAMC_KSPACE_AUTO && EPT > 2)) EPT = 0;
+            if (B > kChainMaxThreads) {
+                if (layout == YAMC_KSPACE_REGISTERS) continue;
+                EPT = -1;
+            }
             if (EPT > 2) continue;
             const int nown_max = (Nmax + G - 1) / G;
             const int qcap = std::min(nown_max, nwork * kCPT) * 2 * kMaxA;  // one filter round of pairs
@@ -1396,10 +1463,11 @@ int max_clusters_t(const LaunchCfg &L, int *out) {
 // kernel instance for (LJ types, entries per thread, split old pass); WHAT(NT, EPT, SPLIT) is
 // a call of a template above
 #ifdef YAMC_ONE_VARIANT  // development builds: a single instantiation compiles in seconds
-#define YAMC_CHAIN_VARIANTS(X) X(3, 0) X(3, 1)
+#define YAMC_CHAIN_VARIANTS(X) X(3, -1) X(3, 0) X(3, 1) X(3, 2)
 #else
 #define YAMC_CHAIN_VARIANTS(X) \
-    X(1, 0) X(1, 1) X(1, 2) X(2, 0) X(2, 1) X(2, 2) X(3, 0) X(3, 1) X(3, 2) X(4, 0) X(4, 1) X(4, 2)
+    X(1, -1) X(1, 0) X(1, 1) X(1, 2) X(2, -1) X(2, 0) X(2, 1) X(2, 2) \
+    X(3, -1) X(3, 0) X(3, 1) X(3, 2) X(4, -1) X(4, 0) X(4, 1) X(4, 2)
 #endif
 
 int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, cudaStream_t stream, int nrep, const ChainArgs &args) {
@@ -1779,6 +1847,8 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.rmax2 = P.rmax2; D.alpha = P.alpha; D.xclb = P.xclb; D.taosp = P.two_alpha_over_sqrt_pi; D.kext = P.kext;
     D.m2k = P.minus_two_kext; D.dr = P.dr; D.d_angle = P.d_angle; D.xlf = P.xlambda_f; D.xlc = P.xlambda_c;
     D.psm = P.pressure_step_multiplier; D.n_store_energy_interval = P.n_store_energy_interval;
+    D.rpre = std::sqrt(P.rmax2);
+    for (int i = 0; i < N; ++i) D.rpre = std::max(D.rpre, H.dhs[i]);
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
@@ -1858,27 +1928,35 @@ int yamc_get_positions(yamc_ctx *c, double *x, double *y, double *z) {
 
 int yamc_set_launch(yamc_ctx *c, int32_t cluster_blocks, int32_t threads) {
     if (!c) return YAMC_EPARAMETER;
-    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > kChainMaxThreads || (threads % 32) ||
+    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > kChainMaxThreadsWide || (threads % 32) ||
         (threads > 0 && threads < 64))
         return YAMC_EPARAMETER;
+    const int oG = c->force_G, oB = c->force_B;
     c->force_G = cluster_blocks;
     c->force_B = threads;
-    c->cfg = LaunchCfg();
-    return pick_launch(c, &c->cfg);
+    LaunchCfg L;
+    const int r = pick_launch(c, &L);
+    if (r) { c->force_G = oG; c->force_B = oB; return r; }  // a refused shape changes nothing
+    c->cfg = L;
+    return YAMC_OK;
 }
 
 int yamc_set_kspace_layout(yamc_ctx *c, int32_t layout) {
     if (!c || layout < YAMC_KSPACE_AUTO || layout > YAMC_KSPACE_STREAMED) return YAMC_EPARAMETER;
+    const int oL = c->force_layout;
     c->force_layout = layout;
-    c->cfg = LaunchCfg();
-    return pick_launch(c, &c->cfg);
+    LaunchCfg L;
+    const int r = pick_launch(c, &L);
+    if (r) { c->force_layout = oL; return r; }
+    c->cfg = L;
+    return YAMC_OK;
 }
 
 int yamc_get_launch(yamc_ctx *c, int32_t out[4]) {
     if (!c || !out) return YAMC_EPARAMETER;
     int r = ensure_cfg(c);
     if (r) return r;
-    out[0] = c->cfg.G; out[1] = c->cfg.B; out[2] = c->cfg.EPT; out[3] = (int32_t)c->cfg.smem;
+    out[0] = c->cfg.G; out[1] = c->cfg.B; out[2] = std::max(c->cfg.EPT, 0); out[3] = (int32_t)c->cfg.smem;
     return YAMC_OK;
 }
 
@@ -2220,26 +2298,32 @@ int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng,
 
 int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads) {
     if (!b) return YAMC_EPARAMETER;
-    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > kChainMaxThreads || (threads % 32) ||
+    if (cluster_blocks < 0 || cluster_blocks > 16 || threads < 0 || threads > kChainMaxThreadsWide || (threads % 32) ||
         (threads > 0 && threads < 64))
         return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(b->device));
+    const int oG = b->force_G, oB = b->force_B;
     b->force_G = cluster_blocks;
     b->force_B = threads;
-    return batch_configure(b);
+    const int r = batch_configure(b);
+    if (r) { b->force_G = oG; b->force_B = oB; batch_configure(b); }
+    return r;
 }
 
 int yamc_batch_set_kspace_layout(yamc_batch *b, int32_t layout) {
     if (!b || layout < YAMC_KSPACE_AUTO || layout > YAMC_KSPACE_STREAMED) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(b->device));
+    const int oL = b->force_layout;
     b->force_layout = layout;
-    return batch_configure(b);
+    const int r = batch_configure(b);
+    if (r) { b->force_layout = oL; batch_configure(b); }
+    return r;
 }
 
 int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]) {
     if (!b || !out || b->groups.empty()) return YAMC_EPARAMETER;
     const BatchGroup &g = b->groups[0];
-    out[0] = g.cfg.G; out[1] = g.cfg.B; out[2] = g.cfg.EPT; out[3] = (int32_t)g.cfg.smem; out[4] = g.max_clusters;
+    out[0] = g.cfg.G; out[1] = g.cfg.B; out[2] = std::max(g.cfg.EPT, 0); out[3] = (int32_t)g.cfg.smem; out[4] = g.max_clusters;
     return YAMC_OK;
 }
 
@@ -2258,7 +2342,7 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     int r = batch_copy_state(b, keep, true);
     if (r) return r;
     const int fG = b->force_G, fB = b->force_B, fL = b->force_layout;
-    const int Bs[] = {kChainMaxThreads, 128};
+    const int Bs[] = {kChainMaxThreadsWide, kChainMaxThreads, 128};
     const int Ls[] = {YAMC_KSPACE_REGISTERS, YAMC_KSPACE_STREAMED};
     double best = -1.0;
     int bestG = 0, bestB = 0, bestL = 0;
