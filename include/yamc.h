@@ -130,6 +130,24 @@ int yamc_get_positions(yamc_ctx *ctx, double *x, double *y, double *z);
 /* sizes: natom, nmol, nk (half-space k), nsigned (signed k entries), ntype */
 int yamc_sizes(yamc_ctx *ctx, int32_t out[5]);
 
+/* Replace the configuration (atom positions in box units, the molecule layout
+   unchanged) and recompute the sums as mc_calc_total_sums does (MC.f90:477-585);
+   e (optional) receives the 8 energy.dat numbers.  The counterpart of loading a
+   new frame into atomic_data before a full recompute. */
+int yamc_set_positions(yamc_ctx *ctx, const double *x, const double *y, const double *z, double e[8]);
+
+/* ---- adjoint forces ----
+   Forces = -gradient of the total energy as implemented, for every atom (kT per
+   box length): real space differentiating the piecewise erfc_Luc that the energy
+   uses (the reference's own real-space forces use the exact erfc derivative,
+   RealSumLocal.f90:104, so they differ at the level of erfc_Luc's error), k-space
+   Coulomb + dispersion as ForceKSpace_coulomb/_LJ (ForceKSpace.f90:59-302) with
+   sin/cos(k r) recomputed per atom, and the external term -2 kext q mu
+   (EwaldSumExternal.f90:84-102).  fx/fy/fz: natom each; mol_f, mol_tau: nmol x 3,
+   the molecular force and the torque about the centre of mass (MC.f90:988-1025,
+   geometry.f90:65-201).  Any output may be NULL. */
+int yamc_forces(yamc_ctx *ctx, double *fx, double *fy, double *fz, double *mol_f, double *mol_tau);
+
 /* ---- per-move drop-in for the body of movemc (MC.f90:831-1322) ---- */
 /* Steps 0-4: old molecular force and torque of molecule imol (1-based). */
 int yamc_move_old(yamc_ctx *ctx, int32_t imol, double f[3], double tau[3]);

@@ -78,6 +78,8 @@ SIGNATURES = {
     "yamc_full_sums": (ctypes.c_int, [_VP, _dp]),
     "yamc_get_positions": (ctypes.c_int, [_VP, _dp, _dp, _dp]),
     "yamc_sizes": (ctypes.c_int, [_VP, _ip]),
+    "yamc_set_positions": (ctypes.c_int, [_VP, _dp, _dp, _dp, _dp]),
+    "yamc_forces": (ctypes.c_int, [_VP, _dp, _dp, _dp, _dp, _dp]),
     "yamc_move_old": (ctypes.c_int, [_VP, ctypes.c_int32, _dp, _dp]),
     "yamc_move_eval": (ctypes.c_int, [_VP, ctypes.c_int32, _dp, _dp, _dp, _dp, _ip, _dp, _dp]),
     "yamc_move_commit": (ctypes.c_int, [_VP, ctypes.c_int32]),

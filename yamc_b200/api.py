@@ -149,6 +149,20 @@ class Engine:
         check(self.lib.yamc_get_positions(self.h, _dptr(x), _dptr(y), _dptr(z)), "yamc_get_positions")
         return x, y, z
 
+    def set_positions(self, x, y, z) -> np.ndarray:
+        """New atom positions (box units); full recompute; returns the 8 energy numbers."""
+        x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+        e = np.zeros(8)
+        check(self.lib.yamc_set_positions(self.h, _dptr(x), _dptr(y), _dptr(z), _dptr(e)), "yamc_set_positions")
+        return e
+
+    def forces(self):
+        """Adjoint forces: (per-atom forces [natom, 3], molecular forces [nmol, 3], torques [nmol, 3])."""
+        fx, fy, fz = (np.zeros(self.natom) for _ in range(3))
+        mf, mt = np.zeros((self.nmol, 3)), np.zeros((self.nmol, 3))
+        check(self.lib.yamc_forces(self.h, _dptr(fx), _dptr(fy), _dptr(fz), _dptr(mf), _dptr(mt)), "yamc_forces")
+        return np.stack([fx, fy, fz], axis=1), mf, mt
+
     # -- per-move drop-in -------------------------------------------------------------------
     def move_old(self, imol: int):
         f, t = np.zeros(3), np.zeros(3)

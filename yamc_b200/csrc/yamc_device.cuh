@@ -99,6 +99,52 @@ __host__ __device__ inline R d_erf_luc(R x, R x2, R ee2) {
     return R(1) - t * (A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)))) * ee2;
 }
 
+// d erfc_Luc(x) / dx of the piecewise function above, piece by piece: the adjoint of the
+// energy as implemented (the reference's own forces use the exact erfc derivative instead,
+// RealSumLocal.f90:104).  erf_Luc = 1 - erfc_Luc on every piece, so -erf_Luc has the same
+// derivative.
+template <class R>
+__host__ __device__ inline R d_erfc_luc_deriv(R x, R x2, R ee2) {
+    const R P = R(0.3275911), A1 = R(0.254829592), A2 = R(-0.284496736), A3 = R(1.421413741),
+            A4 = R(-1.453152027), A5 = R(1.061405429), pi05 = R(1.7724538509055);
+    if (x < R(0.455))  // 1 - (2/sqrt(pi)) (x - x^3/3 + x^5/10 - x^7/42 + x^9/216)
+        return -(R(2) / pi05) * (R(1) - x2 * (R(1) - x2 * (R(0.5) - x2 * (R(1) / R(6) - x2 * (R(1) / R(24))))));
+    if (x > R(3)) {    // (x^-1 - 0.5 x^-3 + 0.75 x^-5) e^{-x^2} / sqrt(pi)
+        const R i1 = rcp(x), i2 = i1 * i1;
+        const R h = i1 * (R(1) - i2 * (R(0.5) - R(0.75) * i2));
+        const R dh = -i2 * (R(1) - i2 * (R(1.5) - R(3.75) * i2));
+        return (dh - R(2) * x * h) * ee2 * (R(1) / pi05);
+    }
+    const R t = rcp(R(1) + P * x);  // t A(t) e^{-x^2}, dt/dx = -P t^2
+    const R A = A1 + t * (A2 + t * (A3 + t * (A4 + t * A5)));
+    const R dA = A2 + t * (R(2) * A3 + t * (R(3) * A4 + t * (R(4) * A5)));
+    return ((-P * t * t) * (A + t * dA) - R(2) * x * t * A) * ee2;
+}
+
+// Radial force factor of the implemented pair energy (F_i += FR (r_i - r_j)): the Coulomb part
+// differentiates qq f(alpha r)/r with f = erfc_Luc (or -erf_Luc inside a molecule), the LJ part
+// is the exact derivative of the dispersion-Ewald terms (the same as the reference's).
+template <class R>
+__host__ __device__ inline R pair_force_adjoint(R r2, R qq_xclb, bool lj, R sigma6, R four_eps, R alpha, bool same_mol) {
+    const R ir = rsq(r2);
+    const R r = r2 * ir;
+    const R ir2 = ir * ir;
+    const R a = alpha * r;
+    const R a2 = a * a;
+    const R e2 = exp(-a2);
+    const R f = same_mol ? -d_erf_luc<R>(a, a2, e2) : d_erfc_luc<R>(a, a2, e2);
+    const R df = d_erfc_luc_deriv<R>(a, a2, e2);
+    R FR = qq_xclb * (f * ir - alpha * df) * ir2;
+    if (lj) {
+        const R so6 = sigma6 * (ir2 * ir2 * ir2);
+        const R C6 = R(1) + a2 * (R(1) + a2 * R(0.5));
+        const R a6 = a2 * a2 * a2;
+        const R C12 = C6 + a6 * (R(1) + a2 * (R(1) + a2 * (R(1) / R(5))) * R(0.25)) * (R(1) / R(6));
+        FR = FR + four_eps * R(6) * so6 * e2 * (R(2) * so6 * (C12 + a6 * a6 * (R(1) / R(720))) - (C6 + a6 * (R(1) / R(6)))) * ir2;
+    }
+    return FR;
+}
+
 // shi_sans_exp_f (Functions.f90:225-289): Shi(x) exp(-x), force-bias acceptance
 __host__ __device__ inline double d_shi_sans_exp(double x) {
     const double dx0 = 0.2;

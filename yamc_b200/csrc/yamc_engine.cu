@@ -1266,6 +1266,108 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     if (G > 1) cluster.sync();  // no CTA leaves while another may still address its shared memory
 }
 
+// ------------------------------------------------------------------------------------------
+// adjoint: forces = -dE/dr of the implemented total energy
+// ------------------------------------------------------------------------------------------
+// Real space: one thread per atom i over all j (tiles in shared memory, increasing j), every
+// pair inside the cutoff, intra-molecular pairs with the -erf_Luc energy; F_i += FR (r_i - r_j).
+__global__ void __launch_bounds__(kFullTile) k_forces_real(DevSys D, double *fx, double *fy, double *fz) {
+    __shared__ double4 tp[kFullTile];
+    __shared__ int2 tm[kFullTile];
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool valid = i < D.N;
+    double4 pi = make_double4(0, 0, 0, 0);
+    int2 mi = make_int2(-1, 0);
+    if (valid) { pi = D.atom[i]; mi = D.meta[i]; }
+    double gx = 0, gy = 0, gz = 0;
+    const int nt = D.nt;
+    for (int t0 = 0; t0 < D.N; t0 += kFullTile) {
+        const int j = t0 + threadIdx.x;
+        if (j < D.N) { tp[threadIdx.x] = D.atom[j]; tm[threadIdx.x] = D.meta[j]; }
+        __syncthreads();
+        const int nj = min(kFullTile, D.N - t0);
+        if (valid) {
+            for (int jj = 0; jj < nj; ++jj) {
+                if (t0 + jj == i) continue;
+                const double4 pj = tp[jj];
+                const int2 mj = tm[jj];
+                const double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                if (r2 >= D.rmax2) continue;
+                const bool lj = mi.y > 0 && mj.y > 0;
+                const int off = lj ? (mi.y - 1) * nt + (mj.y - 1) : 0;
+                const double FR = pair_force_adjoint<double>(r2, D.xclb * pi.w * pj.w, lj, lj ? D.lj_sig6[off] : 0.0,
+                                                             lj ? D.lj_feps[off] : 0.0, D.alpha, mi.x == mj.x);
+                gx = gx + dx * FR; gy = gy + dy * FR; gz = gz + dz * FR;
+            }
+        }
+        __syncthreads();
+    }
+    if (valid) { fx[i] = gx; fy[i] = gy; fz[i] = gz; }
+}
+
+// k space (ForceKSpace_coulomb / _LJ, ForceKSpace.f90:59-302, over the signed entries): one
+// warp per atom, the lanes over the entries; sin/cos(k r) come from the atom's per-axis tables,
+// recomputed here instead of stored per atom and k.  Adds to fx/fy/fz.
+constexpr int kForceAtoms = 8;  // atoms (warps) per block
+
+template <int NT>
+__global__ void __launch_bounds__(32 * kForceAtoms) k_forces_kspace(DevSys D, double *fx, double *fy, double *fz) {
+    extern __shared__ double2 ftab[];  // [kForceAtoms][3][KM]
+    const int KM = D.kmax + 1;
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int i = blockIdx.x * kForceAtoms + w;
+    if (i >= D.N) return;
+    const double4 p = D.atom[i];
+    const int ta = D.meta[i].y;
+    double2 *T = ftab + (size_t)w * 3 * KM;
+    for (int idx = lane; idx < 3 * KM; idx += 32) {
+        const int d = idx / KM, m = idx % KM;
+        const double u = d == 0 ? p.x : (d == 1 ? p.y : p.z);
+        double sn, cs;
+        sincospi(2.0 * (double)m * u, &sn, &cs);
+        if (m == 0) { sn = 0.0; cs = 1.0; }
+        T[idx] = make_double2(cs, sn);
+    }
+    __syncwarp();
+    const double q = p.w, iq = q != 0.0 ? 1.0 / q : 0.0;
+    const int S = D.S;
+    double gx = 0, gy = 0, gz = 0;
+    for (int e = lane; e < S; e += 32) {
+        const int4 kv = D.kvec[e];
+        double c = 0, sn = 0;
+        double wgt = 0;
+        if (q != 0.0) {
+            entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, q, c, sn);
+            const double2 C = D.rho[e];
+            wgt = D.ebeta[e] * (C.x * sn - C.y * c);
+        }
+        if (ta > 0) {
+            double cl, sl;
+            if (q != 0.0) { cl = c * iq; sl = sn * iq; }
+            else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, 1.0, cl, sl);
+#pragma unroll
+            for (int t = 0; t < NT; ++t) {
+                int pr = 0;
+#pragma unroll
+                for (int u = 0; u < NT; ++u)
+                    if (u == ta - 1) pr = pair_idx<NT>(u, t);
+                const double2 Ct = D.rho[(size_t)(1 + t) * S + e];
+                wgt += D.ebetalj[(size_t)pr * S + e] * (Ct.x * sl - Ct.y * cl);
+            }
+        }
+        const double f = kFourPi * wgt;
+        gx = gx + f * kv.x; gy = gy + f * kv.y; gz = gz + f * kv.z;
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+        gx += __shfl_xor_sync(0xffffffffu, gx, o);
+        gy += __shfl_xor_sync(0xffffffffu, gy, o);
+        gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    }
+    if (lane == 0) { fx[i] += gx; fy[i] += gy; fz[i] += gz; }
+}
+
 // per-move API commit: rho += delta (Step 14, MC.f90:1245)
 __global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1365,6 +1467,7 @@ struct yamc_ctx {
     double api_dmu[3] = {};
     long long *d_prof = nullptr;
     bool prof_on = false;
+    double *d_gx = nullptr, *d_gy = nullptr, *d_gz = nullptr;  // adjoint forces
 };
 
 namespace {
@@ -1597,6 +1700,16 @@ void energies_from(const double *sc, double kext, double e[8]) {
 int ensure_cfg(yamc_ctx *c) {
     if (c->cfg.G) return YAMC_OK;
     return pick_launch(c, &c->cfg);
+}
+
+template <int NT>
+int launch_forces_kspace(yamc_ctx *c) {
+    const size_t sm = sizeof(double2) * kForceAtoms * 3 * (c->H.kmax + 1);
+    CUDA_TRY(cudaFuncSetAttribute(k_forces_kspace<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+    k_forces_kspace<NT><<<(c->H.N + kForceAtoms - 1) / kForceAtoms, 32 * kForceAtoms, sm, c->stream>>>(c->hsys, c->d_gx,
+                                                                                                      c->d_gy, c->d_gz);
+    CUDA_TRY(cudaGetLastError());
+    return YAMC_OK;
 }
 
 ChainArgs base_args(yamc_ctx *c, int mode) {
@@ -1878,7 +1991,7 @@ int yamc_destroy(yamc_ctx *c) {
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->uu, c->fx, c->fy,
                     c->fz, c->part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
-                    c->d_prof, c->spec};
+                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -2378,6 +2491,75 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     for (yamc_ctx *c : b->reps) c->pos_valid = false;
     if (best_moves_per_s) *best_moves_per_s = best;
     return r;
+}
+
+// ---------------------------------------------------------------- adjoint forces
+
+int yamc_forces(yamc_ctx *c, double *fx, double *fy, double *fz, double *mol_f, double *mol_tau) {
+    if (!c) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    HostSystem &H = c->H;
+    const int N = H.N;
+    int r;
+    if (!c->d_gx && ((r = dalloc(&c->d_gx, N)) || (r = dalloc(&c->d_gy, N)) || (r = dalloc(&c->d_gz, N)))) return r;
+    if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
+    k_forces_real<<<(N + kFullTile - 1) / kFullTile, kFullTile, 0, c->stream>>>(c->hsys, c->d_gx, c->d_gy, c->d_gz);
+    CUDA_TRY(cudaGetLastError());
+    switch (H.nt) {
+        case 1: r = launch_forces_kspace<1>(c); break;
+        case 2: r = launch_forces_kspace<2>(c); break;
+        case 3: r = launch_forces_kspace<3>(c); break;
+        default: r = launch_forces_kspace<4>(c); break;
+    }
+    if (r) return r;
+    std::vector<double> gx(N), gy(N), gz(N);
+    CUDA_TRY(cudaMemcpyAsync(gx.data(), c->d_gx, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(gy.data(), c->d_gy, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(gz.data(), c->d_gz, sizeof(double) * N, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    // external term: F = -2 kext q mu (EwaldSumExternal.f90:84-102)
+    const double mx = c->sc[SC_MU_X], my = c->sc[SC_MU_Y], mz = c->sc[SC_MU_Z], m2k = H.p.minus_two_kext;
+    for (int i = 0; i < N; ++i) {
+        gx[i] = gx[i] + m2k * H.q[i] * mx; gy[i] = gy[i] + m2k * H.q[i] * my; gz[i] = gz[i] + m2k * H.q[i] * mz;
+        if (fx) fx[i] = gx[i];
+        if (fy) fy[i] = gy[i];
+        if (fz) fz[i] = gz[i];
+    }
+    if (mol_f || mol_tau) {
+        for (int m = 0; m < H.M; ++m) {
+            const int a0 = H.first[m], na = H.natoms[m];
+            if (na > kMaxA) { set_error("molecule with more than 4 atoms"); return YAMC_ELIMITS; }
+            double x[kMaxA], y[kMaxA], z[kMaxA], ms[kMaxA], ax[kMaxA], ay[kMaxA], az[kMaxA], F[3], T[3];
+            for (int a = 0; a < na; ++a) {
+                x[a] = H.x[a0 + a]; y[a] = H.y[a0 + a]; z[a] = H.z[a0 + a]; ms[a] = H.mass[a0 + a];
+                ax[a] = gx[a0 + a]; ay[a] = gy[a0 + a]; az[a] = gz[a0 + a];
+            }
+            mol_force_torque(na, x, y, z, ms, ax, ay, az, F, T);
+            for (int k = 0; k < 3; ++k) {
+                if (mol_f) mol_f[3 * m + k] = F[k];
+                if (mol_tau) mol_tau[3 * m + k] = T[k];
+            }
+        }
+    }
+    return YAMC_OK;
+}
+
+int yamc_set_positions(yamc_ctx *c, const double *x, const double *y, const double *z, double e[8]) {
+    if (!c || !x || !y || !z) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
+    HostSystem &H = c->H;
+    std::vector<double4> a(H.N);
+    for (int i = 0; i < H.N; ++i) {
+        H.x[i] = x[i]; H.y[i] = y[i]; H.z[i] = z[i];
+        a[i] = make_double4(x[i], y[i], z[i], H.q[i]);
+    }
+    int r = upload(c->atom, a.data(), H.N, c->stream);
+    if (r) return r;
+    c->pos_valid = true;
+    if ((r = pull_state(c)) || (r = full_sums(c))) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (e) energies_from(c->sc, H.p.kext, e);
+    return YAMC_OK;
 }
 
 int yamc_phase_cycles(yamc_ctx *c, int32_t mode, int64_t *out, int32_t n) {
