@@ -179,6 +179,13 @@ int yamc_run_chain_device(yamc_ctx *ctx, const float *d_rng, int64_t n_rng, int6
                           int64_t n_moves, int64_t *moves_done, yamc_move_record *d_log,
                           double *d_rows, int32_t max_rows, int32_t *n_rows);
 
+/* Mixed form (params.precision = YAMC_MIXED): rho(k) and the k-space energies are
+   recomputed in FP64 from the positions after every `accepted_moves` accepted
+   moves (default 10000; 0 = never), bounding the drift of the running sums that
+   FP32 deltas update.  yamc_refresh_count returns how many refreshes ran. */
+int yamc_set_refresh(yamc_ctx *ctx, int64_t accepted_moves);
+int yamc_refresh_count(yamc_ctx *ctx, int64_t *count);
+
 /* ---- launch configuration and diagnostics ---- */
 /* Threads per block and blocks per cluster of the persistent chain kernel
    (0 = autotuned); takes effect on the next yamc_run_chain. */

@@ -89,6 +89,8 @@ SIGNATURES = {
     "yamc_run_chain_device": (ctypes.c_int, [_VP, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
                                              ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_int32, _ip]),
+    "yamc_set_refresh": (ctypes.c_int, [_VP, ctypes.c_int64]),
+    "yamc_refresh_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "yamc_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
     "yamc_set_kspace_layout": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_get_launch": (ctypes.c_int, [_VP, _ip]),

@@ -211,6 +211,16 @@ class Engine:
     def set_launch(self, cluster_blocks: int = 0, threads: int = 0) -> None:
         check(self.lib.yamc_set_launch(self.h, int(cluster_blocks), int(threads)), "yamc_set_launch")
 
+    def set_refresh(self, accepted_moves: int) -> None:
+        """Mixed form: FP64 recomputation of rho(k) every `accepted_moves` accepted moves."""
+        check(self.lib.yamc_set_refresh(self.h, int(accepted_moves)), "yamc_set_refresh")
+
+    @property
+    def refresh_count(self) -> int:
+        v = ctypes.c_int64(0)
+        check(self.lib.yamc_refresh_count(self.h, ctypes.byref(v)), "yamc_refresh_count")
+        return v.value
+
     def set_kspace_layout(self, layout: int) -> None:
         """_lib.YAMC_KSPACE_AUTO / _REGISTERS / _STREAMED"""
         check(self.lib.yamc_set_kspace_layout(self.h, int(layout)), "yamc_set_kspace_layout")

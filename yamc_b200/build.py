@@ -13,8 +13,9 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libyamc_b200.so")
-SOURCES = ["yamc_engine.cu", "yamc_static.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
-HEADERS = ["yamc_device.cuh", "yamc_internal.h", os.path.join("..", "..", "include", "yamc.h")]
+SOURCES = ["yamc_chain_t1.cu", "yamc_chain_t2.cu", "yamc_chain_t3.cu", "yamc_chain_t4.cu", "yamc_engine.cu",
+           "yamc_static.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
+HEADERS = ["yamc_chain.cuh", "yamc_device.cuh", "yamc_internal.h", os.path.join("..", "..", "include", "yamc.h")]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -41,15 +42,36 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
+    """Compile every source to an object in parallel (the chain kernel's variants sit in one
+    file per LJ type count), then link the shared library."""
     if not force and not stale():
         return LIB
-    cmd = [nvcc(), *NVCC_FLAGS, "-shared", "-o", LIB + ".tmp",
-           *[os.path.join(CSRC, s) for s in SOURCES], "-lcudart"]
-    res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
-    log = res.stdout + res.stderr
+    from concurrent.futures import ThreadPoolExecutor
+    objdir = os.path.join(HERE, "_build")
+    os.makedirs(objdir, exist_ok=True)
+
+    def compile_one(src):
+        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
+        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", obj, os.path.join(CSRC, src)]
+        res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+        return obj, cmd, res
+
+    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, SOURCES))
+    log = ""
+    failed = False
+    for obj, cmd, res in results:
+        log += " ".join(cmd) + "\n" + res.stdout + res.stderr
+        failed = failed or res.returncode != 0
+    if not failed:
+        cmd = [nvcc(), "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB + ".tmp",
+               *[obj for obj, _, _ in results], "-lcudart"]
+        res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
+        log += " ".join(cmd) + "\n" + res.stdout + res.stderr
+        failed = res.returncode != 0
     with open(os.path.join(HERE, "build.log"), "w") as f:
-        f.write(" ".join(cmd) + "\n" + log)
-    if res.returncode != 0:
+        f.write(log)
+    if failed:
         sys.stderr.write(log)
         raise RuntimeError("nvcc failed (see yamc_b200/build.log)")
     if verbose:

@@ -1,0 +1,1231 @@
+// The persistent chain kernel (run_mc + movemc on the device) and its launch helpers.
+// Included by the engine (types and declarations) and by one instantiation file per LJ type
+// count (yamc_chain_t1.cu .. yamc_chain_t4.cu), so the kernel variants compile in parallel.
+#pragma once
+
+#include <cooperative_groups.h>
+#include <cuda_pipeline.h>
+#include <cuda_runtime.h>
+
+#include <string>
+
+#include "yamc_device.cuh"
+#include "yamc_internal.h"
+
+#define CUDA_TRY(expr)                                                                        \
+    do {                                                                                      \
+        cudaError_t _e = (expr);                                                              \
+        if (_e != cudaSuccess) {                                                              \
+            yamc::set_error(std::string(#expr) + ": " + cudaGetErrorString(_e));              \
+            return YAMC_ECUDA;                                                                \
+        }                                                                                     \
+    } while (0)
+
+namespace yamc {
+
+namespace cg = cooperative_groups;
+
+struct LaunchCfg {
+    int G = 0, B = 0, EPT = 0;  // EPT: entries per worker in registers; 0 streamed; -1 streamed, 512 threads
+    int nown_max = 0, qcap = 0;
+    size_t smem = 0;
+};
+
+// ------------------------------------------------------------------------------------------
+// the chain kernel
+// ------------------------------------------------------------------------------------------
+// One thread-block cluster runs one Markov chain.  Warp 0 of every CTA is the control warp:
+// its lane 0 draws the random numbers, proposes moves and takes the Metropolis decision
+// (redundantly in every CTA, on identical data, so the CTAs agree without talking).  The
+// other warps are workers: they run the fused real-space + k-space pass of the current move
+// over the CTA's atoms and k-vector entries.  For unbiased moves the control warp prepares
+// the next move while the workers run the current pass: the next move starts either where the
+// current one ends after a hard-core overlap (no acceptance draw) or one draw later, and when
+// the next molecule is the one being moved its old positions depend on the decision, so lanes
+// 0-2 prepare the (at most) three candidates and the decision picks one.
+enum ChainMode { MODE_RUN = 0, MODE_OLD = 1, MODE_EVAL = 2 };
+
+// per-replica run control, in device memory
+struct RunSlot {
+    const float *rng;       // stream positions [rng_off, n_rng)
+    long long rng_off;
+    long long n_rng;
+    long long cursor;       // in: start cursor; out: cursor after the last completed move
+    long long n_moves;      // moves requested
+    long long moves_done;   // out
+    yamc_move_record *log;  // optional, n_moves records
+    double *rows;           // optional energy rows (9 doubles)
+    int max_rows, n_rows;
+    int status, accepted;
+    long long acc_limit;    // > 0: return after this many accepted moves (the mixed form's rho refresh)
+};
+
+struct ChainArgs {
+    const DevSys *sys;  // [R]
+    RunSlot *run;       // [R]
+    int G;              // CTAs per chain (cluster size)
+    int mode;
+    int nown_max;       // atoms staged per CTA (interleaved ownership: atom j lives in CTA j % G)
+    int qcap;           // pair queue capacity per CTA
+    // per-move API (R == 1): imol (1-based) and proposed positions in, results out
+    const double *api_in;  // [0] imol, [1 + 3a + c] coordinate c of atom a
+    double *api_out;       // the reduction vector of the pass (RV_* layout)
+    double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas
+    long long *prof;       // optional per-phase cycle counters (PH_* layout), CTA 0
+};
+
+// phases timed when ChainArgs::prof is set (control lane 0 or worker thread 32 of CTA 0)
+enum Phase { PH_CHOOSE = 0, PH_SPECULATE, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE,
+             PH_CLUSTER, PH_DECIDE, PH_COMMIT, PH_COUNT };
+
+// reduction vector of one pass
+constexpr int RV_EW = 0, RV_LJ6 = 1, RV_LJ12 = 2, RV_DUC = 3, RV_DUL = 4, RV_OVL = 5, RV_F = 6;
+constexpr int kNV = 6 + 3 * kMaxA;
+
+enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
+
+struct Slot { double x, y, z, q, iq, dhs; int type, pad; };
+constexpr int kMaxSpecies = 8;
+constexpr int kCPT = 4;   // atoms each worker thread tests per filter round
+constexpr int kWin = 256; // random-stream window held in shared memory
+constexpr int kCtl = 32;  // threads of the control warp
+constexpr int kChainMaxThreads = 256;  // one CTA per SM, up to 255 registers per thread
+constexpr int kChainMaxThreadsWide = 512;  // streamed k entries, 16 warps, up to 128 registers per thread
+
+// a prepared move: the molecule, its atoms at the old and proposed positions, the proposal
+struct Cand {
+    int valid, imol, first, na;
+    long long cur_start;  // stream position at the start of the move
+    long long cur_prop;   // stream position after the proposal
+    double mu_old[3];     // dipole of the molecule at the old positions
+    Slot slot[2 * kMaxA]; // [0, na): proposed positions, [na, 2na): old positions
+    double mass[kMaxA];
+    MoveState mv;
+};
+
+struct ChainShared {
+    Cand cand[4];         // the move being evaluated (cand[icur]) and up to three prepared next moves
+    int icur;             // buffer of the move being evaluated
+    int spec[3];          // buffers of the candidates: after an overlap / after a draw / accepted same molecule
+    int abort, accepted, overlap, last_mol, spec_ok;
+    long long cursor;     // stream position after the last completed move
+    long long icycle, mic;
+    double eold[3], fold[3 * kMaxA];
+    double sc[SC_COUNT];
+    double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (staged copies may lag in other CTAs)
+    int qcount;
+    int wcount[64];       // per-warp pair counts and their exclusive prefix
+    double tot[kNV];
+    double du[4];
+    int flags;
+    // molecule species (runs of identical consecutive molecules): first molecule, count, atoms, first atom
+    int nspec;
+    int sp_m0[kMaxSpecies], sp_cnt[kMaxSpecies], sp_na[kMaxSpecies], sp_a0[kMaxSpecies];
+    Slot sp_atom[kMaxSpecies][kMaxA];
+    double sp_mass[kMaxSpecies][kMaxA];
+    // two windows of the random stream
+    long long wbase[2];
+    int wn[2];
+    int wnext;
+};
+
+__device__ __forceinline__ void worker_sync(int nwork) {
+    asm volatile("bar.sync 1, %0;" ::"r"(nwork) : "memory");
+}
+
+template <int I>
+struct IntC { static constexpr int value = I; };
+
+// calls f(IntC<I>) for I in [B, E): loop indices known at compile time
+template <int B, int E, class F>
+__device__ __forceinline__ void static_for(F &&f) {
+    if constexpr (B < E) {
+        f(IntC<B>{});
+        static_for<B + 1, E>(f);
+    }
+}
+
+template <int NT>
+struct NPair { static constexpr int value = NT * (NT + 1) / 2; };
+
+// row of the packed upper triangle t1 <= t2 (the host's pair_index enumeration)
+template <int NT>
+__host__ __device__ constexpr int pair_idx(int a, int b) {
+    return a <= b ? a * NT - a * (a - 1) / 2 + (b - a) : b * NT - b * (b - 1) / 2 + (a - b);
+}
+
+// Arithmetic of a pass: MX = false is the plain FP64 method; MX = true the mixed form (pair
+// terms, erfc_Luc, phases and per-thread sums in FP32; rho(k), the cross-warp and cross-CTA
+// sums, the energy bookkeeping and the Metropolis test in FP64).
+template <bool MX> struct Prec { using R = double; using R2 = double2; };
+template <> struct Prec<true> { using R = float; using R2 = float2; };
+
+__device__ __forceinline__ double2 mk2(double x, double y) { return make_double2(x, y); }
+__device__ __forceinline__ float2 mk2(float x, float y) { return make_float2(x, y); }
+template <class R2> __device__ __forceinline__ R2 cvt2(double2 v);
+template <> __device__ __forceinline__ double2 cvt2<double2>(double2 v) { return v; }
+template <> __device__ __forceinline__ float2 cvt2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+__device__ __forceinline__ double2 to_d2(double2 v) { return v; }
+__device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
+
+// Per-thread partial sums of a pass: FP64; in the mixed form FP64 for the pair terms (which
+// reach tens of kT) and FP32 with two-sum compensation (the running sum and its rounding
+// error, added in FP64 when the warp reduces) for the FP32 k-space terms.
+template <bool MX>
+struct Acc {
+    double v[kNV];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < kNV; ++i) v[i] = 0.0;
+    }
+    __device__ __forceinline__ void add(int i, double x) { v[i] += x; }
+    __device__ __forceinline__ void flag(int i) { v[i] = 1.0; }
+    __device__ __forceinline__ double get(int i) const { return v[i]; }
+};
+template <>
+struct Acc<true> {
+    double d[kNV];
+    float s[kNV], c[kNV];
+    __device__ __forceinline__ void zero() {
+#pragma unroll
+        for (int i = 0; i < kNV; ++i) { d[i] = 0.0; s[i] = 0.f; c[i] = 0.f; }
+    }
+    __device__ __forceinline__ void add(int i, double x) { d[i] += x; }
+    __device__ __forceinline__ void add(int i, float x) {  // TwoSum (Knuth)
+        const float t = s[i] + x;
+        const float bp = t - s[i];
+        c[i] += (s[i] - (t - bp)) + (x - bp);
+        s[i] = t;
+    }
+    __device__ __forceinline__ void flag(int i) { d[i] = 1.0; }
+    __device__ __forceinline__ double get(int i) const { return d[i] + ((double)s[i] + (double)c[i]); }
+};
+
+template <int NT, int EPT, bool MX = false>
+struct EntryRegs {
+    using R = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+    int e[EPT];
+    int kx[EPT], ky[EPT], kz[EPT];
+    R beta[EPT];
+    R bl[EPT][NPair<NT>::value];  // beta_LJ of every type pair for this entry
+    double2 rho[EPT][1 + NT];     // FP64 in both forms
+    R2 mold[EPT][1 + NT];
+    R2 dl[EPT][1 + NT];
+};
+
+// EPT <= 0: the streamed layout (EPT == -1: the same with 512-thread CTAs) -- no entry lives in
+// registers; each worker loops over its entries and reads k, beta, beta_LJ and rho from memory
+// (L2-resident) every pass.  The register block of one (never touched) entry only keeps the
+// code uniform.
+template <int NT, int EPT, bool MX = false>
+using RegsOf = EntryRegs<NT, (EPT > 0 ? EPT : 1), MX>;
+
+// Phase tables of slots [s0, s1) of move m: T[slot][axis][k] = (cos, sin)(2 pi k u), by the
+// workers.  The FP32 form reduces 2 k u modulo 2 in FP64 before the FP32 sincospi.
+template <bool MX>
+__device__ __forceinline__ void build_tables(typename Prec<MX>::R2 *tab, const Cand &m, int s0, int s1, int KM, int wtid,
+                                             int nwork) {
+    using R = typename Prec<MX>::R;
+    const int n = (s1 - s0) * 3 * KM;
+    for (int idx = wtid; idx < n; idx += nwork) {
+        const int sl = s0 + idx / (3 * KM), r = idx % (3 * KM), d = r / KM, k = r % KM;
+        const double u = d == 0 ? m.slot[sl].x : (d == 1 ? m.slot[sl].y : m.slot[sl].z);
+        R s, c;
+        if constexpr (MX) {
+            double t = 2.0 * (double)k * u;
+            t = t - 2.0 * rint(0.5 * t);
+            sincospif((float)t, &s, &c);
+        } else {
+            sincospi(2.0 * (double)k * u, &s, &c);
+        }
+        if (k == 0) { s = R(0); c = R(1); }
+        tab[(sl * 3 + d) * KM + k] = mk2(c, s);
+    }
+}
+
+// Molecule phase sums of one entry over slots [s0, s0+na) -- RhoSquared_addAtom per atom:
+// Coulomb phase q (cos, sin), LJ phase = Coulomb phase * (1/q) (the unit phase when q == 0),
+// accumulated per LJ type in atom order.  ph/phl keep the per-atom phases for the forces.
+template <int NT, bool MX>
+__device__ __forceinline__ void mol_phase_sum(const typename Prec<MX>::R2 *tab, const Cand &m, int s0, int na, int KM,
+                                              int kx, int ky, int kz, typename Prec<MX>::R2 (&out)[1 + NT],
+                                              typename Prec<MX>::R2 (&ph)[kMaxA], typename Prec<MX>::R2 (&phl)[kMaxA]) {
+    using R = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+#pragma unroll
+    for (int t = 0; t <= NT; ++t) out[t] = mk2(R(0), R(0));
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        ph[a] = mk2(R(0), R(0));
+        phl[a] = mk2(R(0), R(0));
+        if (a < na) {
+            const Slot &sl = m.slot[s0 + a];
+            const R2 *T = tab + (size_t)(s0 + a) * 3 * KM;
+            const R q = (R)sl.q;
+            R c = 0, s = 0;
+            if (sl.q != 0.0) {
+                entry_phase<R, R2>(T, T + KM, T + 2 * KM, kx, ky, kz, q, c, s);
+                out[0].x = out[0].x + c; out[0].y = out[0].y + s;
+            }
+            ph[a] = mk2(c, s);
+            if (sl.type > 0) {
+                R cl, sl2;
+                if (sl.q != 0.0) { const R iq = (R)sl.iq; cl = c * iq; sl2 = s * iq; }
+                else entry_phase<R, R2>(T, T + KM, T + 2 * KM, kx, ky, kz, R(1), cl, sl2);
+#pragma unroll
+                for (int t = 0; t < NT; ++t)
+                    if (t == sl.type - 1) { out[1 + t].x = out[1 + t].x + cl; out[1 + t].y = out[1 + t].y + sl2; }
+                phl[a] = mk2(cl, sl2);
+            }
+        }
+    }
+}
+
+// k-space force on the molecule's atoms from one entry: 4 pi beta (C sin - S cos) k per atom,
+// Coulomb with the q-weighted phase, plus the dispersion terms of the atom's LJ type against
+// every type's structure factor (ForceKSpace.f90:59-302).
+template <int NT, bool MX>
+__device__ __forceinline__ void entry_forces(const Cand &m, int s0, int na, int kx, int ky, int kz,
+                                             typename Prec<MX>::R beta,
+                                             const typename Prec<MX>::R (&bl)[NPair<NT>::value],
+                                             const typename Prec<MX>::R2 (&C)[1 + NT],
+                                             const typename Prec<MX>::R2 (&ph)[kMaxA],
+                                             const typename Prec<MX>::R2 (&phl)[kMaxA], Acc<MX> &acc) {
+    using R = typename Prec<MX>::R;
+    const R fourpi = (R)kFourPi;
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        if (a < na) {
+            const int ta = m.slot[s0 + a].type;
+            R w = fourpi * ((C[0].x * ph[a].y - C[0].y * ph[a].x) * beta);
+            if (ta > 0) {
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    R b = R(0);
+#pragma unroll
+                    for (int u = 0; u < NT; ++u)
+                        if (u == ta - 1) b = bl[pair_idx<NT>(u, t)];
+                    w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * b);
+                }
+            }
+            acc.add(RV_F + 3 * a, w * (R)kx);
+            acc.add(RV_F + 3 * a + 1, w * (R)ky);
+            acc.add(RV_F + 3 * a + 2, w * (R)kz);
+        }
+    }
+}
+
+// One signed entry of a pass: the molecule's phase sums at the old positions (into mold) and/or
+// the new ones, the delta (into dl), dU_k Coulomb + LJ against rho, and the k-space forces.
+template <int NT, int KIND, bool FORCES, bool MX>
+__device__ __forceinline__ void kspace_entry(const typename Prec<MX>::R2 *tab, const Cand &m, int na, int KM, int kx,
+                                             int ky, int kz, typename Prec<MX>::R beta,
+                                             const typename Prec<MX>::R (&bl)[NPair<NT>::value],
+                                             const double2 (&rho)[1 + NT], typename Prec<MX>::R2 (&mold)[1 + NT],
+                                             typename Prec<MX>::R2 (&dl)[1 + NT], Acc<MX> &acc) {
+    using R = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+    R2 ph[kMaxA], phl[kMaxA];
+    R2 C[1 + NT];
+#pragma unroll
+    for (int t = 0; t <= NT; ++t) C[t] = cvt2<R2>(rho[t]);
+    if constexpr (KIND != PASS_NEW) mol_phase_sum<NT, MX>(tab, m, na, na, KM, kx, ky, kz, mold, ph, phl);
+    if constexpr (KIND == PASS_OLD) {
+        if constexpr (FORCES) entry_forces<NT, MX>(m, na, na, kx, ky, kz, beta, bl, C, ph, phl, acc);
+    } else {
+        R2 mnew[1 + NT];
+        mol_phase_sum<NT, MX>(tab, m, 0, na, KM, kx, ky, kz, mnew, ph, phl);
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) dl[t] = mk2(mnew[t].x - mold[t].x, mnew[t].y - mold[t].y);
+        {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
+            const R2 Cc = C[0], d = dl[0];
+            acc.add(RV_DUC, (((Cc.x + Cc.x) + d.x) * d.x + ((Cc.y + Cc.y) + d.y) * d.y) * beta);
+        }
+        // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
+        // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
+#pragma unroll
+        for (int t1 = 0; t1 < NT; ++t1) {
+            const R2 C1 = C[1 + t1], D1 = dl[1 + t1];
+            const R tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
+#pragma unroll
+            for (int t2 = 0; t2 < NT; ++t2) {
+                const R2 D2 = dl[1 + t2];
+                if (D2.x == R(0) && D2.y == R(0)) continue;
+                acc.add(RV_DUL, (tc * D2.x + ts * D2.y) * bl[pair_idx<NT>(t1, t2)]);
+            }
+        }
+        if constexpr (KIND == PASS_NEW && FORCES) {  // against total_new = rho + delta (MC.f90:1136-1163)
+            R2 Cn[1 + NT];
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) Cn[t] = mk2(C[t].x + dl[t].x, C[t].y + dl[t].y);
+            entry_forces<NT, MX>(m, 0, na, kx, ky, kz, beta, bl, Cn, ph, phl, acc);
+        }
+    }
+}
+
+// The workers' part of one pass over the molecule's slots: k-space over their entries, real
+// space over the CTA's atoms (pairs inside the cutoff laid out in the queue by a prefix sum
+// over threads -- a deterministic order -- then evaluated item i by worker i % nwork), and a
+// per-warp reduction into red[worker warp][value].  Worker-only barriers (bar 1).
+template <int NT, int EPT, int KIND, bool FORCES, bool MX>
+__device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
+                                            const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue,
+                                            int *nearbuf,
+                                            double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
+                                            long long *prof) {
+    constexpr int NVMAX = FORCES ? kNV : RV_F;
+    const Cand &m = sh.cand[sh.icur];
+    const int na = m.na;
+    const int KM = D.kmax + 1;
+    const int nt = D.nt;
+    const int imol0 = m.imol - 1;
+    const int nwork = blockDim.x - kCtl;
+    const int wtid = threadIdx.x - kCtl;
+    const int lane = threadIdx.x & 31;
+    const int wwarp = wtid >> 5, nww = nwork >> 5;
+    const int s_lo = (KIND == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
+    const int s_hi = (KIND == PASS_NEW) ? na : 2 * na;
+    using Rt = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+    R2 *tab = reinterpret_cast<R2 *>(tab_raw);
+    const bool pf = prof && wtid == 0;
+    long long t_mark = pf ? clock64() : 0;
+#define YAMC_WPH(ph) do { if (pf) { const long long t_now = clock64(); prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+
+    build_tables<MX>(tab, m, s_lo, s_hi, KM, wtid, nwork);
+    worker_sync(nwork);
+    YAMC_WPH(PH_TABLES);
+
+    Acc<MX> acc;
+    acc.zero();
+
+    if constexpr (EPT > 0) {
+        static_for<0, EPT>([&](auto kc) {
+            constexpr int k = decltype(kc)::value;
+            if (R.e[k] < 0) return;
+            kspace_entry<NT, KIND, FORCES, MX>(tab, m, na, KM, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k],
+                                               R.mold[k], R.dl[k], acc);
+        });
+    } else {
+        // streamed layout: entries e0, e0 + estep, ... read from memory, the next entry's loads in
+        // flight while the current one computes; the old sums and the deltas go to the chain's
+        // scratch for the next pass and the commit
+        const int S = D.S;
+        double2 *mold_g = D.scratch;
+        double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
+        int4 kv_n = make_int4(0, 0, 0, 0);
+        Rt beta_n = Rt(0), bl_n[NPair<NT>::value];
+        double2 rho_n[1 + NT];
+        R2 mold_n[1 + NT];
+        auto fetch = [&](int e) {
+            kv_n = D.kvec[e];
+            beta_n = (Rt)D.ebeta[e];
+#pragma unroll
+            for (int p = 0; p < NPair<NT>::value; ++p) bl_n[p] = (Rt)D.ebetalj[(size_t)p * S + e];
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) {
+                rho_n[t] = D.rho[(size_t)t * S + e];
+                mold_n[t] = (KIND == PASS_NEW) ? cvt2<R2>(mold_g[(size_t)t * S + e]) : mk2(Rt(0), Rt(0));
+            }
+        };
+        if (e0 < S) fetch(e0);
+        for (int e = e0; e < S; e += estep) {
+            const int kx = kv_n.x, ky = kv_n.y, kz = kv_n.z;
+            const Rt beta = beta_n;
+            Rt bl[NPair<NT>::value];
+            double2 rho[1 + NT];
+            R2 mold[1 + NT], dl[1 + NT];
+#pragma unroll
+            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = bl_n[p];
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) { rho[t] = rho_n[t]; mold[t] = mold_n[t]; }
+            if (e + estep < S) fetch(e + estep);
+            kspace_entry<NT, KIND, FORCES, MX>(tab, m, na, KM, kx, ky, kz, beta, bl, rho, mold, dl, acc);
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) {
+                if (KIND == PASS_OLD) mold_g[(size_t)t * S + e] = to_d2(mold[t]);
+                else dl_g[(size_t)t * S + e] = to_d2(dl[t]);
+            }
+        }
+    }
+    YAMC_WPH(PH_KSPACE);
+
+    // bounding spheres of the molecule at its new (slot 0) and old (slot na) positions: an atom
+    // farther than rpre + radius from a centre is outside the cutoff and every hard core of all
+    // that position's slots (triangle inequality on the periodic box), so its slot tests are skipped
+    double rp2;
+    {
+        double rad2 = 0.0;
+        for (int a = 1; a < na; ++a) {
+            const double dx = m.slot[a].x - m.slot[0].x, dy = m.slot[a].y - m.slot[0].y, dz = m.slot[a].z - m.slot[0].z;
+            rad2 = fmax(rad2, dx * dx + dy * dy + dz * dz);
+            const double ex = m.slot[na + a].x - m.slot[na].x, ey = m.slot[na + a].y - m.slot[na].y,
+                         ez = m.slot[na + a].z - m.slot[na].z;
+            rad2 = fmax(rad2, ex * ex + ey * ey + ez * ez);
+        }
+        const double rp = (D.rpre + sqrt(rad2)) * (1.0 + 1e-9);
+        rp2 = rp * rp;
+    }
+    const double cnx = m.slot[0].x, cny = m.slot[0].y, cnz = m.slot[0].z;
+    const double cox = m.slot[na].x, coy = m.slot[na].y, coz = m.slot[na].z;
+
+    const int round_atoms = nwork * kCPT;
+    int *nb = nearbuf + wwarp * 32 * kCPT;  // this warp's near atoms of the round
+    for (int c0 = 0; c0 < nown; c0 += round_atoms) {
+        // near atoms of the warp's 32 x kCPT candidates, compacted in (c, lane) order
+        int nnear = 0;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            const int jl = c0 + c * nwork + wtid;
+            bool near = false;
+            if (jl < nown && meta_s[jl].x != imol0) {
+                const double4 pj = atom_s[jl];
+                if (KIND != PASS_OLD) {
+                    const double dx = min_image(cnx - pj.x), dy = min_image(cny - pj.y), dz = min_image(cnz - pj.z);
+                    near = dx * dx + dy * dy + dz * dz < rp2;
+                }
+                if (KIND != PASS_NEW) {
+                    const double dx = min_image(cox - pj.x), dy = min_image(coy - pj.y), dz = min_image(coz - pj.z);
+                    near = near || dx * dx + dy * dy + dz * dz < rp2;
+                }
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, near);
+            if (near) nb[nnear + __popc(bal & ((1u << lane) - 1u))] = jl;
+            nnear += __popc(bal);
+        }
+        __syncwarp();
+        // slot tests of the near atoms, densely: lane takes entries lane, lane + 32, ...
+        unsigned masks = 0;  // kCPT slot masks of 8 bits
+        int count = 0;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            const int k = c * 32 + lane;
+            if (k < nnear) {
+                const int jl = nb[k];
+                const double4 pj = atom_s[jl];
+                const int tj = meta_s[jl].y;
+                const double dj = dhs_s[jl];
+                unsigned msk = 0;
+                for (int s = s_lo; s < s_hi; ++s) {
+                    const Slot &sl = m.slot[s];
+                    const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (KIND != PASS_OLD && s < na && sl.type > 0 && tj > 0) {  // hard core (EwaldSumRealSpace.f90:409)
+                        const double d12 = (sl.dhs + dj) / 2;
+                        if (r2 < d12 * d12) acc.flag(RV_OVL);
+                    }
+                    if (r2 < D.rmax2) msk |= 1u << s;
+                }
+                masks |= msk << (8 * c);
+                count += __popc(msk);
+            }
+        }
+        int incl = count;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= o) incl += y;
+        }
+        if (lane == 31) sh.wcount[wwarp] = incl;
+        worker_sync(nwork);
+        if (wwarp == 0) {
+            const int v = lane < nww ? sh.wcount[lane] : 0;
+            int x = v;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const int y = __shfl_up_sync(0xffffffffu, x, o);
+                if (lane >= o) x += y;
+            }
+            if (lane < nww) sh.wcount[32 + lane] = x - v;
+            if (lane == 31) sh.qcount = x;
+        }
+        worker_sync(nwork);
+        int pos = sh.wcount[32 + wwarp] + incl - count;
+#pragma unroll
+        for (int c = 0; c < kCPT; ++c) {
+            unsigned msk = (masks >> (8 * c)) & 0xffu;
+            const int jl = msk ? nb[c * 32 + lane] : 0;
+            while (msk) {
+                const int s = __ffs(msk) - 1;
+                msk &= msk - 1;
+                queue[pos++] = (jl << 3) | s;
+            }
+        }
+        worker_sync(nwork);
+        YAMC_WPH(PH_FILTER);
+        const int nq = sh.qcount;
+        for (int qi = wtid; qi < nq; qi += nwork) {
+            const int item = queue[qi];
+            const int jl = item >> 3, s = item & 7;
+            const Slot &sl = m.slot[s];
+            const double4 pj = atom_s[jl];
+            const int tj = meta_s[jl].y;
+            const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const bool lj = sl.type > 0 && tj > 0;
+            const int off = lj ? (sl.type - 1) * nt + (tj - 1) : 0;
+            const double qq = D.xclb * sl.q * pj.w;
+            const double s6 = lj ? lj_s[off] : 0.0, fe = lj ? lj_s[nt * nt + off] : 0.0;
+            const bool isnew = s < na;
+            const double sign = (KIND == PASS_BOTH && !isnew) ? -1.0 : 1.0;
+            const PairTerm<double> t = MX ? pair_term_mx<FORCES>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false)
+                                          : pair_term<double, FORCES>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
+            acc.add(RV_EW, sign * t.ew); acc.add(RV_LJ6, sign * t.lj6); acc.add(RV_LJ12, sign * t.lj12);
+            if constexpr (FORCES) {
+                const int a = isnew ? s : s - na;
+#pragma unroll
+                for (int aa = 0; aa < kMaxA; ++aa)
+                    if (aa == a) {
+                        acc.add(RV_F + 3 * aa, dx * t.FR);
+                        acc.add(RV_F + 3 * aa + 1, dy * t.FR);
+                        acc.add(RV_F + 3 * aa + 2, dz * t.FR);
+                    }
+            }
+        }
+        worker_sync(nwork);
+        YAMC_WPH(PH_PAIRS);
+    }
+
+    // per-warp reduction (xor tree) into red[worker warp][value]
+    const int nv = FORCES ? (RV_F + 3 * na) : RV_F;
+#pragma unroll
+    for (int v = 0; v < NVMAX; ++v) {
+        if (v < nv) {
+            double x = acc.get(v);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = (v == RV_OVL) ? fmax(x, y) : x + y;
+            }
+            if (lane == 0) red[wwarp * kNV + v] = x;
+        }
+    }
+#undef YAMC_WPH
+}
+
+// Control warp, after the workers' per-warp partials: trees over the worker warps, then over the
+// cluster's CTAs in a fixed order, so every CTA holds bit-identical totals in sh.tot.  Called by
+// all threads (the cluster barrier needs everyone).
+__device__ __forceinline__ void reduce_pass(ChainShared &sh, const double *red, double *xch, int nv, int G, int rank,
+                                            int xpar, cg::cluster_group &cluster) {
+    const int lane = threadIdx.x & 31;
+    const int nww = (blockDim.x - kCtl) >> 5;
+    if (threadIdx.x < kCtl) {
+        for (int v = 0; v < nv; ++v) {
+            double x = lane < nww ? red[lane * kNV + v] : 0.0;
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                x = (v == RV_OVL) ? fmax(x, y) : x + y;
+            }
+            if (G > 1) {
+                if (lane < G) {
+                    double *dst = cluster.map_shared_rank(xch, lane);
+                    dst[(xpar * G + rank) * kNV + v] = x;
+                }
+            } else if (lane == 0) {
+                sh.tot[v] = x;
+            }
+        }
+    }
+    if (G > 1) {
+        cluster.sync();
+        if (threadIdx.x < kCtl) {
+            for (int v = 0; v < nv; ++v) {
+                double x = lane < G ? xch[(xpar * G + lane) * kNV + v] : 0.0;
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double y = __shfl_xor_sync(0xffffffffu, x, o);
+                    x = (v == RV_OVL) ? fmax(x, y) : x + y;
+                }
+                if (lane == 0) sh.tot[v] = x;
+            }
+        }
+    }
+}
+
+// Control lane work: molecule choice (run_mc draws) and the static atom data of the chosen
+// molecule at its current positions.  `moving` is the molecule of the move in flight (0-based,
+// -1 if none) whose positions come from `moving_pos` (its old or its proposed positions).
+struct ChooseCtx {
+    const DevSys *D;
+    const RunSlot *run;
+    const float *w0, *w1;
+    const double4 *atom_s;
+    int G;
+};
+
+__device__ inline RngReader make_reader(const ChooseCtx &X, const ChainShared &sh, long long cur) {
+    return RngReader{X.run->rng, X.run->rng_off, X.run->n_rng, cur, 0, X.w0, sh.wbase[0], sh.wn[0],
+                     X.w1, sh.wbase[1], sh.wn[1]};
+}
+
+__device__ inline void stage_molecule(const ChooseCtx &X, ChainShared &sh, Cand &C, int imol, int moving,
+                                      const Slot *moving_pos, cg::cluster_group &cluster) {
+    const DevSys &D = *X.D;
+    int sp = -1;
+    for (int q = 0; q < sh.nspec; ++q)
+        if (imol - 1 >= sh.sp_m0[q] && imol - 1 < sh.sp_m0[q] + sh.sp_cnt[q]) { sp = q; break; }
+    int first, nam;
+    if (sp >= 0) { nam = sh.sp_na[sp]; first = sh.sp_a0[sp] + (imol - 1 - sh.sp_m0[sp]) * nam; }
+    else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
+    C.imol = imol; C.first = first; C.na = nam;
+    double mx = 0, my = 0, mz = 0;
+    for (int a = 0; a < nam; ++a) {
+        const int j = first + a;
+        Slot s;
+        if (sp >= 0) { s = sh.sp_atom[sp][a]; C.mass[a] = sh.sp_mass[sp][a]; }
+        else {
+            const double q = D.atom[j].w;
+            s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y; s.pad = 0;
+            C.mass[a] = D.mass[j];
+        }
+        if (imol - 1 == moving) { s.x = moving_pos[a].x; s.y = moving_pos[a].y; s.z = moving_pos[a].z; }
+        else if (imol - 1 == sh.last_mol) { s.x = sh.lx[a]; s.y = sh.ly[a]; s.z = sh.lz[a]; }
+        else {
+            const double4 *src = (X.G > 1) ? cluster.map_shared_rank(X.atom_s, j % X.G) : X.atom_s;
+            const double4 p = src[j / X.G];
+            s.x = p.x; s.y = p.y; s.z = p.z;
+        }
+        C.slot[nam + a] = s;  // old positions
+        C.slot[a] = s;        // proposed positions, replaced by propose()
+        // dipole of the molecule at the old positions (EwaldSumExternal_calc_mu)
+        mx = mx + s.q * s.x; my = my + s.q * s.y; mz = mz + s.q * s.z;
+    }
+    C.mu_old[0] = mx; C.mu_old[1] = my; C.mu_old[2] = mz;
+}
+
+// run_mc's draws before movemc: the per-cycle pressure draw, the exchange draw, the molecule
+// draw (runmc.f90:206, 232, 258).  Returns the 1-based molecule, or 0 when the stream ran out.
+__device__ inline int draw_molecule(const DevSys &D, RngReader &rng, bool cycle_start) {
+    if (cycle_start) (void)rng.next();
+    (void)rng.next();
+    const double r = rng.next();
+    if (rng.out) return 0;
+    return choose_molecule_guess(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
+}
+
+// movemc Step 5 (MC.f90:1031-1067) for a staged molecule; F/T are the old molecular force and
+// torque (zero for unbiased moves)
+__device__ inline void propose(const DevSys &D, Cand &C, RngReader &rng, const double F[3], const double T[3]) {
+    const int na = C.na;
+    MoveState &m = C.mv;
+    mcm_init_old(m, F, T);
+    mcm_choose_displacement(m, rng, D.xlf, D.dr);
+    if (!rng.out) mcm_choose_rotation(m, rng, D.xlc, D.d_angle);
+    double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        const Slot &o = C.slot[a < na ? na + a : na];
+        xo[a] = o.x; yo[a] = o.y; zo[a] = o.z;
+    }
+    place_molecule(m, na, xo, yo, zo, C.mass, xn, yn, zn);
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a)
+        if (a < na) { C.slot[a].x = xn[a]; C.slot[a].y = yn[a]; C.slot[a].z = zn[a]; }
+}
+
+// SPLIT = false: unbiased device-resident chain only (one fused pass per move, speculation);
+// SPLIT = true: force-biased moves and the per-move API (old pass + new pass with forces).
+template <int NT, int EPT, bool SPLIT, bool MX>
+__global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThreads, 1) k_chain(ChainArgs A) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ ChainShared sh;
+    __shared__ float rwin[2][kWin];
+
+    cg::cluster_group cluster = cg::this_cluster();
+    const int G = A.G;
+    const int rank = G > 1 ? (int)cluster.block_rank() : 0;
+    const int rep = blockIdx.x / G;
+    const DevSys D = A.sys[rep];
+    RunSlot *run = A.run + rep;
+    const int B = blockDim.x;
+    const int tid = threadIdx.x;
+    const int KM = D.kmax + 1;
+    const int S = D.S;
+    const int nt = D.nt;
+    const int nwork = B - kCtl;
+    const int wtid = tid - kCtl;
+    const bool ctl = tid < kCtl;
+    const int lane = tid & 31;
+
+    // shared memory carve-up (chain_smem_bytes on the host computes the same sizes)
+    double2 *tab = reinterpret_cast<double2 *>(smem_raw);                     // [2 kMaxA][3][KM]
+    double4 *atom_s = reinterpret_cast<double4 *>(tab + 2 * kMaxA * 3 * KM);  // [nown_max]
+    double *dhs_s = reinterpret_cast<double *>(atom_s + A.nown_max);          // [nown_max]
+    int2 *meta_s = reinterpret_cast<int2 *>(dhs_s + A.nown_max);              // [nown_max]
+    int *queue = reinterpret_cast<int *>(meta_s + A.nown_max);                // [qcap]
+    int *nearbuf = queue + ((A.qcap + 1) & ~1);                               // [B/32][32 kCPT]
+    double *red = reinterpret_cast<double *>(nearbuf + B * kCPT);             // [B/32][kNV]
+    double *xch = red + (B / 32) * kNV;                                       // [2][G][kNV]
+    double *lj_s = xch + 2 * G * kNV;                                         // [2][nt*nt]
+
+    // atoms of this CTA: j = rank + G * local (interleaved, so every CTA holds a spatial mix)
+    const int nown = (D.N - rank + G - 1) / G;
+    for (int i = tid; i < nown; i += B) {
+        const int j = rank + G * i;
+        atom_s[i] = D.atom[j]; dhs_s[i] = D.dhs[j]; meta_s[i] = D.meta[j];
+    }
+    for (int i = tid; i < nt * nt; i += B) { lj_s[i] = D.lj_sig6[i]; lj_s[nt * nt + i] = D.lj_feps[i]; }
+
+    // the workers' k-vector entries; rho stays in registers for the whole launch
+    using Rt = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+    RegsOf<NT, EPT, MX> R;
+    const int gwork = G * nwork;
+    const int e0 = rank * nwork + wtid;  // this worker's entries: e0 + k * gwork
+#pragma unroll
+    for (int k = 0; k < EPT; ++k) {
+        const int e = ctl ? S : rank * nwork + wtid + k * gwork;
+        R.e[k] = e < S ? e : -1;
+        R.kx[k] = R.ky[k] = R.kz[k] = 0;
+        R.beta[k] = 0;
+        if (e < S) {
+            const int4 kv = D.kvec[e];
+            R.kx[k] = kv.x; R.ky[k] = kv.y; R.kz[k] = kv.z;
+            R.beta[k] = (Rt)D.ebeta[e];
+        }
+#pragma unroll
+        for (int p = 0; p < NPair<NT>::value; ++p) R.bl[k][p] = e < S ? (Rt)D.ebetalj[(size_t)p * S + e] : Rt(0);
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) {
+            R.rho[k][t] = e < S ? D.rho[(size_t)t * S + e] : make_double2(0, 0);
+            R.mold[k][t] = (A.mode == MODE_EVAL && e < S) ? cvt2<R2>(A.scratch[(size_t)t * S + e]) : mk2(Rt(0), Rt(0));
+            R.dl[k][t] = mk2(Rt(0), Rt(0));
+        }
+    }
+    const long long n_rng = run->n_rng;
+    if (tid == 0) {
+        for (int c = 0; c < SC_COUNT; ++c) sh.sc[c] = D.scal[c];
+        sh.icycle = D.cnt[CN_ICYCLE];
+        sh.mic = D.cnt[CN_MOVE_IN_CYCLE];
+        sh.cursor = run->cursor;
+        sh.last_mol = -1;
+        sh.abort = 0;
+        sh.qcount = 0;
+        sh.wnext = 0;
+        sh.icur = 0;
+        sh.spec_ok = 0;
+        // static atom data of each molecule species, taken from its first molecule
+        sh.nspec = D.nspec <= kMaxSpecies ? D.nspec : 0;
+        for (int sp = 0; sp < sh.nspec; ++sp) {
+            const int4 c = D.spec[sp];
+            sh.sp_m0[sp] = c.x; sh.sp_cnt[sp] = c.y; sh.sp_na[sp] = c.z; sh.sp_a0[sp] = c.w;
+            for (int a = 0; a < c.z; ++a) {
+                const int j = c.w + a;
+                Slot t;
+                t.x = t.y = t.z = 0.0;
+                t.q = D.atom[j].w; t.iq = t.q != 0.0 ? 1.0 / t.q : 0.0;
+                t.dhs = D.dhs[j]; t.type = D.meta[j].y; t.pad = 0;
+                sh.sp_atom[sp][a] = t;
+                sh.sp_mass[sp][a] = D.mass[j];
+            }
+        }
+    }
+    // first random window at the start cursor
+    if (ctl && A.mode == MODE_RUN) {
+        const long long base = run->cursor;
+        const long long avail = n_rng - base;
+        const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
+        for (int i = lane; i < nw; i += 32) rwin[0][i] = run->rng[base + i - run->rng_off];
+        if (lane == 0) { sh.wbase[0] = base; sh.wn[0] = nw; sh.wbase[1] = -1; sh.wn[1] = 0; sh.wnext = 1; }
+    }
+    __syncthreads();
+    const bool biased = SPLIT && (D.xlf > 0.0 || D.xlc > 0.0);
+    const bool speculate = !SPLIT;
+    const ChooseCtx X{&D, run, rwin[0], rwin[1], atom_s, G};
+
+    long long moves_done = 0;
+    int n_acc = 0, rows = 0;
+    long long acc_seen = 0;  // accepted moves of this launch, known to every thread
+    const long long acc_limit = (A.mode == MODE_RUN) ? run->acc_limit : 0;
+    int xpar = 0;  // parity of the cluster exchange buffer, flipped after every pass
+    const long long n_moves = (A.mode == MODE_RUN) ? run->n_moves : 1;
+    long long *prof = (A.prof && rank == 0) ? A.prof : nullptr;
+    const bool pc = prof && tid == 0;
+    long long t_mark = 0;
+#define YAMC_PH(ph) do { if (pc) { const long long t_now = clock64(); prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+
+    // ---------------------------------------------------------------- the first move of the launch
+    bool have_next = false;  // sh.cur already prepared by the previous iteration's speculation
+    for (long long it = 0; it < n_moves; ++it) {
+        if (pc) t_mark = clock64();
+        if (!have_next) {
+            // choose the molecule and stage its atoms (no move in flight)
+            if (tid == 0) {
+                Cand &C = sh.cand[sh.icur];
+                C.cur_start = sh.cursor;
+                int imol;
+                if (A.mode == MODE_RUN) {
+                    RngReader rng = make_reader(X, sh, sh.cursor);
+                    imol = draw_molecule(D, rng, sh.mic == 0);
+                    C.valid = imol > 0;
+                    C.cur_prop = rng.cur;
+                    if (!imol) imol = 1;
+                } else {
+                    imol = (int)A.api_in[0];
+                    C.valid = 1;
+                    C.cur_prop = sh.cursor;
+                }
+                stage_molecule(X, sh, C, imol, -1, nullptr, cluster);
+                sh.abort = C.valid ? 0 : 1;
+            }
+            __syncthreads();
+            if (sh.abort) break;
+            YAMC_PH(PH_CHOOSE);
+            const int na0 = sh.cand[sh.icur].na;
+            // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
+            if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+                __syncthreads();
+                reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
+                xpar ^= 1;
+                __syncthreads();
+                if (tid == 0) {
+                    sh.eold[0] = sh.tot[RV_EW]; sh.eold[1] = sh.tot[RV_LJ6]; sh.eold[2] = sh.tot[RV_LJ12];
+                    for (int a = 0; a < na0; ++a) {  // external-field force -2 kext q mu (MC.f90:988-997)
+                        const double q = sh.cand[sh.icur].slot[na0 + a].q;
+                        sh.fold[3 * a] = sh.tot[RV_F + 3 * a] + D.m2k * q * sh.sc[SC_MU_X];
+                        sh.fold[3 * a + 1] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * sh.sc[SC_MU_Y];
+                        sh.fold[3 * a + 2] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * sh.sc[SC_MU_Z];
+                    }
+                }
+                if (A.mode == MODE_OLD) {
+#pragma unroll
+                    for (int k = 0; k < EPT; ++k)
+                        if (R.e[k] >= 0) {
+#pragma unroll
+                            for (int t = 0; t <= NT; ++t) A.scratch[(size_t)t * S + R.e[k]] = to_d2(R.mold[k][t]);
+                        }
+                    __syncthreads();
+                    if (tid == 0 && rank == 0) {
+                        for (int c = 0; c < 3; ++c) A.api_out[c] = sh.eold[c];
+                        for (int c = 0; c < 3 * na0; ++c) A.api_out[RV_F + c] = sh.fold[c];
+                    }
+                    moves_done = 1;
+                    break;
+                }
+            }
+            // the proposal (movemc Step 5)
+            if (tid == 0) {
+                Cand &C = sh.cand[sh.icur];
+                if (A.mode == MODE_RUN) {
+                    RngReader rng = make_reader(X, sh, C.cur_prop);
+                    double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+                    if (biased) {
+                        double xo[kMaxA], yo[kMaxA], zo[kMaxA], fx[kMaxA], fy[kMaxA], fz[kMaxA];
+                        for (int a = 0; a < na0; ++a) {
+                            xo[a] = C.slot[na0 + a].x; yo[a] = C.slot[na0 + a].y; zo[a] = C.slot[na0 + a].z;
+                            fx[a] = sh.fold[3 * a]; fy[a] = sh.fold[3 * a + 1]; fz[a] = sh.fold[3 * a + 2];
+                        }
+                        mol_force_torque(na0, xo, yo, zo, C.mass, fx, fy, fz, F, T);
+                    }
+                    propose(D, C, rng, F, T);
+                    C.cur_prop = rng.cur;
+                    if (rng.out) { C.valid = 0; sh.abort = 1; }
+                } else {  // MODE_EVAL: positions from the host
+                    for (int a = 0; a < na0; ++a) {
+                        C.slot[a].x = A.api_in[1 + 3 * a]; C.slot[a].y = A.api_in[2 + 3 * a]; C.slot[a].z = A.api_in[3 + 3 * a];
+                    }
+                }
+            }
+            __syncthreads();
+            if (sh.abort) break;
+            YAMC_PH(PH_PROPOSE);
+        }
+        const int na = sh.cand[sh.icur].na;
+        const bool split = SPLIT;
+
+        // ------------------------------------------------ the pass over the new positions
+        if (!ctl) {
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+        } else if (speculate && it + 1 < n_moves) {
+            // prepare the next move's candidates while the workers run: lane 0 after an overlap
+            // (no acceptance draw), lanes 1-2 after the acceptance draw, lane 2 with the molecule
+            // in flight at its proposed positions (used only if it is chosen again and accepted)
+            const Cand &M = sh.cand[sh.icur];
+            const long long c1 = M.cur_prop;
+            const bool next_cycle = (sh.mic + 1 == D.M);
+            // the window of the stream the candidates read: make sure it covers c1 onwards
+            {
+                const int b = sh.wnext;
+                const bool covered0 = sh.wbase[0] >= 0 && c1 >= sh.wbase[0] && c1 + kWin / 2 <= sh.wbase[0] + sh.wn[0];
+                const bool covered1 = sh.wbase[1] >= 0 && c1 >= sh.wbase[1] && c1 + kWin / 2 <= sh.wbase[1] + sh.wn[1];
+                if (!covered0 && !covered1) {
+                    const long long avail = n_rng - c1;
+                    const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
+                    __syncwarp();
+                    for (int i = lane; i < nw; i += 32) rwin[b][i] = run->rng[c1 + i - run->rng_off];
+                    __syncwarp();
+                    if (lane == 0) { sh.wbase[b] = c1; sh.wn[b] = nw; sh.wnext = b ^ 1; }
+                    __syncwarp();
+                }
+            }
+            if (lane < 3) {
+                const int buf = (sh.icur + 1 + lane) & 3;
+                if (lane == 0) { sh.spec[0] = (sh.icur + 1) & 3; sh.spec[1] = (sh.icur + 2) & 3; sh.spec[2] = (sh.icur + 3) & 3; }
+                Cand &C = sh.cand[buf];
+                RngReader rng = make_reader(X, sh, c1);
+                if (lane > 0) (void)rng.next();  // the acceptance draw (MonteCarloMove.f90:553)
+                C.cur_start = rng.cur;
+                const int imol = rng.out ? 0 : draw_molecule(D, rng, next_cycle);
+                C.valid = imol > 0;
+                const Slot *moving = (lane == 2) ? &M.slot[0] : &M.slot[M.na];
+                stage_molecule(X, sh, C, imol > 0 ? imol : 1, M.imol - 1, moving, cluster);
+                const double Z[3] = {0, 0, 0};
+                if (C.valid) propose(D, C, rng, Z, Z);
+                C.cur_prop = rng.cur;
+                if (rng.out) C.valid = 0;
+            }
+            if (pc) { const long long t_now = clock64(); prof[PH_SPECULATE] += t_now - t_mark; t_mark = t_now; }
+        }
+        __syncthreads();
+        reduce_pass(sh, red, xch, split ? RV_F + 3 * na : RV_F, G, rank, xpar, cluster);
+        xpar ^= 1;
+        YAMC_PH(PH_REDUCE);
+
+        if (A.mode == MODE_EVAL) {
+#pragma unroll
+            for (int k = 0; k < EPT; ++k)
+                if (R.e[k] >= 0) {
+#pragma unroll
+                    for (int t = 0; t <= NT; ++t) A.scratch[(size_t)(1 + nt + t) * S + R.e[k]] = to_d2(R.dl[k][t]);
+                }
+            __syncthreads();
+            if (tid == 0 && rank == 0)
+                for (int v = 0; v < RV_F + 3 * na; ++v) A.api_out[v] = sh.tot[v];
+            moves_done = 1;
+            break;
+        }
+
+        // ------------------------------------------------ Metropolis (Steps 7-13) and commit (Step 14)
+        if (tid == 0) {
+            const Cand &M = sh.cand[sh.icur];
+            const bool overlap = sh.tot[RV_OVL] > 0.0;
+            int flags = overlap ? 2 : 0;
+            double du_real = 0, du_kc = 0, du_kl = 0, du_ext = 0, dmx = 0, dmy = 0, dmz = 0;
+            double dew = 0, dlj6 = 0, dlj12 = 0;
+            int acc = 0;
+            long long cur_after = M.cur_prop;
+            bool out = false;
+            if (!overlap) {
+                RngReader rng = make_reader(X, sh, M.cur_prop);
+                if (biased) {
+                    dew = sh.tot[RV_EW] - sh.eold[0]; dlj6 = sh.tot[RV_LJ6] - sh.eold[1]; dlj12 = sh.tot[RV_LJ12] - sh.eold[2];
+                    du_real = (sh.tot[RV_EW] + sh.tot[RV_LJ12] - sh.tot[RV_LJ6]) - (sh.eold[0] + sh.eold[2] - sh.eold[1]);
+                } else {
+                    dew = sh.tot[RV_EW]; dlj6 = sh.tot[RV_LJ6]; dlj12 = sh.tot[RV_LJ12];
+                    du_real = dew + dlj12 - dlj6;
+                }
+                du_kc = sh.tot[RV_DUC];
+                du_kl = sh.tot[RV_DUL];
+                double mx = 0, my = 0, mz = 0;
+                for (int a = 0; a < na; ++a) { mx = mx + M.slot[a].q * M.slot[a].x; my = my + M.slot[a].q * M.slot[a].y; mz = mz + M.slot[a].q * M.slot[a].z; }
+                dmx = mx - M.mu_old[0]; dmy = my - M.mu_old[1]; dmz = mz - M.mu_old[2];
+                const double mux = sh.sc[SC_MU_X], muy = sh.sc[SC_MU_Y], muz = sh.sc[SC_MU_Z];
+                // EwaldSumExternal_calc_dU (EwaldSumExternal.f90:68-82)
+                du_ext = D.kext * ((2 * mux + dmx) * dmx + (2 * muy + dmy) * dmy + (2 * muz + dmz) * dmz);
+                double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
+                if (biased) {
+                    double fx[kMaxA], fy[kMaxA], fz[kMaxA], x[kMaxA], y[kMaxA], z[kMaxA];
+                    for (int a = 0; a < na; ++a) {
+                        const double q = M.slot[a].q;
+                        fx[a] = sh.tot[RV_F + 3 * a] + D.m2k * q * (mux + dmx);
+                        fy[a] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * (muy + dmy);
+                        fz[a] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * (muz + dmz);
+                        x[a] = M.slot[a].x; y[a] = M.slot[a].y; z[a] = M.slot[a].z;
+                    }
+                    mol_force_torque(na, x, y, z, M.mass, fx, fy, fz, F, T);
+                }
+                const double du_total = du_real + (du_kc + du_kl) + du_ext;
+                MoveState mv = M.mv;
+                mcm_init_new(mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
+                acc = mcm_accept(mv, du_total, D.xlf, D.xlc, rng);
+                out = rng.out != 0;
+                cur_after = rng.cur;
+                flags |= acc;
+            }
+            sh.accepted = 0;
+            if (out) {
+                sh.abort = 1;  // the interrupted move restarts from its first draw (sh.cursor unchanged)
+            } else {
+                sh.accepted = acc;
+                if (acc) {
+                    sh.sc[SC_UU_EW] += dew; sh.sc[SC_UU_LJ6] += dlj6; sh.sc[SC_UU_LJ12] += dlj12;
+                    sh.sc[SC_EK_C] += du_kc; sh.sc[SC_EK_LJ] += du_kl;
+                    sh.sc[SC_MU_X] += dmx; sh.sc[SC_MU_Y] += dmy; sh.sc[SC_MU_Z] += dmz;
+                    sh.sc[SC_N_MV_ACC] += 1.0;
+                    sh.last_mol = M.imol - 1;
+                    for (int a = 0; a < na; ++a) { sh.lx[a] = M.slot[a].x; sh.ly[a] = M.slot[a].y; sh.lz[a] = M.slot[a].z; }
+                    // this CTA's staged copy of the moved atoms; every reader of the old copy (this
+                    // move's pass, the candidates prepared during it, in any CTA) has passed the barriers
+                    for (int a = 0; a < na; ++a) {
+                        const int j = M.first + a;
+                        if (j % G == rank) {
+                            double4 p = atom_s[j / G];
+                            p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
+                            atom_s[j / G] = p;
+                        }
+                    }
+                    ++n_acc;
+                }
+                sh.sc[SC_N_MV_STEPS] += 1.0;
+                sh.cursor = cur_after;
+                if (rank == 0) {
+                    if (acc)
+                        for (int a = 0; a < na; ++a) {
+                            double4 p = D.atom[M.first + a];
+                            p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
+                            D.atom[M.first + a] = p;
+                        }
+                    if (run->log) {
+                        yamc_move_record rec;
+                        rec.imol = M.imol; rec.flags = flags; rec.cursor = cur_after;
+                        rec.du_real = du_real; rec.du_k_coul = du_kc; rec.du_k_lj = du_kl; rec.du_ext = du_ext;
+                        run->log[it] = rec;
+                    }
+                }
+                // cycle bookkeeping and energy.dat rows (runmc.f90:230-279)
+                sh.mic += 1;
+                if (sh.mic == D.M) {
+                    sh.mic = 0;
+                    const double fr = sh.sc[SC_N_MV_STEPS] / D.M + sh.sc[SC_N_VOL_STEPS];
+                    if (fmod(fr, D.n_store_energy_interval) < 1e-10 && rank == 0 && run->rows && rows < run->max_rows) {
+                        const double *sc = sh.sc;
+                        const double uext = D.kext * (sc[SC_MU_X] * sc[SC_MU_X] + sc[SC_MU_Y] * sc[SC_MU_Y] + sc[SC_MU_Z] * sc[SC_MU_Z]);
+                        const double utew = sc[SC_UU_EW] + sc[SC_EK_C] + sc[SC_TAIL_C] + uext;
+                        const double utlj = sc[SC_UU_LJ12] - sc[SC_UU_LJ6] + sc[SC_EK_LJ] + sc[SC_TAIL_LJ12] - sc[SC_TAIL_LJ6];
+                        double *row = run->rows + 9 * (size_t)rows;
+                        row[0] = (double)sh.icycle; row[1] = utew + utlj; row[2] = utew; row[3] = utlj;
+                        row[4] = sc[SC_UU_EW]; row[5] = sc[SC_UU_LJ6]; row[6] = sc[SC_UU_LJ12];
+                        row[7] = sc[SC_EK_C]; row[8] = sc[SC_EK_LJ];
+                        ++rows;
+                    }
+                    sh.icycle += 1;
+                }
+                // the next move: the prepared candidate that matches what happened
+                sh.spec_ok = 0;
+                if (speculate && it + 1 < n_moves) {
+                    const int sel = overlap ? 0 : ((acc && sh.cand[sh.spec[2]].imol == M.imol) ? 2 : 1);
+                    const int buf = sh.spec[sel];
+                    const Cand &C = sh.cand[buf];
+                    if (C.valid && C.cur_start == sh.cursor) {
+                        sh.icur = buf;
+                        sh.spec_ok = 1;
+                    }
+                }
+            }
+        }
+        __syncthreads();
+        YAMC_PH(PH_DECIDE);
+        if (sh.abort) break;
+        if (sh.accepted) {
+            // commit: rho += delta (MC.f90:1245), in registers or in memory by the entry's owner
+#pragma unroll
+            for (int k = 0; k < EPT; ++k)
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) { R.rho[k][t].x += R.dl[k][t].x; R.rho[k][t].y += R.dl[k][t].y; }
+            if constexpr (EPT <= 0) {
+                if (!ctl) {
+                    const double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
+                    for (int e = e0; e < S; e += gwork)
+#pragma unroll
+                        for (int t = 0; t <= NT; ++t) {
+                            double2 r = D.rho[(size_t)t * S + e];
+                            const double2 d = dl_g[(size_t)t * S + e];
+                            r.x += d.x; r.y += d.y;
+                            D.rho[(size_t)t * S + e] = r;
+                        }
+                }
+            }
+        }
+        ++moves_done;
+        have_next = sh.spec_ok != 0;
+        acc_seen += sh.accepted;
+        __syncthreads();
+        YAMC_PH(PH_COMMIT);
+        if (acc_limit > 0 && acc_seen >= acc_limit) break;  // same decision in every CTA
+    }
+#undef YAMC_PH
+
+    if (A.mode == MODE_RUN) {  // write back the register and shared state
+#pragma unroll
+        for (int k = 0; k < EPT; ++k)
+            if (R.e[k] >= 0) {
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) D.rho[(size_t)t * S + R.e[k]] = R.rho[k][t];
+            }
+        if (tid == 0 && rank == 0) {
+            for (int c = 0; c < SC_COUNT; ++c) D.scal[c] = sh.sc[c];
+            D.cnt[CN_ICYCLE] = sh.icycle;
+            D.cnt[CN_MOVE_IN_CYCLE] = sh.mic;
+            run->cursor = sh.cursor;
+            run->moves_done = moves_done;
+            run->n_rows = rows;
+            run->accepted = n_acc;
+            run->status = sh.abort ? YAMC_ERNG_EXHAUSTED : YAMC_OK;
+        }
+    } else if (tid == 0 && rank == 0) {
+        run->moves_done = moves_done;
+        run->status = YAMC_OK;
+    }
+    if (G > 1) cluster.sync();  // no CTA leaves while another may still address its shared memory
+}
+
+// nrep chains of one launch shape: nrep clusters of L.G CTAs, chain r on cluster r
+template <int NT, int EPT, bool SPLIT, bool MX>
+int launch_chain_t(const LaunchCfg &L, cudaStream_t stream, int nrep, const ChainArgs &args) {
+    auto kfn = k_chain<NT, EPT, SPLIT, MX>;
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    if (L.G > 8) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.G * nrep, 1, 1);
+    cfg.blockDim = dim3(L.B, 1, 1);
+    cfg.dynamicSmemBytes = L.smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = L.G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaLaunchKernelEx(&cfg, kfn, args));
+    return YAMC_OK;
+}
+
+// clusters of shape L that can be resident at once (0 if the shape does not launch)
+template <int NT, int EPT, bool SPLIT, bool MX>
+int max_clusters_t(const LaunchCfg &L, int *out) {
+    auto kfn = k_chain<NT, EPT, SPLIT, MX>;
+    CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)L.smem));
+    if (L.G > 8) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeNonPortableClusterSizeAllowed, 1));
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(L.G, 1, 1);
+    cfg.blockDim = dim3(L.B, 1, 1);
+    cfg.dynamicSmemBytes = L.smem;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = L.G;
+    attr[0].val.clusterDim.y = 1;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CUDA_TRY(cudaOccupancyMaxActiveClusters(out, kfn, &cfg));
+    return YAMC_OK;
+}
+
+
+// one instantiation file per LJ type count: every (entries per thread, split, mixed) variant
+int launch_chain_t1(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
+int launch_chain_t2(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
+int launch_chain_t3(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
+int launch_chain_t4(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
+int max_clusters_t1(const LaunchCfg &L, bool split, bool mx, int *out);
+int max_clusters_t2(const LaunchCfg &L, bool split, bool mx, int *out);
+int max_clusters_t3(const LaunchCfg &L, bool split, bool mx, int *out);
+int max_clusters_t4(const LaunchCfg &L, bool split, bool mx, int *out);
+
+}  // namespace yamc

@@ -220,6 +220,37 @@ __host__ __device__ inline PairTerm<R> pair_term(R r2, R qq_xclb, bool lj, R sig
     return t;
 }
 
+// The mixed form's pair term: the one transcendental, exp(-alpha^2 r^2), in FP32 (its argument
+// formed in FP64, so the FP32 rounding of alpha^2 r^2 costs at most an ulp of the argument);
+// 1/r, the erfc_Luc polynomials and the products in FP64.  Rounding each pair term to FP32, or
+// the A&S polynomial in FP32, would put the per-move dE error above 1e-4 kT.
+template <bool WANT_FR>
+__device__ inline PairTerm<double> pair_term_mx(double r2, double qq_xclb, bool lj, double sigma6, double four_eps,
+                                                double alpha, double taosp, bool same_mol) {
+    PairTerm<double> t;
+    const double ir = rsq(r2);
+    const double r = r2 * ir;
+    const double ir2 = ir * ir;
+    const double a = alpha * r;
+    const double a2 = a * a;
+    const double e2 = (double)expf(-(float)a2);
+    const double erfc_a = same_mol ? -d_erf_luc<double>(a, a2, e2) : d_erfc_luc<double>(a, a2, e2);
+    t.ew = qq_xclb * erfc_a * ir;
+    t.FR = WANT_FR ? qq_xclb * (erfc_a * ir + taosp * e2) * ir2 : 0.0;
+    t.lj6 = 0.0; t.lj12 = 0.0;
+    if (lj) {
+        const double so6 = sigma6 * (ir2 * ir2 * ir2);
+        const double C6 = 1.0 + a2 * (1.0 + a2 * 0.5);
+        const double a6 = a2 * a2 * a2;
+        const double C12 = C6 + a6 * (1.0 + a2 * (1.0 + a2 * (1.0 / 5.0)) * 0.25) * (1.0 / 6.0);
+        t.lj6 = four_eps * so6 * e2 * C6;
+        t.lj12 = four_eps * (so6 * so6) * e2 * C12;
+        if (WANT_FR)
+            t.FR = t.FR + four_eps * 6.0 * so6 * e2 * (2.0 * so6 * (C12 + a6 * a6 * (1.0 / 720.0)) - (C6 + a6 * (1.0 / 6.0))) * ir2;
+    }
+    return t;
+}
+
 // minimum image by one conditional wrap per axis (EwaldSumRealSpace.f90:394-401)
 template <class R>
 __host__ __device__ inline R min_image(R d) {
