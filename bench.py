@@ -18,6 +18,7 @@ device-resident run_mc segment of --moves moves on one independent chain per GPU
 from __future__ import annotations
 
 import argparse
+import contextlib
 import json
 import math
 import os
@@ -214,7 +215,7 @@ def main():
         import datetime
         import torch.distributed as dist
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
-    from yamc_b200 import api, rng as grng
+    from yamc_b200 import _lib, api, rng as grng
 
     dev = f"cuda:{local}"
     n_steps = args.warmup + args.steps
@@ -226,20 +227,41 @@ def main():
         flush.fill_(1.0)
         torch.cuda.synchronize()
 
-    # ---------------- one chain alone: the latency of the move (reported beside the batch)
-    eng = api.Engine.from_files(files, device=local)
-    s0 = grng.gfortran_stream(12345 + 1000 * rank, per_move * args.moves * 3 + 100000)
-    d_s0 = torch.from_numpy(s0).to(dev)
-    c0, _, _ = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves)
-    single_ms = []
-    for _ in range(2):
-        l2_flush()
-        c0, done, st = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves, cursor=c0)
-        assert st == 0 and done == args.moves
-        single_ms.append(eng.last_kernel_ms)
-    single = {"moves_per_s": args.moves / (np.mean(single_ms) / 1e3), "launch": eng.launch}
-    del d_s0
-    eng.close()
+    # ---------------- one chain alone: the latency of the move, FP64 and mixed (beside the batch)
+    def single_chain(precision):
+        eng = api.Engine.from_files(files, device=local, precision=precision)
+        s0 = grng.gfortran_stream(12345 + 1000 * rank, per_move * args.moves * 3 + 100000)
+        d_s0 = torch.from_numpy(s0).to(dev)
+        c0, _, _ = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves)
+        ms = []
+        for _ in range(2):
+            l2_flush()
+            c0, done, st = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves, cursor=c0)
+            assert st == 0 and done == args.moves
+            ms.append(eng.last_kernel_ms)
+        out = {"moves_per_s": args.moves / (np.mean(ms) / 1e3), "launch": eng.launch}
+        eng.close()
+        return out
+
+    single = {"fp64": single_chain(_lib.YAMC_FP64), "mixed": single_chain(_lib.YAMC_MIXED)}
+
+    # ---------------- dE of the mixed form against the FP64 form, move by move on the same stream
+    # (both chains take the same decisions until a draw falls within the dE error of its
+    # threshold; the comparison runs up to there)
+    n_chk = 4000
+    chk = grng.gfortran_stream(4242 + rank, 40 * n_chk + 10000)
+    logs = {}
+    for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
+        eng = api.Engine.from_files(files, device=local, precision=prec)
+        logs[prec] = eng.run_chain(chk, n_chk)[0]
+        eng.close()
+    lf, lm = logs[_lib.YAMC_FP64], logs[_lib.YAMC_MIXED]
+    same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
+    k_same = n_chk if same.all() else int(np.argmin(same))
+    cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
+    de = np.abs(sum(lm[c][:k_same] for c in cols) - sum(lf[c][:k_same] for c in cols))
+    de_err = {"max_kT": float(de.max()) if k_same else None, "rms_kT": float(np.sqrt((de ** 2).mean())) if k_same else None,
+              "moves_compared": k_same, "bar_kT": 1e-4}
 
     # ---------------- the batch: R independent chains of the workload, one graph launch per step
     # R = the most chains any launch shape keeps resident at once (the tuner then picks the shape)
@@ -258,34 +280,45 @@ def main():
     R = max(R, 1)
     rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=3 + 101 * rank + r,
                                                 rng_seed=12345 + 1000 * rank + r) for r in range(1, R)]
-    b = api.Batch([api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files], device=local)
+    rep_inputs = [api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files]
     streams = [grng.gfortran_stream(12345 + 1000 * rank + 7 * r, n_stream) for r in range(R)]
     d_streams = [torch.from_numpy(x).to(dev) for x in streams]
     d_ptrs = [t.data_ptr() for t in d_streams]
     n_rng = [t.numel() for t in d_streams]
-    cur = np.zeros(R, dtype=np.int64)
-    b.tune(d_ptrs, n_rng, cur, max(200, args.moves // 20))
 
-    # ---------------- device-resident value
-    kernel_ms = []
-    for w in range(args.warmup):
-        b.run_device(d_ptrs, n_rng, cur, args.moves)
-        l2_flush()
-    if ws > 1:
-        dist.barrier()
-    torch.cuda.synchronize()
-    with Clocks(local) as clk:
-        for s in range(args.steps):
-            done, st, s_all = b.run_device(d_ptrs, n_rng, cur, args.moves)
-            assert s_all == 0 and (done == args.moves).all(), (s_all, done)
-            kernel_ms.append(b.last_kernel_ms)
+    def timed_batch(precision, clk=None):
+        b = api.Batch(rep_inputs, device=local, precision=precision)
+        cur = np.zeros(R, dtype=np.int64)
+        b.tune(d_ptrs, n_rng, cur, max(200, args.moves // 20))
+        for w in range(args.warmup):
+            b.run_device(d_ptrs, n_rng, cur, args.moves)
             l2_flush()
-    torch.cuda.synchronize()
-    t_dev = sum(kernel_ms) / 1e3
-    if ws > 1:
-        t = torch.tensor([t_dev], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_dev = float(t.item())
+        if ws > 1:
+            dist.barrier()
+        torch.cuda.synchronize()
+        ms, counts = [], []
+        ctx = clk if clk is not None else contextlib.nullcontext()
+        with ctx:
+            for s in range(args.steps):
+                done, st, s_all = b.run_device(d_ptrs, n_rng, cur, args.moves)
+                assert s_all == 0 and (done == args.moves).all(), (s_all, done)
+                ms.append(b.last_kernel_ms)
+                counts.append(b.last_launches)
+                l2_flush()
+        torch.cuda.synchronize()
+        t = sum(ms) / 1e3
+        if ws > 1:
+            tt = torch.tensor([t], device=dev)
+            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+            t = float(tt.item())
+        return b, cur, ms, t, counts
+
+    b64, _, ms64, t64, _ = timed_batch(_lib.YAMC_FP64)
+    value_fp64 = ws * R * args.steps * args.moves / t64
+    launch_fp64 = b64.launch
+    b64.close()
+    clk = Clocks(local)
+    b, cur, kernel_ms, t_dev, launch_counts = timed_batch(_lib.YAMC_MIXED, clk)
     value = ws * R * args.steps * args.moves / t_dev
 
     # ---------------- end to end through the C ABI with host buffers
@@ -341,10 +374,15 @@ def main():
     line = {
         "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
         "config": {"workload": f"{args.workload}: {spec.n_water} SPC/E + {spec.n_na} Na + {spec.n_cl} Cl, "
                                f"{spec.natom} atoms, L={spec.box} A, alpha={spec.alpha}/A, rc={spec.rc} A, "
-                               f"kmax={spec.kmax}", "method": "plain FP64, unbiased moves",
+                               f"kmax={spec.kmax}",
+                   "method": "mixed precision (FP32 phases, k-space terms and pair exp; FP64 rho, sums, "
+                             "Metropolis; FP64 rho refresh every 1e4 accepted moves), unbiased moves",
+                   "fp64": {"value": value_fp64, "unit": "moves/s", "launch": launch_fp64},
+                   "mixed_over_fp64": value / value_fp64,
+                   "de_error_vs_fp64": de_err,
                    "moves_per_step_per_chain": args.moves, "chains_per_gpu": R,
                    "parallelism": "independent replicas (one cluster per chain)",
                    "launch": launch, "l2": "256 MB write between steps", "accept_fraction": p_acc,
@@ -353,7 +391,7 @@ def main():
                      "traffic": TRAFFIC_PER_MOVE * moves_launch, "peak_source": which,
                      "algorithmic_bytes_per_move": bpm},
         "e2e": {"value": e2e, "unit": "moves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": args.steps,
+        "gpu_launches": int(sum(launch_counts)),
         "clocks": clk.summary(),
     }
     if not args.no_cpu_baseline:

@@ -179,10 +179,11 @@ int yamc_run_chain_device(yamc_ctx *ctx, const float *d_rng, int64_t n_rng, int6
                           int64_t n_moves, int64_t *moves_done, yamc_move_record *d_log,
                           double *d_rows, int32_t max_rows, int32_t *n_rows);
 
-/* Mixed form (params.precision = YAMC_MIXED): rho(k) and the k-space energies are
-   recomputed in FP64 from the positions after every `accepted_moves` accepted
-   moves (default 10000; 0 = never), bounding the drift of the running sums that
-   FP32 deltas update.  yamc_refresh_count returns how many refreshes ran. */
+/* Mixed form (params.precision = YAMC_MIXED): the chain kernel recomputes rho(k)
+   and the k-space energies in FP64 from the positions after every
+   `accepted_moves` accepted moves (default 10000; 0 = never), bounding the drift
+   of the running sums that FP32 deltas update.  yamc_refresh_count returns how
+   many refreshes ran. */
 int yamc_set_refresh(yamc_ctx *ctx, int64_t accepted_moves);
 int yamc_refresh_count(yamc_ctx *ctx, int64_t *count);
 
@@ -249,7 +250,10 @@ int yamc_batch_set_kspace_layout(yamc_batch *b, int32_t layout);
 /* out: cluster blocks, threads, entries per thread, shared memory bytes, clusters
    resident at once (of the first group) */
 int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]);
+/* device time (ms, CUDA events on the batch stream) of the last run, and the kernels it
+   launched (one chain launch per variant group) */
 int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms);
+int yamc_batch_last_launches(yamc_batch *b, int32_t *n);
 
 /* ---- allocation-free real-space sums ----
    No counterpart in the reference: an extra entry point for callers that cannot

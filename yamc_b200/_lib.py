@@ -107,6 +107,7 @@ SIGNATURES = {
     "yamc_batch_set_kspace_layout": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_batch_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_batch_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
+    "yamc_batch_last_launches": (ctypes.c_int, [_VP, _ip]),
     "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +
                                    [ctypes.c_int32] + [_VP] * 8),
     "yamc_error_string": (ctypes.c_char_p, [ctypes.c_int]),

@@ -352,6 +352,12 @@ class Batch:
         check(self.lib.yamc_batch_last_kernel_ms(self.h, ctypes.byref(v)), "yamc_batch_last_kernel_ms")
         return v.value
 
+    @property
+    def last_launches(self) -> int:
+        v = ctypes.c_int32(0)
+        check(self.lib.yamc_batch_last_launches(self.h, ctypes.byref(v)), "yamc_batch_last_launches")
+        return v.value
+
 
 class _ReplicaView(Engine):
     """A replica of a Batch seen through the per-context calls; the batch owns it."""

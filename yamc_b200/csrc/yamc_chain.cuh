@@ -57,7 +57,6 @@ struct RunSlot {
     double *rows;           // optional energy rows (9 doubles)
     int max_rows, n_rows;
     int status, accepted;
-    long long acc_limit;    // > 0: return after this many accepted moves (the mixed form's rho refresh)
 };
 
 struct ChainArgs {
@@ -726,6 +725,121 @@ __device__ inline void propose(const DevSys &D, Cand &C, RngReader &rng, const d
         if (a < na) { C.slot[a].x = xn[a]; C.slot[a].y = yn[a]; C.slot[a].z = zn[a]; }
 }
 
+// The mixed form's FP64 recomputation of rho(k) (RhoSquared_addAtoms, RhoSquared.f90:188-243)
+// inside the chain, by all threads of every CTA of the cluster: the worker threads recompute the
+// entries they own from every atom's FP64 position (D.atom, kept current by rank 0), with the
+// atoms' per-axis phase tables built in chunks in the scratch region; then the k-space energies
+// (EwaldSumKSpace_calc_coulomb_energy / _calc_LJ_energy, EwaldSumKSpace.f90:389-526) are
+// reduced over the cluster into the engine scalars.
+template <int NT, int EPT, class Regs>
+__device__ __noinline__ void refresh_in_chain(const DevSys &D, Regs &R, double2 *scr, int scr_atoms, int e0, int estep,
+                                              int G, int rank, ChainShared &sh, double *red, double *xch, int xpar,
+                                              cg::cluster_group &cluster) {
+    const int tid = threadIdx.x, B = blockDim.x;
+    const bool ctl = tid < kCtl;
+    const int lane = tid & 31, wwarp = (tid - kCtl) >> 5;
+    const int KM = D.kmax + 1, S = D.S, N = D.N;
+    const int CH = scr_atoms < 64 ? scr_atoms : 64;
+    double2 *tabs = scr;                                                  // [CH][3][KM]
+    double *sq = reinterpret_cast<double *>(tabs + (size_t)CH * 3 * KM);  // [CH]
+    int *st = reinterpret_cast<int *>(sq + CH);                           // [CH]
+    // the positions rank 0 wrote for accepted moves are visible to every CTA after this barrier
+    __threadfence();
+    if (G > 1) cluster.sync(); else __syncthreads();
+    constexpr int EB = EPT > 0 ? EPT : 4;  // entries per batch
+    const int nbatch = EPT > 0 ? 1 : (S + estep * EB - 1) / (estep * EB);
+    double ekc = 0.0, ekl = 0.0;
+    for (int b = 0; b < nbatch; ++b) {
+        int ent[EB];
+        int4 kv[EB];
+        double2 acc[EB][1 + NT];
+#pragma unroll
+        for (int j = 0; j < EB; ++j) {
+            int e;
+            if constexpr (EPT > 0) e = R.e[j];
+            else e = e0 + (b * EB + j) * estep;
+            ent[j] = (!ctl && e >= 0 && e < S) ? e : -1;
+            kv[j] = ent[j] >= 0 ? D.kvec[ent[j]] : make_int4(0, 0, 0, 0);
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) acc[j][t] = make_double2(0.0, 0.0);
+        }
+        for (int a0 = 0; a0 < N; a0 += CH) {
+            const int na = min(CH, N - a0);
+            for (int idx = tid; idx < na * 3 * KM; idx += B) {
+                const int a = idx / (3 * KM), r = idx % (3 * KM), d = r / KM, m = r % KM;
+                const double4 p = D.atom[a0 + a];
+                const double u = d == 0 ? p.x : (d == 1 ? p.y : p.z);
+                double sn, cs;
+                sincospi(2.0 * (double)m * u, &sn, &cs);
+                if (m == 0) { sn = 0.0; cs = 1.0; }
+                tabs[(a * 3 + d) * KM + m] = make_double2(cs, sn);
+            }
+            for (int a = tid; a < na; a += B) { sq[a] = D.atom[a0 + a].w; st[a] = D.meta[a0 + a].y; }
+            __syncthreads();
+            if (!ctl) {
+                for (int a = 0; a < na; ++a) {
+                    const double2 *T = tabs + (size_t)a * 3 * KM;
+                    const double q = sq[a];
+                    const int ty = st[a];
+#pragma unroll
+                    for (int j = 0; j < EB; ++j) {
+                        if (ent[j] < 0) continue;
+                        double c = 0, s = 0;
+                        if (q != 0.0) {
+                            entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv[j].x, kv[j].y, kv[j].z, q, c, s);
+                            acc[j][0].x = acc[j][0].x + c; acc[j][0].y = acc[j][0].y + s;
+                        }
+                        if (ty > 0) {
+                            double cl, sl;
+                            if (q != 0.0) { const double iq = 1.0 / q; cl = c * iq; sl = s * iq; }
+                            else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv[j].x, kv[j].y, kv[j].z, 1.0, cl, sl);
+#pragma unroll
+                            for (int t = 0; t < NT; ++t)
+                                if (t == ty - 1) { acc[j][1 + t].x = acc[j][1 + t].x + cl; acc[j][1 + t].y = acc[j][1 + t].y + sl; }
+                        }
+                    }
+                }
+            }
+            __syncthreads();
+        }
+#pragma unroll
+        for (int j = 0; j < EB; ++j) {
+            const int e = ent[j];
+            if (e < 0) continue;
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) {
+                if constexpr (EPT > 0) R.rho[j][t] = acc[j][t];
+                else D.rho[(size_t)t * S + e] = acc[j][t];
+            }
+            ekc += D.ebeta[e] * (acc[j][0].x * acc[j][0].x + acc[j][0].y * acc[j][0].y);
+#pragma unroll
+            for (int t1 = 0; t1 < NT; ++t1)
+#pragma unroll
+                for (int t2 = t1; t2 < NT; ++t2) {
+                    double l = D.ebetalj[(size_t)pair_idx<NT>(t1, t2) * S + e] *
+                               (acc[j][1 + t1].x * acc[j][1 + t2].x + acc[j][1 + t1].y * acc[j][1 + t2].y);
+                    if (t1 != t2) l = l + l;
+                    ekl += l;
+                }
+        }
+    }
+    // k-space energies over the cluster (the pass reduction with two values)
+    if (!ctl) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            ekc += __shfl_xor_sync(0xffffffffu, ekc, o);
+            ekl += __shfl_xor_sync(0xffffffffu, ekl, o);
+        }
+        if (lane == 0)
+            for (int v = 0; v <= RV_DUL; ++v) red[wwarp * kNV + v] = v == RV_DUC ? ekc : (v == RV_DUL ? ekl : 0.0);
+    }
+    __syncthreads();
+    reduce_pass(sh, red, xch, RV_DUL + 1, G, rank, xpar, cluster);
+    __syncthreads();
+    if (tid == 0) { sh.sc[SC_EK_C] = sh.tot[RV_DUC]; sh.sc[SC_EK_LJ] = sh.tot[RV_DUL]; }
+    __syncthreads();
+}
+
 // SPLIT = false: unbiased device-resident chain only (one fused pass per move, speculation);
 // SPLIT = true: force-biased moves and the per-move API (old pass + new pass with forces).
 template <int NT, int EPT, bool SPLIT, bool MX>
@@ -758,6 +872,10 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     int *queue = reinterpret_cast<int *>(meta_s + A.nown_max);                // [qcap]
     int *nearbuf = queue + ((A.qcap + 1) & ~1);                               // [B/32][32 kCPT]
     double *red = reinterpret_cast<double *>(nearbuf + B * kCPT);             // [B/32][kNV]
+    // the mixed form's rho refresh reuses the pair queue and near buffer as atom phase tables
+    double2 *scr = reinterpret_cast<double2 *>((reinterpret_cast<uintptr_t>(queue) + 15) & ~uintptr_t(15));
+    const int scr_atoms = (int)(((reinterpret_cast<char *>(red) - reinterpret_cast<char *>(scr))) /
+                                (long)(sizeof(double2) * 3 * KM + sizeof(double) + sizeof(int)));
     double *xch = red + (B / 32) * kNV;                                       // [2][G][kNV]
     double *lj_s = xch + 2 * G * kNV;                                         // [2][nt*nt]
 
@@ -838,8 +956,9 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
 
     long long moves_done = 0;
     int n_acc = 0, rows = 0;
-    long long acc_seen = 0;  // accepted moves of this launch, known to every thread
-    const long long acc_limit = (A.mode == MODE_RUN) ? run->acc_limit : 0;
+    // mixed form: accepted moves since the last FP64 recomputation of rho(k), known to every thread
+    long long acc_since = D.cnt[CN_ACC_SINCE_REFRESH], refreshes = 0;
+    const long long refresh_every = (MX && A.mode == MODE_RUN) ? D.refresh_every : 0;
     int xpar = 0;  // parity of the cluster exchange buffer, flipped after every pass
     const long long n_moves = (A.mode == MODE_RUN) ? run->n_moves : 1;
     long long *prof = (A.prof && rank == 0) ? A.prof : nullptr;
@@ -1143,10 +1262,17 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
         }
         ++moves_done;
         have_next = sh.spec_ok != 0;
-        acc_seen += sh.accepted;
         __syncthreads();
         YAMC_PH(PH_COMMIT);
-        if (acc_limit > 0 && acc_seen >= acc_limit) break;  // same decision in every CTA
+        if constexpr (MX) {
+            acc_since += sh.accepted;  // the same decisions in every CTA: every thread agrees
+            if (refresh_every > 0 && acc_since >= refresh_every) {
+                refresh_in_chain<NT, EPT>(D, R, scr, scr_atoms, e0, gwork, G, rank, sh, red, xch, xpar, cluster);
+                xpar ^= 1;
+                acc_since = 0;
+                ++refreshes;
+            }
+        }
     }
 #undef YAMC_PH
 
@@ -1160,6 +1286,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
         if (tid == 0 && rank == 0) {
             for (int c = 0; c < SC_COUNT; ++c) D.scal[c] = sh.sc[c];
             D.cnt[CN_ICYCLE] = sh.icycle;
+            D.cnt[CN_ACC_SINCE_REFRESH] = acc_since;
+            D.cnt[CN_REFRESHES] += refreshes;
             D.cnt[CN_MOVE_IN_CYCLE] = sh.mic;
             run->cursor = sh.cursor;
             run->moves_done = moves_done;

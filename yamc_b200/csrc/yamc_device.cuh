@@ -18,6 +18,7 @@ struct DevSys {
     int N, M, S, nt, kmax, npair, freq_monotone, n_species;
     double rmax2, alpha, xclb, taosp, kext, m2k, dr, d_angle, xlf, xlc, psm, n_store_energy_interval;
     double rpre;           // max(cutoff, largest hard-core diameter), box units: the pair filter's reach
+    long long refresh_every;  // mixed form: FP64 recomputation of rho(k) every this many accepted moves (0 = never)
     double4 *atom;         // x, y, z (box units), q
     const int2 *meta;      // 0-based molecule, LJ type (0 = none)
     const double *dhs;     // hard-core diameter / BoxLength
@@ -44,7 +45,7 @@ enum Scal {
     SC_N_MV_STEPS, SC_N_MV_ACC, SC_N_VOL_STEPS, SC_COUNT
 };
 // run_mc counters (int64)
-enum Cnt { CN_ICYCLE = 0, CN_MOVE_IN_CYCLE, CN_COUNT };
+enum Cnt { CN_ICYCLE = 0, CN_MOVE_IN_CYCLE, CN_ACC_SINCE_REFRESH, CN_REFRESHES, CN_COUNT };
 
 // ------------------------------------------------------------------ arithmetic helpers
 // 1/y rounded to nearest (the same value as the IEEE division 1/y) and 1/sqrt(y) (within an

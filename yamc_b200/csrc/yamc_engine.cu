@@ -395,8 +395,8 @@ struct yamc_ctx {
     long long *d_prof = nullptr;
     bool prof_on = false;
     double *d_gx = nullptr, *d_gy = nullptr, *d_gz = nullptr;  // adjoint forces
-    // mixed form: FP64 recomputation of rho(k) every refresh_every accepted moves
-    long long refresh_every = 10000, acc_since_refresh = 0, refreshes = 0;
+    // mixed form: FP64 recomputation of rho(k) every refresh_every accepted moves (in the chain kernel)
+    long long refresh_every = 10000;
 };
 
 namespace {
@@ -577,37 +577,6 @@ void energies_from(const double *sc, double kext, double e[8]) {
     e[3] = sc[SC_UU_EW]; e[4] = sc[SC_UU_LJ6]; e[5] = sc[SC_UU_LJ12]; e[6] = sc[SC_EK_C]; e[7] = sc[SC_EK_LJ];
 }
 
-// Mixed form: rho(k) again from the FP64 positions (RhoSquared_addAtoms) and the k-space
-// energies from it, replacing the running sums that FP32 deltas updated.
-int refresh_rho(yamc_ctx *c, cudaStream_t s) {
-    const HostSystem &H = c->H;
-    const int nbk = (H.S + 255) / 256;
-    cudaStream_t keep = c->stream;
-    c->stream = s;
-    int r = YAMC_OK;
-    switch (H.nt) {
-        case 1: r = launch_rho_full<1>(c); if (!r) r = launch_kspace_energy<1>(c, nbk); break;
-        case 2: r = launch_rho_full<2>(c); if (!r) r = launch_kspace_energy<2>(c, nbk); break;
-        case 3: r = launch_rho_full<3>(c); if (!r) r = launch_kspace_energy<3>(c, nbk); break;
-        default: r = launch_rho_full<4>(c); if (!r) r = launch_kspace_energy<4>(c, nbk); break;
-    }
-    c->stream = keep;
-    if (r) return r;
-    std::vector<double> pk((size_t)nbk * 2);
-    CUDA_TRY(cudaMemcpyAsync(pk.data(), c->part, sizeof(double) * pk.size(), cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaMemcpyAsync(c->sc, c->scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    double ekc = 0, ekl = 0;
-    for (int b = 0; b < nbk; ++b) { ekc += pk[2 * b]; ekl += pk[2 * b + 1]; }
-    c->sc[SC_EK_C] = ekc;
-    c->sc[SC_EK_LJ] = ekl;
-    CUDA_TRY(cudaMemcpyAsync(c->scal, c->sc, sizeof(double) * SC_COUNT, cudaMemcpyHostToDevice, s));
-    CUDA_TRY(cudaStreamSynchronize(s));
-    c->acc_since_refresh = 0;
-    c->refreshes += 1;
-    return YAMC_OK;
-}
-
 bool is_mixed(const yamc_ctx *c) { return c->H.p.precision == YAMC_MIXED; }
 
 int ensure_cfg(yamc_ctx *c) {
@@ -663,6 +632,7 @@ struct yamc_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
     cudaGraphExec_t graph = nullptr;
     float last_ms = 0.f;
+    int last_launches = 0;  // kernels launched by the last run (chain launches + refresh kernels)
     int force_G = 0, force_B = 0, force_layout = YAMC_KSPACE_AUTO;
     float *d_rng = nullptr;
     size_t rng_cap = 0;
@@ -735,54 +705,37 @@ int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, c
                int64_t *cursors, int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log) {
     int r = batch_build_graph(b);
     if (r) return r;
-    const size_t R = b->reps.size();
-    std::vector<long long> done(R, 0);
-    std::vector<int> st(R, YAMC_OK);
-    std::vector<char> active(R, 1);
+    for (BatchGroup &g : b->groups) {
+        // the replicas' DevSys again (their refresh settings may have changed since the batch began)
+        std::vector<DevSys> hs(g.idx.size());
+        for (size_t k = 0; k < g.idx.size(); ++k) hs[k] = b->reps[g.idx[k]]->hsys;
+        if ((r = upload(g.d_sys, hs.data(), hs.size(), b->stream))) return r;
+        for (size_t k = 0; k < g.idx.size(); ++k) {
+            const int i = g.idx[k];
+            RunSlot &rs = g.h_run[k];
+            rs = RunSlot{};
+            rs.rng = rng[i]; rs.rng_off = rng_off[i]; rs.n_rng = n_rng[i];
+            rs.cursor = cursors[i]; rs.n_moves = n_moves;
+            rs.log = d_log ? d_log + (size_t)i * n_moves : nullptr;
+        }
+    }
     CUDA_TRY(cudaEventRecord(b->ev0, b->stream));
-    // one graph launch, or (mixed replicas) launches that end at each replica's refresh budget
-    while (true) {
-        for (BatchGroup &g : b->groups)
-            for (size_t k = 0; k < g.idx.size(); ++k) {
-                const int i = g.idx[k];
-                const yamc_ctx *c = b->reps[i];
-                RunSlot &rs = g.h_run[k];
-                rs = RunSlot{};
-                rs.rng = rng[i]; rs.rng_off = rng_off[i]; rs.n_rng = n_rng[i];
-                rs.cursor = cursors[i]; rs.n_moves = active[i] ? n_moves - done[i] : 0;
-                rs.log = d_log ? d_log + (size_t)i * n_moves + done[i] : nullptr;
-                rs.acc_limit = (is_mixed(c) && c->refresh_every > 0) ? c->refresh_every - c->acc_since_refresh : 0;
-            }
-        CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
-        CUDA_TRY(cudaStreamSynchronize(b->stream));
-        bool more = false;
-        for (BatchGroup &g : b->groups)
-            for (size_t k = 0; k < g.idx.size(); ++k) {
-                const int i = g.idx[k];
-                yamc_ctx *c = b->reps[i];
-                const RunSlot &rs = g.h_run[k];
-                cursors[i] = rs.cursor;
-                done[i] += rs.moves_done;
-                st[i] = rs.status;
-                c->pos_valid = false;
-                if (is_mixed(c) && c->refresh_every > 0) {
-                    c->acc_since_refresh += rs.accepted;
-                    if (c->acc_since_refresh >= c->refresh_every && (r = refresh_rho(c, b->stream))) return r;
-                }
-                if (rs.status != YAMC_OK || done[i] >= n_moves) active[i] = 0;
-                more = more || active[i];
-            }
-        if (!more) break;
-    }
+    CUDA_TRY(cudaGraphLaunch(b->graph, b->stream));
     CUDA_TRY(cudaEventRecord(b->ev1, b->stream));
-    CUDA_TRY(cudaEventSynchronize(b->ev1));
+    CUDA_TRY(cudaStreamSynchronize(b->stream));
     cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
+    b->last_launches = (int)b->groups.size();
     int worst = YAMC_OK;
-    for (size_t i = 0; i < R; ++i) {
-        if (moves_done) moves_done[i] = done[i];
-        if (status) status[i] = st[i];
-        if (st[i] != YAMC_OK && (worst == YAMC_OK || worst == YAMC_ERNG_EXHAUSTED)) worst = st[i];
-    }
+    for (BatchGroup &g : b->groups)
+        for (size_t k = 0; k < g.idx.size(); ++k) {
+            const int i = g.idx[k];
+            const RunSlot &rs = g.h_run[k];
+            cursors[i] = rs.cursor;
+            if (moves_done) moves_done[i] = rs.moves_done;
+            if (status) status[i] = rs.status;
+            b->reps[i]->pos_valid = false;
+            if (rs.status != YAMC_OK && (worst == YAMC_OK || worst == YAMC_ERNG_EXHAUSTED)) worst = rs.status;
+        }
     return worst;
 }
 
@@ -897,6 +850,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.rmax2 = P.rmax2; D.alpha = P.alpha; D.xclb = P.xclb; D.taosp = P.two_alpha_over_sqrt_pi; D.kext = P.kext;
     D.m2k = P.minus_two_kext; D.dr = P.dr; D.d_angle = P.d_angle; D.xlf = P.xlambda_f; D.xlc = P.xlambda_c;
     D.psm = P.pressure_step_multiplier; D.n_store_energy_interval = P.n_store_energy_interval;
+    D.refresh_every = P.precision == YAMC_MIXED ? c->refresh_every : 0;
     D.rpre = std::sqrt(P.rmax2);
     for (int i = 0; i < N; ++i) D.rpre = std::max(D.rpre, H.dhs[i]);
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
@@ -1021,53 +975,42 @@ static int run_chain_impl(yamc_ctx *c, const float *d_rng, long long rng_off, lo
                           int32_t *n_rows) {
     int r = ensure_cfg(c);
     if (r) return r;
-    const bool refresh = is_mixed(c) && c->refresh_every > 0;
-    long long done = 0;
-    int rows = 0;
-    int status = YAMC_OK;
+    RunSlot rs{};
+    rs.rng = d_rng; rs.rng_off = rng_off; rs.n_rng = n_rng; rs.cursor = *cursor; rs.n_moves = n_moves;
+    rs.log = d_log; rs.rows = d_rows; rs.max_rows = max_rows;
+    if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
+    ChainArgs a = base_args(c, MODE_RUN);
     CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
-    // one launch, or (mixed form) launches that end at the refresh budget of accepted moves
-    while (true) {
-        RunSlot rs{};
-        rs.rng = d_rng; rs.rng_off = rng_off; rs.n_rng = n_rng; rs.cursor = *cursor; rs.n_moves = n_moves - done;
-        rs.log = d_log ? d_log + done : nullptr;
-        rs.rows = d_rows ? d_rows + 9 * (size_t)rows : nullptr;
-        rs.max_rows = max_rows - rows;
-        rs.acc_limit = refresh ? c->refresh_every - c->acc_since_refresh : 0;
-        if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
-        ChainArgs a = base_args(c, MODE_RUN);
-        if ((r = launch_chain(c, a))) return r;
-        RunSlot back{};
-        CUDA_TRY(cudaMemcpyAsync(&back, c->d_run, sizeof(RunSlot), cudaMemcpyDeviceToHost, c->stream));
-        CUDA_TRY(cudaStreamSynchronize(c->stream));
-        c->pos_valid = false;
-        *cursor = back.cursor;
-        done += back.moves_done;
-        rows += back.n_rows;
-        status = back.status;
-        if (refresh) {
-            c->acc_since_refresh += back.accepted;
-            if (c->acc_since_refresh >= c->refresh_every && (r = refresh_rho(c, c->stream))) return r;
-        }
-        if (status != YAMC_OK || done >= n_moves || !refresh) break;
-    }
+    if ((r = launch_chain(c, a))) return r;
     CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
-    CUDA_TRY(cudaEventSynchronize(c->ev1));
+    RunSlot back{};
+    CUDA_TRY(cudaMemcpyAsync(&back, c->d_run, sizeof(RunSlot), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     cudaEventElapsedTime(&c->last_ms, c->ev0, c->ev1);
-    if (moves_done) *moves_done = done;
-    if (n_rows) *n_rows = rows;
-    return status;
+    c->pos_valid = false;
+    *cursor = back.cursor;
+    if (moves_done) *moves_done = back.moves_done;
+    if (n_rows) *n_rows = back.n_rows;
+    return back.status;
 }
 
 int yamc_set_refresh(yamc_ctx *c, int64_t accepted_moves) {
     if (!c || accepted_moves < 0) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(c->device));
     c->refresh_every = accepted_moves;
+    c->hsys.refresh_every = is_mixed(c) ? accepted_moves : 0;
+    int r = upload(c->d_sys, &c->hsys, 1, c->stream);
+    if (r) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     return YAMC_OK;
 }
 
 int yamc_refresh_count(yamc_ctx *c, int64_t *count) {
     if (!c || !count) return YAMC_EPARAMETER;
-    *count = c->refreshes;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int r = pull_state(c);
+    if (r) return r;
+    *count = c->cnt_h[CN_REFRESHES];
     return YAMC_OK;
 }
 
@@ -1412,6 +1355,12 @@ int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]) {
     return YAMC_OK;
 }
 
+int yamc_batch_last_launches(yamc_batch *b, int32_t *n) {
+    if (!b || !n) return YAMC_EPARAMETER;
+    *n = b->last_launches;
+    return YAMC_OK;
+}
+
 int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms) {
     if (!b || !ms) return YAMC_EPARAMETER;
     *ms = b->last_ms;
@@ -1426,6 +1375,7 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     BatchBackup keep;
     int r = batch_copy_state(b, keep, true);
     if (r) return r;
+
     const int fG = b->force_G, fB = b->force_B, fL = b->force_layout;
     const int Bs[] = {kChainMaxThreadsWide, kChainMaxThreads, 128};
     const int Ls[] = {YAMC_KSPACE_REGISTERS, YAMC_KSPACE_STREAMED};
@@ -1445,6 +1395,7 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
             r = yamc_batch_run_device(b, d_rng, n_rng, cur.data(), n_moves, done.data(), nullptr, nullptr);
             const int rr = batch_copy_state(b, keep, false);
             if (rr) return rr;
+
             if (r != YAMC_OK && r != YAMC_ERNG_EXHAUSTED) return r;
             double moves = 0;
             for (size_t i = 0; i < R; ++i) moves += (double)done[i];
