@@ -180,6 +180,85 @@ def run_reference(args, files, spec_name):
     print(json.dumps(line), flush=True)
 
 
+def target_block(local, rank, moves=2000, steps=3, warmup=2):
+    """The north-star comparison on 4096 SPC/E + 76 Na + 76 Cl (12,440 atoms, L = 50 A,
+    alpha = 0.28/A, rc = 12 A, kmax = 15): one plain FP64 chain (unbiased moves, the drop-in)
+    against a batch of mixed-precision force-biased chains (lambda = 0.1), all resident at once,
+    with the mixed chains' dE against FP64 chains on the same random stream."""
+    import torch
+    from yamc_b200 import _lib, api, rng as grng, systems
+    dev = f"cuda:{local}"
+    spec_b = systems.WORKLOADS["nacl4k"]                      # force-biased, lambda = 0.1
+    spec_p = systems.SystemSpec(**{**spec_b.__dict__, "name": "nacl4k_plain", "xlambda": 0.0})
+    base = f"/tmp/yamc_bench_target_r{rank}_{os.getpid()}"
+    fp = systems.write_system(spec_p, base + "_plain", seed=5)
+    per_move = 40
+    # one plain FP64 chain
+    eng = api.Engine.from_files(fp, device=local)
+    s0 = torch.from_numpy(grng.gfortran_stream(99, per_move * moves * (steps + warmup) + 10000)).to(dev)
+    cur = 0
+    ms = []
+    for w in range(warmup + steps):
+        cur, done, st = eng.run_chain_device(s0.data_ptr(), s0.numel(), moves, cursor=cur)
+        assert st == 0 and done == moves
+        if w >= warmup:
+            ms.append(eng.last_kernel_ms)
+    plain = moves * steps / (sum(ms) / 1e3)
+    plain_launch = eng.launch
+    eng.close()
+    del s0
+    # dE of mixed vs FP64 force-biased chains on the same stream
+    fb = systems.write_system(spec_b, base + "_b0", seed=5)
+    n_chk = 1500
+    chk = grng.gfortran_stream(4243, 60 * n_chk + 10000)
+    logs = {}
+    for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
+        e = api.Engine.from_files(fb, device=local, precision=prec)
+        logs[prec] = e.run_chain(chk, n_chk)[0]
+        e.close()
+    lf, lm = logs[_lib.YAMC_FP64], logs[_lib.YAMC_MIXED]
+    same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
+    k = n_chk if same.all() else int(np.argmin(same))
+    cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
+    de = np.abs(sum(lm[c][:k] for c in cols) - sum(lf[c][:k] for c in cols)) if k else np.zeros(1)
+    # the mixed force-biased batch: as many chains as one shape keeps resident
+    inp0 = api.load_inputs(fb["parameters"], fb["composition"], fb["moltab"])
+    probe = api.Batch([inp0], device=local, precision=_lib.YAMC_MIXED)
+    R = 1
+    for G in range(1, 17):
+        try:
+            probe.set_launch(G, 0)
+        except Exception:
+            continue
+        R = max(R, probe.launch["resident_clusters"])
+    probe.close()
+    R = min(R, 148)
+    files = [fb] + [systems.write_system(spec_b, f"{base}_b{r}", seed=5 + 13 * r, rng_seed=777 + r) for r in range(1, R)]
+    b = api.Batch([api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in files], device=local,
+                  precision=_lib.YAMC_MIXED)
+    ds = [torch.from_numpy(grng.gfortran_stream(1000 + r, per_move * moves * (steps + warmup + 1) + 10000)).to(dev)
+          for r in range(R)]
+    ptrs, nr = [t.data_ptr() for t in ds], [t.numel() for t in ds]
+    curs = np.zeros(R, dtype=np.int64)
+    b.tune(ptrs, nr, curs, 200)
+    ms = []
+    for w in range(warmup + steps):
+        done, st, s_all = b.run_device(ptrs, nr, curs, moves)
+        assert s_all == 0 and (done == moves).all(), (s_all, done)
+        if w >= warmup:
+            ms.append(b.last_kernel_ms)
+    batched = R * moves * steps / (sum(ms) / 1e3)
+    out = {"workload": "nacl4k: 4096 SPC/E + 76 Na + 76 Cl, 12440 atoms, L=50 A, alpha=0.28/A, rc=12 A, kmax=15",
+           "plain_fp64_one_chain": {"value": plain, "unit": "moves/s", "launch": plain_launch},
+           "mixed_batched_force_biased": {"value": batched, "unit": "moves/s", "chains": R, "launch": b.launch,
+                                          "lambda": 0.1},
+           "ratio": batched / plain,
+           "de_error_mixed_vs_fp64_force_biased": {"max_kT": float(de.max()), "moves_compared": k},
+           "moves_per_step_per_chain": moves, "steps": steps}
+    b.close()
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -191,6 +270,7 @@ def main():
     ap.add_argument("--ref-moves", type=int, default=1500)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replicas", type=int, default=0, help="chains per GPU (0 = as many clusters as are resident)")
+    ap.add_argument("--no-target", action="store_true", help="skip the 4096-water mixed/batched/force-biased block")
     args = ap.parse_args()
 
     from yamc_b200 import systems
@@ -394,6 +474,8 @@ def main():
         "gpu_launches": int(sum(launch_counts)),
         "clocks": clk.summary(),
     }
+    if not args.no_target:
+        line["north_star_target"] = target_block(local, rank)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(files)
     print(json.dumps(line), flush=True)
