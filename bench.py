@@ -46,6 +46,24 @@ def dist_env():
     return ws, rank, local
 
 
+def max_over_ranks(x: float, device) -> float:
+    """The largest of every rank's x (the job's time is its slowest rank's); x itself at N = 1."""
+    ws, _, _ = dist_env()
+    if ws == 1:
+        return x
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_seeds(rank: int, r: int):
+    """(initial-configuration seed, random-stream seed) of chain r on rank `rank`: distinct for
+    every (rank, chain) of the job, so replicas are independent across GPUs too."""
+    return 3 + 1000 * rank + r, 12345 + 100000 * rank + 7 * r
+
+
 def peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -277,7 +295,7 @@ def main():
     ws, rank, local = dist_env()
     spec = systems.WORKLOADS[args.workload]
     wdir = f"/tmp/yamc_bench_{args.workload}_r{rank}_{os.getpid()}"
-    files = systems.write_system(spec, wdir, seed=3 + rank, rng_seed=12345 + rank)
+    files = systems.write_system(spec, wdir, seed=replica_seeds(rank, 0)[0], rng_seed=replica_seeds(rank, 0)[1])
 
     if args.impl == "reference":
         if ws > 1:
@@ -310,7 +328,7 @@ def main():
     # ---------------- one chain alone: the latency of the move, FP64 and mixed (beside the batch)
     def single_chain(precision):
         eng = api.Engine.from_files(files, device=local, precision=precision)
-        s0 = grng.gfortran_stream(12345 + 1000 * rank, per_move * args.moves * 3 + 100000)
+        s0 = grng.gfortran_stream(replica_seeds(rank, 0)[1], per_move * args.moves * 3 + 100000)
         d_s0 = torch.from_numpy(s0).to(dev)
         c0, _, _ = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves)
         ms = []
@@ -358,10 +376,10 @@ def main():
         R = min(148, max(resident.values(), default=1))
     probe.close()
     R = max(R, 1)
-    rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=3 + 101 * rank + r,
-                                                rng_seed=12345 + 1000 * rank + r) for r in range(1, R)]
+    rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=replica_seeds(rank, r)[0],
+                                                rng_seed=replica_seeds(rank, r)[1]) for r in range(1, R)]
     rep_inputs = [api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files]
-    streams = [grng.gfortran_stream(12345 + 1000 * rank + 7 * r, n_stream) for r in range(R)]
+    streams = [grng.gfortran_stream(replica_seeds(rank, r)[1], n_stream) for r in range(R)]
     d_streams = [torch.from_numpy(x).to(dev) for x in streams]
     d_ptrs = [t.data_ptr() for t in d_streams]
     n_rng = [t.numel() for t in d_streams]
@@ -386,11 +404,7 @@ def main():
                 counts.append(b.last_launches)
                 l2_flush()
         torch.cuda.synchronize()
-        t = sum(ms) / 1e3
-        if ws > 1:
-            tt = torch.tensor([t], device=dev)
-            dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-            t = float(tt.item())
+        t = max_over_ranks(sum(ms) / 1e3, dev)
         return b, cur, ms, t, counts
 
     b64, _, ms64, t64, _ = timed_batch(_lib.YAMC_FP64)
@@ -427,11 +441,7 @@ def main():
         assert s_all == 0 and (done == args.moves).all(), (s_all, done)
         e_moves += int(done.sum())
         l2_flush()
-    t_e2e = sum(e_times)
-    if ws > 1:
-        t = torch.tensor([t_e2e], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        t_e2e = float(t.item())
+    t_e2e = max_over_ranks(sum(e_times), dev)
     e2e = ws * e_moves / t_e2e
     d2h = R * (run_slot + 8 * 17 + 8 * 2)  # run slot + engine scalars + counters per replica
 
