@@ -92,10 +92,10 @@ def test_chain_streamed_spce256(spce_files):
 
 @pytest.mark.parametrize("cluster", [1, 3])
 def test_chain_streamed_wide(spce_files, cluster):
-    """Streamed entries with 512-thread CTAs (15 worker warps)."""
-    o, olog, ocur, eng, glog, gcur = _run_pair(spce_files, 5000, cluster=cluster, threads=512,
+    """Streamed entries with 384-thread CTAs (11 worker warps)."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(spce_files, 5000, cluster=cluster, threads=384,
                                                layout=_lib.YAMC_KSPACE_STREAMED)
-    assert eng.launch["threads"] == 512 and eng.launch["entries_per_thread"] == 0
+    assert eng.launch["threads"] == 384 and eng.launch["entries_per_thread"] == 0
     compare_logs(glog, olog)
     assert rel_close(eng.energies(), o.energies(), 1e-9)
 

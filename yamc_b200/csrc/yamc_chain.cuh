@@ -21,12 +21,19 @@
         }                                                                                     \
     } while (0)
 
+#ifndef YAMC_WIDE_THREADS
+#define YAMC_WIDE_THREADS 384  // threads of the wide streamed variant (up to 170 registers each)
+#endif
+#ifndef YAMC_KSPACE_UNROLL
+#define YAMC_KSPACE_UNROLL 1  // streamed k entries handled per loop iteration
+#endif
+
 namespace yamc {
 
 namespace cg = cooperative_groups;
 
 struct LaunchCfg {
-    int G = 0, B = 0, EPT = 0;  // EPT: entries per worker in registers; 0 streamed; -1 streamed, 512 threads
+    int G = 0, B = 0, EPT = 0;  // EPT: entries per worker in registers; 0 streamed; -1 streamed, wide CTAs
     int nown_max = 0, qcap = 0;
     size_t smem = 0;
 };
@@ -89,7 +96,7 @@ constexpr int kCPT = 4;   // atoms each worker thread tests per filter round
 constexpr int kWin = 256; // random-stream window held in shared memory
 constexpr int kCtl = 32;  // threads of the control warp
 constexpr int kChainMaxThreads = 256;  // one CTA per SM, up to 255 registers per thread
-constexpr int kChainMaxThreadsWide = 512;  // streamed k entries, 16 warps, up to 128 registers per thread
+constexpr int kChainMaxThreadsWide = YAMC_WIDE_THREADS;  // streamed k entries, more warps, fewer registers
 
 // a prepared move: the molecule, its atoms at the old and proposed positions, the proposal
 struct Cand {
@@ -213,15 +220,24 @@ struct EntryRegs {
     R2 dl[EPT][1 + NT];
 };
 
-// EPT <= 0: the streamed layout (EPT == -1: the same with 512-thread CTAs) -- no entry lives in
+// EPT <= 0: the streamed layout (EPT == -1: the same with wide CTAs) -- no entry lives in
 // registers; each worker loops over its entries and reads k, beta, beta_LJ and rho from memory
 // (L2-resident) every pass.  The register block of one (never touched) entry only keeps the
 // code uniform.
 template <int NT, int EPT, bool MX = false>
 using RegsOf = EntryRegs<NT, (EPT > 0 ? EPT : 1), MX>;
 
-// Phase tables of slots [s0, s1) of move m: T[slot][axis][k] = (cos, sin)(2 pi k u), by the
-// workers.  The FP32 form reduces 2 k u modulo 2 in FP64 before the FP32 sincospi.
+// The per-move phase tables of the molecule's slots, T[slot][axis][m] = (cos, sin)(2 pi m u),
+// and tmask: the LJ types the moving molecule carries.
+template <bool MX>
+struct PhaseTabs {
+    const typename Prec<MX>::R2 *T;
+    int KM;
+    int tmask;
+};
+
+// Phase tables of slots [s0, s1) of move m, by the workers.  The FP32 form reduces 2 k u
+// modulo 2 in FP64 before the FP32 sincospi.
 template <bool MX>
 __device__ __forceinline__ void build_tables(typename Prec<MX>::R2 *tab, const Cand &m, int s0, int s1, int KM, int wtid,
                                              int nwork) {
@@ -247,11 +263,12 @@ __device__ __forceinline__ void build_tables(typename Prec<MX>::R2 *tab, const C
 // Coulomb phase q (cos, sin), LJ phase = Coulomb phase * (1/q) (the unit phase when q == 0),
 // accumulated per LJ type in atom order.  ph/phl keep the per-atom phases for the forces.
 template <int NT, bool MX>
-__device__ __forceinline__ void mol_phase_sum(const typename Prec<MX>::R2 *tab, const Cand &m, int s0, int na, int KM,
-                                              int kx, int ky, int kz, typename Prec<MX>::R2 (&out)[1 + NT],
+__device__ __forceinline__ void mol_phase_sum(const PhaseTabs<MX> &pt, const Cand &m, int s0, int na, int kx, int ky,
+                                              int kz, typename Prec<MX>::R2 (&out)[1 + NT],
                                               typename Prec<MX>::R2 (&ph)[kMaxA], typename Prec<MX>::R2 (&phl)[kMaxA]) {
     using R = typename Prec<MX>::R;
     using R2 = typename Prec<MX>::R2;
+    const int KM = pt.KM;
 #pragma unroll
     for (int t = 0; t <= NT; ++t) out[t] = mk2(R(0), R(0));
 #pragma unroll
@@ -260,7 +277,7 @@ __device__ __forceinline__ void mol_phase_sum(const typename Prec<MX>::R2 *tab, 
         phl[a] = mk2(R(0), R(0));
         if (a < na) {
             const Slot &sl = m.slot[s0 + a];
-            const R2 *T = tab + (size_t)(s0 + a) * 3 * KM;
+            const R2 *T = pt.T + (size_t)(s0 + a) * 3 * KM;
             const R q = (R)sl.q;
             R c = 0, s = 0;
             if (sl.q != 0.0) {
@@ -318,7 +335,7 @@ __device__ __forceinline__ void entry_forces(const Cand &m, int s0, int na, int 
 // One signed entry of a pass: the molecule's phase sums at the old positions (into mold) and/or
 // the new ones, the delta (into dl), dU_k Coulomb + LJ against rho, and the k-space forces.
 template <int NT, int KIND, bool FORCES, bool MX>
-__device__ __forceinline__ void kspace_entry(const typename Prec<MX>::R2 *tab, const Cand &m, int na, int KM, int kx,
+__device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Cand &m, int na, int kx,
                                              int ky, int kz, typename Prec<MX>::R beta,
                                              const typename Prec<MX>::R (&bl)[NPair<NT>::value],
                                              const double2 (&rho)[1 + NT], typename Prec<MX>::R2 (&mold)[1 + NT],
@@ -329,12 +346,12 @@ __device__ __forceinline__ void kspace_entry(const typename Prec<MX>::R2 *tab, c
     R2 C[1 + NT];
 #pragma unroll
     for (int t = 0; t <= NT; ++t) C[t] = cvt2<R2>(rho[t]);
-    if constexpr (KIND != PASS_NEW) mol_phase_sum<NT, MX>(tab, m, na, na, KM, kx, ky, kz, mold, ph, phl);
+    if constexpr (KIND != PASS_NEW) mol_phase_sum<NT, MX>(pt, m, na, na, kx, ky, kz, mold, ph, phl);
     if constexpr (KIND == PASS_OLD) {
         if constexpr (FORCES) entry_forces<NT, MX>(m, na, na, kx, ky, kz, beta, bl, C, ph, phl, acc);
     } else {
         R2 mnew[1 + NT];
-        mol_phase_sum<NT, MX>(tab, m, 0, na, KM, kx, ky, kz, mnew, ph, phl);
+        mol_phase_sum<NT, MX>(pt, m, 0, na, kx, ky, kz, mnew, ph, phl);
 #pragma unroll
         for (int t = 0; t <= NT; ++t) dl[t] = mk2(mnew[t].x - mold[t].x, mnew[t].y - mold[t].y);
         {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
@@ -349,8 +366,8 @@ __device__ __forceinline__ void kspace_entry(const typename Prec<MX>::R2 *tab, c
             const R tc = (C1.x + C1.x) + D1.x, ts = (C1.y + C1.y) + D1.y;
 #pragma unroll
             for (int t2 = 0; t2 < NT; ++t2) {
+                if (!((pt.tmask >> t2) & 1)) continue;
                 const R2 D2 = dl[1 + t2];
-                if (D2.x == R(0) && D2.y == R(0)) continue;
                 acc.add(RV_DUL, (tc * D2.x + ts * D2.y) * bl[pair_idx<NT>(t1, t2)]);
             }
         }
@@ -395,6 +412,10 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
     build_tables<MX>(tab, m, s_lo, s_hi, KM, wtid, nwork);
     worker_sync(nwork);
     YAMC_WPH(PH_TABLES);
+    int tmask = 0;
+    for (int a = 0; a < na; ++a)
+        if (m.slot[a].type > 0) tmask |= 1 << (m.slot[a].type - 1);
+    const PhaseTabs<MX> pt{tab, KM, tmask};
 
     Acc<MX> acc;
     acc.zero();
@@ -403,7 +424,7 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
         static_for<0, EPT>([&](auto kc) {
             constexpr int k = decltype(kc)::value;
             if (R.e[k] < 0) return;
-            kspace_entry<NT, KIND, FORCES, MX>(tab, m, na, KM, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k],
+            kspace_entry<NT, KIND, FORCES, MX>(pt, m, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k],
                                                R.mold[k], R.dl[k], acc);
         });
     } else {
@@ -413,38 +434,58 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
         const int S = D.S;
         double2 *mold_g = D.scratch;
         double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
-        int4 kv_n = make_int4(0, 0, 0, 0);
-        Rt beta_n = Rt(0), bl_n[NPair<NT>::value];
-        double2 rho_n[1 + NT];
-        R2 mold_n[1 + NT];
-        auto fetch = [&](int e) {
-            kv_n = D.kvec[e];
-            beta_n = (Rt)D.ebeta[e];
+        // U entries per iteration: their independent dependency chains interleave
+        constexpr int U = YAMC_KSPACE_UNROLL;
+        int4 kv_n[U];
+        Rt beta_n[U], bl_n[U][NPair<NT>::value];
+        double2 rho_n[U][1 + NT];
+        R2 mold_n[U][1 + NT];
+        auto fetch = [&](int j, int e) {
+            kv_n[j] = D.kvec[e];
+            beta_n[j] = (Rt)D.ebeta[e];
 #pragma unroll
-            for (int p = 0; p < NPair<NT>::value; ++p) bl_n[p] = (Rt)D.ebetalj[(size_t)p * S + e];
+            for (int p = 0; p < NPair<NT>::value; ++p) bl_n[j][p] = (Rt)D.ebetalj[(size_t)p * S + e];
 #pragma unroll
             for (int t = 0; t <= NT; ++t) {
-                rho_n[t] = D.rho[(size_t)t * S + e];
-                mold_n[t] = (KIND == PASS_NEW) ? cvt2<R2>(mold_g[(size_t)t * S + e]) : mk2(Rt(0), Rt(0));
+                rho_n[j][t] = D.rho[(size_t)t * S + e];
+                mold_n[j][t] = (KIND == PASS_NEW) ? cvt2<R2>(mold_g[(size_t)t * S + e]) : mk2(Rt(0), Rt(0));
             }
         };
-        if (e0 < S) fetch(e0);
-        for (int e = e0; e < S; e += estep) {
-            const int kx = kv_n.x, ky = kv_n.y, kz = kv_n.z;
-            const Rt beta = beta_n;
-            Rt bl[NPair<NT>::value];
-            double2 rho[1 + NT];
-            R2 mold[1 + NT], dl[1 + NT];
+        const int step = U * estep;
 #pragma unroll
-            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = bl_n[p];
+        for (int j = 0; j < U; ++j)
+            if (e0 + j * estep < S) fetch(j, e0 + j * estep);
+        for (int e = e0; e < S; e += step) {
+            int kx[U], ky[U], kz[U];
+            Rt beta[U], bl[U][NPair<NT>::value];
+            double2 rho[U][1 + NT];
+            R2 mold[U][1 + NT], dl[U][1 + NT];
 #pragma unroll
-            for (int t = 0; t <= NT; ++t) { rho[t] = rho_n[t]; mold[t] = mold_n[t]; }
-            if (e + estep < S) fetch(e + estep);
-            kspace_entry<NT, KIND, FORCES, MX>(tab, m, na, KM, kx, ky, kz, beta, bl, rho, mold, dl, acc);
+            for (int j = 0; j < U; ++j) {
+                kx[j] = kv_n[j].x; ky[j] = kv_n[j].y; kz[j] = kv_n[j].z;
+                beta[j] = beta_n[j];
 #pragma unroll
-            for (int t = 0; t <= NT; ++t) {
-                if (KIND == PASS_OLD) mold_g[(size_t)t * S + e] = to_d2(mold[t]);
-                else dl_g[(size_t)t * S + e] = to_d2(dl[t]);
+                for (int p = 0; p < NPair<NT>::value; ++p) bl[j][p] = bl_n[j][p];
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) { rho[j][t] = rho_n[j][t]; mold[j][t] = mold_n[j][t]; }
+            }
+#pragma unroll
+            for (int j = 0; j < U; ++j)
+                if (e + step + j * estep < S) fetch(j, e + step + j * estep);
+#pragma unroll
+            for (int j = 0; j < U; ++j)
+                if (e + j * estep < S)
+                    kspace_entry<NT, KIND, FORCES, MX>(pt, m, na, kx[j], ky[j], kz[j], beta[j], bl[j], rho[j], mold[j],
+                                                       dl[j], acc);
+#pragma unroll
+            for (int j = 0; j < U; ++j) {
+                const int ej = e + j * estep;
+                if (ej >= S) continue;
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) {
+                    if (KIND == PASS_OLD) mold_g[(size_t)t * S + ej] = to_d2(mold[j][t]);
+                    else dl_g[(size_t)t * S + ej] = to_d2(dl[j][t]);
+                }
             }
         }
     }
@@ -468,6 +509,15 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
     }
     const double cnx = m.slot[0].x, cny = m.slot[0].y, cnz = m.slot[0].z;
     const double cox = m.slot[na].x, coy = m.slot[na].y, coz = m.slot[na].z;
+    // a pass over both positions tests one sphere around the midpoint of the two centres that
+    // holds both spheres (the centre may have been wrapped: the shift is taken by minimum image)
+    double cbx = cox, cby = coy, cbz = coz, rb2 = rp2;
+    if (KIND == PASS_BOTH) {
+        const double hx = 0.5 * min_image(cnx - cox), hy = 0.5 * min_image(cny - coy), hz = 0.5 * min_image(cnz - coz);
+        cbx = cox + hx; cby = coy + hy; cbz = coz + hz;
+        const double rb = (sqrt(rp2) + sqrt(hx * hx + hy * hy + hz * hz)) * (1.0 + 1e-9);
+        rb2 = rb * rb;
+    }
 
     const int round_atoms = nwork * kCPT;
     int *nb = nearbuf + wwarp * 32 * kCPT;  // this warp's near atoms of the round
@@ -480,13 +530,15 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
             bool near = false;
             if (jl < nown && meta_s[jl].x != imol0) {
                 const double4 pj = atom_s[jl];
-                if (KIND != PASS_OLD) {
+                if (KIND == PASS_BOTH) {
+                    const double dx = min_image(cbx - pj.x), dy = min_image(cby - pj.y), dz = min_image(cbz - pj.z);
+                    near = dx * dx + dy * dy + dz * dz < rb2;
+                } else if (KIND == PASS_NEW) {
                     const double dx = min_image(cnx - pj.x), dy = min_image(cny - pj.y), dz = min_image(cnz - pj.z);
                     near = dx * dx + dy * dy + dz * dz < rp2;
-                }
-                if (KIND != PASS_NEW) {
+                } else {
                     const double dx = min_image(cox - pj.x), dy = min_image(coy - pj.y), dz = min_image(coz - pj.z);
-                    near = near || dx * dx + dy * dy + dz * dz < rp2;
+                    near = dx * dx + dy * dy + dz * dz < rp2;
                 }
             }
             const unsigned bal = __ballot_sync(0xffffffffu, near);

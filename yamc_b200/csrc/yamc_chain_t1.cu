@@ -5,7 +5,7 @@
 namespace yamc {
 
 #ifdef YAMC_ONE_VARIANT  // development builds: fewer instantiations
-#define YAMC_EPTS(X) X(0) X(2)
+#define YAMC_EPTS(X) X(-1) X(0) X(2)
 #else
 #define YAMC_EPTS(X) X(-1) X(0) X(1) X(2)
 #endif

@@ -406,7 +406,7 @@ namespace {
 // from large to small when large_first (the shortest move for a lone chain), else from small to
 // large; B from 256 to 128 threads; force_G / force_B pin either (0 = free).
 int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, int force_G, int force_B, int layout,
-                    LaunchCfg *out, bool large_first = true) {
+                    bool mx, LaunchCfg *out, bool large_first = true) {
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, device));
     const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
@@ -426,7 +426,7 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
             const int nwork = B - kCtl;  // warp 0 is the control warp
             int EPT = (Smax + G * nwork - 1) / (G * nwork);
             // entries in registers (at most 2 per worker) or streamed from memory (EPT 0; EPT -1
-            // for 512-thread CTAs, which only the streamed layout runs)
+            // for the wide CTAs, which only the streamed layout runs)
             if (layout == YAMC_KSPACE_STREAMED || (layout == YAMC_KSPACE_AUTO && EPT > 2)) EPT = 0;
             if (B > kChainMaxThreads) {
                 if (layout == YAMC_KSPACE_REGISTERS) continue;
@@ -445,8 +445,10 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
     return YAMC_ELIMITS;
 }
 
+bool is_mixed(const yamc_ctx *c) { return c->H.p.precision == YAMC_MIXED; }
+
 int pick_launch(yamc_ctx *c, LaunchCfg *out) {
-    return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, c->force_layout, out);
+    return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, c->force_layout, is_mixed(c), out);
 }
 
 int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, bool mx, cudaStream_t stream, int nrep,
@@ -577,7 +579,6 @@ void energies_from(const double *sc, double kext, double e[8]) {
     e[3] = sc[SC_UU_EW]; e[4] = sc[SC_UU_LJ6]; e[5] = sc[SC_UU_LJ12]; e[6] = sc[SC_EK_C]; e[7] = sc[SC_EK_LJ];
 }
 
-bool is_mixed(const yamc_ctx *c) { return c->H.p.precision == YAMC_MIXED; }
 
 int ensure_cfg(yamc_ctx *c) {
     if (c->cfg.G) return YAMC_OK;
@@ -653,7 +654,7 @@ int batch_configure(yamc_batch *b) {
     for (BatchGroup &g : b->groups) {
         std::vector<const HostSystem *> hs;
         for (int i : g.idx) hs.push_back(&b->reps[i]->H);
-        int r = pick_launch_for(hs, b->device, b->force_G, b->force_B, b->force_layout, &g.cfg);
+        int r = pick_launch_for(hs, b->device, b->force_G, b->force_B, b->force_layout, g.mx, &g.cfg);
         if (r) return r;
         if ((r = max_clusters_cfg(g.cfg, g.nt, g.split, g.mx, &g.max_clusters))) return r;
     }
