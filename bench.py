@@ -277,6 +277,54 @@ def target_block(local, rank, moves=2000, steps=3, warmup=2):
     return out
 
 
+def config4_block(local, rank, n_replicas=96, moves=10000):
+    """Ragged replicas (water log-uniform 216..4096, NaCl 0..2 M, density 0.0334 +- 2 %, T 280..360 K,
+    alpha = 5.6/L, cutoff min(12 A, L/2), one k-set), mixed precision, force-biased (lambda = 0.1),
+    all in one batch: one graph launch per kernel-variant group, launch shape from the autotuner,
+    `moves` trial moves per replica.  dE of the mixed form against FP64 on two replicas."""
+    import torch
+    from yamc_b200 import _lib, api, rng as grng, systems
+    dev = f"cuda:{local}"
+    specs = systems.batch_specs(n_replicas, seed=7)
+    base = f"/tmp/yamc_bench_c4_r{rank}_{os.getpid()}"
+    files = [systems.write_system(sp, f"{base}_{i}", seed=11 + i, rng_seed=900 + i) for i, sp in enumerate(specs)]
+    inputs = [api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in files]
+    b = api.Batch(inputs, device=local, precision=_lib.YAMC_MIXED)
+    per_move = 40
+    ds = [torch.from_numpy(grng.gfortran_stream(5000 + i, per_move * (moves + 400) + 10000)).to(dev)
+          for i in range(n_replicas)]
+    ptrs, nr = [t.data_ptr() for t in ds], [t.numel() for t in ds]
+    cur = np.zeros(n_replicas, dtype=np.int64)
+    b.tune(ptrs, nr, cur, 200)
+    done, st, s_all = b.run_device(ptrs, nr, cur, 200)  # warm-up
+    done, st, s_all = b.run_device(ptrs, nr, cur, moves)
+    assert s_all == 0 and (done == moves).all(), (s_all, done)
+    ms = b.last_kernel_ms
+    launch = b.groups
+    b.close()
+    # mixed against FP64 on the smallest and the largest replica, same random stream
+    de = []
+    natoms = [inp.natom for inp in inputs]
+    for i in (int(np.argmin(natoms)), int(np.argmax(natoms))):
+        chk = grng.gfortran_stream(6000 + i, 60 * 1000 + 10000)
+        logs = []
+        for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
+            e = api.Engine(inputs[i], device=local, precision=prec)
+            logs.append(e.run_chain(chk, 1000)[0])
+            e.close()
+        lf, lm = logs
+        same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
+        k = 1000 if same.all() else int(np.argmin(same))
+        cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
+        if k:
+            de.append(float(np.abs(sum(lm[c][:k] for c in cols) - sum(lf[c][:k] for c in cols)).max()))
+    return {"workload": f"{n_replicas} ragged replicas: water 216..4096 (log-uniform), NaCl 0..2 M, T 280..360 K, "
+                        f"alpha = 5.6/L, kmax {specs[0].kmax}; {min(natoms)}..{max(natoms)} atoms",
+            "method": "mixed precision, force-biased (lambda = 0.1), one batch", "moves_per_replica": moves,
+            "value": n_replicas * moves / (ms / 1e3), "unit": "moves/s", "ms": ms, "launch": launch,
+            "de_error_vs_fp64_max_kT": max(de) if de else None}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -289,6 +337,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replicas", type=int, default=0, help="chains per GPU (0 = as many clusters as are resident)")
     ap.add_argument("--no-target", action="store_true", help="skip the 4096-water mixed/batched/force-biased block")
+    ap.add_argument("--no-config4", action="store_true", help="skip the 96 ragged replicas block")
     args = ap.parse_args()
 
     from yamc_b200 import systems
@@ -486,6 +535,8 @@ def main():
     }
     if not args.no_target:
         line["north_star_target"] = target_block(local, rank)
+    if not args.no_config4:
+        line["batch_ragged_96"] = config4_block(local, rank)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(files)
     print(json.dumps(line), flush=True)

@@ -239,10 +239,15 @@ int yamc_batch_run_device(yamc_batch *b, const float *const *d_rng, const int64_
    [cursors[i], n_rng[i]) is copied to the device) and the log in host memory. */
 int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng, int64_t *cursors,
                    int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *log);
-/* Autotuner: times every launch shape (k-space layout x cluster size x threads per block) that fits
-   all replicas on n_moves moves of each and keeps the one with the highest
-   aggregate moves/s.  The replicas' state is put back after every trial, so the
-   chains do not advance. */
+/* Replicas are grouped by kernel variant (LJ type count, force bias, precision)
+   and size class (atom count up to 1024 / 2048 / 4096 / 8192 / more); each group
+   is one cluster launch with a shape of its own, the groups run concurrently.
+   Autotuner: for each group alone, times every launch shape (k-space layout x
+   cluster size x threads per block) that fits its replicas on n_moves moves of
+   each and keeps the one with the most moves/s per SM it occupies (the groups
+   share the GPU).  The replicas' state is put back after every trial, so the
+   chains do not advance.  best_moves_per_s: the sum of the chosen shapes' rates
+   measured alone. */
 int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng,
                     const int64_t *cursors, int64_t n_moves, double *best_moves_per_s);
 int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads);
@@ -250,6 +255,10 @@ int yamc_batch_set_kspace_layout(yamc_batch *b, int32_t layout);
 /* out: cluster blocks, threads, entries per thread, shared memory bytes, clusters
    resident at once (of the first group) */
 int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]);
+/* the groups: their number, and per group the out[5] above plus its replica count
+   and precision (1 = mixed) */
+int yamc_batch_groups(yamc_batch *b, int32_t *n);
+int yamc_batch_group_launch(yamc_batch *b, int32_t group, int32_t out[7]);
 /* device time (ms, CUDA events on the batch stream) of the last run, and the kernels it
    launched (one chain launch per variant group) */
 int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms);

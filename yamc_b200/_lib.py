@@ -106,6 +106,8 @@ SIGNATURES = {
     "yamc_batch_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),
     "yamc_batch_set_kspace_layout": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_batch_get_launch": (ctypes.c_int, [_VP, _ip]),
+    "yamc_batch_groups": (ctypes.c_int, [_VP, _ip]),
+    "yamc_batch_group_launch": (ctypes.c_int, [_VP, ctypes.c_int32, _ip]),
     "yamc_batch_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_batch_last_launches": (ctypes.c_int, [_VP, _ip]),
     "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +

@@ -347,6 +347,20 @@ class Batch:
                 "smem_bytes": int(out[3]), "resident_clusters": int(out[4])}
 
     @property
+    def groups(self):
+        """Launch shape of every group (kernel variant x size class) of the batch."""
+        n = ctypes.c_int32(0)
+        check(self.lib.yamc_batch_groups(self.h, ctypes.byref(n)), "yamc_batch_groups")
+        out = []
+        for g in range(n.value):
+            v = np.zeros(7, dtype=np.int32)
+            check(self.lib.yamc_batch_group_launch(self.h, g, _iptr(v)), "yamc_batch_group_launch")
+            out.append({"cluster_blocks": int(v[0]), "threads": int(v[1]), "entries_per_thread": int(v[2]),
+                        "smem_bytes": int(v[3]), "resident_clusters": int(v[4]), "replicas": int(v[5]),
+                        "mixed": bool(v[6])})
+        return out
+
+    @property
     def last_kernel_ms(self) -> float:
         v = ctypes.c_double(0)
         check(self.lib.yamc_batch_last_kernel_ms(self.h, ctypes.byref(v)), "yamc_batch_last_kernel_ms")

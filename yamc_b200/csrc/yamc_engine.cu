@@ -20,6 +20,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -409,7 +410,8 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
                     bool mx, LaunchCfg *out, bool large_first = true) {
     cudaDeviceProp prop;
     CUDA_TRY(cudaGetDeviceProperties(&prop, device));
-    const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - 1024;
+    // the kernel's static shared memory (ChainShared and the two random-stream windows) comes first
+    const size_t smem_max = prop.sharedMemPerBlockOptin - sizeof(ChainShared) - sizeof(float) * 2 * kWin - 256;
     int Smax = 0, Nmax = 0, Nmin = 1 << 30, kmax = 0, nt = 0;
     for (const HostSystem *h : hosts) {
         Smax = std::max(Smax, h->S); Nmax = std::max(Nmax, h->N); Nmin = std::min(Nmin, h->N);
@@ -615,6 +617,8 @@ struct BatchGroup {
     int nt = 0;
     bool split = false;
     bool mx = false;            // mixed precision
+    int size_class = 0;         // replicas of similar atom counts share a launch shape
+    int fG = 0, fB = 0, fL = YAMC_KSPACE_AUTO;  // the group's tuned shape (0 / AUTO: the batch's)
     LaunchCfg cfg;
     int max_clusters = 0;       // resident at once for cfg
     DevSys *d_sys = nullptr;    // [n]
@@ -654,7 +658,10 @@ int batch_configure(yamc_batch *b) {
     for (BatchGroup &g : b->groups) {
         std::vector<const HostSystem *> hs;
         for (int i : g.idx) hs.push_back(&b->reps[i]->H);
-        int r = pick_launch_for(hs, b->device, b->force_G, b->force_B, b->force_layout, g.mx, &g.cfg);
+        const int G = g.fG ? g.fG : b->force_G, B = g.fB ? g.fB : b->force_B;
+        const int L = g.fL != YAMC_KSPACE_AUTO ? g.fL : b->force_layout;
+        // a batch prefers the smallest cluster that fits: more chains resident at once
+        int r = pick_launch_for(hs, b->device, G, B, L, g.mx, &g.cfg, false);
         if (r) return r;
         if ((r = max_clusters_cfg(g.cfg, g.nt, g.split, g.mx, &g.max_clusters))) return r;
     }
@@ -703,10 +710,13 @@ int batch_build_graph(yamc_batch *b) {
 
 // one step of every replica: replica i's stream holds positions [rng_off[i], n_rng[i]) at rng[i]
 int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, const int64_t *n_rng,
-               int64_t *cursors, int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log) {
+               int64_t *cursors, int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log,
+               int only_group = -1) {
     int r = batch_build_graph(b);
     if (r) return r;
-    for (BatchGroup &g : b->groups) {
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        BatchGroup &g = b->groups[gi];
+        const bool on = only_group < 0 || (int)gi == only_group;  // a group left out runs no moves
         // the replicas' DevSys again (their refresh settings may have changed since the batch began)
         std::vector<DevSys> hs(g.idx.size());
         for (size_t k = 0; k < g.idx.size(); ++k) hs[k] = b->reps[g.idx[k]]->hsys;
@@ -716,7 +726,7 @@ int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, c
             RunSlot &rs = g.h_run[k];
             rs = RunSlot{};
             rs.rng = rng[i]; rs.rng_off = rng_off[i]; rs.n_rng = n_rng[i];
-            rs.cursor = cursors[i]; rs.n_moves = n_moves;
+            rs.cursor = cursors[i]; rs.n_moves = on ? n_moves : 0;
             rs.log = d_log ? d_log + (size_t)i * n_moves : nullptr;
         }
     }
@@ -1219,15 +1229,17 @@ static int batch_create_impl(yamc_batch *b, int32_t n, const yamc_system *system
         const HostSystem &H = b->reps[i]->H;
         const bool split = split_variant(H, MODE_RUN);
         const bool mx = H.p.precision == YAMC_MIXED;
+        const int cls = H.N <= 1024 ? 0 : H.N <= 2048 ? 1 : H.N <= 4096 ? 2 : H.N <= 8192 ? 3 : 4;
         size_t k = 0;
-        while (k < b->groups.size() &&
-               !(b->groups[k].nt == H.nt && b->groups[k].split == split && b->groups[k].mx == mx))
+        while (k < b->groups.size() && !(b->groups[k].nt == H.nt && b->groups[k].split == split &&
+                                         b->groups[k].mx == mx && b->groups[k].size_class == cls))
             ++k;
         if (k == b->groups.size()) {
             b->groups.emplace_back();
             b->groups.back().nt = H.nt;
             b->groups.back().split = split;
             b->groups.back().mx = mx;
+            b->groups.back().size_class = cls;
         }
         b->groups[k].idx.push_back(i);
     }
@@ -1334,8 +1346,14 @@ int yamc_batch_set_launch(yamc_batch *b, int32_t cluster_blocks, int32_t threads
     const int oG = b->force_G, oB = b->force_B;
     b->force_G = cluster_blocks;
     b->force_B = threads;
+    std::vector<std::array<int, 3>> keep;
+    for (BatchGroup &g : b->groups) { keep.push_back({g.fG, g.fB, g.fL}); g.fG = 0; g.fB = 0; g.fL = YAMC_KSPACE_AUTO; }
     const int r = batch_configure(b);
-    if (r) { b->force_G = oG; b->force_B = oB; batch_configure(b); }
+    if (r) {
+        b->force_G = oG; b->force_B = oB;
+        for (size_t k = 0; k < keep.size(); ++k) { b->groups[k].fG = keep[k][0]; b->groups[k].fB = keep[k][1]; b->groups[k].fL = keep[k][2]; }
+        batch_configure(b);
+    }
     return r;
 }
 
@@ -1376,45 +1394,68 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     BatchBackup keep;
     int r = batch_copy_state(b, keep, true);
     if (r) return r;
-
-    const int fG = b->force_G, fB = b->force_B, fL = b->force_layout;
+    for (size_t i = 0; i < R; ++i)
+        if (!d_rng[i] || n_rng[i] < 0 || cursors[i] < 0 || cursors[i] > n_rng[i]) return YAMC_EPARAMETER;
     const int Bs[] = {kChainMaxThreadsWide, kChainMaxThreads, 128};
     const int Ls[] = {YAMC_KSPACE_REGISTERS, YAMC_KSPACE_STREAMED};
-    double best = -1.0;
-    int bestG = 0, bestB = 0, bestL = 0;
-    std::vector<int64_t> cur(R), done(R);
-    for (int L : Ls)
-    for (int G = 1; G <= 16; ++G) {
-        for (int B : Bs) {
-            if (fL != YAMC_KSPACE_AUTO && L != fL) continue;
-            b->force_G = G; b->force_B = B; b->force_layout = L;
-            if (batch_configure(b) != YAMC_OK) continue;  // shape does not fit
-            bool ok = true;
-            for (const BatchGroup &g : b->groups) ok = ok && g.cfg.G == G && g.cfg.B == B && g.max_clusters > 0;
-            if (!ok) continue;
-            for (size_t i = 0; i < R; ++i) cur[i] = cursors[i];
-            r = yamc_batch_run_device(b, d_rng, n_rng, cur.data(), n_moves, done.data(), nullptr, nullptr);
-            const int rr = batch_copy_state(b, keep, false);
-            if (rr) return rr;
-
-            if (r != YAMC_OK && r != YAMC_ERNG_EXHAUSTED) return r;
-            double moves = 0;
-            for (size_t i = 0; i < R; ++i) moves += (double)done[i];
-            const double rate = b->last_ms > 0 ? moves / (1e-3 * b->last_ms) : 0.0;
-            if (rate > best) { best = rate; bestG = G; bestB = B; bestL = L; }
+    std::vector<int64_t> cur(R), done(R), off(R, 0);
+    double total = 0.0;
+    // every group on its own (the others run no moves): the shape with its highest moves/s
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        BatchGroup &g = b->groups[gi];
+        const int f0 = g.fG, f1 = g.fB, f2 = g.fL;
+        double best = -1.0, brate = 0.0;
+        int bG = 0, bB = 0, bL = 0;
+        for (int L : Ls)
+            for (int G = 1; G <= 16; ++G)
+                for (int B : Bs) {
+                    if (b->force_layout != YAMC_KSPACE_AUTO && L != b->force_layout) continue;
+                    g.fG = G; g.fB = B; g.fL = L;
+                    if (batch_configure(b) != YAMC_OK) continue;  // shape does not fit
+                    if (g.cfg.G != G || g.cfg.B != B || g.max_clusters <= 0) continue;
+                    for (size_t i = 0; i < R; ++i) cur[i] = cursors[i];
+                    r = batch_step(b, d_rng, off.data(), n_rng, cur.data(), n_moves, done.data(), nullptr, nullptr,
+                                   (int)gi);
+                    const int rr = batch_copy_state(b, keep, false);
+                    if (rr) return rr;
+                    if (r != YAMC_OK && r != YAMC_ERNG_EXHAUSTED) return r;
+                    double moves = 0;
+                    for (int i : g.idx) moves += (double)done[i];
+                    const double rate = b->last_ms > 0 ? moves / (1e-3 * b->last_ms) : 0.0;
+                    // per SM occupied: the groups share the GPU, so the shape that does the most with
+                    // the SMs it holds wins, not the one that is fastest on an empty GPU
+                    const int nrep = (int)g.idx.size();
+                    const double sms = (double)std::min(nrep, g.max_clusters) * G;
+                    const double eff = rate / sms;
+                    if (eff > best) { best = eff; bG = G; bB = B; bL = L; brate = rate; }
+                }
+        if (best < 0) {
+            g.fG = f0; g.fB = f1; g.fL = f2;
+            batch_configure(b);
+            set_error("no launch shape fits the replicas of a batch group");
+            return YAMC_ELIMITS;
         }
+        g.fG = bG; g.fB = bB; g.fL = bL;
+        total += brate;
     }
-    if (best < 0) {
-        b->force_G = fG; b->force_B = fB; b->force_layout = fL;
-        batch_configure(b);
-        set_error("no launch shape fits every replica of the batch");
-        return YAMC_ELIMITS;
-    }
-    b->force_G = bestG; b->force_B = bestB; b->force_layout = bestL;
     r = batch_configure(b);
     for (yamc_ctx *c : b->reps) c->pos_valid = false;
-    if (best_moves_per_s) *best_moves_per_s = best;
+    if (best_moves_per_s) *best_moves_per_s = total;
     return r;
+}
+
+int yamc_batch_groups(yamc_batch *b, int32_t *n) {
+    if (!b || !n) return YAMC_EPARAMETER;
+    *n = (int32_t)b->groups.size();
+    return YAMC_OK;
+}
+
+int yamc_batch_group_launch(yamc_batch *b, int32_t group, int32_t out[7]) {
+    if (!b || !out || group < 0 || group >= (int)b->groups.size()) return YAMC_EPARAMETER;
+    const BatchGroup &g = b->groups[group];
+    out[0] = g.cfg.G; out[1] = g.cfg.B; out[2] = std::max(g.cfg.EPT, 0); out[3] = (int32_t)g.cfg.smem;
+    out[4] = g.max_clusters; out[5] = (int32_t)g.idx.size(); out[6] = g.mx ? 1 : 0;
+    return YAMC_OK;
 }
 
 // ---------------------------------------------------------------- adjoint forces
