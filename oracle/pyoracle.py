@@ -104,6 +104,8 @@ def lib(fast: bool = False):
         L.orc_move_eval.restype = ctypes.c_int32
         L.orc_move_commit.argtypes = [ctypes.c_void_p]
         L.orc_move_commit.restype = ctypes.c_int32
+        L.orc_set_move_weights.argtypes = [ctypes.c_void_p, dp, ctypes.c_int32]
+        L.orc_set_move_weights.restype = ctypes.c_int32
         L.orc_force_kspace_atom.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_double,
                                             ctypes.c_double, dp]
         _libs[name] = L
@@ -176,6 +178,12 @@ class Oracle:
         self.L.orc_get_atoms(self.h, x.ctypes.data, y.ctypes.data, z.ctypes.data, q.ctypes.data,
                              t.ctypes.data, m.ctypes.data)
         return x, y, z, q, t, m
+
+    def set_move_weights(self, w) -> None:
+        """init_freq with a frequencies file: BiasedRandom_init on the molecules' move weights."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        if self.L.orc_set_move_weights(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), w.size) != 0:
+            raise ValueError("one weight per molecule")
 
     def mols(self):
         f = np.zeros(self.nmol, dtype=np.int32)

@@ -1635,6 +1635,23 @@ orc_state *orc_create(const orc_params *pin, const char *composition_path, const
     return s;
 }
 
+/* BiasedRandom_init (BiasedRandom.f90:44-79) on given move weights (init_freq with a frequencies
+   file, runmc.f90:25-67): probabilities w/S (flat when S == 0), running-sum intervals, and
+   end = -1 for a zero weight when S > 0. */
+int32_t orc_set_move_weights(orc_state *s, const double *w, int32_t n) {
+    if (n != s->nmol) return -3;
+    double S = 0;
+    for (int i = 0; i < n; i++) S = S + w[i];
+    double *prob = malloc(sizeof(double) * n);
+    for (int i = 0; i < n; i++) prob[i] = (S == 0) ? 1.0 / n : w[i] / S;
+    s->freq_beg[0] = 0.0; s->freq_end[0] = prob[0];
+    for (int i = 1; i < n; i++) { s->freq_beg[i] = s->freq_end[i - 1]; s->freq_end[i] = s->freq_beg[i] + prob[i]; }
+    if (S > 0)
+        for (int i = 0; i < n; i++) if (w[i] == 0) s->freq_end[i] = -1.0;
+    free(prob);
+    return 0;
+}
+
 void orc_destroy(orc_state *s) {
     if (!s) return;
     int nt = s->lj.ntype;

@@ -74,6 +74,7 @@ double orc_shi_sans_exp(double x);
 int32_t orc_grid_count(int32_t kmax);
 
 /* ---- system ---- */
+int32_t orc_set_move_weights(orc_state *s, const double *w, int32_t n);
 orc_state *orc_create(const orc_params *p, const char *composition_path, const char *moltab_path,
                       int32_t *status);
 void orc_destroy(orc_state *s);

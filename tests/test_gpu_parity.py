@@ -225,3 +225,32 @@ def test_per_move_api_matches_oracle(which, layout, request):
         if acc:
             o.move_commit()
     assert rel_close(eng.energies(), o.energies(), 1e-9)
+
+
+@pytest.mark.parametrize("zero", [False, True])
+def test_weighted_molecule_choice(tiny_files, tmp_path, zero):
+    """A frequencies file with move weights only (no exchange): BiasedRandom_choose on uneven
+    intervals; with a zero weight the intervals are no longer monotone (end = -1) and the
+    device takes the reference's linear scan."""
+    from yamc_b200 import formats
+    inp = api.load_inputs(tiny_files["parameters"], tiny_files["composition"], tiny_files["moltab"])
+    n = inp.nmol
+    lines = [f"1-{n - 4} 1.0 0.0", f"{n - 3}-{n} 5.0 0.0"]
+    if zero:
+        lines = ["1-3 1.0 0.0", "4-4 0.0 0.0", f"5-{n - 4} 1.0 0.0", f"{n - 3}-{n} 5.0 0.0"]
+    (tmp_path / "freq").write_text(f"{len(lines)}\n" + "\n".join(lines) + "\n")
+    mv, xc = formats.read_freq_file(str(tmp_path / "freq"), n)
+    inp.move_weights = mv
+    o = pyoracle.Oracle(tiny_files)
+    o.set_move_weights(mv)
+    buf = grng.gfortran_stream(31, 200000)
+    olog, _, ocur = o.run_mc(buf, 3000)
+    eng = api.Engine(inp)
+    glog, _, gcur, done, st = eng.run_chain(buf, 3000)
+    assert st == 0 and done == 3000
+    compare_logs(glog, olog)
+    assert gcur == ocur
+    counts = np.bincount(glog["imol"], minlength=n + 1)[1:]
+    assert counts[-4:].mean() > 3 * counts[: n - 4].mean()
+    if zero:
+        assert counts[3] == 0

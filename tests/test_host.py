@@ -98,3 +98,23 @@ def test_workload_sizes():
         assert kmax == w.kmax
     b = systems.batch_specs(96)
     assert len(b) == 96 and min(x.n_water for x in b) >= 216 and max(x.n_water for x in b) <= 4096
+
+
+def test_freq_file_reader(tmp_path):
+    """read_freq_file (runmc.f90:70-173): comments, intervals, coverage and crossing checks."""
+    import numpy as np
+    import pytest
+    from yamc_b200 import formats
+    p = tmp_path / "freq.txt"
+    p.write_text("# frequencies\n\n3\n1-4 1.0 0.0\n5-5 0.0 0.0\n6-8 2.5 0.0\n")
+    mv, xc = formats.read_freq_file(str(p), 8)
+    assert np.array_equal(mv, [1, 1, 1, 1, 0, 2.5, 2.5, 2.5]) and np.all(xc == 0)
+    p.write_text("2\n1-4 1.0 0.0\n4-8 1.0 0.0\n")
+    with pytest.raises(ValueError, match="crossing"):
+        formats.read_freq_file(str(p), 8)
+    p.write_text("1\n1-6 1.0 0.0\n")
+    with pytest.raises(ValueError, match="not all"):
+        formats.read_freq_file(str(p), 8)
+    p.write_text("1\n1-9 1.0 0.0\n")
+    with pytest.raises(ValueError, match="inconsistent"):
+        formats.read_freq_file(str(p), 8)

@@ -134,3 +134,42 @@ def read_energy_dat(path: str) -> np.ndarray:
             if len(t) >= 9:
                 rows.append([float(v) for v in t[:9]])
     return np.array(rows, dtype=np.float64).reshape(-1, 9)
+
+
+def read_freq_file(path: str, nmol: int):
+    """The frequencies file of run_mc (read_freq_file, runmc.f90:70-173): comment ('#') and empty
+    lines, then the number of records, then records "first-last move_prob xchange_prob" with
+    1-based molecule intervals that must not overlap and must cover every molecule.  Returns
+    (move weights, exchange weights), one per molecule; the move weights are yamc_system's
+    move_weights.  Raises ValueError where the reference throws ERROR_PARAMETER / ERROR_IO."""
+    import numpy as np
+    with open(path) as f:
+        lines = f.read().splitlines()
+    it = iter(lines)
+    head = None
+    for line in it:
+        if line.strip() and "#" not in line:
+            head = line
+            break
+    if head is None:
+        raise ValueError(f"read_freq_file: unexpected end of file {path}")
+    nrec = int(head.split()[0])
+    mv = np.full(nmol, -1.0)
+    xc = np.full(nmol, -1.0)
+    for _ in range(nrec):
+        try:
+            rec = next(it)
+        except StopIteration:
+            raise ValueError(f"read_freq_file: unexpected end of file {path}")
+        tok = rec.replace("-", " ").split()
+        first, last, mp, xp = int(tok[0]), int(tok[1]), float(tok[2]), float(tok[3])
+        if last > nmol:
+            raise ValueError(f"read_freq_file: {path} is inconsistent with the composition")
+        for j in range(first - 1, last):
+            if mv[j] > 0:
+                raise ValueError(f"read_freq_file: crossing intervals in {path}")
+            mv[j] = mp
+            xc[j] = xp
+    if np.any(mv < 0):
+        raise ValueError(f"read_freq_file: not all frequences defined ({path} is inconsistent with composition?)")
+    return mv, xc
