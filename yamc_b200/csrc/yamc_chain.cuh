@@ -92,7 +92,8 @@ enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
 
 struct Slot { double x, y, z, q, iq, dhs; int type, pad; };
 constexpr int kMaxSpecies = 8;
-constexpr int kCPT = 4;   // atoms each worker thread tests per filter round
+constexpr int kCPT = 8;   // atoms each worker thread tests per filter round
+constexpr int kQueueMax = 4096;  // pair-queue chunk (items); a round's pairs are consumed in chunks
 constexpr int kWin = 256; // random-stream window held in shared memory
 constexpr int kCtl = 32;  // threads of the control warp
 constexpr int kChainMaxThreads = 256;  // one CTA per SM, up to 255 registers per thread
@@ -547,7 +548,7 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
         }
         __syncwarp();
         // slot tests of the near atoms, densely: lane takes entries lane, lane + 32, ...
-        unsigned masks = 0;  // kCPT slot masks of 8 bits
+        unsigned long long masks = 0;  // kCPT slot masks of 8 bits
         int count = 0;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
@@ -568,7 +569,7 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
                     }
                     if (r2 < D.rmax2) msk |= 1u << s;
                 }
-                masks |= msk << (8 * c);
+                masks |= (unsigned long long)msk << (8 * c);
                 count += __popc(msk);
             }
         }
@@ -592,49 +593,58 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
             if (lane == 31) sh.qcount = x;
         }
         worker_sync(nwork);
-        int pos = sh.wcount[32 + wwarp] + incl - count;
-#pragma unroll
-        for (int c = 0; c < kCPT; ++c) {
-            unsigned msk = (masks >> (8 * c)) & 0xffu;
-            const int jl = msk ? nb[c * 32 + lane] : 0;
-            while (msk) {
-                const int s = __ffs(msk) - 1;
-                msk &= msk - 1;
-                queue[pos++] = (jl << 3) | s;
-            }
-        }
-        worker_sync(nwork);
-        YAMC_WPH(PH_FILTER);
+        // the round's pairs in queue order (thread order by the prefix sums), consumed in chunks of
+        // qcap: each thread writes its items that fall in the chunk, the workers evaluate them
+        const int base = sh.wcount[32 + wwarp] + incl - count;
         const int nq = sh.qcount;
-        for (int qi = wtid; qi < nq; qi += nwork) {
-            const int item = queue[qi];
-            const int jl = item >> 3, s = item & 7;
-            const Slot &sl = m.slot[s];
-            const double4 pj = atom_s[jl];
-            const int tj = meta_s[jl].y;
-            const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
-            const double r2 = dx * dx + dy * dy + dz * dz;
-            const bool lj = sl.type > 0 && tj > 0;
-            const int off = lj ? (sl.type - 1) * nt + (tj - 1) : 0;
-            const double qq = D.xclb * sl.q * pj.w;
-            const double s6 = lj ? lj_s[off] : 0.0, fe = lj ? lj_s[nt * nt + off] : 0.0;
-            const bool isnew = s < na;
-            const double sign = (KIND == PASS_BOTH && !isnew) ? -1.0 : 1.0;
-            const PairTerm<double> t = MX ? pair_term_mx<FORCES>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false)
-                                          : pair_term<double, FORCES>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
-            acc.add(RV_EW, sign * t.ew); acc.add(RV_LJ6, sign * t.lj6); acc.add(RV_LJ12, sign * t.lj12);
-            if constexpr (FORCES) {
-                const int a = isnew ? s : s - na;
+        for (int q0 = 0; q0 < nq; q0 += qcap) {
+            if (base < q0 + qcap && base + count > q0) {
+                int pos = base;
 #pragma unroll
-                for (int aa = 0; aa < kMaxA; ++aa)
-                    if (aa == a) {
-                        acc.add(RV_F + 3 * aa, dx * t.FR);
-                        acc.add(RV_F + 3 * aa + 1, dy * t.FR);
-                        acc.add(RV_F + 3 * aa + 2, dz * t.FR);
+                for (int c = 0; c < kCPT; ++c) {
+                    unsigned msk = (unsigned)(masks >> (8 * c)) & 0xffu;
+                    const int jl = msk ? nb[c * 32 + lane] : 0;
+                    while (msk) {
+                        const int s = __ffs(msk) - 1;
+                        msk &= msk - 1;
+                        if (pos >= q0 && pos < q0 + qcap) queue[pos - q0] = (jl << 3) | s;
+                        ++pos;
                     }
+                }
             }
+            worker_sync(nwork);
+            if (q0 == 0) YAMC_WPH(PH_FILTER);
+            const int nc = min(qcap, nq - q0);
+            for (int qi = wtid; qi < nc; qi += nwork) {
+                const int item = queue[qi];
+                const int jl = item >> 3, s = item & 7;
+                const Slot &sl = m.slot[s];
+                const double4 pj = atom_s[jl];
+                const int tj = meta_s[jl].y;
+                const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const bool lj = sl.type > 0 && tj > 0;
+                const int off = lj ? (sl.type - 1) * nt + (tj - 1) : 0;
+                const double qq = D.xclb * sl.q * pj.w;
+                const double s6 = lj ? lj_s[off] : 0.0, fe = lj ? lj_s[nt * nt + off] : 0.0;
+                const bool isnew = s < na;
+                const double sign = (KIND == PASS_BOTH && !isnew) ? -1.0 : 1.0;
+                const PairTerm<double> t = MX ? pair_term_mx<FORCES>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false)
+                                              : pair_term<double, FORCES>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
+                acc.add(RV_EW, sign * t.ew); acc.add(RV_LJ6, sign * t.lj6); acc.add(RV_LJ12, sign * t.lj12);
+                if constexpr (FORCES) {
+                    const int a = isnew ? s : s - na;
+#pragma unroll
+                    for (int aa = 0; aa < kMaxA; ++aa)
+                        if (aa == a) {
+                            acc.add(RV_F + 3 * aa, dx * t.FR);
+                            acc.add(RV_F + 3 * aa + 1, dy * t.FR);
+                            acc.add(RV_F + 3 * aa + 2, dz * t.FR);
+                        }
+                }
+            }
+            worker_sync(nwork);
         }
-        worker_sync(nwork);
         YAMC_WPH(PH_PAIRS);
     }
 

@@ -436,7 +436,7 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
             }
             if (EPT > 2) continue;
             const int nown_max = (Nmax + G - 1) / G;
-            const int qcap = std::min(nown_max, nwork * kCPT) * 2 * kMaxA;  // one filter round of pairs
+            const int qcap = std::min(kQueueMax, std::min(nown_max, nwork * kCPT) * 2 * kMaxA);  // pair-queue chunk
             const size_t sm = chain_smem_bytes(G, B, kmax, nt, nown_max, qcap);
             if (sm > smem_max) continue;
             out->G = G; out->B = B; out->EPT = EPT; out->nown_max = nown_max; out->qcap = qcap; out->smem = sm;
