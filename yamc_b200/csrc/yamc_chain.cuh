@@ -670,38 +670,42 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
 // all threads (the cluster barrier needs everyone).
 __device__ __forceinline__ void reduce_pass(ChainShared &sh, const double *red, double *xch, int nv, int G, int rank,
                                             int xpar, cg::cluster_group &cluster) {
+    // lane v of the control warp owns value v: the worker warps' partials in warp order, then
+    // (cluster) every CTA's sum in rank order -- the same order in every CTA
     const int lane = threadIdx.x & 31;
     const int nww = (blockDim.x - kCtl) >> 5;
     if (threadIdx.x < kCtl) {
-        for (int v = 0; v < nv; ++v) {
-            double x = lane < nww ? red[lane * kNV + v] : 0.0;
-#pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
-                const double y = __shfl_xor_sync(0xffffffffu, x, o);
-                x = (v == RV_OVL) ? fmax(x, y) : x + y;
+        double x = 0.0;
+        if (lane < nv) {
+            for (int w = 0; w < nww; ++w) {
+                const double y = red[w * kNV + lane];
+                x = (lane == RV_OVL) ? fmax(x, y) : x + y;
             }
-            if (G > 1) {
-                if (lane < G) {
-                    double *dst = cluster.map_shared_rank(xch, lane);
-                    dst[(xpar * G + rank) * kNV + v] = x;
+        }
+        if (G > 1) {
+            // value v of this CTA to every rank's exchange row; lanes cover (v, r) pairs
+            for (int idx = 0; idx < nv * G; idx += 32) {
+                const int my = idx + lane;
+                const int v = my % nv, r = my / nv;
+                const double xv = __shfl_sync(0xffffffffu, x, v < 32 ? v : 0);
+                if (my < nv * G) {
+                    double *dst = cluster.map_shared_rank(xch, r);
+                    dst[(xpar * G + rank) * kNV + v] = xv;
                 }
-            } else if (lane == 0) {
-                sh.tot[v] = x;
             }
+        } else if (lane < nv) {
+            sh.tot[lane] = x;
         }
     }
     if (G > 1) {
         cluster.sync();
-        if (threadIdx.x < kCtl) {
-            for (int v = 0; v < nv; ++v) {
-                double x = lane < G ? xch[(xpar * G + lane) * kNV + v] : 0.0;
-#pragma unroll
-                for (int o = 16; o > 0; o >>= 1) {
-                    const double y = __shfl_xor_sync(0xffffffffu, x, o);
-                    x = (v == RV_OVL) ? fmax(x, y) : x + y;
-                }
-                if (lane == 0) sh.tot[v] = x;
+        if (threadIdx.x < kCtl && lane < nv) {
+            double x = 0.0;
+            for (int r = 0; r < G; ++r) {
+                const double y = xch[(xpar * G + r) * kNV + lane];
+                x = (lane == RV_OVL) ? fmax(x, y) : x + y;
             }
+            sh.tot[lane] = x;
         }
     }
 }
@@ -1221,9 +1225,16 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     mol_force_torque(na, x, y, z, M.mass, fx, fy, fz, F, T);
                 }
                 const double du_total = du_real + (du_kc + du_kl) + du_ext;
-                MoveState mv = M.mv;
-                mcm_init_new(mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
-                acc = mcm_accept(mv, du_total, D.xlf, D.xlc, rng);
+                if (biased || SPLIT) {
+                    MoveState mv = M.mv;
+                    mcm_init_new(mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
+                    acc = mcm_accept(mv, du_total, D.xlf, D.xlc, rng);
+                } else {
+                    // MonteCarloMove_accept_or_decline without bias: every bias term is an exact 0
+                    // or 1 (cold = qold = cnew = qnew = 1), so the factor is exp(-dU) bit for bit
+                    const double factor = exp(-du_total);
+                    acc = rng.next() > factor ? 0 : 1;
+                }
                 out = rng.out != 0;
                 cur_after = rng.cur;
                 flags |= acc;
