@@ -1127,9 +1127,9 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
             else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
         } else if (speculate && it + 1 < n_moves) {
-            // prepare the next move's candidates while the workers run: lane 0 after an overlap
-            // (no acceptance draw), lanes 1-2 after the acceptance draw, lane 2 with the molecule
-            // in flight at its proposed positions (used only if it is chosen again and accepted)
+            // prepare the next move's candidates while the workers run: lanes 1-2 after the
+            // acceptance draw, lane 2 with the molecule in flight at its proposed positions (used
+            // only if it is chosen again and accepted)
             const Cand &M = sh.cand[sh.icur];
             const long long c1 = M.cur_prop;
             const bool next_cycle = (sh.mic + 1 == D.M);
@@ -1148,12 +1148,17 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     __syncwarp();
                 }
             }
-            if (lane < 3) {
+            if (lane == 0) {
+                // the candidate after an overlap is not prepared: overlaps are rare, and a third
+                // lane on its own random numbers diverges from lanes 1-2 (which draw the same
+                // numbers and run in step); an overlap takes the unspeculated path instead
+                sh.spec[0] = (sh.icur + 1) & 3; sh.spec[1] = (sh.icur + 2) & 3; sh.spec[2] = (sh.icur + 3) & 3;
+                sh.cand[(sh.icur + 1) & 3].valid = 0;
+            } else if (lane < 3) {
                 const int buf = (sh.icur + 1 + lane) & 3;
-                if (lane == 0) { sh.spec[0] = (sh.icur + 1) & 3; sh.spec[1] = (sh.icur + 2) & 3; sh.spec[2] = (sh.icur + 3) & 3; }
                 Cand &C = sh.cand[buf];
                 RngReader rng = make_reader(X, sh, c1);
-                if (lane > 0) (void)rng.next();  // the acceptance draw (MonteCarloMove.f90:553)
+                (void)rng.next();  // the acceptance draw (MonteCarloMove.f90:553)
                 C.cur_start = rng.cur;
                 const int imol = rng.out ? 0 : draw_molecule(D, rng, next_cycle);
                 C.valid = imol > 0;
@@ -1267,10 +1272,9 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 sh.cursor = cur_after;
                 if (rank == 0) {
                     if (acc)
-                        for (int a = 0; a < na; ++a) {
-                            double4 p = D.atom[M.first + a];
-                            p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
-                            D.atom[M.first + a] = p;
+                        for (int a = 0; a < na; ++a) {  // x, y, z of the double4 (q unchanged): no read
+                            double *pa = reinterpret_cast<double *>(D.atom + M.first + a);
+                            pa[0] = M.slot[a].x; pa[1] = M.slot[a].y; pa[2] = M.slot[a].z;
                         }
                     if (run->log) {
                         yamc_move_record rec;
