@@ -93,6 +93,17 @@ typedef struct {
     double du_real, du_k_coul, du_k_lj, du_ext; /* movemc Steps 7, 10, 11, 11A */
 } yamc_move_record;
 
+/* One NPT volume step (mcvol, MC.f90:701-825), an optional output of yamc_run_mc. */
+typedef struct {
+    int64_t cycle;   /* run_mc cycle number of the step */
+    int32_t flags;   /* bit0 accepted, bit1 hard-core overlap at the new volume (rejected) */
+    int32_t pad;
+    int64_t cursor;  /* RNG cursor after the step */
+    double box_old, box_new; /* BoxLength before the step and the one tried (Angstrom) */
+    double du, arg;  /* U_new - U_old (kT; 0 on overlap) and the acceptance exponent
+                        -dU - P dV + (nmol+1) ln(V_new/V_old) */
+} yamc_volume_record;
+
 /* ---- parameters (parameters.f90) ---- */
 /* Parameters_read (parameters.f90:266-305) on top of the defaults (:18-72). */
 int yamc_params_read(const char *path, const char *extra, yamc_params *p);
@@ -178,6 +189,36 @@ int yamc_run_chain(yamc_ctx *ctx, const float *rng, int64_t n_rng, int64_t *curs
 int yamc_run_chain_device(yamc_ctx *ctx, const float *d_rng, int64_t n_rng, int64_t *cursor,
                           int64_t n_moves, int64_t *moves_done, yamc_move_record *d_log,
                           double *d_rows, int32_t max_rows, int32_t *n_rows);
+
+/* ---- NPT: volume moves (mcvol, MC.f90:701-825) ----
+   yamc_run_mc is run_mc (runmc.f90:178-334) by cycles, with the volume cycles of an NPT run
+   (pressure_step_multiplier > 0): each cycle draws rnd = rand()*(psm+1); when psm > 0 and
+   rnd > psm the cycle is one volume step, otherwise nmol movemc calls on the device.  A volume
+   step draws lambda, scales the box (scale_box, scale_box.f90:6-62), recomputes the parameters,
+   the LJ tables and beta_LJ for the new length, scales beta by xclb_new/xclb_old, redoes the
+   full sums on the device and takes the Metropolis test
+   exp(-dU - P dV + (nmol+1) ln(V_new/V_old)), drawing only when that is not above 1; a
+   rejected step restores the state as mc_restore_state does.  rng is a HOST pointer (copied to
+   the device inside the call).  log: up to max_log movemc records (whole cycles only); vlog: up
+   to max_vlog volume records; rows: energy.dat rows (frame + 8 columns, as yamc_run_chain).
+   Returns YAMC_ERNG_EXHAUSTED when the stream runs out (an interrupted volume step is undone and
+   its cycle draw given back; an interrupted move cycle resumes where it stopped).  With
+   pressure_step_multiplier 0 it is the NVT loop of yamc_run_chain counted in cycles, and
+   yamc_run_chain refuses NPT parameters. */
+int yamc_run_mc(yamc_ctx *ctx, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_cycles,
+                int64_t *cycles_done, yamc_move_record *log, int64_t max_log, int64_t *n_log,
+                yamc_volume_record *vlog, int64_t max_vlog, int64_t *n_vlog, double *rows,
+                int32_t max_rows, int32_t *n_rows);
+/* The volume step as a drop-in for the body of mcvol, for a host that draws its own random
+   numbers: yamc_volume_eval takes the new box length (Angstrom; MC.f90:738-746 compute it from
+   lambda), does MC.f90:756-785 and returns dU = U_new - U_old and the overlap flag;
+   yamc_volume_commit then keeps the new box (accepted != 0) or restores the old one
+   (MC.f90:807-818). */
+int yamc_volume_eval(yamc_ctx *ctx, double new_box_length, double *du, int32_t *overlap);
+int yamc_volume_commit(yamc_ctx *ctx, int32_t accepted);
+/* The parameters as they stand (BoxLength and everything Parameters_recalc derives from it
+   change with accepted volume steps). */
+int yamc_get_params(yamc_ctx *ctx, yamc_params *p);
 
 /* Mixed form (params.precision = YAMC_MIXED): the chain kernel recomputes rho(k)
    and the k-space energies in FP64 from the positions after every

@@ -54,6 +54,10 @@ MOVE_DTYPE = np.dtype([("imol", np.int32), ("flags", np.int32), ("cursor", np.in
                        ("f_new", np.float64, 3), ("t_new", np.float64, 3)])
 assert MOVE_DTYPE.itemsize == ctypes.sizeof(MoveRec)
 
+# orc_vol_rec: one mcvol step
+VOL_DTYPE = np.dtype([("cycle", np.int64), ("flags", np.int32), ("pad", np.int32), ("cursor", np.int64),
+                      ("box_old", np.float64), ("box_new", np.float64), ("du", np.float64), ("arg", np.float64)])
+
 _libs = {}
 
 
@@ -98,6 +102,15 @@ def lib(fast: bool = False):
         L.orc_movemc.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
                                  P(ctypes.c_int64), P(MoveRec)]
         L.orc_movemc.restype = ctypes.c_int32
+        L.orc_run_cycles.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, P(ctypes.c_int64),
+                                     ctypes.c_int64, P(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int64,
+                                     P(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int64, P(ctypes.c_int64),
+                                     ctypes.c_void_p, ctypes.c_int32, P(ctypes.c_int32)]
+        L.orc_run_cycles.restype = ctypes.c_int32
+        L.orc_mcvol.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, P(ctypes.c_int64), ctypes.c_void_p]
+        L.orc_mcvol.restype = ctypes.c_int32
+        L.orc_box_length.argtypes = [ctypes.c_void_p]
+        L.orc_box_length.restype = ctypes.c_double
         L.orc_move_old.argtypes = [ctypes.c_void_p, ctypes.c_int32, dp, dp]
         L.orc_move_old.restype = ctypes.c_int32
         L.orc_move_eval.argtypes = [ctypes.c_void_p, dp, dp, dp, dp, P(ctypes.c_int32), dp, dp]
@@ -216,6 +229,40 @@ class Oracle:
         if r != 0:
             raise RuntimeError(f"orc_run_mc returned {r}")
         return log, rows[: nrows.value], cur.value
+
+    def run_cycles(self, rng: np.ndarray, n_cycles: int, cursor: int = 0, max_rows: int = 0,
+                   allow_exhausted: bool = False):
+        """run_mc by cycles, NPT volume steps included: (move log, volume log, energy rows,
+        cursor, cycles done)."""
+        rng = np.ascontiguousarray(rng, dtype=np.float32)
+        max_log = n_cycles * self.nmol
+        log = np.zeros(max(max_log, 1), dtype=MOVE_DTYPE)
+        vlog = np.zeros(max(n_cycles, 1), dtype=VOL_DTYPE)
+        rows = np.zeros((max(max_rows, 1), 9))
+        nrows = ctypes.c_int32(0)
+        nlog = ctypes.c_int64(0)
+        nv = ctypes.c_int64(0)
+        done = ctypes.c_int64(0)
+        cur = ctypes.c_int64(cursor)
+        r = self.L.orc_run_cycles(self.h, rng.ctypes.data, rng.size, ctypes.byref(cur), n_cycles, ctypes.byref(done),
+                                  log.ctypes.data, max_log, ctypes.byref(nlog), vlog.ctypes.data, n_cycles,
+                                  ctypes.byref(nv), rows.ctypes.data, max_rows, ctypes.byref(nrows))
+        if r != 0 and not (allow_exhausted and r == -6):
+            raise RuntimeError(f"orc_run_cycles returned {r}")
+        return log[: nlog.value], vlog[: nv.value], rows[: nrows.value], cur.value, done.value
+
+    def mcvol(self, rng: np.ndarray, cursor: int = 0):
+        rng = np.ascontiguousarray(rng, dtype=np.float32)
+        rec = np.zeros(1, dtype=VOL_DTYPE)
+        cur = ctypes.c_int64(cursor)
+        r = self.L.orc_mcvol(self.h, rng.ctypes.data, rng.size, ctypes.byref(cur), rec.ctypes.data)
+        if r != 0:
+            raise RuntimeError(f"orc_mcvol returned {r}")
+        return rec[0], cur.value
+
+    @property
+    def box_length(self) -> float:
+        return self.L.orc_box_length(self.h)
 
     def movemc(self, imol: int, rng: np.ndarray, cursor: int = 0):
         rng = np.ascontiguousarray(rng, dtype=np.float32)

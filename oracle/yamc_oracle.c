@@ -449,6 +449,19 @@ static void lj_fill_index(ljtypes_t *L, int i, int j, double sigma12, double eps
     L->four_eps[o21] = 4 * epsilon12;
 }
 
+/* LJTypes_fill_LJ_tab (LJTypes.f90:273-308): Lorentz-Berthelot tables from the type list */
+static void lj_fill_tab(ljtypes_t *L) {
+    int nt = L->ntype;
+    for (int i = 1; i <= nt; i++) {
+        double s1 = L->sigma[i - 1], e1 = L->epsilon[i - 1];
+        lj_fill_index(L, i, i, s1, e1);
+        for (int j = i + 1; j <= nt; j++) {
+            double s2 = L->sigma[j - 1], e2 = L->epsilon[j - 1];
+            lj_fill_index(L, i, j, (s1 + s2) / 2, sqrt(e1 * e2));
+        }
+    }
+}
+
 /* LJTypes_fill (LJTypes.f90:134-200) + LJTypes_fill_LJ_tab (:273-308) */
 static int lj_fill(ljtypes_t *L, const double *sig, const double *eps, int n) {
     int nt = 0;
@@ -470,15 +483,14 @@ static int lj_fill(ljtypes_t *L, const double *sig, const double *eps, int n) {
     int n2 = nt * nt > 0 ? nt * nt : 1;
     L->lj6 = calloc(n2, sizeof(double)); L->lj12 = calloc(n2, sizeof(double));
     L->four_eps = calloc(n2, sizeof(double)); L->sigma6 = calloc(n2, sizeof(double)); L->sigma2 = calloc(n2, sizeof(double));
-    for (int i = 1; i <= nt; i++) {
-        double s1 = L->sigma[i - 1], e1 = L->epsilon[i - 1];
-        lj_fill_index(L, i, i, s1, e1);
-        for (int j = i + 1; j <= nt; j++) {
-            double s2 = L->sigma[j - 1], e2 = L->epsilon[j - 1];
-            lj_fill_index(L, i, j, (s1 + s2) / 2, sqrt(e1 * e2));
-        }
-    }
+    lj_fill_tab(L);
     return 0;
+}
+
+/* LJTypes_scale_sigma (LJTypes.f90:238-252): every type's sigma times c, tables refilled */
+static void lj_scale_sigma(ljtypes_t *L, double c) {
+    for (int i = 0; i < L->ntype; i++) L->sigma[i] = L->sigma[i] * c;
+    lj_fill_tab(L);
 }
 
 /* ------------------------------------------------------------------ */
@@ -531,7 +543,7 @@ struct orc_state {
     /* run_mc state */
     double *freq_beg, *freq_end;
     int64_t icycle, move_in_cycle;
-    double n_mv_steps, n_mv_accepted, n_vol_steps;
+    double n_mv_steps, n_mv_accepted, n_vol_steps, n_vol_accepted;
     /* RNG binding for the current call */
     const float *rng; int64_t n_rng; int64_t *cursor; int rng_out;
 };
@@ -1415,13 +1427,40 @@ int32_t orc_movemc(orc_state *s, int32_t imol, const float *rng, int64_t n_rng, 
     return r;
 }
 
+/* energy.dat row at the end of a cycle (runmc.f90:276-279), frame = the cycle number */
+static void cycle_end(orc_state *s, double *rows, int32_t max_rows, int32_t *n_rows) {
+    if (fmod(s->n_mv_steps / s->nmol + s->n_vol_steps, s->p.n_store_energy_interval) < 1e-10) {
+        if (rows && n_rows && *n_rows < max_rows) {
+            double e[8];
+            orc_energies(s, e);
+            double *row = rows + 9 * (size_t)(*n_rows);
+            row[0] = (double)s->icycle;
+            for (int c = 0; c < 8; c++) row[1 + c] = e[c];
+            (*n_rows)++;
+        }
+    }
+    s->icycle++;
+}
+
+static int32_t run_moves(orc_state *s, int64_t n_moves, orc_move_rec *log, double *rows, int32_t max_rows,
+                         int32_t *n_rows);
+
 /* run_mc (runmc.f90:178-334), NVT single-molecule moves only */
 int32_t orc_run_mc(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_moves,
                    orc_move_rec *log, double *rows, int32_t max_rows, int32_t *n_rows) {
     s->rng = rng; s->n_rng = n_rng; s->cursor = cursor; s->rng_out = 0;
-    if (s->p.pressure_step_multiplier > 0) return -4; /* mcvol is outside this path */
+    if (s->p.pressure_step_multiplier > 0) return -4; /* NPT runs through orc_run_cycles */
     if (n_rows) *n_rows = 0;
+    return run_moves(s, n_moves, log, rows, max_rows, n_rows);
+}
+
+/* the movemc calls of run_mc's move cycles (runmc.f90:224-272): the cycle's pressure draw
+   at a cycle start (a move cycle: the caller has checked it), the exchange draw, the
+   molecule choice, movemc */
+static int32_t run_moves(orc_state *s, int64_t n_moves, orc_move_rec *log, double *rows, int32_t max_rows,
+                         int32_t *n_rows) {
     for (int64_t m = 0; m < n_moves; m++) {
+        const int64_t c_move = *s->cursor;  /* an interrupted move resumes from here */
         if (s->move_in_cycle == 0) {
             double rnd = orc_rand(s) * (s->p.pressure_step_multiplier + 1);
             (void)rnd;
@@ -1429,29 +1468,230 @@ int32_t orc_run_mc(orc_state *s, const float *rng, int64_t n_rng, int64_t *curso
         double rnd = orc_rand(s);
         (void)rnd; /* compared with xchange_probability = 0: never an exchange */
         int imol = biased_choose(s);
-        if (s->rng_out) return -6;
+        if (s->rng_out) { *s->cursor = c_move; return -6; }
         orc_move_rec rec;
         int r = movemc(s, imol, &rec);
+        if (r == -6) *s->cursor = c_move;
         if (r) return r;
-        rec.cursor = *cursor;
+        rec.cursor = *s->cursor;
         if (rec.flags & 1) s->n_mv_accepted += 1;
         s->n_mv_steps += 1;
         if (log) log[m] = rec;
         s->move_in_cycle++;
         if (s->move_in_cycle == s->nmol) {
             s->move_in_cycle = 0;
-            if (fmod(s->n_mv_steps / s->nmol + s->n_vol_steps, s->p.n_store_energy_interval) < 1e-10) {
-                if (rows && n_rows && *n_rows < max_rows) {
-                    double e[8];
-                    orc_energies(s, e);
-                    double *row = rows + 9 * (size_t)(*n_rows);
-                    row[0] = (double)s->icycle;
-                    for (int c = 0; c < 8; c++) row[1 + c] = e[c];
-                    (*n_rows)++;
-                }
-            }
-            s->icycle++;
+            cycle_end(s, rows, max_rows, n_rows);
         }
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ */
+/* NPT volume move: mcvol (MC.f90:701-825)                              */
+/* ------------------------------------------------------------------ */
+/* TMCState (MC.f90:149-255): what mc_save_state keeps; the parameters, the LJ
+   type list and beta are kept too, only to undo a step that ran out of random
+   numbers (the reference has no such case) */
+typedef struct {
+    double U_tail, U_tail_coul, U_tail_lj6, U_tail_lj12, U_ext, U_total, U_total_ew, U_total_lj;
+    double E_k, E_k_coul, E_k_lj, uu_ew, uu_lj6, uu_lj12, uu_ew_intra, uu_lj6_intra, uu_lj12_intra;
+    double *xx, *yy, *zz, *sigma, *fx, *fy, *fz, *uu;
+    rho_t rho;
+    double mu_x, mu_y, mu_z;
+    orc_params p;
+    double lj_sigma[MAX_LJ_TYPE];
+    double *beta;
+} mcstate_t;
+
+static void mcstate_save(orc_state *s, mcstate_t *t) {
+    int N = s->N, nk = s->g.nk, nt = s->lj.ntype;
+    t->U_tail = s->U_tail; t->U_tail_coul = s->U_tail_coul; t->U_tail_lj6 = s->U_tail_lj6; t->U_tail_lj12 = s->U_tail_lj12;
+    t->U_ext = s->U_ext; t->U_total = s->U_total; t->U_total_ew = s->U_total_ew; t->U_total_lj = s->U_total_lj;
+    t->E_k = s->E_k; t->E_k_coul = s->E_k_coul; t->E_k_lj = s->E_k_lj;
+    t->uu_ew = s->uu_ew; t->uu_lj6 = s->uu_lj6; t->uu_lj12 = s->uu_lj12;
+    t->uu_ew_intra = s->uu_ew_intra; t->uu_lj6_intra = s->uu_lj6_intra; t->uu_lj12_intra = s->uu_lj12_intra;
+    double **dst[8] = {&t->xx, &t->yy, &t->zz, &t->sigma, &t->fx, &t->fy, &t->fz, &t->uu};
+    double *src[8] = {s->xx, s->yy, s->zz, s->sigma, s->fx, s->fy, s->fz, s->uu};
+    for (int a = 0; a < 8; a++) { *dst[a] = malloc(sizeof(double) * N); memcpy(*dst[a], src[a], sizeof(double) * N); }
+    rho_alloc(&t->rho, nk, nt);
+    rho_copy(&t->rho, &s->rho_total, nk, nt);
+    memcpy(t->rho.present, s->rho_total.present, sizeof t->rho.present);
+    t->mu_x = s->mu_x; t->mu_y = s->mu_y; t->mu_z = s->mu_z;
+    t->p = s->p;
+    memcpy(t->lj_sigma, s->lj.sigma, sizeof t->lj_sigma);
+    t->beta = malloc(sizeof(double) * nk);
+    memcpy(t->beta, s->beta, sizeof(double) * nk);
+}
+
+/* mc_restore_state (MC.f90:205-255) */
+static void mcstate_restore(orc_state *s, const mcstate_t *t) {
+    int N = s->N, nk = s->g.nk, nt = s->lj.ntype;
+    s->U_tail = t->U_tail; s->U_tail_coul = t->U_tail_coul; s->U_tail_lj6 = t->U_tail_lj6; s->U_tail_lj12 = t->U_tail_lj12;
+    s->U_ext = t->U_ext; s->U_total = t->U_total; s->U_total_ew = t->U_total_ew; s->U_total_lj = t->U_total_lj;
+    s->E_k = t->E_k; s->E_k_coul = t->E_k_coul; s->E_k_lj = t->E_k_lj;
+    s->uu_ew = t->uu_ew; s->uu_lj6 = t->uu_lj6; s->uu_lj12 = t->uu_lj12;
+    s->uu_ew_intra = t->uu_ew_intra; s->uu_lj6_intra = t->uu_lj6_intra; s->uu_lj12_intra = t->uu_lj12_intra;
+    double *dst[8] = {s->xx, s->yy, s->zz, s->sigma, s->fx, s->fy, s->fz, s->uu};
+    const double *src[8] = {t->xx, t->yy, t->zz, t->sigma, t->fx, t->fy, t->fz, t->uu};
+    for (int a = 0; a < 8; a++) memcpy(dst[a], src[a], sizeof(double) * N);
+    rho_copy(&s->rho_total, &t->rho, nk, nt);
+    s->mu_x = t->mu_x; s->mu_y = t->mu_y; s->mu_z = t->mu_z;
+}
+
+static void mcstate_free(orc_state *s, mcstate_t *t) {
+    free(t->xx); free(t->yy); free(t->zz); free(t->sigma); free(t->fx); free(t->fy); free(t->fz); free(t->uu);
+    rho_free(&t->rho, s->lj.ntype);
+    free(t->beta);
+}
+
+/* scale_box (scale_box.f90:6-62): molecule centres of mass keep their box coordinates,
+   the atoms' offsets from them scale by L_old / L_new (bond lengths in Angstrom stay);
+   single-atom molecules are left as they are; atomic sigma (box units) scales too */
+static void scale_box(orc_state *s, double new_L) {
+    double c = s->p.BoxLength / new_L;
+    for (int m = 0; m < s->nmol; m++) {
+        int f = s->first_atom[m], l = s->last_atom[m], n = l - f + 1;
+        if (n == 1) continue;
+        double xc, yc, zc;
+        center_of_mass(&s->xx[f], &s->yy[f], &s->zz[f], &s->mass[f], n, &xc, &yc, &zc);
+        for (int j = f; j <= l; j++) {
+            s->xx[j] = (s->xx[j] - xc) * c + xc;
+            s->yy[j] = (s->yy[j] - yc) * c + yc;
+            s->zz[j] = (s->zz[j] - zc) * c + zc;
+        }
+    }
+    for (int i = 0; i < s->N; i++) s->sigma[i] = s->sigma[i] * c;
+}
+
+/* mc_calc_total_sums with scale_beta (MC.f90:477-585, EwaldSumKSpace_init :197-223):
+   beta is scaled instead of recomputed (alpha*L, hence beta6/beta12, stays fixed) */
+static int full_sums_scaled(orc_state *s, double scale_beta) {
+    int ov = realspace_calc(s, 1, NULL, NULL, NULL, NULL, 0, 0);
+    if (scale_beta > (double)1e-9f)
+        for (int k = 0; k < s->g.nk; k++) s->beta[k] = s->beta[k] * scale_beta;
+    else { init_beta(s); init_beta_lj(s); }
+    kspace_total_energy(s);
+    calc_mu(s->xx, s->yy, s->zz, s->charge, s->N, &s->mu_x, &s->mu_y, &s->mu_z);
+    tails(s);
+    total_energy(s);
+    return ov;
+}
+
+/* mcvol (MC.f90:701-825): a random walk in ln V, Frenkel & Smit algorithm 11.
+   Draws: lambda, then the acceptance draw only when the probability is not above 1
+   (`(proba > 1) .or. (rand() < proba)`, evaluated left to right with short-circuit as
+   gfortran's optimised builds do); an overlap gives proba = -1, so it draws and rejects.
+   Returns 0, or -6 when the random buffer ran out (the state is put back exactly). */
+static int mcvol(orc_state *s, orc_vol_rec *rec) {
+    int64_t cur0 = *s->cursor;
+    double old_L = s->p.BoxLength;
+    double old_V = old_L * old_L * old_L;
+    double lambda = 2 * orc_rand(s) - 1.0;
+    if (s->rng_out) return -6;
+    double log_new_V = log(old_V) + lambda * s->p.log_max_volume_scaling;
+    double new_V = exp(log_new_V);
+    double new_L = pow(new_V, 1.0 / 3.0);
+    double U_old = total_energy(s);
+    mcstate_t st;
+    mcstate_save(s, &st);
+    scale_box(s, new_L);
+    double xclb_old = s->p.xclb;
+    orc_params_recalc(&s->p, new_L);
+    double xclb_new = s->p.xclb;
+    lj_scale_sigma(&s->lj, old_L / new_L);
+    init_beta_lj(s);
+    int ov = full_sums_scaled(s, xclb_new / xclb_old);
+    double proba, dU = 0, arg = 0;
+    if (!ov) {
+        double U_new = total_energy(s);
+        dU = U_new - U_old;
+        double dV = new_V - old_V;
+        arg = -dU - s->p.pressure_angstr_kT * dV + (s->nmol + 1) * log(new_V / old_V);
+        proba = exp(arg);
+    } else {
+        proba = -1.0;
+    }
+    int acc = 1;
+    if (!(proba > 1)) {
+        double r = orc_rand(s);
+        if (s->rng_out) {  /* undo exactly and rewind to before lambda */
+            mcstate_restore(s, &st);
+            s->p = st.p;
+            memcpy(s->lj.sigma, st.lj_sigma, sizeof st.lj_sigma);
+            lj_fill_tab(&s->lj);
+            memcpy(s->beta, st.beta, sizeof(double) * s->g.nk);
+            init_beta_lj(s);
+            total_energy(s);
+            mcstate_free(s, &st);
+            *s->cursor = cur0;
+            return -6;
+        }
+        acc = r < proba;
+    }
+    if (!acc) {
+        mcstate_restore(s, &st);
+        orc_params_recalc(&s->p, old_L);
+        lj_scale_sigma(&s->lj, new_L / old_L);
+        init_beta_lj(s);
+        for (int k = 0; k < s->g.nk; k++) s->beta[k] = s->beta[k] * xclb_old / xclb_new;
+        total_energy(s);
+    }
+    mcstate_free(s, &st);
+    rec->flags = (acc ? 1 : 0) | (ov ? 2 : 0);
+    rec->pad = 0;
+    rec->box_old = old_L; rec->box_new = new_L; rec->du = dU; rec->arg = arg;
+    rec->cursor = *s->cursor;
+    return 0;
+}
+
+int32_t orc_mcvol(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, orc_vol_rec *rec) {
+    s->rng = rng; s->n_rng = n_rng; s->cursor = cursor; s->rng_out = 0;
+    rec->cycle = s->icycle;
+    return mcvol(s, rec);
+}
+
+/* run_mc (runmc.f90:178-334) by cycles, NPT included: each cycle draws
+   rnd = rand()*(pressure_step_multiplier+1); above pressure_step_multiplier (when it is
+   positive) the cycle is one mcvol, otherwise nmol movemc calls.  A call that starts in
+   the middle of a move cycle finishes that cycle first (it counts as one of n_cycles). */
+int32_t orc_run_cycles(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_cycles,
+                       int64_t *cycles_done, orc_move_rec *log, int64_t max_log, int64_t *n_log,
+                       orc_vol_rec *vlog, int64_t max_vlog, int64_t *n_vlog, double *rows, int32_t max_rows,
+                       int32_t *n_rows) {
+    s->rng = rng; s->n_rng = n_rng; s->cursor = cursor; s->rng_out = 0;
+    if (n_rows) *n_rows = 0;
+    if (n_log) *n_log = 0;
+    if (n_vlog) *n_vlog = 0;
+    if (cycles_done) *cycles_done = 0;
+    double psm = s->p.pressure_step_multiplier;
+    for (int64_t c = 0; c < n_cycles; c++) {
+        if (s->move_in_cycle == 0) {
+            int64_t c0 = *cursor;
+            double rnd = orc_rand(s) * (psm + 1);
+            if (s->rng_out) { *cursor = c0; return -6; }
+            if (psm > 0 && rnd > psm) {
+                orc_vol_rec vr;
+                vr.cycle = s->icycle;
+                int r = mcvol(s, &vr);
+                if (r) { *cursor = c0; return r; }
+                if (vr.flags & 1) s->n_vol_accepted += 1;
+                s->n_vol_steps += 1;
+                if (vlog && n_vlog && *n_vlog < max_vlog) vlog[(*n_vlog)++] = vr;
+                cycle_end(s, rows, max_rows, n_rows);
+                if (cycles_done) (*cycles_done)++;
+                continue;
+            }
+            *cursor = c0;  /* a move cycle: run_moves takes the draw again */
+        }
+        int64_t mic0 = s->move_in_cycle;
+        int64_t n = s->nmol - mic0;
+        int64_t room = log ? max_log - *n_log : 0;
+        orc_move_rec *lg = (log && room >= n) ? log + *n_log : NULL;
+        int r = run_moves(s, n, lg, rows, max_rows, n_rows);
+        if (r == -6 && lg) *n_log += s->move_in_cycle - mic0;  /* the moves done before the stream ran out */
+        if (r) return r;
+        if (lg) *n_log += n;
+        if (cycles_done) (*cycles_done)++;
     }
     return 0;
 }
@@ -1720,3 +1960,4 @@ void orc_force_kspace_atom(orc_state *s, int32_t atom1, double x, double y, doub
     f[0] = fk[0] + fl[0]; f[1] = fk[1] + fl[1]; f[2] = fk[2] + fl[2];
     rho_free(&tmp, s->lj.ntype);
 }
+double orc_box_length(const orc_state *s) { return s->p.BoxLength; }

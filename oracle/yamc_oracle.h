@@ -59,6 +59,16 @@ typedef struct {
     double f_old[3], t_old[3], f_new[3], t_new[3];
 } orc_move_rec;
 
+/* one mcvol step (MC.f90:701-825) written by orc_run_cycles / orc_mcvol */
+typedef struct {
+    int64_t cycle;      /* run_mc cycle number */
+    int32_t flags;      /* bit0 accepted, bit1 hard-core overlap at the new volume */
+    int32_t pad;
+    int64_t cursor;     /* RNG cursor after the step */
+    double box_old, box_new;  /* BoxLength before and tried (Angstrom) */
+    double du, arg;     /* U_new - U_old (kT) and the acceptance exponent */
+} orc_vol_rec;
+
 /* ---- parameters ---- */
 void orc_params_defaults(orc_params *p);
 int orc_params_read(orc_params *p, const char *path);
@@ -103,6 +113,18 @@ double orc_mu(const orc_state *s, int32_t c);
 int32_t orc_run_mc(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor,
                    int64_t n_moves, orc_move_rec *log, double *rows, int32_t max_rows,
                    int32_t *n_rows);
+/* run_mc by cycles with NPT volume steps (pressure_step_multiplier > 0); move records
+   go to log (when max_log leaves room for the whole cycle), volume steps to vlog.
+   Returns 0 or -6 (buffer exhausted; an interrupted volume step is undone and its
+   cycle draw given back, an interrupted move cycle resumes mid-cycle). */
+int32_t orc_run_cycles(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_cycles,
+                       int64_t *cycles_done, orc_move_rec *log, int64_t max_log, int64_t *n_log,
+                       orc_vol_rec *vlog, int64_t max_vlog, int64_t *n_vlog, double *rows, int32_t max_rows,
+                       int32_t *n_rows);
+/* a single mcvol with its draws from the RNG buffer */
+int32_t orc_mcvol(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, orc_vol_rec *rec);
+/* current BoxLength (Angstrom) and the molecule-atom distances in Angstrom follow from it */
+double orc_box_length(const orc_state *s);
 /* a single movemc(imol) with the proposal drawn from the RNG buffer */
 int32_t orc_movemc(orc_state *s, int32_t imol, const float *rng, int64_t n_rng,
                    int64_t *cursor, orc_move_rec *rec);

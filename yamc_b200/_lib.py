@@ -62,6 +62,17 @@ MOVE_RECORD_DTYPE = np.dtype([("imol", np.int32), ("flags", np.int32), ("cursor"
                               ("du_k_lj", np.float64), ("du_ext", np.float64)])
 assert MOVE_RECORD_DTYPE.itemsize == ctypes.sizeof(MoveRecord)
 
+class VolumeRecord(ctypes.Structure):
+    _fields_ = [("cycle", ctypes.c_int64), ("flags", ctypes.c_int32), ("pad", ctypes.c_int32),
+                ("cursor", ctypes.c_int64), ("box_old", ctypes.c_double), ("box_new", ctypes.c_double),
+                ("du", ctypes.c_double), ("arg", ctypes.c_double)]
+
+
+VOLUME_RECORD_DTYPE = np.dtype([("cycle", np.int64), ("flags", np.int32), ("pad", np.int32), ("cursor", np.int64),
+                                ("box_old", np.float64), ("box_new", np.float64), ("du", np.float64),
+                                ("arg", np.float64)])
+assert VOLUME_RECORD_DTYPE.itemsize == ctypes.sizeof(VolumeRecord)
+
 # every entry point declared in include/yamc.h, with (restype, argtypes)
 _VP = ctypes.c_void_p
 _PPP = ctypes.POINTER(ctypes.c_void_p)
@@ -89,6 +100,13 @@ SIGNATURES = {
     "yamc_run_chain_device": (ctypes.c_int, [_VP, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64),
                                              ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p,
                                              ctypes.c_void_p, ctypes.c_int32, _ip]),
+    "yamc_run_mc": (ctypes.c_int, [_VP, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64), ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int64,
+                                   ctypes.POINTER(ctypes.c_int64), ctypes.c_void_p, ctypes.c_int32, _ip]),
+    "yamc_volume_eval": (ctypes.c_int, [_VP, ctypes.c_double, _dp, _ip]),
+    "yamc_volume_commit": (ctypes.c_int, [_VP, ctypes.c_int32]),
+    "yamc_get_params": (ctypes.c_int, [_VP, ctypes.POINTER(YamcParams)]),
     "yamc_set_refresh": (ctypes.c_int, [_VP, ctypes.c_int64]),
     "yamc_refresh_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "yamc_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),

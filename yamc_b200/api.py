@@ -196,6 +196,42 @@ class Engine:
             check(st, "yamc_run_chain")
         return rec[: done.value], rows[: nrow.value], cur.value, done.value, st
 
+    def run_mc(self, rng: np.ndarray, n_cycles: int, cursor: int = 0, log: bool = True, max_rows: int = 0):
+        """run_mc by cycles, NPT volume steps included (pressure_step_multiplier > 0).
+        Returns (move log, volume log, rows, cursor, cycles_done, status)."""
+        rng = np.ascontiguousarray(rng, dtype=np.float32)
+        cur = ctypes.c_int64(int(cursor))
+        done, nlog, nvlog = ctypes.c_int64(0), ctypes.c_int64(0), ctypes.c_int64(0)
+        nrow = ctypes.c_int32(0)
+        max_log = int(n_cycles) * self.nmol if log else 0
+        rec = np.zeros(max(max_log, 1), dtype=MOVE_RECORD_DTYPE)
+        vrec = np.zeros(max(int(n_cycles), 1), dtype=_lib.VOLUME_RECORD_DTYPE)
+        rows = np.zeros((max(max_rows, 1), 9))
+        st = self.lib.yamc_run_mc(self.h, rng.ctypes.data, rng.size, ctypes.byref(cur), int(n_cycles), ctypes.byref(done),
+                                  rec.ctypes.data if log else None, max_log, ctypes.byref(nlog), vrec.ctypes.data,
+                                  int(n_cycles), ctypes.byref(nvlog), rows.ctypes.data if max_rows else None,
+                                  int(max_rows), ctypes.byref(nrow))
+        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+            check(st, "yamc_run_mc")
+        return rec[: nlog.value], vrec[: nvlog.value], rows[: nrow.value], cur.value, done.value, st
+
+    def volume_eval(self, new_box_length: float):
+        """mcvol up to the acceptance test for a given new box length: (dU, overlap)."""
+        du = ctypes.c_double(0)
+        ov = ctypes.c_int32(0)
+        check(self.lib.yamc_volume_eval(self.h, float(new_box_length), ctypes.byref(du), ctypes.byref(ov)),
+              "yamc_volume_eval")
+        return du.value, bool(ov.value)
+
+    def volume_commit(self, accepted: bool) -> None:
+        check(self.lib.yamc_volume_commit(self.h, int(bool(accepted))), "yamc_volume_commit")
+
+    @property
+    def params(self) -> "_lib.YamcParams":
+        p = _lib.YamcParams()
+        check(self.lib.yamc_get_params(self.h, ctypes.byref(p)), "yamc_get_params")
+        return p
+
     def run_chain_device(self, d_rng_ptr: int, n_rng: int, n_moves: int, cursor: int = 0, d_log_ptr: int = 0):
         cur = ctypes.c_int64(int(cursor))
         done = ctypes.c_int64(0)

@@ -396,6 +396,17 @@ struct yamc_ctx {
     long long *d_prof = nullptr;
     bool prof_on = false;
     double *d_gx = nullptr, *d_gy = nullptr, *d_gz = nullptr;  // adjoint forces
+    // NPT volume move: rho(k) as it was before the step, accepted volume steps
+    double2 *rho_save = nullptr;
+    double n_vol_accepted = 0;
+    int vol_stage = 0;  // 1 between yamc_volume_eval and yamc_volume_commit
+    struct VolSaved {
+        yamc_params p{};
+        std::vector<double> x, y, z, sigma, type_sigma, beta, ebetalj, lj6, lj12, four_eps, sigma6, sigma2, dhs;
+        double sc[SC_COUNT] = {};
+        double tail_c = 0, tail6 = 0, tail12 = 0;
+        double old_L = 0, new_L = 0, xclb_old = 0, xclb_new = 0, U_old = 0;
+    } vol;
     // mixed form: FP64 recomputation of rho(k) every refresh_every accepted moves (in the chain kernel)
     long long refresh_every = 10000;
 };
@@ -525,8 +536,10 @@ int push_state(yamc_ctx *c) {
     return YAMC_OK;
 }
 
-// mc_calc_total_sums (MC.f90:477-585) on the device
-int full_sums(yamc_ctx *c) {
+// mc_calc_total_sums (MC.f90:477-585) on the device.  A hard-core overlap is an error
+// (YAMC_EOVERLAP_INIT) unless overlap is given, which then receives it (the volume move's
+// case: the sums are still completed, as the reference completes them).
+int full_sums(yamc_ctx *c, int *overlap = nullptr) {
     HostSystem &H = c->H;
     int r = sync_positions(c);
     if (r) return r;
@@ -539,7 +552,8 @@ int full_sums(yamc_ctx *c) {
     double tot[kFullParts] = {};
     for (int b = 0; b < nbr; ++b)
         for (int v = 0; v < kFullParts; ++v) tot[v] = (v == 6) ? std::max(tot[v], pr[b * kFullParts + v]) : tot[v] + pr[b * kFullParts + v];
-    if (tot[6] > 0) { set_error("hard-core overlap in the configuration"); return YAMC_EOVERLAP_INIT; }
+    if (overlap) *overlap = tot[6] > 0;
+    else if (tot[6] > 0) { set_error("hard-core overlap in the configuration"); return YAMC_EOVERLAP_INIT; }
     switch (H.nt) {
         case 1: r = launch_rho_full<1>(c); break;
         case 2: r = launch_rho_full<2>(c); break;
@@ -893,7 +907,7 @@ int yamc_destroy(yamc_ctx *c) {
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->uu, c->fx, c->fy,
                     c->fz, c->part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
-                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz};
+                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->rho_save};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1028,6 +1042,10 @@ int yamc_refresh_count(yamc_ctx *c, int64_t *count) {
 int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_t *cursor, int64_t n_moves,
                           int64_t *moves_done, yamc_move_record *d_log, double *d_rows, int32_t max_rows, int32_t *n_rows) {
     if (!c || !d_rng || !cursor || n_moves < 0) return YAMC_EPARAMETER;
+    if (c->H.p.pressure_step_multiplier > 0) {
+        set_error("pressure_step_multiplier > 0 (NPT): volume cycles run through yamc_run_mc");
+        return YAMC_EWRONG_FUNCTION;
+    }
     CUDA_TRY(cudaSetDevice(c->device));
     return run_chain_impl(c, d_rng, 0, n_rng, cursor, n_moves, moves_done, d_log, d_rows, max_rows, n_rows);
 }
@@ -1035,6 +1053,10 @@ int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_
 int yamc_run_chain(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_moves, int64_t *moves_done,
                    yamc_move_record *log, double *rows, int32_t max_rows, int32_t *n_rows) {
     if (!c || !rng || !cursor || n_moves < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
+    if (c->H.p.pressure_step_multiplier > 0) {
+        set_error("pressure_step_multiplier > 0 (NPT): volume cycles run through yamc_run_mc");
+        return YAMC_EWRONG_FUNCTION;
+    }
     CUDA_TRY(cudaSetDevice(c->device));
     const size_t nr = (size_t)(n_rng - *cursor);
     if (nr > c->rng_cap) {
@@ -1070,6 +1092,311 @@ int yamc_run_chain(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor
     if (log && done) CUDA_TRY(cudaMemcpy(log, c->d_log, sizeof(yamc_move_record) * done, cudaMemcpyDeviceToHost));
     if (rows && nrow) CUDA_TRY(cudaMemcpy(rows, c->d_rows, sizeof(double) * 9 * nrow, cudaMemcpyDeviceToHost));
     if (moves_done) *moves_done = done;
+    if (n_rows) *n_rows = nrow;
+    return st;
+}
+
+// ---------------------------------------------------------------- NPT volume move
+
+// rand() of random.f90:65-93 on the host: the next value of the stream, values outside
+// [1e-14, 1 - 1e-14] drawn again; false when the stream runs out
+static bool host_rand(const float *rng, int64_t n_rng, int64_t *cursor, double *out) {
+    float v = 0.0f;
+    while ((double)v < 1e-14 || (double)v > 1.0 - 1e-14) {
+        if (*cursor >= n_rng) return false;
+        v = rng[(*cursor)++];
+    }
+    *out = (double)v;
+    return true;
+}
+
+// the device data that depend on the box length, from the host copy: positions, hard-core
+// diameters / L, beta and beta_LJ per signed entry, the LJ tables and the scalar parameters
+static int upload_box(yamc_ctx *c) {
+    HostSystem &H = c->H;
+    const int N = H.N, S = H.S, nt = H.nt;
+    std::vector<double4> a(N);
+    for (int i = 0; i < N; ++i) a[i] = make_double4(H.x[i], H.y[i], H.z[i], H.q[i]);
+    for (int e = 0; e < S; ++e) H.ebeta[e] = H.beta[H.ekk[e]];
+    int r;
+    if ((r = upload(c->atom, a.data(), N, c->stream)) || (r = upload(c->dhs, H.dhs.data(), N, c->stream)) ||
+        (r = upload(c->ebeta, H.ebeta.data(), S, c->stream)) ||
+        (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) ||
+        (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
+        (r = upload(c->lj_feps, H.four_eps.data(), nt * nt, c->stream)))
+        return r;
+    DevSys &D = c->hsys;
+    const yamc_params &P = H.p;
+    D.rmax2 = P.rmax2; D.alpha = P.alpha; D.xclb = P.xclb; D.taosp = P.two_alpha_over_sqrt_pi; D.kext = P.kext;
+    D.m2k = P.minus_two_kext; D.dr = P.dr; D.d_angle = P.d_angle;
+    D.rpre = std::sqrt(P.rmax2);
+    for (int i = 0; i < N; ++i) D.rpre = std::max(D.rpre, H.dhs[i]);
+    if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
+    c->pos_valid = true;
+    return YAMC_OK;
+}
+
+// scale_box (scale_box.f90:6-62) on the host copy: each molecule's centre of mass
+// (center_of_mass, geometry.f90:170-201) keeps its box coordinates, its atoms' offsets scale
+// by L_old / L_new (bond lengths in Angstrom stay), one-atom molecules stay; sigma scales too
+static void scale_box_host(HostSystem &H, double new_L) {
+    const double c = H.p.BoxLength / new_L;
+    for (int m = 0; m < H.M; ++m) {
+        const int f = H.first[m], n = H.natoms[m];
+        if (n == 1) continue;
+        double sx = 0, sy = 0, sz = 0, tm = 0;
+        for (int a = f; a < f + n; ++a) {
+            sx = sx + H.mass[a] * H.x[a]; sy = sy + H.mass[a] * H.y[a]; sz = sz + H.mass[a] * H.z[a];
+            tm = tm + H.mass[a];
+        }
+        const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
+        for (int a = f; a < f + n; ++a) {
+            H.x[a] = (H.x[a] - xc) * c + xc;
+            H.y[a] = (H.y[a] - yc) * c + yc;
+            H.z[a] = (H.z[a] - zc) * c + zc;
+        }
+    }
+    for (int i = 0; i < H.N; ++i) H.sigma[i] = H.sigma[i] * c;
+}
+
+// mcvol up to the acceptance test (MC.f90:735-799): save the state (mc_save_state), scale
+// the box, Parameters_recalc, LJTypes_scale_sigma, EwaldSumKSpace_initBetaLJ and the full
+// sums with beta scaled by xclb_new / xclb_old (mc_calc_total_sums with scale_beta; alpha*L
+// is fixed, so beta6/beta12 and the k-set do not change)
+static int volume_eval(yamc_ctx *c, double new_L, double *du, int *overlap) {
+    HostSystem &H = c->H;
+    auto &v = c->vol;
+    int r;
+    if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
+    double e[8];
+    energies_from(c->sc, H.p.kext, e);
+    v.U_old = e[0];
+    v.p = H.p; v.x = H.x; v.y = H.y; v.z = H.z; v.sigma = H.sigma; v.type_sigma = H.type_sigma; v.beta = H.beta;
+    v.ebetalj = H.ebetalj; v.lj6 = H.lj6; v.lj12 = H.lj12; v.four_eps = H.four_eps; v.sigma6 = H.sigma6;
+    v.sigma2 = H.sigma2; v.dhs = H.dhs;
+    std::copy(c->sc, c->sc + SC_COUNT, v.sc);
+    v.tail_c = H.U_tail_coul; v.tail6 = H.U_tail_lj6; v.tail12 = H.U_tail_lj12;
+    const size_t nrho = (size_t)(1 + H.nt) * H.S;
+    if (!c->rho_save && (r = dalloc(&c->rho_save, nrho))) return r;
+    CUDA_TRY(cudaMemcpyAsync(c->rho_save, c->rho, sizeof(double2) * nrho, cudaMemcpyDeviceToDevice, c->stream));
+    v.old_L = H.p.BoxLength; v.new_L = new_L;
+    scale_box_host(H, new_L);
+    v.xclb_old = H.p.xclb;
+    if ((r = yamc_params_recalc(&H.p, new_L))) return r;
+    v.xclb_new = H.p.xclb;
+    for (double &t : H.type_sigma) t = t * (v.old_L / new_L);
+    fill_lj_tables(H);
+    fill_beta_lj(H);
+    const double scale_beta = v.xclb_new / v.xclb_old;  // positive: the recompute branch of EwaldSumKSpace_init is never taken
+    for (double &b : H.beta) b = b * scale_beta;
+    for (int i = 0; i < H.N; ++i) H.dhs[i] = H.hc[i] / new_L;
+    compute_tails(H);
+    if ((r = upload_box(c))) return r;
+    int ov = 0;
+    if ((r = full_sums(c, &ov))) return r;
+    energies_from(c->sc, H.p.kext, e);
+    *du = ov ? 0.0 : e[0] - v.U_old;
+    *overlap = ov;
+    c->vol_stage = 1;
+    return YAMC_OK;
+}
+
+// the end of mcvol (MC.f90:801-823): an accepted step keeps the new box; a rejected one
+// takes mc_restore_state and puts the parameters, LJ tables and beta back as the reference
+// does (sigma scaled by L_new / L_old, beta by xclb_old / xclb_new, both to rounding).
+// exact != 0 instead restores every table bit for bit (a step abandoned because the random
+// stream ran out, which the reference never meets).
+static int volume_commit(yamc_ctx *c, bool accepted, bool exact) {
+    HostSystem &H = c->H;
+    auto &v = c->vol;
+    c->vol_stage = 0;
+    if (accepted) {
+        CUDA_TRY(cudaStreamSynchronize(c->stream));
+        return YAMC_OK;
+    }
+    H.x = v.x; H.y = v.y; H.z = v.z; H.sigma = v.sigma;
+    std::copy(v.sc, v.sc + SC_COUNT, c->sc);
+    H.U_tail_coul = v.tail_c; H.U_tail_lj6 = v.tail6; H.U_tail_lj12 = v.tail12;
+    if (exact) {
+        H.p = v.p; H.type_sigma = v.type_sigma; H.beta = v.beta; H.ebetalj = v.ebetalj; H.lj6 = v.lj6;
+        H.lj12 = v.lj12; H.four_eps = v.four_eps; H.sigma6 = v.sigma6; H.sigma2 = v.sigma2;
+    } else {
+        int r = yamc_params_recalc(&H.p, v.old_L);
+        if (r) return r;
+        for (double &t : H.type_sigma) t = t * (v.new_L / v.old_L);
+        fill_lj_tables(H);
+        fill_beta_lj(H);
+        for (double &b : H.beta) b = b * v.xclb_old / v.xclb_new;
+    }
+    H.dhs = v.dhs;
+    const size_t nrho = (size_t)(1 + H.nt) * H.S;
+    CUDA_TRY(cudaMemcpyAsync(c->rho, c->rho_save, sizeof(double2) * nrho, cudaMemcpyDeviceToDevice, c->stream));
+    int r;
+    if ((r = upload_box(c)) || (r = push_state(c))) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return YAMC_OK;
+}
+
+// one whole mcvol (MC.f90:701-825) with its draws from a host stream: lambda, then the
+// acceptance draw only when the probability is not above 1 (`(proba > 1) .or. (rand() <
+// proba)` with the short-circuit of gfortran's optimised builds); an overlap gives
+// proba = -1, so it draws and rejects.  On exhaustion the step is undone and the cursor
+// put back to where it was.
+static int volume_step(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, yamc_volume_record *rec) {
+    const int64_t cur0 = *cursor;
+    double u;
+    if (!host_rand(rng, n_rng, cursor, &u)) {
+        *cursor = cur0;
+        set_error("random stream exhausted at a volume step");
+        return YAMC_ERNG_EXHAUSTED;
+    }
+    const double old_L = c->H.p.BoxLength, old_V = old_L * old_L * old_L;
+    const double lambda = 2 * u - 1.0;
+    const double log_new_V = std::log(old_V) + lambda * c->H.p.log_max_volume_scaling;
+    const double new_V = std::exp(log_new_V);
+    const double new_L = std::pow(new_V, 1.0 / 3.0);
+    double du = 0;
+    int ov = 0;
+    int r = volume_eval(c, new_L, &du, &ov);
+    if (r) return r;
+    double proba, arg = 0;
+    if (!ov) {
+        const double dV = new_V - old_V;
+        arg = -du - c->H.p.pressure_angstr_kT * dV + (c->H.M + 1) * std::log(new_V / old_V);
+        proba = std::exp(arg);
+    } else {
+        proba = -1.0;
+    }
+    bool acc = true;
+    if (!(proba > 1)) {
+        double x;
+        if (!host_rand(rng, n_rng, cursor, &x)) {
+            if ((r = volume_commit(c, false, true))) return r;
+            *cursor = cur0;
+            set_error("random stream exhausted inside a volume step (undone)");
+            return YAMC_ERNG_EXHAUSTED;
+        }
+        acc = x < proba;
+    }
+    if ((r = volume_commit(c, acc, false))) return r;
+    rec->flags = (acc ? 1 : 0) | (ov ? 2 : 0);
+    rec->pad = 0;
+    rec->cursor = *cursor;
+    rec->box_old = old_L; rec->box_new = new_L; rec->du = du; rec->arg = arg;
+    return YAMC_OK;
+}
+
+int yamc_volume_eval(yamc_ctx *c, double new_box_length, double *du, int32_t *overlap) {
+    if (!c || !du || !overlap || !(new_box_length > 0)) return YAMC_EPARAMETER;
+    if (c->api_stage || c->vol_stage) { set_error("a move or volume step is pending"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    int ov = 0;
+    const int r = volume_eval(c, new_box_length, du, &ov);
+    *overlap = ov;
+    return r;
+}
+
+int yamc_volume_commit(yamc_ctx *c, int32_t accepted) {
+    if (!c) return YAMC_EPARAMETER;
+    if (!c->vol_stage) { set_error("no volume step is pending"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    return volume_commit(c, accepted != 0, false);
+}
+
+int yamc_get_params(yamc_ctx *c, yamc_params *p) {
+    if (!c || !p) return YAMC_EPARAMETER;
+    *p = c->H.p;
+    return YAMC_OK;
+}
+
+int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_cycles, int64_t *cycles_done,
+                yamc_move_record *log, int64_t max_log, int64_t *n_log, yamc_volume_record *vlog, int64_t max_vlog,
+                int64_t *n_vlog, double *rows, int32_t max_rows, int32_t *n_rows) {
+    if (!c || !rng || !cursor || n_cycles < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
+    if (c->api_stage || c->vol_stage) { set_error("a move or volume step is pending"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    HostSystem &H = c->H;
+    const int64_t base = *cursor;
+    const size_t nr = (size_t)(n_rng - base);
+    int r;
+    if (nr > c->rng_cap) {
+        if (c->d_rng) cudaFree(c->d_rng);
+        c->d_rng = nullptr;
+        c->rng_cap = 0;
+        if ((r = dalloc(&c->d_rng, nr))) return r;
+        c->rng_cap = nr;
+    }
+    if (nr) CUDA_TRY(cudaMemcpyAsync(c->d_rng, rng + base, nr * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+    if (log && (size_t)H.M > c->log_cap) {
+        if (c->d_log) cudaFree(c->d_log);
+        c->d_log = nullptr;
+        c->log_cap = 0;
+        if ((r = dalloc(&c->d_log, (size_t)H.M))) return r;
+        c->log_cap = (size_t)H.M;
+    }
+    if (rows && c->rows_cap < 1) {
+        if ((r = dalloc(&c->d_rows, 9))) return r;
+        c->rows_cap = 1;
+    }
+    int64_t done = 0, nlog = 0, nvlog = 0;
+    int32_t nrow = 0;
+    int st = YAMC_OK;
+    if ((r = pull_state(c))) return r;
+    const double psm = H.p.pressure_step_multiplier;
+    for (int64_t cyc = 0; cyc < n_cycles; ++cyc) {
+        if (c->cnt_h[CN_MOVE_IN_CYCLE] == 0) {
+            // the cycle's draw (runmc.f90:206-207): above pressure_step_multiplier, a volume step
+            const int64_t c0 = *cursor;
+            double u;
+            if (!host_rand(rng, n_rng, cursor, &u)) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
+            if (psm > 0 && u * (psm + 1) > psm) {
+                yamc_volume_record vr{};
+                vr.cycle = c->cnt_h[CN_ICYCLE];
+                r = volume_step(c, rng, n_rng, cursor, &vr);
+                if (r == YAMC_ERNG_EXHAUSTED) { *cursor = c0; st = r; break; }
+                if (r) return r;
+                if (vr.flags & 1) c->n_vol_accepted += 1;
+                c->sc[SC_N_VOL_STEPS] += 1;
+                if (vlog && nvlog < max_vlog) vlog[nvlog++] = vr;
+                // energy.dat row at the cycle's end (runmc.f90:276-279)
+                const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
+                if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && nrow < max_rows) {
+                    double e[8];
+                    energies_from(c->sc, H.p.kext, e);
+                    double *row = rows + 9 * (size_t)nrow;
+                    row[0] = (double)c->cnt_h[CN_ICYCLE];
+                    for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
+                    ++nrow;
+                }
+                c->cnt_h[CN_ICYCLE] += 1;
+                if ((r = push_state(c))) return r;
+                ++done;
+                continue;
+            }
+            *cursor = c0;  // a move cycle: the chain kernel takes the cycle's draw itself
+        }
+        const int64_t n = H.M - c->cnt_h[CN_MOVE_IN_CYCLE];
+        const bool keep_log = log && nlog + n <= max_log;
+        const bool want_row = rows && nrow < max_rows;
+        int64_t mdone = 0;
+        int32_t kr = 0;
+        st = run_chain_impl(c, c->d_rng, base, n_rng, cursor, n, &mdone, keep_log ? c->d_log : nullptr,
+                            want_row ? c->d_rows : nullptr, want_row ? 1 : 0, &kr);
+        if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
+        if (keep_log && mdone)
+            CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record) * mdone, cudaMemcpyDeviceToHost));
+        if (keep_log) nlog += mdone;
+        if (want_row && kr) {
+            CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9, cudaMemcpyDeviceToHost));
+            ++nrow;
+        }
+        if ((r = pull_state(c))) return r;
+        if (st == YAMC_ERNG_EXHAUSTED) break;
+        ++done;
+    }
+    if (cycles_done) *cycles_done = done;
+    if (n_log) *n_log = nlog;
+    if (n_vlog) *n_vlog = nvlog;
     if (n_rows) *n_rows = nrow;
     return st;
 }
@@ -1217,6 +1544,10 @@ static int batch_create_impl(yamc_batch *b, int32_t n, const yamc_system *system
     CUDA_TRY(cudaEventCreate(&b->ev1));
     CUDA_TRY(cudaEventCreateWithFlags(&b->fork, cudaEventDisableTiming));
     for (int i = 0; i < n; ++i) {
+        if (params[i].pressure_step_multiplier > 0) {
+            set_error("replica " + std::to_string(i) + ": batched replicas run NVT (pressure_step_multiplier 0)");
+            return YAMC_EPARAMETER;
+        }
         yamc_ctx *c = nullptr;
         const int r = yamc_create(&systems[i], &params[i], b->device, &c);
         if (r) {

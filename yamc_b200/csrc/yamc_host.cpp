@@ -256,6 +256,73 @@ int grid_count(int kmax) {
     return n;
 }
 
+// ---------------------------------------------------------------- box-dependent tables
+
+// LJTypes_fill_LJ_tab (LJTypes.f90:273-308) with LJTypes_fill_LJ_tab_index (:202-232):
+// Lorentz-Berthelot tables from the type list (type_sigma in box units, type_eps in kT)
+void fill_lj_tables(HostSystem &H) {
+    const int nt = H.nt, n2 = std::max(1, nt * nt);
+    H.lj6.assign(n2, 0); H.lj12.assign(n2, 0); H.four_eps.assign(n2, 0); H.sigma6.assign(n2, 0); H.sigma2.assign(n2, 0);
+    auto fill = [&](int i, int j, double s12, double e12) {
+        const double s2 = s12 * s12, s6 = s2 * s2 * s2;
+        for (int pass = 0; pass < (i == j ? 1 : 2); ++pass) {
+            const int o = pass == 0 ? (i - 1) * nt + (j - 1) : (j - 1) * nt + (i - 1);
+            H.lj6[o] = 4 * e12 * s6;
+            H.lj12[o] = H.lj6[o] * s6;
+            H.sigma2[o] = s2; H.sigma6[o] = s6; H.four_eps[o] = 4 * e12;
+        }
+    };
+    const std::vector<double> &ts = H.type_sigma, &te = H.type_eps;
+    for (int i = 1; i <= nt; ++i) {
+        fill(i, i, ts[i - 1], te[i - 1]);
+        for (int j = i + 1; j <= nt; ++j) fill(i, j, (ts[i - 1] + ts[j - 1]) / 2, std::sqrt(te[i - 1] * te[j - 1]));
+    }
+}
+
+// EwaldSumKSpace_initBetaLJ (EwaldSumKSpace.f90:352-386), one row per t1 <= t2, per signed entry
+void fill_beta_lj(HostSystem &H) {
+    const int nt = H.nt;
+    H.ebetalj.assign((size_t)std::max(1, H.npair) * H.S, 0.0);
+    for (int t1 = 1; t1 <= nt; ++t1)
+        for (int t2 = t1; t2 <= nt; ++t2) {
+            const int o = (t1 - 1) * nt + (t2 - 1), pidx = H.pair_index[o];
+            for (int e = 0; e < H.S; ++e) {
+                const int k = H.ekk[e];
+                H.ebetalj[(size_t)pidx * H.S + e] = H.lj12[o] * H.beta12[k] - H.lj6[o] * H.beta6[k];
+            }
+        }
+}
+
+// ewald_sum_coulomb_tail / ewald_sum_lj_tails (EwaldSumTails.f90:18-127); molecule counts
+// are read by LJ type (EwaldSumTails.f90:88)
+void compute_tails(HostSystem &H) {
+    const yamc_params &p = H.p;
+    const int N = H.N, nt = H.nt;
+    const double alpha = p.alpha;
+    double sq = 0;
+    for (int i = 0; i < N; ++i) sq = sq + H.q[i] * H.q[i];
+    H.U_tail_coul = -(p.xclb * p.alpha_over_sqrt_pi * sq);
+    const double a3 = powi(alpha, 3), a6 = a3 * a3, a9 = a3 * a6, a12 = a6 * a6;
+    const double pisp = std::pow(kPi, 1.5);
+    double sij6 = 0, sij12 = 0, sj6 = 0, sj12 = 0;
+    for (int t1 = 1; t1 <= nt; ++t1)
+        for (int t2 = t1; t2 <= nt; ++t2) {
+            const int o = (t1 - 1) * nt + (t2 - 1);
+            const int n1n2 = H.mol_numbers[t1 - 1] * H.mol_numbers[t2 - 1];
+            double l6 = H.lj6[o] * n1n2, l12 = H.lj12[o] * n1n2;
+            if (t1 != t2) { l6 = l6 + l6; l12 = l12 + l12; }
+            sij6 = sij6 + l6; sij12 = sij12 + l12;
+        }
+    for (int t = 1; t <= nt; ++t) {
+        const int o = (t - 1) * nt + (t - 1);
+        sj6 = sj6 + H.lj6[o] * H.mol_numbers[t - 1];
+        sj12 = sj12 + H.lj12[o] * H.mol_numbers[t - 1];
+    }
+    H.U_tail_lj6 = pisp * a3 / 6.0 * sij6 - a6 / 12.0 * sj6;
+    H.U_tail_lj12 = pisp * a9 / 1080.0 * sij12 - a12 / 1440.0 * sj12;
+
+}
+
 // ---------------------------------------------------------------- system set-up
 
 int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSystem *hs) {
@@ -329,26 +396,13 @@ int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSyst
     }
     const int nt = (int)ts.size();
     H.nt = nt;
+    H.type_sigma = ts; H.type_eps = te;
     H.type_by_index.assign(N, 0);
     for (int i = 0; i < N; ++i)
         for (int t = 0; t < nt; ++t)
             if (std::fabs(H.sigma[i] - ts[t]) < 1e-8 && std::fabs(H.eps[i] - te[t]) < 1e-8) { H.type_by_index[i] = t + 1; break; }
-    // LJTypes_fill_LJ_tab (:273-308) with LJTypes_fill_LJ_tab_index (:202-232), Lorentz-Berthelot
+    fill_lj_tables(H);
     const int n2 = std::max(1, nt * nt);
-    H.lj6.assign(n2, 0); H.lj12.assign(n2, 0); H.four_eps.assign(n2, 0); H.sigma6.assign(n2, 0); H.sigma2.assign(n2, 0);
-    auto fill = [&](int i, int j, double s12, double e12) {
-        const double s2 = s12 * s12, s6 = s2 * s2 * s2;
-        for (int pass = 0; pass < (i == j ? 1 : 2); ++pass) {
-            const int o = pass == 0 ? (i - 1) * nt + (j - 1) : (j - 1) * nt + (i - 1);
-            H.lj6[o] = 4 * e12 * s6;
-            H.lj12[o] = H.lj6[o] * s6;
-            H.sigma2[o] = s2; H.sigma6[o] = s6; H.four_eps[o] = 4 * e12;
-        }
-    };
-    for (int i = 1; i <= nt; ++i) {
-        fill(i, i, ts[i - 1], te[i - 1]);
-        for (int j = i + 1; j <= nt; ++j) fill(i, j, (ts[i - 1] + ts[j - 1]) / 2, std::sqrt(te[i - 1] * te[j - 1]));
-    }
     H.pair_index.assign(n2, 0);
     H.npair = nt * (nt + 1) / 2;
     for (int t1 = 1, pidx = 0; t1 <= nt; ++t1)
@@ -403,16 +457,7 @@ int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSyst
     H.S = (int)H.ekk.size();
     H.ebeta.resize(H.S);
     for (int e = 0; e < H.S; ++e) H.ebeta[e] = H.beta[H.ekk[e]];
-    // EwaldSumKSpace_initBetaLJ (EwaldSumKSpace.f90:352-386), one row per t1 <= t2
-    H.ebetalj.assign((size_t)std::max(1, H.npair) * H.S, 0.0);
-    for (int t1 = 1; t1 <= nt; ++t1)
-        for (int t2 = t1; t2 <= nt; ++t2) {
-            const int o = (t1 - 1) * nt + (t2 - 1), pidx = H.pair_index[o];
-            for (int e = 0; e < H.S; ++e) {
-                const int k = H.ekk[e];
-                H.ebetalj[(size_t)pidx * H.S + e] = H.lj12[o] * H.beta12[k] - H.lj6[o] * H.beta6[k];
-            }
-        }
+    fill_beta_lj(H);
 
     // EwaldSumTails (EwaldSumTails.f90:18-127); molecule counts are read by LJ type
     H.mol_numbers.assign(sys->mol_numbers, sys->mol_numbers + std::max(0, sys->n_species));
@@ -420,27 +465,7 @@ int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSyst
         set_error("the LJ tails need mol_numbers for every LJ type (EwaldSumTails.f90:88)");
         return YAMC_EPARAMETER;
     }
-    double sq = 0;
-    for (int i = 0; i < N; ++i) sq = sq + H.q[i] * H.q[i];
-    H.U_tail_coul = -(p.xclb * p.alpha_over_sqrt_pi * sq);
-    const double a3 = powi(alpha, 3), a6 = a3 * a3, a9 = a3 * a6, a12 = a6 * a6;
-    const double pisp = std::pow(kPi, 1.5);
-    double sij6 = 0, sij12 = 0, sj6 = 0, sj12 = 0;
-    for (int t1 = 1; t1 <= nt; ++t1)
-        for (int t2 = t1; t2 <= nt; ++t2) {
-            const int o = (t1 - 1) * nt + (t2 - 1);
-            const int n1n2 = H.mol_numbers[t1 - 1] * H.mol_numbers[t2 - 1];
-            double l6 = H.lj6[o] * n1n2, l12 = H.lj12[o] * n1n2;
-            if (t1 != t2) { l6 = l6 + l6; l12 = l12 + l12; }
-            sij6 = sij6 + l6; sij12 = sij12 + l12;
-        }
-    for (int t = 1; t <= nt; ++t) {
-        const int o = (t - 1) * nt + (t - 1);
-        sj6 = sj6 + H.lj6[o] * H.mol_numbers[t - 1];
-        sj12 = sj12 + H.lj12[o] * H.mol_numbers[t - 1];
-    }
-    H.U_tail_lj6 = pisp * a3 / 6.0 * sij6 - a6 / 12.0 * sj6;
-    H.U_tail_lj12 = pisp * a9 / 1080.0 * sij12 - a12 / 1440.0 * sj12;
+    compute_tails(H);
 
     // BiasedRandom_init (BiasedRandom.f90:44-79) on the move weights (init_freq)
     std::vector<double> w(M, 1.0);

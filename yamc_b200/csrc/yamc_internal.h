@@ -30,6 +30,7 @@ struct HostSystem {
     std::vector<int> molnum;          // 0-based molecule of each atom
     std::vector<int> type_by_index;   // 0 = no LJ, 1..nt
     std::vector<int> first, natoms;   // per molecule, 0-based first atom
+    std::vector<double> type_sigma, type_eps;                  // per LJ type (box units, kT)
     std::vector<double> lj6, lj12, four_eps, sigma6, sigma2;  // nt*nt, offset (t1-1)*nt + t2-1
     std::vector<int> kx, ky, kz;      // half-space list (FourierGrid_init order)
     std::vector<double> beta, beta6, beta12;  // per half-space k, the (1+sgn(kx)) factor folded in
@@ -48,6 +49,11 @@ struct HostSystem {
 };
 
 int prepare_host_system(const yamc_system *sys, const yamc_params *p, HostSystem *hs);
+// the tables that depend on the box length: LJ tables from type_sigma/type_eps, beta_LJ per
+// signed entry from them and beta6/beta12, the tails (used again by the volume move)
+void fill_lj_tables(HostSystem &H);
+void fill_beta_lj(HostSystem &H);
+void compute_tails(HostSystem &H);
 
 // Functions.f90 restated (host)
 double erfc_luc(double x, double x2, double ee2);
