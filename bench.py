@@ -325,6 +325,42 @@ def config4_block(local, rank, n_replicas=96, moves=10000):
             "de_error_vs_fp64_max_kT": max(de) if de else None}
 
 
+def npt_block(local, rank, cycles=12):
+    """NPT run_mc on nacl1m as the reference's own parameters.prm runs it (a volume step on
+    average once every pressure_step_multiplier + 1 = 6 cycles), through yamc_run_mc: move
+    cycles as chain-kernel launches, volume steps as a host-built box rescale plus the full
+    sums on the device.  Reported: moves/s over the whole run and the mean time of a volume
+    step (host clock; both include the volume steps' host work)."""
+    from yamc_b200 import api, rng as grng, systems
+    base = f"/tmp/yamc_bench_npt_r{rank}_{os.getpid()}"
+    files = systems.write_system(systems.WORKLOADS["nacl1m"], base, seed=3)
+    extra = "pressure_step_multiplier=5,max_volume_scaling=1.002,pressure=100000"
+    eng = api.Engine.from_files(files, extra=extra, device=local)
+    buf = grng.gfortran_stream(4242, 40 * 2124 * (cycles + 2) + 100000)
+    log, vlog, _, cur, done, st = eng.run_mc(buf, 2)  # warm-up (kernel shape, first launch)
+    t0 = time.perf_counter()
+    log, vlog, _, cur, done, st = eng.run_mc(buf, cycles, cursor=cur)
+    t = time.perf_counter() - t0
+    assert st == 0 and done == cycles, (st, done)
+    L = eng.current_params().BoxLength
+    tv = []
+    for k in range(6):
+        t1 = time.perf_counter()
+        eng.volume_eval(L * (1.0 + 0.0005 * (1 if k % 2 else -1)))
+        eng.volume_commit(False)
+        tv.append(time.perf_counter() - t1)
+    t2 = time.perf_counter()
+    eng.full_sums()
+    t_full = time.perf_counter() - t2
+    eng.close()
+    return {"workload": "nacl1m (6220 atoms), NPT: pressure 1 bar, pressure_step_multiplier 5, "
+                        "max_volume_scaling 1.002, FP64, unbiased moves",
+            "cycles": cycles, "volume_steps": int(len(vlog)), "volume_accepted": int((vlog["flags"] & 1).sum()),
+            "moves": int(len(log)), "moves_per_s": len(log) / t, "wall_s": t,
+            "volume_step_ms": 1e3 * float(np.median(tv)), "full_sums_ms": 1e3 * t_full,
+            "box_length_A": L}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -338,6 +374,7 @@ def main():
     ap.add_argument("--replicas", type=int, default=0, help="chains per GPU (0 = as many clusters as are resident)")
     ap.add_argument("--no-target", action="store_true", help="skip the 4096-water mixed/batched/force-biased block")
     ap.add_argument("--no-config4", action="store_true", help="skip the 96 ragged replicas block")
+    ap.add_argument("--no-npt", action="store_true", help="skip the NPT run_mc block")
     args = ap.parse_args()
 
     from yamc_b200 import systems
@@ -537,6 +574,8 @@ def main():
         line["north_star_target"] = target_block(local, rank)
     if not args.no_config4:
         line["batch_ragged_96"] = config4_block(local, rank)
+    if not args.no_npt:
+        line["npt_run_mc"] = npt_block(local, rank)
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(files)
     print(json.dumps(line), flush=True)

@@ -226,8 +226,8 @@ class Engine:
     def volume_commit(self, accepted: bool) -> None:
         check(self.lib.yamc_volume_commit(self.h, int(bool(accepted))), "yamc_volume_commit")
 
-    @property
-    def params(self) -> "_lib.YamcParams":
+    def current_params(self) -> "_lib.YamcParams":
+        """The parameters as they stand now (BoxLength follows accepted volume steps)."""
         p = _lib.YamcParams()
         check(self.lib.yamc_get_params(self.h, ctypes.byref(p)), "yamc_get_params")
         return p

@@ -61,87 +61,108 @@ __device__ inline void block_sum(double *vals, int nv, double *sh) {
     __syncthreads();
 }
 
-// EwaldSumRealSpace_calc on the full sum (EwaldSumRealSpace.f90:233-500, j0 = i+1):
-// one thread per atom i runs over all j (tiles staged in shared memory), so per-atom
-// uu(i) and F(i) accumulate in increasing j order like the reference; the energy
-// totals count each pair once (j > i), intra-molecular pairs with -erf_Luc.
-__global__ void __launch_bounds__(kFullTile) k_realspace_full(DevSys D, double *uu, double *fx, double *fy, double *fz,
-                                                             double *part) {
+// EwaldSumRealSpace_calc on the full sum (EwaldSumRealSpace.f90:233-500, j0 = i+1): the
+// energy totals of every pair once.  One block per pair of atom tiles (ti <= tj, the upper
+// triangle, listed in tpairs), so the grid grows as (N/256)^2/2 and fills the GPU even for a
+// few thousand atoms; the j tile sits in shared memory, each thread owns one atom i and runs
+// over it (j > i on the diagonal tile).  Intra-molecular pairs use -erf_Luc and count in the
+// intra totals too; LJ-LJ pairs of different molecules closer than their mean hard-core
+// diameter set the overlap flag.  One partial per block (part[blk*8 + v]), reduced in block
+// order by k_sum_parts.  (The reference's per-atom uu/F of the full sum are not needed: the
+// chain kernel evaluates the moved molecule's old energy directly.)
+__global__ void __launch_bounds__(kFullTile) k_realspace_full(DevSys D, const int2 *tpairs, double *part) {
     __shared__ double4 tp[kFullTile];
     __shared__ int2 tm[kFullTile];
     __shared__ double td[kFullTile];
     __shared__ double red[(kFullTile / 32 + 1) * kFullParts];
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    const int2 tt = tpairs[blockIdx.x];
+    const int i = tt.x * kFullTile + threadIdx.x, j0 = tt.y * kFullTile;
     const bool valid = i < D.N;
     double4 pi = make_double4(0, 0, 0, 0);
     int2 mi = make_int2(-1, 0);
     double di = 0;
     if (valid) { pi = D.atom[i]; mi = D.meta[i]; di = D.dhs[i]; }
-    double u = 0, gx = 0, gy = 0, gz = 0;
     double acc[kFullParts] = {0, 0, 0, 0, 0, 0, 0, 0};
     const int nt = D.nt;
-    for (int t0 = 0; t0 < D.N; t0 += kFullTile) {
-        const int j = t0 + threadIdx.x;
+    {
+        const int j = j0 + threadIdx.x;
         if (j < D.N) { tp[threadIdx.x] = D.atom[j]; tm[threadIdx.x] = D.meta[j]; td[threadIdx.x] = D.dhs[j]; }
-        __syncthreads();
-        const int nj = min(kFullTile, D.N - t0);
-        if (valid) {
-            for (int jj = 0; jj < nj; ++jj) {
-                const int jg = t0 + jj;
-                if (jg == i) continue;
-                const double4 pj = tp[jj];
-                const int2 mj = tm[jj];
-                const bool same = mi.x == mj.x;
-                const double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
-                const double r2 = dx * dx + dy * dy + dz * dz;
-                if (!same && mi.y > 0 && mj.y > 0) {
-                    const double d12 = (di + td[jj]) / 2;
-                    if (r2 < d12 * d12) acc[6] = 1.0;
-                }
-                if (r2 >= D.rmax2) continue;
-                const bool lj = mi.y > 0 && mj.y > 0;
-                const int off = lj ? (mi.y - 1) * nt + (mj.y - 1) : 0;
-                const PairTerm<double> t = pair_term<double, true>(r2, D.xclb * pi.w * pj.w, lj, lj ? D.lj_sig6[off] : 0.0,
-                                                                    lj ? D.lj_feps[off] : 0.0, D.alpha, D.taosp, same);
-                if (jg > i) {
-                    acc[0] += t.ew; acc[1] += t.lj6; acc[2] += t.lj12;
-                    if (same) { acc[3] += t.ew; acc[4] += t.lj6; acc[5] += t.lj12; }
-                }
-                if (!same) {
-                    u = u + (t.ew + t.lj12 - t.lj6);
-                    gx = gx + dx * t.FR; gy = gy + dy * t.FR; gz = gz + dz * t.FR;
-                }
-            }
-        }
-        __syncthreads();
     }
-    if (valid) { uu[i] = u; fx[i] = gx; fy[i] = gy; fz[i] = gz; }
+    __syncthreads();
+    const int nj = min(kFullTile, D.N - j0);
+    if (valid) {
+        const int jstart = tt.x == tt.y ? threadIdx.x + 1 : 0;  // j > i
+        for (int jj = jstart; jj < nj; ++jj) {
+            const double4 pj = tp[jj];
+            const int2 mj = tm[jj];
+            const bool same = mi.x == mj.x;
+            const double dx = min_image(pi.x - pj.x), dy = min_image(pi.y - pj.y), dz = min_image(pi.z - pj.z);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const bool lj = mi.y > 0 && mj.y > 0;
+            if (!same && lj) {
+                const double d12 = (di + td[jj]) / 2;
+                if (r2 < d12 * d12) acc[6] = 1.0;
+            }
+            if (r2 >= D.rmax2) continue;
+            const int off = lj ? (mi.y - 1) * nt + (mj.y - 1) : 0;
+            const PairTerm<double> t = pair_term<double, false>(r2, D.xclb * pi.w * pj.w, lj, lj ? D.lj_sig6[off] : 0.0,
+                                                                 lj ? D.lj_feps[off] : 0.0, D.alpha, D.taosp, same);
+            acc[0] += t.ew; acc[1] += t.lj6; acc[2] += t.lj12;
+            if (same) { acc[3] += t.ew; acc[4] += t.lj6; acc[5] += t.lj12; }
+        }
+    }
     block_sum<kFullTile>(acc, kFullParts, red);
-    if (threadIdx.x < kFullParts) part[blockIdx.x * kFullParts + threadIdx.x] = acc[threadIdx.x];
+    if (threadIdx.x < kFullParts) part[(size_t)blockIdx.x * kFullParts + threadIdx.x] = acc[threadIdx.x];
 }
 
-// RhoSquared_addAtoms (RhoSquared.f90:188-243): for each signed entry the sum over all atoms,
-// in atom order, of the charge-weighted phase (Coulomb) and of the unit phase per LJ type,
-// the LJ phase being the Coulomb one times 1/q like RhoSquared_addAtom (RhoSquared.f90:173-176).
+// part[b*nv + v] over b in [0, nb) -> out[v]: thread t adds blocks t, t+256, ... in order, then
+// a fixed tree over the threads (deterministic); value vmax is a flag, reduced by max
+constexpr int kSumThreads = 256;
+__global__ void __launch_bounds__(kSumThreads) k_sum_parts(const double *part, int nb, int nv, int vmax, double *out) {
+    __shared__ double sh[kSumThreads];
+    for (int v = 0; v < nv; ++v) {
+        double x = 0;
+        for (int b = threadIdx.x; b < nb; b += kSumThreads) {
+            const double y = part[(size_t)b * nv + v];
+            x = v == vmax ? fmax(x, y) : x + y;
+        }
+        sh[threadIdx.x] = x;
+        __syncthreads();
+        for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+            if (threadIdx.x < w) sh[threadIdx.x] = v == vmax ? fmax(sh[threadIdx.x], sh[threadIdx.x + w]) : sh[threadIdx.x] + sh[threadIdx.x + w];
+            __syncthreads();
+        }
+        if (threadIdx.x == 0) out[v] = sh[0];
+        __syncthreads();
+    }
+}
+
+// RhoSquared_addAtoms (RhoSquared.f90:188-243): for each signed entry the sum over atoms, in
+// atom order within a slice, of the charge-weighted phase (Coulomb) and of the unit phase per
+// LJ type, the LJ phase being the Coulomb one times 1/q like RhoSquared_addAtom
+// (RhoSquared.f90:173-176).  Grid: entry blocks x atom slices (blockIdx.y), so a few thousand
+// entries still fill the GPU; slice s writes its partial sums to
+// part[((1+t) * nslice + s) * S + e], and k_rho_reduce adds the slices in order.
 constexpr int kRhoBlock = 128;
 constexpr int kRhoChunk = 32;
 
 template <int NT>
-__global__ void __launch_bounds__(kRhoBlock) k_rho_full(DevSys D, double2 *rho) {
+__global__ void __launch_bounds__(kRhoBlock) k_rho_full(DevSys D, int slice_atoms, double2 *part) {
     extern __shared__ double2 stab[];  // [kRhoChunk][3][kmax+1]
     __shared__ double sq[kRhoChunk];
     __shared__ int st[kRhoChunk];
     const int KM = D.kmax + 1;
     const int e = blockIdx.x * blockDim.x + threadIdx.x;
     const bool valid = e < D.S;
+    const int abeg = blockIdx.y * slice_atoms, aend = min(D.N, abeg + slice_atoms);
     int4 kv = make_int4(0, 0, 0, 0);
     if (valid) kv = D.kvec[e];
     double cC = 0, sC = 0;
     double cL[NT > 0 ? NT : 1], sL[NT > 0 ? NT : 1];
 #pragma unroll
     for (int t = 0; t < NT; ++t) { cL[t] = 0; sL[t] = 0; }
-    for (int a0 = 0; a0 < D.N; a0 += kRhoChunk) {
-        const int na = min(kRhoChunk, D.N - a0);
+    for (int a0 = abeg; a0 < aend; a0 += kRhoChunk) {
+        const int na = min(kRhoChunk, aend - a0);
         for (int idx = threadIdx.x; idx < na * 3 * KM; idx += blockDim.x) {
             const int a = idx / (3 * KM), r = idx % (3 * KM), d = r / KM, m = r % KM;
             const double4 p = D.atom[a0 + a];
@@ -176,10 +197,24 @@ __global__ void __launch_bounds__(kRhoBlock) k_rho_full(DevSys D, double2 *rho) 
         __syncthreads();
     }
     if (valid) {
-        rho[e] = make_double2(cC, sC);
+        const size_t ns = gridDim.y, s0 = blockIdx.y;
+        part[s0 * D.S + e] = make_double2(cC, sC);
 #pragma unroll
-        for (int t = 0; t < NT; ++t) rho[(size_t)(1 + t) * D.S + e] = make_double2(cL[t], sL[t]);
+        for (int t = 0; t < NT; ++t) part[((1 + t) * ns + s0) * D.S + e] = make_double2(cL[t], sL[t]);
     }
+}
+
+// rho[(t)*S + e] = sum over slices s in order of part[(t*nslice + s)*S + e], t over 1+nt rows
+__global__ void k_rho_reduce(const double2 *part, int nslice, int S, int nrow, double2 *rho) {
+    const int idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= nrow * S) return;
+    const int t = idx / S, e = idx % S;
+    double c = 0, s = 0;
+    for (int k = 0; k < nslice; ++k) {
+        const double2 v = part[((size_t)t * nslice + k) * S + e];
+        c = c + v.x; s = s + v.y;
+    }
+    rho[idx] = make_double2(c, s);
 }
 
 // EwaldSumKSpace_calc_coulomb_energy / _calc_LJ_energy (EwaldSumKSpace.f90:389-526) per entry,
@@ -370,7 +405,11 @@ struct yamc_ctx {
     double *freq_beg = nullptr, *freq_end = nullptr, *scal = nullptr;
     long long *cnt = nullptr;
     int4 *spec = nullptr;
-    double *uu = nullptr, *fx = nullptr, *fy = nullptr, *fz = nullptr, *part = nullptr;
+    double *part = nullptr, *sums = nullptr;  // block partials of the full sums, their totals
+    int2 *tpairs = nullptr;                    // atom-tile pairs of the real-space full sum
+    int ntpairs = 0;
+    double2 *rho_part = nullptr;               // per-slice rho(k) sums of the full recompute
+    int rho_slices = 1, rho_slice_atoms = 0;
     DevSys hsys{};
     DevSys *d_sys = nullptr;
     RunSlot *d_run = nullptr;
@@ -501,7 +540,11 @@ int launch_rho_full(yamc_ctx *c) {
     const int KM = c->H.kmax + 1;
     const size_t sm = sizeof(double2) * kRhoChunk * 3 * KM;
     CUDA_TRY(cudaFuncSetAttribute(k_rho_full<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_rho_full<NT><<<(c->H.S + kRhoBlock - 1) / kRhoBlock, kRhoBlock, sm, c->stream>>>(c->hsys, c->rho);
+    const dim3 grid((c->H.S + kRhoBlock - 1) / kRhoBlock, c->rho_slices);
+    k_rho_full<NT><<<grid, kRhoBlock, sm, c->stream>>>(c->hsys, c->rho_slice_atoms, c->rho_part);
+    CUDA_TRY(cudaGetLastError());
+    const int n = (1 + NT) * c->H.S;
+    k_rho_reduce<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho_part, c->rho_slices, c->H.S, 1 + NT, c->rho);
     CUDA_TRY(cudaGetLastError());
     return YAMC_OK;
 }
@@ -543,15 +586,13 @@ int full_sums(yamc_ctx *c, int *overlap = nullptr) {
     HostSystem &H = c->H;
     int r = sync_positions(c);
     if (r) return r;
-    const int nbr = (H.N + kFullTile - 1) / kFullTile;
-    k_realspace_full<<<nbr, kFullTile, 0, c->stream>>>(c->hsys, c->uu, c->fx, c->fy, c->fz, c->part);
+    k_realspace_full<<<c->ntpairs, kFullTile, 0, c->stream>>>(c->hsys, c->tpairs, c->part);
     CUDA_TRY(cudaGetLastError());
-    std::vector<double> pr((size_t)nbr * kFullParts);
-    CUDA_TRY(cudaMemcpyAsync(pr.data(), c->part, sizeof(double) * pr.size(), cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(c->part, c->ntpairs, kFullParts, 6, c->sums);
+    CUDA_TRY(cudaGetLastError());
     double tot[kFullParts] = {};
-    for (int b = 0; b < nbr; ++b)
-        for (int v = 0; v < kFullParts; ++v) tot[v] = (v == 6) ? std::max(tot[v], pr[b * kFullParts + v]) : tot[v] + pr[b * kFullParts + v];
+    CUDA_TRY(cudaMemcpyAsync(tot, c->sums, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (overlap) *overlap = tot[6] > 0;
     else if (tot[6] > 0) { set_error("hard-core overlap in the configuration"); return YAMC_EOVERLAP_INIT; }
     switch (H.nt) {
@@ -570,11 +611,12 @@ int full_sums(yamc_ctx *c, int *overlap = nullptr) {
         default: r = launch_kspace_energy<4>(c, nbk); break;
     }
     if (r) return r;
-    std::vector<double> pk((size_t)nbk * 2);
-    CUDA_TRY(cudaMemcpyAsync(pk.data(), c->part, sizeof(double) * pk.size(), cudaMemcpyDeviceToHost, c->stream));
+    k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(c->part, nbk, 2, -1, c->sums + kFullParts);
+    CUDA_TRY(cudaGetLastError());
+    double ek[2];
+    CUDA_TRY(cudaMemcpyAsync(ek, c->sums + kFullParts, sizeof(ek), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    double ekc = 0, ekl = 0;
-    for (int b = 0; b < nbk; ++b) { ekc += pk[2 * b]; ekl += pk[2 * b + 1]; }
+    const double ekc = ek[0], ekl = ek[1];
     // EwaldSumExternal_calc_mu over all atoms, in atom order (EwaldSumExternal.f90:34-52)
     double mx = 0, my = 0, mz = 0;
     for (int i = 0; i < H.N; ++i) { mx = mx + H.q[i] * H.x[i]; my = my + H.q[i] * H.y[i]; mz = mz + H.q[i] * H.z[i]; }
@@ -844,12 +886,32 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->ebetalj, (size_t)H.npair * S)) || (r = dalloc(&c->pair_index, nt * nt)) ||
         (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
         (r = dalloc(&c->scratch, (size_t)2 * (1 + nt) * S)) || (r = dalloc(&c->freq_beg, M)) || (r = dalloc(&c->freq_end, M)) ||
-        (r = dalloc(&c->scal, SC_COUNT)) || (r = dalloc(&c->cnt, CN_COUNT)) || (r = dalloc(&c->uu, N)) ||
-        (r = dalloc(&c->fx, N)) || (r = dalloc(&c->fy, N)) || (r = dalloc(&c->fz, N)) ||
-        (r = dalloc(&c->part, (size_t)std::max((N + kFullTile - 1) / kFullTile * kFullParts, (S + 255) / 256 * 2))) ||
+        (r = dalloc(&c->scal, SC_COUNT)) || (r = dalloc(&c->cnt, CN_COUNT)) ||
         (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->api_in, 1 + 3 * kMaxA)) ||
         (r = dalloc(&c->api_out, kNV)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
+    // full-sum work split: atom-tile pairs of the real-space sum; atom slices of rho(k) so that
+    // entry blocks x slices cover the SMs about twice
+    int nsm = 148;
+    CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    {
+        const int T = (N + kFullTile - 1) / kFullTile;
+        std::vector<int2> tp;
+        tp.reserve((size_t)T * (T + 1) / 2);
+        for (int ti = 0; ti < T; ++ti)
+            for (int tj = ti; tj < T; ++tj) tp.push_back(make_int2(ti, tj));
+        c->ntpairs = (int)tp.size();
+        const int eb = (S + kRhoBlock - 1) / kRhoBlock;
+        const int chunks = (N + kRhoChunk - 1) / kRhoChunk;
+        const int want = std::max(1, std::min(chunks, (2 * nsm + eb - 1) / eb));
+        c->rho_slice_atoms = ((chunks + want - 1) / want) * kRhoChunk;
+        c->rho_slices = (N + c->rho_slice_atoms - 1) / c->rho_slice_atoms;
+        if ((r = dalloc(&c->tpairs, tp.size())) || (r = upload(c->tpairs, tp.data(), tp.size(), c->stream)) ||
+            (r = dalloc(&c->part, std::max((size_t)c->ntpairs * kFullParts, (size_t)(S + 255) / 256 * 2))) ||
+            (r = dalloc(&c->sums, kFullParts + 2)) ||
+            (r = dalloc(&c->rho_part, (size_t)(1 + nt) * c->rho_slices * S)))
+            return r;
+    }
     std::vector<double4> a(N);
     std::vector<int2> m(N);
     for (int i = 0; i < N; ++i) { a[i] = make_double4(H.x[i], H.y[i], H.z[i], H.q[i]); m[i] = make_int2(H.molnum[i], H.type_by_index[i]); }
@@ -905,8 +967,8 @@ int yamc_destroy(yamc_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
-                    c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->uu, c->fx, c->fy,
-                    c->fz, c->part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
+                    c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
+                    c->tpairs, c->rho_part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
                     c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->rho_save};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);

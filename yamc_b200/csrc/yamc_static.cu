@@ -15,8 +15,8 @@
 // arithmetic, the same tile order and the same deterministic block reduction, but it reads
 // the reference's structure-of-arrays atom data directly instead of the engine's packed
 // double4 layout, and a second one-block kernel adds the block partials in block order on
-// the device (the engine adds them on the host in the same order), so the totals agree bit
-// for bit with yamc_full_sums.
+// the device.  The engine's own full sum splits the pairs differently (blocks over pairs of
+// atom tiles), so the totals agree with yamc_full_sums to rounding, not bit for bit.
 #include <cuda_runtime.h>
 
 #include <cstdint>
