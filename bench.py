@@ -34,9 +34,10 @@ sys.path.insert(0, ROOT)
 METRIC = "MC trial moves/s (SPC/E+NaCl Ewald); mixed vs FP64 GPU at |ΔE err|≤1e-4 kT"
 
 
-# DRAM bytes per move of the chain kernel from the ncu capture of one 2,000-move launch on
-# nacl1m (dram__bytes_read.sum + dram__bytes_write.sum = 1.193 MB), used for roofline.traffic
-TRAFFIC_PER_MOVE = 597.0
+# DRAM bytes per move of the chain kernel in the timed shape (mixed, streamed, cluster of 2 x 384
+# threads) from the ncu capture of one 1,000-move launch on nacl1m (dram__bytes_read.sum +
+# dram__bytes_write.sum = 1.145 MB), used for roofline.traffic
+TRAFFIC_PER_MOVE = 1145.0
 
 
 def dist_env():

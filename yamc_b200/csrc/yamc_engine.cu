@@ -247,9 +247,11 @@ __global__ void __launch_bounds__(256) k_kspace_energy(DevSys D, const double2 *
 // ------------------------------------------------------------------------------------------
 // adjoint: forces = -dE/dr of the implemented total energy
 // ------------------------------------------------------------------------------------------
-// Real space: one thread per atom i over all j (tiles in shared memory, increasing j), every
-// pair inside the cutoff, intra-molecular pairs with the -erf_Luc energy; F_i += FR (r_i - r_j).
-__global__ void __launch_bounds__(kFullTile) k_forces_real(DevSys D, double *fx, double *fy, double *fz) {
+// Real space: one thread per atom i over the j tiles of one slice (blockIdx.y; tiles in shared
+// memory, increasing j), every pair inside the cutoff, intra-molecular pairs with the -erf_Luc
+// energy; F_i += FR (r_i - r_j).  Slices let a few thousand atoms fill the GPU: slice s writes
+// its partial forces to pf[(c * nslice + s) * N + i] (c = x, y, z), k_forces_reduce adds them.
+__global__ void __launch_bounds__(kFullTile) k_forces_real(DevSys D, int slice_tiles, double *pf) {
     __shared__ double4 tp[kFullTile];
     __shared__ int2 tm[kFullTile];
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -259,11 +261,12 @@ __global__ void __launch_bounds__(kFullTile) k_forces_real(DevSys D, double *fx,
     if (valid) { pi = D.atom[i]; mi = D.meta[i]; }
     double gx = 0, gy = 0, gz = 0;
     const int nt = D.nt;
-    for (int t0 = 0; t0 < D.N; t0 += kFullTile) {
+    const int jbeg = blockIdx.y * slice_tiles * kFullTile, jend = min(D.N, jbeg + slice_tiles * kFullTile);
+    for (int t0 = jbeg; t0 < jend; t0 += kFullTile) {
         const int j = t0 + threadIdx.x;
-        if (j < D.N) { tp[threadIdx.x] = D.atom[j]; tm[threadIdx.x] = D.meta[j]; }
+        if (j < jend) { tp[threadIdx.x] = D.atom[j]; tm[threadIdx.x] = D.meta[j]; }
         __syncthreads();
-        const int nj = min(kFullTile, D.N - t0);
+        const int nj = min(kFullTile, jend - t0);
         if (valid) {
             for (int jj = 0; jj < nj; ++jj) {
                 if (t0 + jj == i) continue;
@@ -281,7 +284,24 @@ __global__ void __launch_bounds__(kFullTile) k_forces_real(DevSys D, double *fx,
         }
         __syncthreads();
     }
-    if (valid) { fx[i] = gx; fy[i] = gy; fz[i] = gz; }
+    if (valid) {
+        const size_t ns = gridDim.y, s0 = blockIdx.y, N = D.N;
+        pf[(0 * ns + s0) * N + i] = gx; pf[(1 * ns + s0) * N + i] = gy; pf[(2 * ns + s0) * N + i] = gz;
+    }
+}
+
+// f{x,y,z}[i] = sum over slices in order of pf[(c * nslice + s) * N + i]
+__global__ void k_forces_reduce(const double *pf, int nslice, int N, double *fx, double *fy, double *fz) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= N) return;
+    double g[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        double x = 0;
+        for (int k = 0; k < nslice; ++k) x = x + pf[((size_t)c * nslice + k) * N + i];
+        g[c] = x;
+    }
+    fx[i] = g[0]; fy[i] = g[1]; fz[i] = g[2];
 }
 
 // k space (ForceKSpace_coulomb / _LJ, ForceKSpace.f90:59-302, over the signed entries): one
@@ -410,6 +430,7 @@ struct yamc_ctx {
     int ntpairs = 0;
     double2 *rho_part = nullptr;               // per-slice rho(k) sums of the full recompute
     int rho_slices = 1, rho_slice_atoms = 0;
+    int nsm = 148;                             // SMs of the device
     DevSys hsys{};
     DevSys *d_sys = nullptr;
     RunSlot *d_run = nullptr;
@@ -435,6 +456,7 @@ struct yamc_ctx {
     long long *d_prof = nullptr;
     bool prof_on = false;
     double *d_gx = nullptr, *d_gy = nullptr, *d_gz = nullptr;  // adjoint forces
+    double *d_fpart = nullptr;                                  // their per-slice real-space parts
     // NPT volume move: rho(k) as it was before the step, accepted volume steps
     double2 *rho_save = nullptr;
     double n_vol_accepted = 0;
@@ -894,6 +916,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     // entry blocks x slices cover the SMs about twice
     int nsm = 148;
     CUDA_TRY(cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device));
+    c->nsm = nsm;
     {
         const int T = (N + kFullTile - 1) / kFullTile;
         std::vector<int2> tp;
@@ -969,7 +992,7 @@ int yamc_destroy(yamc_ctx *c) {
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
                     c->tpairs, c->rho_part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
-                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->rho_save};
+                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
@@ -1859,9 +1882,17 @@ int yamc_forces(yamc_ctx *c, double *fx, double *fy, double *fz, double *mol_f, 
     HostSystem &H = c->H;
     const int N = H.N;
     int r;
-    if (!c->d_gx && ((r = dalloc(&c->d_gx, N)) || (r = dalloc(&c->d_gy, N)) || (r = dalloc(&c->d_gz, N)))) return r;
+    // real space over atom tiles x j slices (about two blocks per SM), the slices added in order
+    const int T = (N + kFullTile - 1) / kFullTile;
+    const int want = std::max(1, std::min(T, (2 * c->nsm + T - 1) / T));
+    const int slice_tiles = (T + want - 1) / want, nslice = (T + slice_tiles - 1) / slice_tiles;
+    if (!c->d_gx && ((r = dalloc(&c->d_gx, N)) || (r = dalloc(&c->d_gy, N)) || (r = dalloc(&c->d_gz, N)) ||
+                     (r = dalloc(&c->d_fpart, (size_t)3 * nslice * N))))
+        return r;
     if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
-    k_forces_real<<<(N + kFullTile - 1) / kFullTile, kFullTile, 0, c->stream>>>(c->hsys, c->d_gx, c->d_gy, c->d_gz);
+    k_forces_real<<<dim3(T, nslice), kFullTile, 0, c->stream>>>(c->hsys, slice_tiles, c->d_fpart);
+    CUDA_TRY(cudaGetLastError());
+    k_forces_reduce<<<(N + 255) / 256, 256, 0, c->stream>>>(c->d_fpart, nslice, N, c->d_gx, c->d_gy, c->d_gz);
     CUDA_TRY(cudaGetLastError());
     switch (H.nt) {
         case 1: r = launch_forces_kspace<1>(c); break;

@@ -1,10 +1,11 @@
 """Full recomputations and NPT volume steps of one workload, for profilers.
 
-    python -m yamc_b200.profile_fullsums WORKLOAD [REPEATS] [VOLUME_STEPS]
+    python -m yamc_b200.profile_fullsums WORKLOAD [REPEATS] [VOLUME_STEPS] [FORCES]
 
 builds the named workload (systems.WORKLOADS) on cuda:0, runs yamc_full_sums once as a
 warm-up and then REPEATS more times (default 3), timing each call on the host (the call
-synchronises), then VOLUME_STEPS volume steps through yamc_volume_eval/_commit (default 0).
+synchronises), then VOLUME_STEPS volume steps through yamc_volume_eval/_commit (default 0)
+and FORCES calls of the adjoint yamc_forces (default 0).
 Capture the kernels of the second call with
 ``ncu -k regex:"k_realspace_full|k_rho_full|k_rho_reduce|k_kspace_energy" -s 4 -c 4``.
 """
@@ -20,6 +21,7 @@ def main(argv):
     name = argv[0]
     reps = int(argv[1]) if len(argv) > 1 else 3
     nvol = int(argv[2]) if len(argv) > 2 else 0
+    nfor = int(argv[3]) if len(argv) > 3 else 0
     with tempfile.TemporaryDirectory() as d:
         files = systems.write_system(systems.WORKLOADS[name], d, seed=3)
         eng = api.Engine.from_files(files)
@@ -39,6 +41,13 @@ def main(argv):
         tv.append(time.perf_counter() - t0)
     if tv:
         print(f"volume step (eval + rejecting commit): {1e3 * min(tv):.3f} ms (best of {nvol})")
+    tf = []
+    for _ in range(nfor):
+        t0 = time.perf_counter()
+        eng.forces()
+        tf.append(time.perf_counter() - t0)
+    if tf:
+        print(f"adjoint forces (yamc_forces, with the host's molecular sums): {1e3 * min(tf):.3f} ms (best of {nfor})")
 
 
 if __name__ == "__main__":
