@@ -436,17 +436,36 @@ def main():
     n_chk = 4000
     chk = grng.gfortran_stream(4242 + rank, 40 * n_chk + 10000)
     logs = {}
+    e_tot = {}
     for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
         eng = api.Engine.from_files(files, device=local, precision=prec)
         logs[prec] = eng.run_chain(chk, n_chk)[0]
+        if prec == _lib.YAMC_MIXED:
+            # the mixed chain's running total energy against an FP64 recomputation of its own configuration
+            e_tot = {"incremental": float(eng.energies()[0]), "fp64_full": float(eng.full_sums()[0])}
         eng.close()
     lf, lm = logs[_lib.YAMC_FP64], logs[_lib.YAMC_MIXED]
     same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
     k_same = n_chk if same.all() else int(np.argmin(same))
     cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
     de = np.abs(sum(lm[c][:k_same] for c in cols) - sum(lf[c][:k_same] for c in cols))
+    # molecular forces of the force-bias path (movemc Steps 3-4) in both forms, same configuration
+    ef = api.Engine.from_files(files, device=local, precision=_lib.YAMC_FP64)
+    em = api.Engine.from_files(files, device=local, precision=_lib.YAMC_MIXED)
+    ferr, fscale, nf = 0.0, 0.0, 0
+    for imol in range(1, ef.nmol + 1, max(1, ef.nmol // 200)):
+        f1, t1 = ef.move_old(imol)
+        f2, t2 = em.move_old(imol)
+        fscale = max(fscale, float(np.abs(f1).max()))
+        ferr = max(ferr, float(np.abs(f2 - f1).max()))
+        nf += 1
+    ef.close()
+    em.close()
     de_err = {"max_kT": float(de.max()) if k_same else None, "rms_kT": float(np.sqrt((de ** 2).mean())) if k_same else None,
-              "moves_compared": k_same, "bar_kT": 1e-4}
+              "moves_compared": k_same, "bar_kT": 1e-4,
+              "force_max_abs_err": ferr, "force_scale": fscale, "molecules_compared": nf,
+              "total_energy_err_kT": abs(e_tot["incremental"] - e_tot["fp64_full"]),
+              "total_energy_kT": e_tot["fp64_full"]}
 
     # ---------------- the batch: R independent chains of the workload, one graph launch per step
     # R = the most chains any launch shape keeps resident at once (the tuner then picks the shape)

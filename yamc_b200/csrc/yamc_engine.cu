@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(kSumThreads) k_sum_parts(const double *part, i
 // (RhoSquared.f90:173-176).  Grid: entry blocks x atom slices (blockIdx.y), so a few thousand
 // entries still fill the GPU; slice s writes its partial sums to
 // part[((1+t) * nslice + s) * S + e], and k_rho_reduce adds the slices in order.
-constexpr int kRhoBlock = 128;
+constexpr int kRhoBlock = 512;  // entries per block: the block's atom tables serve 512 entries
 constexpr int kRhoChunk = 32;
 
 template <int NT>
@@ -189,8 +189,11 @@ __global__ void __launch_bounds__(kRhoBlock) k_rho_full(DevSys D, int slice_atom
                     if (q != 0.0) { const double iq = 1.0 / q; cl = c * iq; sl = s * iq; }
                     else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, 1.0, cl, sl);
 #pragma unroll
-                    for (int tt = 0; tt < NT; ++tt)
-                        if (tt == t - 1) { cL[tt] = cL[tt] + cl; sL[tt] = sL[tt] + sl; }
+                    for (int tt = 0; tt < NT; ++tt) {  // selects, not an indexed store: the sums stay in registers
+                        const bool hit = tt == t - 1;
+                        cL[tt] = hit ? cL[tt] + cl : cL[tt];
+                        sL[tt] = hit ? sL[tt] + sl : sL[tt];
+                    }
                 }
             }
         }
@@ -305,22 +308,34 @@ __global__ void k_forces_reduce(const double *pf, int nslice, int N, double *fx,
 }
 
 // k space (ForceKSpace_coulomb / _LJ, ForceKSpace.f90:59-302, over the signed entries): one
-// warp per atom, the lanes over the entries; sin/cos(k r) come from the atom's per-axis tables,
+// warp per kForceAPW atoms, the lanes over the entries, so each entry's k, rho and beta rows are
+// loaded once for kForceAPW atoms; sin/cos(k r) come from the atoms' per-axis tables,
 // recomputed here instead of stored per atom and k.  Adds to fx/fy/fz.
-constexpr int kForceAtoms = 8;  // atoms (warps) per block
+constexpr int kForceWarps = 8;  // warps per block
+constexpr int kForceAPW = 4;    // atoms per warp
 
 template <int NT>
-__global__ void __launch_bounds__(32 * kForceAtoms) k_forces_kspace(DevSys D, double *fx, double *fy, double *fz) {
-    extern __shared__ double2 ftab[];  // [kForceAtoms][3][KM]
+__global__ void __launch_bounds__(32 * kForceWarps, 2) k_forces_kspace(DevSys D, double *fx, double *fy, double *fz) {
+    extern __shared__ double2 ftab[];  // [kForceWarps][kForceAPW][3][KM]
     const int KM = D.kmax + 1;
     const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int i = blockIdx.x * kForceAtoms + w;
-    if (i >= D.N) return;
-    const double4 p = D.atom[i];
-    const int ta = D.meta[i].y;
-    double2 *T = ftab + (size_t)w * 3 * KM;
-    for (int idx = lane; idx < 3 * KM; idx += 32) {
-        const int d = idx / KM, m = idx % KM;
+    const int i0 = (blockIdx.x * kForceWarps + w) * kForceAPW;
+    if (i0 >= D.N) return;
+    const int na = min(kForceAPW, D.N - i0);
+    double2 *T = ftab + (size_t)w * kForceAPW * 3 * KM;
+    double q[kForceAPW], iq[kForceAPW];
+    int ta[kForceAPW];
+#pragma unroll
+    for (int a = 0; a < kForceAPW; ++a) {
+        q[a] = 0; iq[a] = 0; ta[a] = 0;
+        if (a < na) {
+            const double4 p = D.atom[i0 + a];
+            q[a] = p.w; iq[a] = p.w != 0.0 ? 1.0 / p.w : 0.0; ta[a] = D.meta[i0 + a].y;
+        }
+    }
+    for (int idx = lane; idx < na * 3 * KM; idx += 32) {
+        const int a = idx / (3 * KM), r = idx % (3 * KM), d = r / KM, m = r % KM;
+        const double4 p = D.atom[i0 + a];
         const double u = d == 0 ? p.x : (d == 1 ? p.y : p.z);
         double sn, cs;
         sincospi(2.0 * (double)m * u, &sn, &cs);
@@ -328,42 +343,56 @@ __global__ void __launch_bounds__(32 * kForceAtoms) k_forces_kspace(DevSys D, do
         T[idx] = make_double2(cs, sn);
     }
     __syncwarp();
-    const double q = p.w, iq = q != 0.0 ? 1.0 / q : 0.0;
     const int S = D.S;
-    double gx = 0, gy = 0, gz = 0;
+    double gx[kForceAPW], gy[kForceAPW], gz[kForceAPW];
+#pragma unroll
+    for (int a = 0; a < kForceAPW; ++a) { gx[a] = 0; gy[a] = 0; gz[a] = 0; }
     for (int e = lane; e < S; e += 32) {
         const int4 kv = D.kvec[e];
-        double c = 0, sn = 0;
-        double wgt = 0;
-        if (q != 0.0) {
-            entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, q, c, sn);
-            const double2 C = D.rho[e];
-            wgt = D.ebeta[e] * (C.x * sn - C.y * c);
-        }
-        if (ta > 0) {
-            double cl, sl;
-            if (q != 0.0) { cl = c * iq; sl = sn * iq; }
-            else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, 1.0, cl, sl);
+        const double2 C = D.rho[e];
+        const double be = D.ebeta[e];
+        double2 Ct[NT > 0 ? NT : 1];
 #pragma unroll
-            for (int t = 0; t < NT; ++t) {
-                int pr = 0;
+        for (int t = 0; t < NT; ++t) Ct[t] = D.rho[(size_t)(1 + t) * S + e];
+        double bl[NT * (NT + 1) / 2 > 0 ? NT * (NT + 1) / 2 : 1];
 #pragma unroll
-                for (int u = 0; u < NT; ++u)
-                    if (u == ta - 1) pr = pair_idx<NT>(u, t);
-                const double2 Ct = D.rho[(size_t)(1 + t) * S + e];
-                wgt += D.ebetalj[(size_t)pr * S + e] * (Ct.x * sl - Ct.y * cl);
+        for (int pr = 0; pr < NT * (NT + 1) / 2; ++pr) bl[pr] = D.ebetalj[(size_t)pr * S + e];
+#pragma unroll
+        for (int a = 0; a < kForceAPW; ++a) {
+            if (a >= na) break;
+            const double2 *Ta = T + (size_t)a * 3 * KM;
+            double c = 0, sn = 0, wgt = 0;
+            if (q[a] != 0.0) {
+                entry_phase<double, double2>(Ta, Ta + KM, Ta + 2 * KM, kv.x, kv.y, kv.z, q[a], c, sn);
+                wgt = be * (C.x * sn - C.y * c);
             }
+            if (ta[a] > 0) {
+                double cl, sl;
+                if (q[a] != 0.0) { cl = c * iq[a]; sl = sn * iq[a]; }
+                else entry_phase<double, double2>(Ta, Ta + KM, Ta + 2 * KM, kv.x, kv.y, kv.z, 1.0, cl, sl);
+#pragma unroll
+                for (int t = 0; t < NT; ++t) {
+                    const int row = pair_idx<NT>(ta[a] - 1, t);
+                    double b = bl[0];  // selects, not an indexed load: bl stays in registers
+#pragma unroll
+                    for (int pr = 1; pr < NT * (NT + 1) / 2; ++pr) b = row == pr ? bl[pr] : b;
+                    wgt += b * (Ct[t].x * sl - Ct[t].y * cl);
+                }
+            }
+            const double f = kFourPi * wgt;
+            gx[a] = gx[a] + f * kv.x; gy[a] = gy[a] + f * kv.y; gz[a] = gz[a] + f * kv.z;
         }
-        const double f = kFourPi * wgt;
-        gx = gx + f * kv.x; gy = gy + f * kv.y; gz = gz + f * kv.z;
     }
 #pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-        gx += __shfl_xor_sync(0xffffffffu, gx, o);
-        gy += __shfl_xor_sync(0xffffffffu, gy, o);
-        gz += __shfl_xor_sync(0xffffffffu, gz, o);
+    for (int a = 0; a < kForceAPW; ++a) {
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) {
+            gx[a] += __shfl_xor_sync(0xffffffffu, gx[a], o);
+            gy[a] += __shfl_xor_sync(0xffffffffu, gy[a], o);
+            gz[a] += __shfl_xor_sync(0xffffffffu, gz[a], o);
+        }
+        if (lane == 0 && a < na) { fx[i0 + a] += gx[a]; fy[i0 + a] += gy[a]; fz[i0 + a] += gz[a]; }
     }
-    if (lane == 0) { fx[i] += gx; fy[i] += gy; fz[i] += gz; }
 }
 
 // per-move API commit: rho += delta (Step 14, MC.f90:1245)
@@ -667,9 +696,10 @@ int ensure_cfg(yamc_ctx *c) {
 
 template <int NT>
 int launch_forces_kspace(yamc_ctx *c) {
-    const size_t sm = sizeof(double2) * kForceAtoms * 3 * (c->H.kmax + 1);
+    const size_t sm = sizeof(double2) * kForceWarps * kForceAPW * 3 * (c->H.kmax + 1);
+    const int per_block = kForceWarps * kForceAPW;
     CUDA_TRY(cudaFuncSetAttribute(k_forces_kspace<NT>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
-    k_forces_kspace<NT><<<(c->H.N + kForceAtoms - 1) / kForceAtoms, 32 * kForceAtoms, sm, c->stream>>>(c->hsys, c->d_gx,
+    k_forces_kspace<NT><<<(c->H.N + per_block - 1) / per_block, 32 * kForceWarps, sm, c->stream>>>(c->hsys, c->d_gx,
                                                                                                       c->d_gy, c->d_gz);
     CUDA_TRY(cudaGetLastError());
     return YAMC_OK;
