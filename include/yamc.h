@@ -220,6 +220,24 @@ int yamc_volume_commit(yamc_ctx *ctx, int32_t accepted);
    change with accepted volume steps). */
 int yamc_get_params(yamc_ctx *ctx, yamc_params *p);
 
+/* ---- exchange moves (mc_xchange, MC.f90:1325-1954) ----
+   init_freq with the exchange column of a frequencies file (runmc.f90:25-173): weights[nmol]
+   give xchange_freq (BiasedRandom_init) and the probability Sxch / (Smv + Sxch) that a move
+   step of run_mc is an exchange step (Smv: the move weights' sum).  With a positive
+   probability yamc_run_mc reads each move's exchange draw on the host and runs exchange steps
+   there (two molecules from xchange_freq, different, swap their centres of mass; acceptance by
+   MonteCarloMove_accept_or_decline_simple) and movemc steps as one-move chain launches; their
+   records have flags bit2 set, imol = the first molecule and the second in flags bits 8..31.
+   yamc_run_chain refuses a context with exchange steps on. */
+int yamc_set_xchange_weights(yamc_ctx *ctx, const double *weights);
+/* The exchange step as a drop-in for the body of mc_xchange, for a host that draws its own
+   random numbers: yamc_xchange_eval(imol1 != imol2, 1-based) returns du = {dU_real, dU_k_coulomb,
+   dU_k_LJ, dU_ext} as the reference forms them (its real-space part holds the 1-2 pair energy
+   change twice, MC.f90:1451-1452, 1639-1642) and *overlap (then du = 0 and the step is
+   rejected without a draw); yamc_xchange_commit keeps the swap (accepted != 0) or drops it. */
+int yamc_xchange_eval(yamc_ctx *ctx, int32_t imol1, int32_t imol2, double du[4], int32_t *overlap);
+int yamc_xchange_commit(yamc_ctx *ctx, int32_t accepted);
+
 /* Mixed form (params.precision = YAMC_MIXED): the chain kernel recomputes rho(k)
    and the k-space energies in FP64 from the positions after every
    `accepted_moves` accepted moves (default 10000; 0 = never), bounding the drift

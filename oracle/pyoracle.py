@@ -109,6 +109,11 @@ def lib(fast: bool = False):
         L.orc_run_cycles.restype = ctypes.c_int32
         L.orc_mcvol.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, P(ctypes.c_int64), ctypes.c_void_p]
         L.orc_mcvol.restype = ctypes.c_int32
+        L.orc_set_xchange_weights.argtypes = [ctypes.c_void_p, dp, ctypes.c_int32]
+        L.orc_set_xchange_weights.restype = ctypes.c_int32
+        L.orc_xchange.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
+                                  P(ctypes.c_int64), P(MoveRec)]
+        L.orc_xchange.restype = ctypes.c_int32
         L.orc_box_length.argtypes = [ctypes.c_void_p]
         L.orc_box_length.restype = ctypes.c_double
         L.orc_move_old.argtypes = [ctypes.c_void_p, ctypes.c_int32, dp, dp]
@@ -197,6 +202,22 @@ class Oracle:
         w = np.ascontiguousarray(w, dtype=np.float64)
         if self.L.orc_set_move_weights(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), w.size) != 0:
             raise ValueError("one weight per molecule")
+
+    def set_xchange_weights(self, w) -> None:
+        """init_freq's exchange weights: xchange_freq and xchange_probability = Sxch/(Smv+Sxch)."""
+        w = np.ascontiguousarray(w, dtype=np.float64)
+        if self.L.orc_set_xchange_weights(self.h, w.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), w.size) != 0:
+            raise ValueError("one weight per molecule")
+
+    def xchange(self, imol1: int, imol2: int, rng: np.ndarray, cursor: int = 0):
+        """One mc_xchange with its acceptance draw from rng: (record, cursor)."""
+        rng = np.ascontiguousarray(rng, dtype=np.float32)
+        rec = MoveRec()
+        cur = ctypes.c_int64(cursor)
+        r = self.L.orc_xchange(self.h, imol1, imol2, rng.ctypes.data, rng.size, ctypes.byref(cur), ctypes.byref(rec))
+        if r != 0:
+            raise RuntimeError(f"orc_xchange returned {r}")
+        return rec, cur.value
 
     def mols(self):
         f = np.zeros(self.nmol, dtype=np.int32)

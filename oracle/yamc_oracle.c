@@ -542,6 +542,8 @@ struct orc_state {
     double U_tail, U_tail_coul, U_tail_lj6, U_tail_lj12, U_ext, U_total, U_total_ew, U_total_lj;
     /* run_mc state */
     double *freq_beg, *freq_end;
+    double *xfreq_beg, *xfreq_end;     /* xchange_freq intervals (BiasedRandom_init on exchange weights) */
+    double smv, xchange_probability;   /* SUM(mv_num) and Sxch / (Smv + Sxch) (init_freq, runmc.f90:25-67) */
     int64_t icycle, move_in_cycle;
     double n_mv_steps, n_mv_accepted, n_vol_steps, n_vol_accepted;
     /* RNG binding for the current call */
@@ -826,8 +828,17 @@ static void rsl_lj(rsl_t *L, double sigma6, double four_eps) {
    full != 0: full sum (i over all atoms, j0 = i+1, uu_back == uu).
    otherwise: partial sum of molecule atoms [first,last] placed at (xn,yn,zn).
    Returns the overlap flag (early return like the reference). */
+/* EwaldSumRealSpace_calc (EwaldSumRealSpace.f90:233-500); the partial form runs j over
+   [jlo, jhi) only (the optional first/last of the reference's call, used by mc_xchange for the
+   1-2 cross sum) */
+static int realspace_calc_j(orc_state *s, int full, partial_t *ps, const double *xn, const double *yn,
+                            const double *zn, int first, int last, int jlo, int jhi);
 static int realspace_calc(orc_state *s, int full, partial_t *ps, const double *xn, const double *yn,
                           const double *zn, int first, int last) {
+    return realspace_calc_j(s, full, ps, xn, yn, zn, first, last, 0, s->N);
+}
+static int realspace_calc_j(orc_state *s, int full, partial_t *ps, const double *xn, const double *yn,
+                            const double *zn, int first, int last, int jlo, int jhi) {
     const orc_params *p = &s->p;
     int ntot = s->N, nt = s->lj.ntype;
     int natom = full ? ntot : (last - first + 1);
@@ -851,14 +862,14 @@ static int realspace_calc(orc_state *s, int full, partial_t *ps, const double *x
     }
     *e_ew = *e_lj6 = *e_lj12 = *e_ewi = *e_lj6i = *e_lj12i = 0;
     for (int i = 0; i < natom; i++) {
-        int j0 = full ? i + 1 : 0;
+        int j0 = full ? i + 1 : jlo;
         int ii = full ? i : i + first;
         int imol = s->molnum[ii], ityp = s->lj.type_by_index[ii];
         double qi = s->charge[ii];
         double dhs_i = s->hard_core[ii] / p->BoxLength;
         int base = ityp > 0 ? (ityp - 1) * nt : -1000;
         double xi = full ? s->xx[i] : xn[i], yi = full ? s->yy[i] : yn[i], zi = full ? s->zz[i] : zn[i];
-        for (int j = j0; j < ntot; j++) {
+        for (int j = j0; j < (full ? ntot : jhi); j++) {
             int jmol = s->molnum[j], jtyp = s->lj.type_by_index[j];
             if (!full && imol == jmol) continue;
             double qj = s->charge[j];
@@ -1419,6 +1430,159 @@ static int biased_choose(orc_state *s) {
     return interval;
 }
 
+/* BiasedRandom_choose on xchange_freq */
+static int biased_choose_x(orc_state *s) {
+    double rnd = orc_rand(s);
+    int interval = 1;
+    for (int i = 0; i < s->nmol; i++)
+        if (rnd > s->xfreq_beg[i] && rnd < s->xfreq_end[i]) { interval = i + 1; break; }
+    return interval;
+}
+
+static void partial_alloc(partial_t *p, int N) {
+    memset(p, 0, sizeof *p);
+    p->uu_back = calloc(N, sizeof(double)); p->fx_back = calloc(N, sizeof(double));
+    p->fy_back = calloc(N, sizeof(double)); p->fz_back = calloc(N, sizeof(double));
+}
+static void partial_free(partial_t *p) { free(p->uu_back); free(p->fx_back); free(p->fy_back); free(p->fz_back); }
+
+/* mc_xchange (MC.f90:1325-1954): molecules imol1 and imol2 (1-based) swap their centres of mass,
+   each keeping its orientation.  The real-space change is, as in the reference, the sum of the
+   two molecules' per-atom energies after minus before (MC.f90:1451-1452, 1639-1642), so the 1-2
+   pair energy enters the acceptance twice (the bookkeeping on acceptance takes it once,
+   :1813-1826).  No acceptance draw after a hard-core overlap; otherwise
+   MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597). */
+static int mc_xchange(orc_state *s, int imol1, int imol2, orc_move_rec *rec) {
+    const orc_params *p = &s->p;
+    int nk = s->g.nk, nt = s->lj.ntype, N = s->N;
+    int m1 = imol1 - 1, m2 = imol2 - 1;
+    int f1 = s->first_atom[m1], l1 = s->last_atom[m1], n1 = l1 - f1 + 1;
+    int f2 = s->first_atom[m2], l2 = s->last_atom[m2], n2 = l2 - f2 + 1;
+    const double *mass1 = s->moltypes[s->mol_type[m1]].mass, *mass2 = s->moltypes[s->mol_type[m2]].mass;
+    memset(rec, 0, sizeof *rec);
+    rec->imol = imol1;
+    /* FOR TEST ONLY (MC.f90:1420): mu from all atoms */
+    calc_mu(s->xx, s->yy, s->zz, s->charge, N, &s->mu_x, &s->mu_y, &s->mu_z);
+    /* Step 2 (:1451-1452) */
+    double S1 = 0, S2 = 0;
+    for (int i = f1; i <= l1; i++) S1 = S1 + s->uu[i];
+    for (int i = f2; i <= l2; i++) S2 = S2 + s->uu[i];
+    double E_old = S1 + S2;
+    /* Step 3 (:1467-1490): old structure factors of both molecules */
+    rho_zero(&s->mol_old, nk, nt);
+    for (int i = f1; i <= l1; i++)
+        rho_add_atom(s, &s->mol_old, s->xx[i], s->yy[i], s->zz[i], s->charge[i], s->lj.type_by_index[i], &s->skr_coul[0], &s->skr_lj[0]);
+    for (int i = f2; i <= l2; i++)
+        rho_add_atom(s, &s->mol_old, s->xx[i], s->yy[i], s->zz[i], s->charge[i], s->lj.type_by_index[i], &s->skr_coul[0], &s->skr_lj[0]);
+    double mo1[3], mo2[3], c1[3], c2[3];
+    calc_mu(s->xx + f1, s->yy + f1, s->zz + f1, s->charge + f1, n1, &mo1[0], &mo1[1], &mo1[2]);
+    calc_mu(s->xx + f2, s->yy + f2, s->zz + f2, s->charge + f2, n2, &mo2[0], &mo2[1], &mo2[2]);
+    center_of_mass(s->xx + f1, s->yy + f1, s->zz + f1, mass1, n1, &c1[0], &c1[1], &c1[2]);
+    center_of_mass(s->xx + f2, s->yy + f2, s->zz + f2, mass2, n2, &c2[0], &c2[1], &c2[2]);
+    /* the swapped positions (:1516-1524), not wrapped into the box */
+    double xn1[MAX_MOL_ATOMS], yn1[MAX_MOL_ATOMS], zn1[MAX_MOL_ATOMS];
+    double xn2[MAX_MOL_ATOMS], yn2[MAX_MOL_ATOMS], zn2[MAX_MOL_ATOMS];
+    double xo1[MAX_MOL_ATOMS], yo1[MAX_MOL_ATOMS], zo1[MAX_MOL_ATOMS];
+    double xo2[MAX_MOL_ATOMS], yo2[MAX_MOL_ATOMS], zo2[MAX_MOL_ATOMS];
+    for (int i = 0; i < n1; i++) {
+        xo1[i] = s->xx[f1 + i]; yo1[i] = s->yy[f1 + i]; zo1[i] = s->zz[f1 + i];
+        xn1[i] = xo1[i] - c1[0] + c2[0]; yn1[i] = yo1[i] - c1[1] + c2[1]; zn1[i] = zo1[i] - c1[2] + c2[2];
+    }
+    for (int i = 0; i < n2; i++) {
+        xo2[i] = s->xx[f2 + i]; yo2[i] = s->yy[f2 + i]; zo2[i] = s->zz[f2 + i];
+        xn2[i] = xo2[i] - c2[0] + c1[0]; yn2[i] = yo2[i] - c2[1] + c1[1]; zn2[i] = zo2[i] - c2[2] + c1[2];
+    }
+    /* real space with both molecules at their new positions (:1534-1570) */
+    partial_t pn1, pn2, pn12;
+    partial_alloc(&pn1, N); partial_alloc(&pn2, N); partial_alloc(&pn12, N);
+    for (int i = 0; i < n1; i++) { s->xx[f1 + i] = xn1[i]; s->yy[f1 + i] = yn1[i]; s->zz[f1 + i] = zn1[i]; }
+    for (int i = 0; i < n2; i++) { s->xx[f2 + i] = xn2[i]; s->yy[f2 + i] = yn2[i]; s->zz[f2 + i] = zn2[i]; }
+    int ov1 = realspace_calc_j(s, 0, &pn1, xn1, yn1, zn1, f1, l1, 0, N);
+    int ov2 = realspace_calc_j(s, 0, &pn2, xn2, yn2, zn2, f2, l2, 0, N);
+    (void)realspace_calc_j(s, 0, &pn12, xn1, yn1, zn1, f1, l1, f2, l2 + 1);
+    for (int i = 0; i < n1; i++) { s->xx[f1 + i] = xo1[i]; s->yy[f1 + i] = yo1[i]; s->zz[f1 + i] = zo1[i]; }
+    for (int i = 0; i < n2; i++) { s->xx[f2 + i] = xo2[i]; s->yy[f2 + i] = yo2[i]; s->zz[f2 + i] = zo2[i]; }
+    rec->flags = 4 | (imol2 << 8);
+    if (ov1 || ov2) {
+        rec->flags |= 2;
+        partial_free(&pn1); partial_free(&pn2); partial_free(&pn12);
+        return 0;
+    }
+    double T1 = 0, T2 = 0;
+    for (int i = 0; i < n1; i++) T1 = T1 + pn1.uu[i];
+    for (int i = 0; i < n2; i++) T2 = T2 + pn2.uu[i];
+    double E_new = T1 + T2;
+    double dU_real = E_new - E_old;
+    /* new structure factors and the k-space change (:1652-1700) */
+    rho_zero(&s->mol_new, nk, nt);
+    for (int i = 0; i < n1; i++)
+        rho_add_atom(s, &s->mol_new, xn1[i], yn1[i], zn1[i], s->charge[f1 + i], s->lj.type_by_index[f1 + i], &s->skr_coul[0], &s->skr_lj[0]);
+    for (int i = 0; i < n2; i++)
+        rho_add_atom(s, &s->mol_new, xn2[i], yn2[i], zn2[i], s->charge[f2 + i], s->lj.type_by_index[f2 + i], &s->skr_coul[0], &s->skr_lj[0]);
+    rho_sub(&s->mol_new, &s->mol_old, nk, nt);
+    double du_kc = kspace_du_coulomb(s, &s->mol_new.coul);
+    double du_kl = kspace_du_lj(s, &s->mol_new);
+    /* external field (:1706-1738) */
+    double mn1[3], mn2[3];
+    calc_mu(xn1, yn1, zn1, s->charge + f1, n1, &mn1[0], &mn1[1], &mn1[2]);
+    calc_mu(xn2, yn2, zn2, s->charge + f2, n2, &mn2[0], &mn2[1], &mn2[2]);
+    double dmx = (mn1[0] - mo1[0]) + (mn2[0] - mo2[0]);
+    double dmy = (mn1[1] - mo1[1]) + (mn2[1] - mo2[1]);
+    double dmz = (mn1[2] - mo1[2]) + (mn2[2] - mo2[2]);
+    double dU_ext = p->kext * ((2 * s->mu_x + dmx) * dmx + (2 * s->mu_y + dmy) * dmy + (2 * s->mu_z + dmz) * dmz);
+    double du_total = dU_real + (du_kc + du_kl) + dU_ext;
+    rec->du_real = dU_real; rec->du_k_coul = du_kc; rec->du_k_lj = du_kl; rec->du_ext = dU_ext;
+    /* MonteCarloMove_accept_or_decline_simple */
+    double factor = exp(-du_total);
+    double xksi = orc_rand(s);
+    if (s->rng_out) { partial_free(&pn1); partial_free(&pn2); partial_free(&pn12); return -6; }
+    int acc = !(xksi > factor);
+    if (acc) {
+        /* :1758-1848 */
+        rho_add(&s->rho_total, &s->mol_new, nk, nt);
+        partial_t po1, po2, po12;
+        partial_alloc(&po1, N); partial_alloc(&po2, N); partial_alloc(&po12, N);
+        realspace_calc_j(s, 0, &po1, xo1, yo1, zo1, f1, l1, 0, N);
+        realspace_calc_j(s, 0, &po2, xo2, yo2, zo2, f2, l2, 0, N);
+        realspace_calc_j(s, 0, &po12, xo1, yo1, zo1, f1, l1, f2, l2 + 1);
+        for (int i = 0; i < N; i++) {
+            s->uu[i] = s->uu[i] + pn1.uu_back[i] - po1.uu_back[i] + pn2.uu_back[i] - po2.uu_back[i];
+            s->fx[i] = s->fx[i] + pn1.fx_back[i] - po1.fx_back[i] + pn2.fx_back[i] - po2.fx_back[i];
+            s->fy[i] = s->fy[i] + pn1.fy_back[i] - po1.fy_back[i] + pn2.fy_back[i] - po2.fy_back[i];
+            s->fz[i] = s->fz[i] + pn1.fz_back[i] - po1.fz_back[i] + pn2.fz_back[i] - po2.fz_back[i];
+        }
+        for (int i = 0; i < n1; i++) {
+            s->uu[f1 + i] = pn1.uu[i]; s->fx[f1 + i] = pn1.fx[i]; s->fy[f1 + i] = pn1.fy[i]; s->fz[f1 + i] = pn1.fz[i];
+        }
+        for (int i = 0; i < n2; i++) {
+            s->uu[f2 + i] = pn2.uu[i]; s->fx[f2 + i] = pn2.fx[i]; s->fy[f2 + i] = pn2.fy[i]; s->fz[f2 + i] = pn2.fz[i];
+        }
+        s->E_k_coul = s->E_k_coul + du_kc;
+        s->E_k_lj = s->E_k_lj + du_kl;
+        s->E_k = s->E_k_coul + s->E_k_lj;
+        s->uu_ew = s->uu_ew + pn1.uu_ew - po1.uu_ew + pn2.uu_ew - po2.uu_ew - (pn12.uu_ew - po12.uu_ew);
+        s->uu_lj6 = s->uu_lj6 + pn1.uu_lj6 - po1.uu_lj6 + pn2.uu_lj6 - po2.uu_lj6 - (pn12.uu_lj6 - po12.uu_lj6);
+        s->uu_lj12 = s->uu_lj12 + pn1.uu_lj12 - po1.uu_lj12 + pn2.uu_lj12 - po2.uu_lj12 - (pn12.uu_lj12 - po12.uu_lj12);
+        s->mu_x = s->mu_x + dmx; s->mu_y = s->mu_y + dmy; s->mu_z = s->mu_z + dmz;
+        total_energy(s);
+        for (int i = 0; i < n1; i++) { s->xx[f1 + i] = xn1[i]; s->yy[f1 + i] = yn1[i]; s->zz[f1 + i] = zn1[i]; }
+        for (int i = 0; i < n2; i++) { s->xx[f2 + i] = xn2[i]; s->yy[f2 + i] = yn2[i]; s->zz[f2 + i] = zn2[i]; }
+        partial_free(&po1); partial_free(&po2); partial_free(&po12);
+        rec->flags |= 1;
+    }
+    partial_free(&pn1); partial_free(&pn2); partial_free(&pn12);
+    return 0;
+}
+
+int32_t orc_xchange(orc_state *s, int32_t imol1, int32_t imol2, const float *rng, int64_t n_rng, int64_t *cursor,
+                    orc_move_rec *rec) {
+    s->rng = rng; s->n_rng = n_rng; s->cursor = cursor; s->rng_out = 0;
+    if (imol1 < 1 || imol1 > s->nmol || imol2 < 1 || imol2 > s->nmol || imol1 == imol2) return -4;
+    int r = mc_xchange(s, imol1, imol2, rec);
+    rec->cursor = *cursor;
+    return r;
+}
+
 int32_t orc_movemc(orc_state *s, int32_t imol, const float *rng, int64_t n_rng, int64_t *cursor, orc_move_rec *rec) {
     s->rng = rng; s->n_rng = n_rng; s->cursor = cursor; s->rng_out = 0;
     if (imol < 1 || imol > s->nmol) return -4;
@@ -1444,6 +1608,8 @@ static void cycle_end(orc_state *s, double *rows, int32_t max_rows, int32_t *n_r
 
 static int32_t run_moves(orc_state *s, int64_t n_moves, orc_move_rec *log, double *rows, int32_t max_rows,
                          int32_t *n_rows);
+static int biased_choose_x(orc_state *s);
+static int mc_xchange(orc_state *s, int imol1, int imol2, orc_move_rec *rec);
 
 /* run_mc (runmc.f90:178-334), NVT single-molecule moves only */
 int32_t orc_run_mc(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_moves,
@@ -1466,11 +1632,19 @@ static int32_t run_moves(orc_state *s, int64_t n_moves, orc_move_rec *log, doubl
             (void)rnd;
         }
         double rnd = orc_rand(s);
-        (void)rnd; /* compared with xchange_probability = 0: never an exchange */
-        int imol = biased_choose(s);
-        if (s->rng_out) { *s->cursor = c_move; return -6; }
         orc_move_rec rec;
-        int r = movemc(s, imol, &rec);
+        int r;
+        if (rnd < s->xchange_probability) {
+            /* exchange step (runmc.f90:238-259): two different molecules from xchange_freq */
+            int imol1 = biased_choose_x(s), imol2 = imol1;
+            while (imol2 == imol1 && !s->rng_out) imol2 = biased_choose_x(s);
+            if (s->rng_out) { *s->cursor = c_move; return -6; }
+            r = mc_xchange(s, imol1, imol2, &rec);
+        } else {
+            int imol = biased_choose(s);
+            if (s->rng_out) { *s->cursor = c_move; return -6; }
+            r = movemc(s, imol, &rec);
+        }
         if (r == -6) *s->cursor = c_move;
         if (r) return r;
         rec.cursor = *s->cursor;
@@ -1869,6 +2043,9 @@ orc_state *orc_create(const orc_params *pin, const char *composition_path, const
     double prob = 1.0 / S;
     s->freq_beg[0] = 0.0; s->freq_end[0] = prob;
     for (int i = 1; i < total_mol; i++) { s->freq_beg[i] = s->freq_end[i - 1]; s->freq_end[i] = s->freq_beg[i] + prob; }
+    s->smv = S;
+    s->xfreq_beg = calloc(total_mol, sizeof(double)); s->xfreq_end = calloc(total_mol, sizeof(double));
+    s->xchange_probability = 0.0;
     s->icycle = 1;
     /* initmc -> mc_calc_total_sums (MC.f90:587-602) */
     if (orc_full_sums(s, NULL)) *status = 1; /* overlap in the initial configuration */
@@ -1878,17 +2055,31 @@ orc_state *orc_create(const orc_params *pin, const char *composition_path, const
 /* BiasedRandom_init (BiasedRandom.f90:44-79) on given move weights (init_freq with a frequencies
    file, runmc.f90:25-67): probabilities w/S (flat when S == 0), running-sum intervals, and
    end = -1 for a zero weight when S > 0. */
-int32_t orc_set_move_weights(orc_state *s, const double *w, int32_t n) {
-    if (n != s->nmol) return -3;
+static double biased_random_init(double *beg, double *end, const double *w, int n) {
     double S = 0;
     for (int i = 0; i < n; i++) S = S + w[i];
     double *prob = malloc(sizeof(double) * n);
     for (int i = 0; i < n; i++) prob[i] = (S == 0) ? 1.0 / n : w[i] / S;
-    s->freq_beg[0] = 0.0; s->freq_end[0] = prob[0];
-    for (int i = 1; i < n; i++) { s->freq_beg[i] = s->freq_end[i - 1]; s->freq_end[i] = s->freq_beg[i] + prob[i]; }
+    beg[0] = 0.0; end[0] = prob[0];
+    for (int i = 1; i < n; i++) { beg[i] = end[i - 1]; end[i] = beg[i] + prob[i]; }
     if (S > 0)
-        for (int i = 0; i < n; i++) if (w[i] == 0) s->freq_end[i] = -1.0;
+        for (int i = 0; i < n; i++) if (w[i] == 0) end[i] = -1.0;
     free(prob);
+    return S;
+}
+
+int32_t orc_set_move_weights(orc_state *s, const double *w, int32_t n) {
+    if (n != s->nmol) return -3;
+    s->smv = biased_random_init(s->freq_beg, s->freq_end, w, n);
+    return 0;
+}
+
+/* init_freq with exchange weights (runmc.f90:25-67): xchange_freq from the exchange weights,
+   xchange_probability = Sxch / (Smv + Sxch) with Smv the move weights' sum */
+int32_t orc_set_xchange_weights(orc_state *s, const double *w, int32_t n) {
+    if (n != s->nmol) return -3;
+    double sx = biased_random_init(s->xfreq_beg, s->xfreq_end, w, n);
+    s->xchange_probability = sx / (s->smv + sx);
     return 0;
 }
 
@@ -1913,7 +2104,7 @@ void orc_destroy(orc_state *s) {
         free(s->ps_new.uu_back); free(s->ps_new.fx_back); free(s->ps_new.fy_back); free(s->ps_new.fz_back);
         grid_free(&s->g);
     }
-    free(s->freq_beg); free(s->freq_end);
+    free(s->freq_beg); free(s->freq_end); free(s->xfreq_beg); free(s->xfreq_end);
     free(s);
 }
 

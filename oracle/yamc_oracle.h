@@ -125,6 +125,13 @@ int32_t orc_run_cycles(orc_state *s, const float *rng, int64_t n_rng, int64_t *c
 int32_t orc_mcvol(orc_state *s, const float *rng, int64_t n_rng, int64_t *cursor, orc_vol_rec *rec);
 /* current BoxLength (Angstrom) and the molecule-atom distances in Angstrom follow from it */
 double orc_box_length(const orc_state *s);
+/* init_freq with exchange weights: xchange_freq and xchange_probability = Sxch/(Smv+Sxch);
+   run_mc then takes an exchange step when the move's first draw is below it */
+int32_t orc_set_xchange_weights(orc_state *s, const double *w, int32_t n);
+/* one mc_xchange (MC.f90:1325-1954) of molecules imol1 != imol2 (1-based); the record has
+   imol = imol1, flags bit0 accepted, bit1 overlap, bit2 exchange, bits 8.. imol2 */
+int32_t orc_xchange(orc_state *s, int32_t imol1, int32_t imol2, const float *rng, int64_t n_rng,
+                    int64_t *cursor, orc_move_rec *rec);
 /* a single movemc(imol) with the proposal drawn from the RNG buffer */
 int32_t orc_movemc(orc_state *s, int32_t imol, const float *rng, int64_t n_rng,
                    int64_t *cursor, orc_move_rec *rec);

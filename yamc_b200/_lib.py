@@ -107,6 +107,9 @@ SIGNATURES = {
     "yamc_volume_eval": (ctypes.c_int, [_VP, ctypes.c_double, _dp, _ip]),
     "yamc_volume_commit": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_get_params": (ctypes.c_int, [_VP, ctypes.POINTER(YamcParams)]),
+    "yamc_set_xchange_weights": (ctypes.c_int, [_VP, _dp]),
+    "yamc_xchange_eval": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, _dp, _ip]),
+    "yamc_xchange_commit": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_set_refresh": (ctypes.c_int, [_VP, ctypes.c_int64]),
     "yamc_refresh_count": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
     "yamc_set_launch": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32]),

@@ -226,6 +226,24 @@ class Engine:
     def volume_commit(self, accepted: bool) -> None:
         check(self.lib.yamc_volume_commit(self.h, int(bool(accepted))), "yamc_volume_commit")
 
+    def set_xchange_weights(self, weights) -> None:
+        """Exchange weights per molecule (the third column of a frequencies file)."""
+        w = np.ascontiguousarray(weights, dtype=np.float64)
+        if w.size != self.nmol:
+            raise ValueError("one exchange weight per molecule")
+        check(self.lib.yamc_set_xchange_weights(self.h, _dptr(w)), "yamc_set_xchange_weights")
+
+    def xchange_eval(self, imol1: int, imol2: int):
+        """mc_xchange up to the acceptance test: (du[4], overlap)."""
+        du = np.zeros(4)
+        ov = ctypes.c_int32(0)
+        check(self.lib.yamc_xchange_eval(self.h, int(imol1), int(imol2), _dptr(du), ctypes.byref(ov)),
+              "yamc_xchange_eval")
+        return du, bool(ov.value)
+
+    def xchange_commit(self, accepted: bool) -> None:
+        check(self.lib.yamc_xchange_commit(self.h, int(bool(accepted))), "yamc_xchange_commit")
+
     def current_params(self) -> "_lib.YamcParams":
         """The parameters as they stand now (BoxLength follows accepted volume steps)."""
         p = _lib.YamcParams()

@@ -395,6 +395,136 @@ __global__ void __launch_bounds__(32 * kForceWarps, 2) k_forces_kspace(DevSys D,
     }
 }
 
+// ------------------------------------------------------------------------------------------
+// exchange move (mc_xchange, MC.f90:1325-1954): two molecules swap centres of mass
+// ------------------------------------------------------------------------------------------
+// The two molecules' atoms (molecule 1 first), at the old and the swapped positions.
+struct XchgIn {
+    int m1, m2, n1, n2;                 // 0-based molecules, their atom counts
+    double4 o[2 * kMaxA], n[2 * kMaxA]; // x, y, z (box units), q
+    int type[2 * kMaxA];                // LJ type (0 = none)
+    double dhs[2 * kMaxA];              // hard-core diameter / L
+};
+constexpr int kXParts = 16;  // (old 1, new 1, old 2, new 2) x (ew, lj6, lj12), then the overlap flag at 12
+
+// Real space of both molecules, old and new, against every atom outside them (the 1-2 pairs are
+// added on the host): one thread per atom j, block partials for k_sum_parts.  Overlap: an LJ site
+// of either molecule, at its new position, inside the mean hard-core diameter of an LJ site j
+// (EwaldSumRealSpace.f90:409-433).
+__global__ void __launch_bounds__(256) k_xchg_real(DevSys D, XchgIn X, double *part) {
+    __shared__ double red[(256 / 32 + 1) * kXParts];
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[kXParts];
+#pragma unroll
+    for (int v = 0; v < kXParts; ++v) acc[v] = 0;
+    if (j < D.N) {
+        const int2 mj = D.meta[j];
+        if (mj.x != X.m1 && mj.x != X.m2) {
+            const double4 pj = D.atom[j];
+            const double dj = D.dhs[j];
+            const int na = X.n1 + X.n2;
+            for (int a = 0; a < na; ++a) {
+                const int set0 = a < X.n1 ? 0 : 2;
+                const int ta = X.type[a];
+                const bool lj = ta > 0 && mj.y > 0;
+                const int off = lj ? (ta - 1) * D.nt + (mj.y - 1) : 0;
+                for (int w = 0; w < 2; ++w) {
+                    const double4 pa = w ? X.n[a] : X.o[a];
+                    const double dx = min_image(pa.x - pj.x), dy = min_image(pa.y - pj.y), dz = min_image(pa.z - pj.z);
+                    const double r2 = dx * dx + dy * dy + dz * dz;
+                    if (w == 1 && lj) {
+                        const double d12 = (X.dhs[a] + dj) / 2;
+                        if (r2 < d12 * d12) acc[12] = 1.0;
+                    }
+                    if (r2 >= D.rmax2) continue;
+                    const PairTerm<double> t = pair_term<double, false>(r2, D.xclb * pa.w * pj.w, lj, lj ? D.lj_sig6[off] : 0.0,
+                                                                         lj ? D.lj_feps[off] : 0.0, D.alpha, D.taosp, false);
+                    const int s = (set0 + w) * 3;
+                    acc[s] += t.ew; acc[s + 1] += t.lj6; acc[s + 2] += t.lj12;
+                }
+            }
+        }
+    }
+    block_sum<256>(acc, kXParts, red);
+    if (threadIdx.x < kXParts) part[(size_t)blockIdx.x * kXParts + threadIdx.x] = acc[threadIdx.x];
+}
+
+// k space: per signed entry the structure factors of both molecules at the new positions minus
+// the old ones (RhoSquared_addAtom per atom, molecule 1 then 2, MC.f90:1467-1490, 1652-1672),
+// written to delta (rows: Coulomb, then LJ types) for the commit, and the entry's terms of
+// EwaldSumKSpace_calc_dU_coulomb / _LJ (EwaldSumKSpace.f90:528-753) against the resident rho.
+template <int NT>
+__global__ void __launch_bounds__(256) k_xchg_kspace(DevSys D, XchgIn X, double2 *delta, double *part) {
+    extern __shared__ double2 xt[];  // [atom][old/new][3][KM]
+    __shared__ double red[(256 / 32 + 1) * 2];
+    const int KM = D.kmax + 1, na = X.n1 + X.n2;
+    for (int idx = threadIdx.x; idx < na * 2 * 3 * KM; idx += blockDim.x) {
+        const int a = idx / (6 * KM), r = idx % (6 * KM), w = r / (3 * KM), r3 = r % (3 * KM), d = r3 / KM, m = r3 % KM;
+        const double4 p = w ? X.n[a] : X.o[a];
+        const double u = d == 0 ? p.x : (d == 1 ? p.y : p.z);
+        double sn, cs;
+        sincospi(2.0 * (double)m * u, &sn, &cs);
+        if (m == 0) { sn = 0.0; cs = 1.0; }
+        xt[idx] = make_double2(cs, sn);
+    }
+    __syncthreads();
+    const int e = blockIdx.x * blockDim.x + threadIdx.x;
+    double acc[2] = {0, 0};
+    if (e < D.S) {
+        const int4 kv = D.kvec[e];
+        double2 sum[2][1 + NT];
+        int tmask = 0;
+#pragma unroll
+        for (int w = 0; w < 2; ++w)
+#pragma unroll
+            for (int t = 0; t <= NT; ++t) sum[w][t] = make_double2(0, 0);
+#pragma unroll
+        for (int w = 0; w < 2; ++w) {
+            for (int a = 0; a < na; ++a) {
+                const double2 *T = xt + (size_t)(a * 2 + w) * 3 * KM;
+                const double q = X.o[a].w;
+                const int ta = X.type[a];
+                double c = 0, sn = 0;
+                if (q != 0.0) {
+                    entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, q, c, sn);
+                    sum[w][0].x = sum[w][0].x + c; sum[w][0].y = sum[w][0].y + sn;
+                }
+                if (ta > 0) {
+                    double cl, sl;
+                    if (q != 0.0) { const double iq = 1.0 / q; cl = c * iq; sl = sn * iq; }
+                    else entry_phase<double, double2>(T, T + KM, T + 2 * KM, kv.x, kv.y, kv.z, 1.0, cl, sl);
+#pragma unroll
+                    for (int t = 0; t < NT; ++t) {
+                        const bool hit = t == ta - 1;
+                        sum[w][1 + t].x = hit ? sum[w][1 + t].x + cl : sum[w][1 + t].x;
+                        sum[w][1 + t].y = hit ? sum[w][1 + t].y + sl : sum[w][1 + t].y;
+                    }
+                    tmask |= 1 << (ta - 1);
+                }
+            }
+        }
+        double2 dl[1 + NT], C[1 + NT];
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) {
+            dl[t] = make_double2(sum[1][t].x - sum[0][t].x, sum[1][t].y - sum[0][t].y);
+            C[t] = D.rho[(size_t)t * D.S + e];
+            delta[(size_t)t * D.S + e] = dl[t];
+        }
+        acc[0] = (((C[0].x + C[0].x) + dl[0].x) * dl[0].x + ((C[0].y + C[0].y) + dl[0].y) * dl[0].y) * D.ebeta[e];
+#pragma unroll
+        for (int t1 = 0; t1 < NT; ++t1) {
+            const double tc = (C[1 + t1].x + C[1 + t1].x) + dl[1 + t1].x, ts = (C[1 + t1].y + C[1 + t1].y) + dl[1 + t1].y;
+#pragma unroll
+            for (int t2 = 0; t2 < NT; ++t2) {
+                if (!((tmask >> t2) & 1)) continue;
+                acc[1] += (tc * dl[1 + t2].x + ts * dl[1 + t2].y) * D.ebetalj[(size_t)pair_idx<NT>(t1, t2) * D.S + e];
+            }
+        }
+    }
+    block_sum<256>(acc, 2, red);
+    if (threadIdx.x < 2) part[(size_t)blockIdx.x * 2 + threadIdx.x] = acc[threadIdx.x];
+}
+
 // per-move API commit: rho += delta (Step 14, MC.f90:1245)
 __global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -490,6 +620,13 @@ struct yamc_ctx {
     double2 *rho_save = nullptr;
     double n_vol_accepted = 0;
     int vol_stage = 0;  // 1 between yamc_volume_eval and yamc_volume_commit
+    // exchange step between yamc_xchange_eval and yamc_xchange_commit (1 evaluated, 2 overlap)
+    int xch_stage = 0;
+    struct XchgPending {
+        int m1 = 0, m2 = 0;
+        double x[2 * kMaxA] = {}, y[2 * kMaxA] = {}, z[2 * kMaxA] = {};  // swapped positions, molecule 1 first
+        double d_ew = 0, d_lj6 = 0, d_lj12 = 0, du_kc = 0, du_kl = 0, dmu[3] = {};
+    } xch;
     struct VolSaved {
         yamc_params p{};
         std::vector<double> x, y, z, sigma, type_sigma, beta, ebetalj, lj6, lj12, four_eps, sigma6, sigma2, dhs;
@@ -960,8 +1097,11 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         c->rho_slice_atoms = ((chunks + want - 1) / want) * kRhoChunk;
         c->rho_slices = (N + c->rho_slice_atoms - 1) / c->rho_slice_atoms;
         if ((r = dalloc(&c->tpairs, tp.size())) || (r = upload(c->tpairs, tp.data(), tp.size(), c->stream)) ||
-            (r = dalloc(&c->part, std::max((size_t)c->ntpairs * kFullParts, (size_t)(S + 255) / 256 * 2))) ||
-            (r = dalloc(&c->sums, kFullParts + 2)) ||
+            // block partials: the full sums' tile pairs, the k-space energy blocks and the
+            // exchange step's atom blocks (kXParts each); the totals of any of them
+            (r = dalloc(&c->part, std::max({(size_t)c->ntpairs * kFullParts, (size_t)(S + 255) / 256 * 2,
+                                            (size_t)(N + 255) / 256 * kXParts}))) ||
+            (r = dalloc(&c->sums, std::max(kFullParts + 2, kXParts))) ||
             (r = dalloc(&c->rho_part, (size_t)(1 + nt) * c->rho_slices * S)))
             return r;
     }
@@ -1157,8 +1297,8 @@ int yamc_refresh_count(yamc_ctx *c, int64_t *count) {
 int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_t *cursor, int64_t n_moves,
                           int64_t *moves_done, yamc_move_record *d_log, double *d_rows, int32_t max_rows, int32_t *n_rows) {
     if (!c || !d_rng || !cursor || n_moves < 0) return YAMC_EPARAMETER;
-    if (c->H.p.pressure_step_multiplier > 0) {
-        set_error("pressure_step_multiplier > 0 (NPT): volume cycles run through yamc_run_mc");
+    if (c->H.p.pressure_step_multiplier > 0 || c->H.xchange_probability > 0) {
+        set_error("NPT volume cycles or exchange steps are on: they run through yamc_run_mc");
         return YAMC_EWRONG_FUNCTION;
     }
     CUDA_TRY(cudaSetDevice(c->device));
@@ -1168,8 +1308,8 @@ int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_
 int yamc_run_chain(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_moves, int64_t *moves_done,
                    yamc_move_record *log, double *rows, int32_t max_rows, int32_t *n_rows) {
     if (!c || !rng || !cursor || n_moves < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
-    if (c->H.p.pressure_step_multiplier > 0) {
-        set_error("pressure_step_multiplier > 0 (NPT): volume cycles run through yamc_run_mc");
+    if (c->H.p.pressure_step_multiplier > 0 || c->H.xchange_probability > 0) {
+        set_error("NPT volume cycles or exchange steps are on: they run through yamc_run_mc");
         return YAMC_EWRONG_FUNCTION;
     }
     CUDA_TRY(cudaSetDevice(c->device));
@@ -1401,9 +1541,216 @@ static int volume_step(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cu
     return YAMC_OK;
 }
 
+// ---------------------------------------------------------------- exchange move
+
+// mc_xchange (MC.f90:1325-1954) up to the acceptance test.  The real-space change follows the
+// reference: the two molecules' per-atom energies after the swap minus before
+// (MC.f90:1451-1452, 1639-1642), each of which holds the 1-2 pair energy, so that pair term
+// enters twice; the device sums both molecules (old and new) against every other atom, the host
+// adds the 1-2 pairs (at most 16).  k space and the external term are the exact two-molecule
+// changes.  du = {dU_real, dU_k_coulomb, dU_k_LJ, dU_ext}.
+static int xchange_eval(yamc_ctx *c, int imol1, int imol2, double du[4], int *overlap) {
+    HostSystem &H = c->H;
+    auto &X = c->xch;
+    int r;
+    if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
+    const int m1 = imol1 - 1, m2 = imol2 - 1;
+    const int f1 = H.first[m1], n1 = H.natoms[m1], f2 = H.first[m2], n2 = H.natoms[m2];
+    XchgIn in{};
+    in.m1 = m1; in.m2 = m2; in.n1 = n1; in.n2 = n2;
+    double cm[2][3];
+    for (int k = 0; k < 2; ++k) {  // center_of_mass (geometry.f90:170-201)
+        const int f = k ? f2 : f1, n = k ? n2 : n1;
+        double sx = 0, sy = 0, sz = 0, tm = 0;
+        for (int a = f; a < f + n; ++a) {
+            sx = sx + H.mass[a] * H.x[a]; sy = sy + H.mass[a] * H.y[a]; sz = sz + H.mass[a] * H.z[a]; tm = tm + H.mass[a];
+        }
+        cm[k][0] = sx / tm; cm[k][1] = sy / tm; cm[k][2] = sz / tm;
+    }
+    for (int a = 0; a < n1 + n2; ++a) {
+        const int k = a < n1 ? 0 : 1, i = k ? f2 + (a - n1) : f1 + a;
+        const double *co = cm[k], *cn = cm[1 - k];
+        in.o[a] = make_double4(H.x[i], H.y[i], H.z[i], H.q[i]);
+        // xnew = xold - x_center(own) + x_center(other), not wrapped (MC.f90:1516-1524)
+        X.x[a] = H.x[i] - co[0] + cn[0]; X.y[a] = H.y[i] - co[1] + cn[1]; X.z[a] = H.z[i] - co[2] + cn[2];
+        in.n[a] = make_double4(X.x[a], X.y[a], X.z[a], H.q[i]);
+        in.type[a] = H.type_by_index[i];
+        in.dhs[a] = H.dhs[i];
+    }
+    X.m1 = m1; X.m2 = m2;
+    const int nb = (H.N + 255) / 256;
+    k_xchg_real<<<nb, 256, 0, c->stream>>>(c->hsys, in, c->part);
+    CUDA_TRY(cudaGetLastError());
+    k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(c->part, nb, kXParts, 12, c->sums);
+    CUDA_TRY(cudaGetLastError());
+    double rs[kXParts];
+    CUDA_TRY(cudaMemcpyAsync(rs, c->sums, sizeof(rs), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    // the 1-2 pairs, old and new, on the host with the device's pair formula
+    const yamc_params &P = H.p;
+    double u12[2][3] = {};
+    bool ov12 = false;
+    for (int w = 0; w < 2; ++w)
+        for (int a = 0; a < n1; ++a)
+            for (int b = n1; b < n1 + n2; ++b) {
+                const double4 pa = w ? in.n[a] : in.o[a], pb = w ? in.n[b] : in.o[b];
+                const double dx = min_image(pa.x - pb.x), dy = min_image(pa.y - pb.y), dz = min_image(pa.z - pb.z);
+                const double r2 = dx * dx + dy * dy + dz * dz;
+                const bool lj = in.type[a] > 0 && in.type[b] > 0;
+                if (w == 1 && lj) {
+                    const double d12 = (in.dhs[a] + in.dhs[b]) / 2;
+                    if (r2 < d12 * d12) ov12 = true;
+                }
+                if (r2 >= P.rmax2) continue;
+                const int off = lj ? (in.type[a] - 1) * H.nt + (in.type[b] - 1) : 0;
+                const PairTerm<double> t = pair_term<double, false>(r2, P.xclb * pa.w * pb.w, lj, lj ? H.sigma6[off] : 0.0,
+                                                                     lj ? H.four_eps[off] : 0.0, P.alpha,
+                                                                     P.two_alpha_over_sqrt_pi, false);
+                u12[w][0] += t.ew; u12[w][1] += t.lj6; u12[w][2] += t.lj12;
+            }
+    *overlap = rs[12] > 0 || ov12;
+    if (*overlap) {
+        du[0] = du[1] = du[2] = du[3] = 0;
+        c->xch_stage = 2;
+        return YAMC_OK;
+    }
+    auto E = [&](const double *v) { return v[0] + v[2] - v[1]; };  // ew + lj12 - lj6
+    const double Eo1 = E(rs + 0), En1 = E(rs + 3), Eo2 = E(rs + 6), En2 = E(rs + 9);
+    const double U12o = E(u12[0]), U12n = E(u12[1]);
+    const double E_old = (Eo1 + U12o) + (Eo2 + U12o), E_new = (En1 + U12n) + (En2 + U12n);
+    du[0] = E_new - E_old;
+    // the bookkeeping change of the totals takes the 1-2 pairs once (MC.f90:1813-1826)
+    X.d_ew = (rs[3] + rs[9] + u12[1][0]) - (rs[0] + rs[6] + u12[0][0]);
+    X.d_lj6 = (rs[4] + rs[10] + u12[1][1]) - (rs[1] + rs[7] + u12[0][1]);
+    X.d_lj12 = (rs[5] + rs[11] + u12[1][2]) - (rs[2] + rs[8] + u12[0][2]);
+    // k space
+    const size_t sm = sizeof(double2) * (size_t)(n1 + n2) * 2 * 3 * (H.kmax + 1);
+    const int nbk = (H.S + 255) / 256;
+    switch (H.nt) {
+        case 1: CUDA_TRY(cudaFuncSetAttribute(k_xchg_kspace<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_xchg_kspace<1><<<nbk, 256, sm, c->stream>>>(c->hsys, in, c->scratch, c->part); break;
+        case 2: CUDA_TRY(cudaFuncSetAttribute(k_xchg_kspace<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_xchg_kspace<2><<<nbk, 256, sm, c->stream>>>(c->hsys, in, c->scratch, c->part); break;
+        case 3: CUDA_TRY(cudaFuncSetAttribute(k_xchg_kspace<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                k_xchg_kspace<3><<<nbk, 256, sm, c->stream>>>(c->hsys, in, c->scratch, c->part); break;
+        default: CUDA_TRY(cudaFuncSetAttribute(k_xchg_kspace<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm));
+                 k_xchg_kspace<4><<<nbk, 256, sm, c->stream>>>(c->hsys, in, c->scratch, c->part); break;
+    }
+    CUDA_TRY(cudaGetLastError());
+    k_sum_parts<<<1, kSumThreads, 0, c->stream>>>(c->part, nbk, 2, -1, c->sums);
+    CUDA_TRY(cudaGetLastError());
+    double ek[2];
+    CUDA_TRY(cudaMemcpyAsync(ek, c->sums, sizeof(ek), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    X.du_kc = ek[0]; X.du_kl = ek[1];
+    du[1] = ek[0]; du[2] = ek[1];
+    // external term (EwaldSumExternal_calc_dU) with dmu = dmu1 + dmu2
+    double dm[2][3] = {};
+    for (int k = 0; k < 2; ++k) {
+        double mo[3] = {}, mn[3] = {};
+        const int a0 = k ? n1 : 0, a1 = k ? n1 + n2 : n1;
+        for (int a = a0; a < a1; ++a) {
+            const double q = in.o[a].w;
+            mo[0] = mo[0] + q * in.o[a].x; mo[1] = mo[1] + q * in.o[a].y; mo[2] = mo[2] + q * in.o[a].z;
+            mn[0] = mn[0] + q * X.x[a]; mn[1] = mn[1] + q * X.y[a]; mn[2] = mn[2] + q * X.z[a];
+        }
+        for (int d = 0; d < 3; ++d) dm[k][d] = mn[d] - mo[d];
+    }
+    for (int d = 0; d < 3; ++d) X.dmu[d] = dm[0][d] + dm[1][d];
+    const double mu[3] = {c->sc[SC_MU_X], c->sc[SC_MU_Y], c->sc[SC_MU_Z]};
+    du[3] = P.kext * ((2 * mu[0] + X.dmu[0]) * X.dmu[0] + (2 * mu[1] + X.dmu[1]) * X.dmu[1] + (2 * mu[2] + X.dmu[2]) * X.dmu[2]);
+    c->xch_stage = 1;
+    return YAMC_OK;
+}
+
+// the acceptance branch of mc_xchange (MC.f90:1758-1848): rho += delta, the two molecules at the
+// swapped positions, the totals and the dipole updated; a rejection changes nothing
+static int xchange_commit(yamc_ctx *c, bool accepted) {
+    HostSystem &H = c->H;
+    const auto &X = c->xch;
+    const int stage = c->xch_stage;
+    c->xch_stage = 0;
+    if (!accepted || stage != 1) return YAMC_OK;
+    const int n = (1 + H.nt) * H.S;
+    k_commit_rho<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, c->scratch, n);
+    CUDA_TRY(cudaGetLastError());
+    const int f1 = H.first[X.m1], n1 = H.natoms[X.m1], f2 = H.first[X.m2], n2 = H.natoms[X.m2];
+    for (int k = 0; k < 2; ++k) {
+        const int f = k ? f2 : f1, na = k ? n2 : n1, a0 = k ? n1 : 0;
+        double4 a[kMaxA];
+        for (int i = 0; i < na; ++i) {
+            H.x[f + i] = X.x[a0 + i]; H.y[f + i] = X.y[a0 + i]; H.z[f + i] = X.z[a0 + i];
+            a[i] = make_double4(H.x[f + i], H.y[f + i], H.z[f + i], H.q[f + i]);
+        }
+        int r = upload(c->atom + f, a, na, c->stream);
+        if (r) return r;
+    }
+    c->sc[SC_UU_EW] = c->sc[SC_UU_EW] + X.d_ew;
+    c->sc[SC_UU_LJ6] = c->sc[SC_UU_LJ6] + X.d_lj6;
+    c->sc[SC_UU_LJ12] = c->sc[SC_UU_LJ12] + X.d_lj12;
+    c->sc[SC_EK_C] = c->sc[SC_EK_C] + X.du_kc;
+    c->sc[SC_EK_LJ] = c->sc[SC_EK_LJ] + X.du_kl;
+    c->sc[SC_MU_X] = c->sc[SC_MU_X] + X.dmu[0];
+    c->sc[SC_MU_Y] = c->sc[SC_MU_Y] + X.dmu[1];
+    c->sc[SC_MU_Z] = c->sc[SC_MU_Z] + X.dmu[2];
+    int r = push_state(c);
+    if (r) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    return YAMC_OK;
+}
+
+// BiasedRandom_choose (BiasedRandom.f90:81-109): the first interval with beg < rnd < end, else 1
+static int host_choose(const std::vector<double> &beg, const std::vector<double> &end, double rnd) {
+    for (size_t i = 0; i < beg.size(); ++i)
+        if (rnd > beg[i] && rnd < end[i]) return (int)i + 1;
+    return 1;
+}
+
+int yamc_set_xchange_weights(yamc_ctx *c, const double *w) {
+    if (!c || !w) return YAMC_EPARAMETER;
+    HostSystem &H = c->H;
+    const int M = H.M;
+    double S = 0;
+    for (int i = 0; i < M; ++i) {
+        if (!(w[i] >= 0)) { set_error("exchange weights must be non-negative"); return YAMC_EPARAMETER; }
+        S = S + w[i];
+    }
+    // BiasedRandom_init (BiasedRandom.f90:44-79) on the exchange weights
+    H.xfreq_beg.assign(M, 0.0); H.xfreq_end.assign(M, 0.0);
+    std::vector<double> prob(M);
+    for (int i = 0; i < M; ++i) prob[i] = (S == 0) ? 1.0 / M : w[i] / S;
+    H.xfreq_beg[0] = 0.0; H.xfreq_end[0] = prob[0];
+    for (int i = 1; i < M; ++i) { H.xfreq_beg[i] = H.xfreq_end[i - 1]; H.xfreq_end[i] = H.xfreq_beg[i] + prob[i]; }
+    if (S > 0)
+        for (int i = 0; i < M; ++i) if (w[i] == 0) H.xfreq_end[i] = -1.0;
+    int nz = 0;
+    for (int i = 0; i < M; ++i) nz += w[i] > 0;
+    if (S > 0 && nz < 2) { set_error("exchange steps need at least two molecules with a positive weight"); return YAMC_EPARAMETER; }
+    H.xchange_probability = S / (H.smv + S);
+    return YAMC_OK;
+}
+
+int yamc_xchange_eval(yamc_ctx *c, int32_t imol1, int32_t imol2, double du[4], int32_t *overlap) {
+    if (!c || !du || !overlap || imol1 < 1 || imol2 < 1 || imol1 > c->H.M || imol2 > c->H.M || imol1 == imol2)
+        return YAMC_EPARAMETER;
+    if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    int ov = 0;
+    const int r = xchange_eval(c, imol1, imol2, du, &ov);
+    *overlap = ov;
+    return r;
+}
+
+int yamc_xchange_commit(yamc_ctx *c, int32_t accepted) {
+    if (!c) return YAMC_EPARAMETER;
+    if (!c->xch_stage) { set_error("no exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(c->device));
+    return xchange_commit(c, accepted != 0);
+}
+
 int yamc_volume_eval(yamc_ctx *c, double new_box_length, double *du, int32_t *overlap) {
     if (!c || !du || !overlap || !(new_box_length > 0)) return YAMC_EPARAMETER;
-    if (c->api_stage || c->vol_stage) { set_error("a move or volume step is pending"); return YAMC_EWRONG_FUNCTION; }
+    if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
     int ov = 0;
     const int r = volume_eval(c, new_box_length, du, &ov);
@@ -1428,7 +1775,7 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
                 yamc_move_record *log, int64_t max_log, int64_t *n_log, yamc_volume_record *vlog, int64_t max_vlog,
                 int64_t *n_vlog, double *rows, int32_t max_rows, int32_t *n_rows) {
     if (!c || !rng || !cursor || n_cycles < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
-    if (c->api_stage || c->vol_stage) { set_error("a move or volume step is pending"); return YAMC_EWRONG_FUNCTION; }
+    if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
     HostSystem &H = c->H;
     const int64_t base = *cursor;
@@ -1489,6 +1836,92 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
                 continue;
             }
             *cursor = c0;  // a move cycle: the chain kernel takes the cycle's draw itself
+        }
+        if (H.xchange_probability > 0) {
+            // exchange steps on: the host reads each move's draws (the cycle's pressure draw at
+            // its start, the exchange draw); an exchange step runs here, a movemc step as a
+            // one-move chain launch that takes those draws itself (runmc.f90:228-272)
+            bool cycle_done = false;
+            while (!cycle_done && st == YAMC_OK) {
+                const int64_t c0 = *cursor;
+                const bool at_start = c->cnt_h[CN_MOVE_IN_CYCLE] == 0;
+                double u = 0, xd = 0;
+                if ((at_start && !host_rand(rng, n_rng, cursor, &u)) || !host_rand(rng, n_rng, cursor, &xd)) {
+                    *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
+                }
+                if (xd < H.xchange_probability) {
+                    double r1 = 0, r2 = 0;
+                    bool out = !host_rand(rng, n_rng, cursor, &r1);
+                    const int imol1 = out ? 1 : host_choose(H.xfreq_beg, H.xfreq_end, r1);
+                    int imol2 = imol1;
+                    while (!out && imol2 == imol1) {
+                        out = !host_rand(rng, n_rng, cursor, &r2);
+                        if (!out) imol2 = host_choose(H.xfreq_beg, H.xfreq_end, r2);
+                    }
+                    if (out) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
+                    double du[4];
+                    int ov = 0;
+                    if ((r = xchange_eval(c, imol1, imol2, du, &ov))) return r;
+                    bool acc = false;
+                    if (!ov) {  // MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597)
+                        const double factor = std::exp(-(du[0] + (du[1] + du[2]) + du[3]));
+                        double xk = 0;
+                        if (!host_rand(rng, n_rng, cursor, &xk)) {
+                            xchange_commit(c, false);
+                            *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
+                        }
+                        acc = !(xk > factor);
+                    }
+                    if ((r = xchange_commit(c, acc))) return r;
+                    if (log && nlog < max_log) {
+                        yamc_move_record &rec = log[nlog++];
+                        rec.imol = imol1; rec.flags = (acc ? 1 : 0) | (ov ? 2 : 0) | 4 | (imol2 << 8); rec.cursor = *cursor;
+                        rec.du_real = du[0]; rec.du_k_coul = du[1]; rec.du_k_lj = du[2]; rec.du_ext = du[3];
+                    }
+                    c->sc[SC_N_MV_STEPS] += 1;
+                    if (acc) c->sc[SC_N_MV_ACC] += 1;
+                    long long mic = c->cnt_h[CN_MOVE_IN_CYCLE] + 1;
+                    if (mic == H.M) {
+                        mic = 0;
+                        const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
+                        if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && nrow < max_rows) {
+                            double e[8];
+                            energies_from(c->sc, H.p.kext, e);
+                            double *row = rows + 9 * (size_t)nrow;
+                            row[0] = (double)c->cnt_h[CN_ICYCLE];
+                            for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
+                            ++nrow;
+                        }
+                        c->cnt_h[CN_ICYCLE] += 1;
+                        cycle_done = true;
+                    }
+                    c->cnt_h[CN_MOVE_IN_CYCLE] = mic;
+                    if ((r = push_state(c))) return r;
+                    CUDA_TRY(cudaStreamSynchronize(c->stream));
+                } else {
+                    *cursor = c0;
+                    const bool keep = log && nlog < max_log;
+                    const bool want_row = rows && nrow < max_rows;
+                    int64_t mdone = 0;
+                    int32_t kr = 0;
+                    st = run_chain_impl(c, c->d_rng, base, n_rng, cursor, 1, &mdone, keep ? c->d_log : nullptr,
+                                        want_row ? c->d_rows : nullptr, want_row ? 1 : 0, &kr);
+                    if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
+                    if (keep && mdone) {
+                        CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record), cudaMemcpyDeviceToHost));
+                        ++nlog;
+                    }
+                    if (want_row && kr) {
+                        CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9, cudaMemcpyDeviceToHost));
+                        ++nrow;
+                    }
+                    if ((r = pull_state(c))) return r;
+                    cycle_done = mdone == 1 && c->cnt_h[CN_MOVE_IN_CYCLE] == 0;
+                }
+            }
+            if (st == YAMC_ERNG_EXHAUSTED) break;
+            ++done;
+            continue;
         }
         const int64_t n = H.M - c->cnt_h[CN_MOVE_IN_CYCLE];
         const bool keep_log = log && nlog + n <= max_log;

@@ -475,6 +475,7 @@ int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSyst
     std::vector<double> prob(M);
     for (int i = 0; i < M; ++i) prob[i] = (S == 0) ? 1.0 / M : w[i] / S;
     H.freq_beg.resize(M); H.freq_end.resize(M);
+    H.smv = S;
     H.freq_beg[0] = 0.0; H.freq_end[0] = prob[0];
     for (int i = 1; i < M; ++i) { H.freq_beg[i] = H.freq_end[i - 1]; H.freq_end[i] = H.freq_beg[i] + prob[i]; }
     if (S > 0)

@@ -42,6 +42,11 @@ struct HostSystem {
     double U_tail_coul = 0, U_tail_lj6 = 0, U_tail_lj12 = 0;
     std::vector<double> freq_beg, freq_end;   // BiasedRandom intervals
     int freq_monotone = 1;                    // intervals increasing (binary search valid)
+    double smv = 0;                           // SUM of the move weights (init_freq's Smv)
+    // exchange moves (init_freq with exchange weights): xchange_freq intervals and the
+    // probability Sxch / (Smv + Sxch) of an exchange step; 0 = no exchange steps
+    std::vector<double> xfreq_beg, xfreq_end;
+    double xchange_probability = 0;
     std::vector<int32_t> mol_numbers;
     int max_mol_atoms = 0;
     // runs of identical consecutive molecules: first molecule, count, atoms each, first atom
