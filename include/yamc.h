@@ -238,6 +238,31 @@ int yamc_set_xchange_weights(yamc_ctx *ctx, const double *weights);
 int yamc_xchange_eval(yamc_ctx *ctx, int32_t imol1, int32_t imol2, double du[4], int32_t *overlap);
 int yamc_xchange_commit(yamc_ctx *ctx, int32_t accepted);
 
+/* ---- radial distribution functions of molecule centres (mcrdf2.f90:110-440) ----
+   The reference computes them offline from the trajectory; here frames are added on the GPU,
+   from host arrays of molecule centres (a trajectory frame) or straight from a context's
+   device-resident positions.  For every frame: every ordered pair (i, j) of centres and, when
+   rmax reaches past L/2, the periodic images, counted per species pair (t1 <= t2) into bins of
+   width dr (count_distances, mcrdf2.f90:110-333).  mol_type[nmol]: 1-based species of each
+   molecule (composition order); mol_numbers[ntypes]: molecules per species.  nbin =
+   aint((rmax - 1e-10)/dr) + 2.  yamc_rdf_result: counts[(t1*ntypes + t2)*nbin + b] (0-based
+   species) and the written g(r) of save_rdfs (mcrdf2.f90:371-440) at r = (b + 1/2) dr:
+   counts / N_frame / <1/V> / N_t1 / N_t2 / dV / (2 if t1 != t2), dV = 4 pi dr (r^2 + r dr) +
+   4/3 pi dr^3.  The reference's interpolated and 1/r^2-weighted histograms, which save_rdfs does
+   not write, are not formed. */
+typedef struct yamc_rdf yamc_rdf;
+int yamc_rdf_create(int32_t nmol, const int32_t *mol_type, int32_t ntypes, const int32_t *mol_numbers,
+                    double dr, double rmax, int32_t device, yamc_rdf **out);
+int yamc_rdf_destroy(yamc_rdf *h);
+int yamc_rdf_nbin(yamc_rdf *h, int32_t *nbin);
+/* centres in box units (HOST arrays, nmol each), box length in Angstrom */
+int yamc_rdf_add_frame(yamc_rdf *h, const double *x, const double *y, const double *z, double box_length);
+/* the context's current configuration: centres of mass (center_of_mass, geometry.f90:170-201)
+   computed on the device from its positions; the context must be on the RDF's device */
+int yamc_rdf_add_ctx(yamc_rdf *h, yamc_ctx *ctx);
+/* g and counts: ntypes*ntypes*nbin each (entries with t1 > t2 are 0); either may be NULL */
+int yamc_rdf_result(yamc_rdf *h, double *g, double *counts, int32_t *n_frames);
+
 /* Mixed form (params.precision = YAMC_MIXED): the chain kernel recomputes rho(k)
    and the k-space energies in FP64 from the positions after every
    `accepted_moves` accepted moves (default 10000; 0 = never), bounding the drift

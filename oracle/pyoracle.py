@@ -114,6 +114,10 @@ def lib(fast: bool = False):
         L.orc_xchange.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_int32, ctypes.c_void_p, ctypes.c_int64,
                                   P(ctypes.c_int64), P(MoveRec)]
         L.orc_xchange.restype = ctypes.c_int32
+        L.orc_rdf_count.argtypes = [ctypes.c_int32] + [ctypes.c_void_p] * 4 + [ctypes.c_int32] + [ctypes.c_double] * 3 + \
+            [ctypes.c_void_p] * 2
+        L.orc_rdf_normalize.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_double, ctypes.c_double, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p]
         L.orc_box_length.argtypes = [ctypes.c_void_p]
         L.orc_box_length.restype = ctypes.c_double
         L.orc_move_old.argtypes = [ctypes.c_void_p, ctypes.c_int32, dp, dp]
@@ -343,3 +347,33 @@ def bet6_bet12(x: float):
 
 def grid_count(kmax: int) -> int:
     return lib().orc_grid_count(kmax)
+
+
+class RDF:
+    """mcrdf2's molecule-centre RDFs (count_distances + save_rdfs, mcrdf2.f90:110-440)."""
+
+    def __init__(self, mol_type, mol_numbers, dr: float = 0.1, rmax: float = 12.0):
+        self.L = lib()
+        self.type = np.ascontiguousarray(mol_type, dtype=np.int32)
+        self.mol_numbers = np.ascontiguousarray(mol_numbers, dtype=np.int32)
+        self.nt = int(self.mol_numbers.size)
+        self.dr, self.rmax = float(dr), float(rmax)
+        self.nbin = int((rmax - 1e-10) / dr) + 2
+        self.cnt4 = np.zeros(self.nt * self.nt * self.nbin)
+        self.n_total = np.zeros(self.nt * self.nt)
+        self.n_frame = 0
+        self.sum_inv_vol = 0.0
+
+    def add_frame(self, x, y, z, box_length: float) -> None:
+        x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+        self.L.orc_rdf_count(x.size, x.ctypes.data, y.ctypes.data, z.ctypes.data, self.type.ctypes.data, self.nt,
+                             box_length, self.dr, self.rmax, self.cnt4.ctypes.data, self.n_total.ctypes.data)
+        self.n_frame += 1
+        self.sum_inv_vol += 1.0 / box_length ** 3
+
+    def g(self) -> np.ndarray:
+        out = np.zeros_like(self.cnt4)
+        self.L.orc_rdf_normalize(self.nt, self.mol_numbers.ctypes.data, self.dr, self.rmax, self.cnt4.ctypes.data,
+                                 self.n_total.ctypes.data, self.n_frame, self.sum_inv_vol / self.n_frame,
+                                 out.ctypes.data)
+        return out.reshape(self.nt, self.nt, self.nbin)

@@ -2152,3 +2152,67 @@ void orc_force_kspace_atom(orc_state *s, int32_t atom1, double x, double y, doub
     rho_free(&tmp, s->lj.ntype);
 }
 double orc_box_length(const orc_state *s) { return s->p.BoxLength; }
+
+/* ------------------------------------------------------------------ */
+/* radial distribution functions: mcrdf2 count_distances / save_rdfs    */
+/* ------------------------------------------------------------------ */
+/* count_distances (mcrdf2.f90:110-333) for one frame: every ordered pair (i, j) of molecule
+   centres (box units) and, when Rmax reaches past L/2, the periodic images up to Nbox boxes
+   away; j shifted by one box where |x_i - x_j| > 0.5 first.  cnt4[(t1*ntypes + t2)*nbin + b]
+   (t1 <= t2, 0-based species) counts the pairs with r in bin b = aint(r/dr), n_total[t1*ntypes+t2]
+   all of them.  The interpolated, 1/r^2 and 1/(r^2 V) histograms of the reference are not
+   formed: its output (save_rdfs) reads only cnt4.  nbin = aint((Rmax - 1e-10)/dr) + 2. */
+void orc_rdf_count(int32_t M, const double *x, const double *y, const double *z, const int32_t *type, int32_t ntypes,
+                   double L, double dr, double rmax, double *cnt4, double *n_total) {
+    int nbin = (int)((rmax - 1e-10) / dr) + 2;
+    double rmax2 = rmax * rmax;
+    int nbox = rmax < L / 2 ? 0 : (int)((rmax - L / 2) / L) + 1;
+    for (int i = 0; i < M; i++) {
+        int ti = type[i] - 1;
+        for (int j = 0; j < M; j++) {
+            int tj = type[j] - 1;
+            double x2 = x[j], y2 = y[j], z2 = z[j];
+            if (x[i] - x2 > 0.5) x2 = x2 + 1.0;
+            if (x[i] - x2 < -0.5) x2 = x2 - 1.0;
+            if (y[i] - y2 > 0.5) y2 = y2 + 1.0;
+            if (y[i] - y2 < -0.5) y2 = y2 - 1.0;
+            if (z[i] - z2 > 0.5) z2 = z2 + 1.0;
+            if (z[i] - z2 < -0.5) z2 = z2 - 1.0;
+            for (int nx = -nbox; nx <= nbox; nx++)
+                for (int ny = -nbox; ny <= nbox; ny++)
+                    for (int nz = -nbox; nz <= nbox; nz++) {
+                        if (i == j && nx == 0 && ny == 0 && nz == 0) continue;
+                        double dx = (x[i] - x2 + nx) * L, dy = (y[i] - y2 + ny) * L, dz = (z[i] - z2 + nz) * L;
+                        double r2 = dx * dx + dy * dy + dz * dz;
+                        if (r2 > rmax2 - 1e-10) continue;
+                        double r = sqrt(r2);
+                        int b = (int)(r / dr);
+                        int off = ti < tj ? ti * ntypes + tj : tj * ntypes + ti;
+                        n_total[off] += 1.0;
+                        if (b < nbin) cnt4[(size_t)off * nbin + b] += 1.0;
+                    }
+        }
+    }
+}
+
+/* save_rdfs (mcrdf2.f90:371-440), the written column: g(r_k + dr/2) = cnt4 / N_frame / <1/V> /
+   N_i / N_j / dV / factor with dV = 4 pi dr (r^2 + r dr) + 4/3 pi dr^3, factor 2 for i != j */
+void orc_rdf_normalize(int32_t ntypes, const int32_t *mol_numbers, double dr, double rmax, const double *cnt4,
+                       const double *n_total, int32_t n_frame, double avg_inv_vol, double *g) {
+    int nbin = (int)((rmax - 1e-10) / dr) + 2;
+    double four_pi_dr = 4.0 * PI * dr, small_ball = 4.0 / 3.0 * PI * dr * dr * dr;
+    for (int i = 0; i < ntypes; i++)
+        for (int j = i; j < ntypes; j++) {
+            int off = i * ntypes + j;
+            double r = 0.0;
+            for (int k = 0; k < nbin; k++) {
+                double dV = four_pi_dr * (r * r + r * dr) + small_ball;
+                double factor = i == j ? 1.0 : 2.0;
+                double v = 0.0;
+                if (n_total[off] > 0)
+                    v = cnt4[(size_t)off * nbin + k] / n_frame / avg_inv_vol / mol_numbers[i] / mol_numbers[j] / dV / factor;
+                g[(size_t)off * nbin + k] = v;
+                r = r + dr;
+            }
+        }
+}

@@ -142,6 +142,14 @@ int32_t orc_move_eval(orc_state *s, const double *xn, const double *yn, const do
                       int32_t *overlap, double f[3], double t[3]);
 int32_t orc_move_commit(orc_state *s);
 
+/* radial distribution functions of molecule centres (mcrdf2.f90:110-440): counts of one frame
+   added to cnt4[(t1*ntypes+t2)*nbin + b] and n_total[t1*ntypes+t2] (t1 <= t2, 0-based species,
+   nbin = aint((Rmax-1e-10)/dr) + 2), and the written g(r) from the accumulated counts */
+void orc_rdf_count(int32_t M, const double *x, const double *y, const double *z, const int32_t *type, int32_t ntypes,
+                   double L, double dr, double rmax, double *cnt4, double *n_total);
+void orc_rdf_normalize(int32_t ntypes, const int32_t *mol_numbers, double dr, double rmax, const double *cnt4,
+                       const double *n_total, int32_t n_frame, double avg_inv_vol, double *g);
+
 /* k-space forces on one atom at (x,y,z) with the current total rho (ForceKSpace.f90) */
 void orc_force_kspace_atom(orc_state *s, int32_t atom1, double x, double y, double z,
                            double f[3]);

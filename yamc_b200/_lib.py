@@ -108,6 +108,13 @@ SIGNATURES = {
     "yamc_volume_commit": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_get_params": (ctypes.c_int, [_VP, ctypes.POINTER(YamcParams)]),
     "yamc_set_xchange_weights": (ctypes.c_int, [_VP, _dp]),
+    "yamc_rdf_create": (ctypes.c_int, [ctypes.c_int32, _ip, ctypes.c_int32, _ip, ctypes.c_double, ctypes.c_double,
+                                       ctypes.c_int32, _PPP]),
+    "yamc_rdf_destroy": (ctypes.c_int, [_VP]),
+    "yamc_rdf_nbin": (ctypes.c_int, [_VP, _ip]),
+    "yamc_rdf_add_frame": (ctypes.c_int, [_VP, _dp, _dp, _dp, ctypes.c_double]),
+    "yamc_rdf_add_ctx": (ctypes.c_int, [_VP, _VP]),
+    "yamc_rdf_result": (ctypes.c_int, [_VP, _dp, _dp, _ip]),
     "yamc_xchange_eval": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.c_int32, _dp, _ip]),
     "yamc_xchange_commit": (ctypes.c_int, [_VP, ctypes.c_int32]),
     "yamc_set_refresh": (ctypes.c_int, [_VP, ctypes.c_int64]),

@@ -442,3 +442,56 @@ class _ReplicaView(Engine):
 
     def close(self) -> None:  # owned by the batch
         self.h = None
+
+
+class RDF:
+    """Molecule-centre radial distribution functions on the GPU (mcrdf2.f90:110-440): frames from
+    host centres (a trajectory frame) or from an Engine's device-resident configuration."""
+
+    def __init__(self, mol_type, mol_numbers, dr: float = 0.1, rmax: float = 12.0, device: int = 0):
+        self.lib = _lib.load()
+        self.mol_type = np.ascontiguousarray(mol_type, dtype=np.int32)
+        self.mol_numbers = np.ascontiguousarray(mol_numbers, dtype=np.int32)
+        self.ntypes = int(self.mol_numbers.size)
+        self.dr, self.rmax = float(dr), float(rmax)
+        self.h = ctypes.c_void_p()
+        check(self.lib.yamc_rdf_create(self.mol_type.size, _iptr(self.mol_type), self.ntypes, _iptr(self.mol_numbers),
+                                       self.dr, self.rmax, int(device), ctypes.byref(self.h)), "yamc_rdf_create")
+        nb = ctypes.c_int32(0)
+        check(self.lib.yamc_rdf_nbin(self.h, ctypes.byref(nb)), "yamc_rdf_nbin")
+        self.nbin = nb.value
+
+    @classmethod
+    def for_engine(cls, eng: "Engine", dr: float = 0.1, rmax: float = 12.0, device: int = 0) -> "RDF":
+        """Species per molecule in composition order from the engine's inputs."""
+        counts = np.asarray(eng.inputs.mol_numbers, dtype=np.int32)
+        mol_type = np.repeat(np.arange(1, counts.size + 1, dtype=np.int32), counts)
+        return cls(mol_type, counts, dr, rmax, device)
+
+    def add_frame(self, x, y, z, box_length: float) -> None:
+        x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in (x, y, z))
+        check(self.lib.yamc_rdf_add_frame(self.h, _dptr(x), _dptr(y), _dptr(z), float(box_length)), "yamc_rdf_add_frame")
+
+    def add_engine(self, eng: "Engine") -> None:
+        check(self.lib.yamc_rdf_add_ctx(self.h, eng.h), "yamc_rdf_add_ctx")
+
+    def result(self):
+        """(r, g[ntypes, ntypes, nbin], counts[ntypes, ntypes, nbin], n_frames); r = bin centres."""
+        g = np.zeros(self.ntypes * self.ntypes * self.nbin)
+        c = np.zeros_like(g)
+        nf = ctypes.c_int32(0)
+        check(self.lib.yamc_rdf_result(self.h, _dptr(g), _dptr(c), ctypes.byref(nf)), "yamc_rdf_result")
+        r = (np.arange(self.nbin) + 0.5) * self.dr
+        shape = (self.ntypes, self.ntypes, self.nbin)
+        return r, g.reshape(shape), c.reshape(shape), nf.value
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.yamc_rdf_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

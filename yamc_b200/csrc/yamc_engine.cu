@@ -525,6 +525,67 @@ __global__ void __launch_bounds__(256) k_xchg_kspace(DevSys D, XchgIn X, double2
     if (threadIdx.x < 2) part[(size_t)blockIdx.x * 2 + threadIdx.x] = acc[threadIdx.x];
 }
 
+// ------------------------------------------------------------------------------------------
+// radial distribution functions of molecule centres (mcrdf2, count_distances, mcrdf2.f90:110-333)
+// ------------------------------------------------------------------------------------------
+// centre of mass of every molecule (center_of_mass, geometry.f90:170-201) from the device positions
+__global__ void k_mol_centres(DevSys D, double *cx, double *cy, double *cz) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= D.M) return;
+    const int2 mo = D.mol[m];
+    double sx = 0, sy = 0, sz = 0, tm = 0;
+    for (int a = mo.x; a < mo.x + mo.y; ++a) {
+        const double4 p = D.atom[a];
+        const double w = D.mass[a];
+        sx = __dadd_rn(sx, __dmul_rn(w, p.x)); sy = __dadd_rn(sy, __dmul_rn(w, p.y));
+        sz = __dadd_rn(sz, __dmul_rn(w, p.z)); tm = __dadd_rn(tm, w);
+    }
+    cx[m] = sx / tm; cy[m] = sy / tm; cz[m] = sz / tm;
+}
+
+// One frame: every ordered pair (i, j) of centres, grid-stride over i*M + j, each block counting
+// into shared-memory histograms (hist[(t1*ntypes + t2)*nbin + b], t1 <= t2, then the per-pair
+// totals) that it adds to the device totals at the end.  The distance arithmetic is written with
+// explicitly rounded operations (no contraction), so the bins match the oracle's exactly.
+__global__ void __launch_bounds__(256) k_rdf_count(const double *cx, const double *cy, const double *cz, const int *type,
+                                                   int M, int ntypes, int nbin, double L, double dr, double rmax2,
+                                                   int nbox, unsigned long long *hist) {
+    extern __shared__ unsigned int hs[];
+    const int npair = ntypes * ntypes, nh = npair * nbin + npair;
+    for (int k = threadIdx.x; k < nh; k += blockDim.x) hs[k] = 0;
+    __syncthreads();
+    const long long total = (long long)M * M;
+    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < total; p += (long long)gridDim.x * blockDim.x) {
+        const int i = (int)(p / M), j = (int)(p % M);
+        const double x1 = cx[i], y1 = cy[i], z1 = cz[i];
+        double x2 = cx[j], y2 = cy[j], z2 = cz[j];
+        if (__dsub_rn(x1, x2) > 0.5) x2 = __dadd_rn(x2, 1.0);
+        if (__dsub_rn(x1, x2) < -0.5) x2 = __dsub_rn(x2, 1.0);
+        if (__dsub_rn(y1, y2) > 0.5) y2 = __dadd_rn(y2, 1.0);
+        if (__dsub_rn(y1, y2) < -0.5) y2 = __dsub_rn(y2, 1.0);
+        if (__dsub_rn(z1, z2) > 0.5) z2 = __dadd_rn(z2, 1.0);
+        if (__dsub_rn(z1, z2) < -0.5) z2 = __dsub_rn(z2, 1.0);
+        const int ti = type[i] - 1, tj = type[j] - 1;
+        const int off = ti < tj ? ti * ntypes + tj : tj * ntypes + ti;
+        for (int nx = -nbox; nx <= nbox; ++nx)
+            for (int ny = -nbox; ny <= nbox; ++ny)
+                for (int nz = -nbox; nz <= nbox; ++nz) {
+                    if (i == j && nx == 0 && ny == 0 && nz == 0) continue;
+                    const double dx = __dmul_rn(__dadd_rn(__dsub_rn(x1, x2), (double)nx), L);
+                    const double dy = __dmul_rn(__dadd_rn(__dsub_rn(y1, y2), (double)ny), L);
+                    const double dz = __dmul_rn(__dadd_rn(__dsub_rn(z1, z2), (double)nz), L);
+                    const double r2 = __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz));
+                    if (r2 > __dsub_rn(rmax2, 1e-10)) continue;
+                    const int b = (int)__ddiv_rn(__dsqrt_rn(r2), dr);
+                    atomicAdd(&hs[npair * nbin + off], 1u);
+                    if (b < nbin) atomicAdd(&hs[off * nbin + b], 1u);
+                }
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < nh; k += blockDim.x)
+        if (hs[k]) atomicAdd(&hist[k], (unsigned long long)hs[k]);
+}
+
 // per-move API commit: rho += delta (Step 14, MC.f90:1245)
 __global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1746,6 +1807,140 @@ int yamc_xchange_commit(yamc_ctx *c, int32_t accepted) {
     if (!c->xch_stage) { set_error("no exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
     return xchange_commit(c, accepted != 0);
+}
+
+// ---------------------------------------------------------------- radial distribution functions
+
+struct yamc_rdf {
+    int device = 0, M = 0, ntypes = 0, nbin = 0, grid = 1, n_frame = 0;
+    double dr = 0, rmax = 0, sum_inv_vol = 0;
+    size_t smem = 0;
+    std::vector<int32_t> mol_numbers;
+    cudaStream_t stream = nullptr;
+    int *type = nullptr;
+    double *cx = nullptr, *cy = nullptr, *cz = nullptr;
+    unsigned long long *hist = nullptr;  // [ntypes^2][nbin] counts, then [ntypes^2] pair totals
+};
+
+static int rdf_frame(yamc_rdf *h, double L) {
+    const int nbox = h->rmax < L / 2 ? 0 : (int)((h->rmax - L / 2) / L) + 1;  // mcrdf2.f90:206-210
+    k_rdf_count<<<h->grid, 256, h->smem, h->stream>>>(h->cx, h->cy, h->cz, h->type, h->M, h->ntypes, h->nbin, L, h->dr,
+                                                      h->rmax * h->rmax, nbox, h->hist);
+    CUDA_TRY(cudaGetLastError());
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    h->n_frame += 1;
+    h->sum_inv_vol += 1.0 / (L * L * L);
+    return YAMC_OK;
+}
+
+int yamc_rdf_destroy(yamc_rdf *h) {
+    if (!h) return YAMC_OK;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    void *ptrs[] = {h->type, h->cx, h->cy, h->cz, h->hist};
+    for (void *p : ptrs) if (p) cudaFree(p);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+    return YAMC_OK;
+}
+
+static int rdf_create_impl(yamc_rdf *h, int32_t nmol, const int32_t *mol_type, int32_t ntypes, const int32_t *mol_numbers,
+                           double dr, double rmax, int32_t device) {
+    if (nmol < 1 || !mol_type || ntypes < 1 || !mol_numbers || !(dr > 0) || !(rmax > dr)) return YAMC_EPARAMETER;
+    for (int i = 0; i < nmol; ++i)
+        if (mol_type[i] < 1 || mol_type[i] > ntypes) { set_error("mol_type outside 1..ntypes"); return YAMC_EPARAMETER; }
+    h->device = device; h->M = nmol; h->ntypes = ntypes; h->dr = dr; h->rmax = rmax;
+    h->nbin = (int)((rmax - 1e-10) / dr) + 2;  // N of count_distances (mcrdf2.f90:140)
+    h->mol_numbers.assign(mol_numbers, mol_numbers + ntypes);
+    const size_t nh = (size_t)ntypes * ntypes * h->nbin + (size_t)ntypes * ntypes;
+    h->smem = sizeof(unsigned int) * nh;
+    CUDA_TRY(cudaSetDevice(device));
+    cudaDeviceProp prop;
+    CUDA_TRY(cudaGetDeviceProperties(&prop, device));
+    if (h->smem > prop.sharedMemPerBlockOptin) { set_error("too many RDF bins x species pairs for one block's histogram"); return YAMC_ELIMITS; }
+    CUDA_TRY(cudaFuncSetAttribute(k_rdf_count, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)h->smem));
+    const long long pairs = (long long)nmol * nmol;
+    h->grid = (int)std::max(1LL, std::min((pairs + 255) / 256, 4LL * prop.multiProcessorCount));
+    CUDA_TRY(cudaStreamCreateWithFlags(&h->stream, cudaStreamNonBlocking));
+    int r;
+    if ((r = dalloc(&h->type, nmol)) || (r = dalloc(&h->cx, nmol)) || (r = dalloc(&h->cy, nmol)) || (r = dalloc(&h->cz, nmol)) ||
+        (r = dalloc(&h->hist, nh)) || (r = upload(h->type, mol_type, nmol, h->stream)))
+        return r;
+    CUDA_TRY(cudaMemsetAsync(h->hist, 0, sizeof(unsigned long long) * nh, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    return YAMC_OK;
+}
+
+int yamc_rdf_create(int32_t nmol, const int32_t *mol_type, int32_t ntypes, const int32_t *mol_numbers, double dr,
+                    double rmax, int32_t device, yamc_rdf **out) {
+    if (!out) return YAMC_EPARAMETER;
+    *out = nullptr;
+    yamc_rdf *h = new yamc_rdf();
+    const int r = rdf_create_impl(h, nmol, mol_type, ntypes, mol_numbers, dr, rmax, device);
+    if (r) { yamc_rdf_destroy(h); return r; }
+    *out = h;
+    return YAMC_OK;
+}
+
+int yamc_rdf_nbin(yamc_rdf *h, int32_t *nbin) {
+    if (!h || !nbin) return YAMC_EPARAMETER;
+    *nbin = h->nbin;
+    return YAMC_OK;
+}
+
+int yamc_rdf_add_frame(yamc_rdf *h, const double *x, const double *y, const double *z, double box_length) {
+    if (!h || !x || !y || !z || !(box_length > 0)) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(h->device));
+    int r;
+    if ((r = upload(h->cx, x, h->M, h->stream)) || (r = upload(h->cy, y, h->M, h->stream)) ||
+        (r = upload(h->cz, z, h->M, h->stream)))
+        return r;
+    return rdf_frame(h, box_length);
+}
+
+int yamc_rdf_add_ctx(yamc_rdf *h, yamc_ctx *c) {
+    if (!h || !c) return YAMC_EPARAMETER;
+    if (c->device != h->device || c->H.M != h->M) { set_error("the context's device or molecule count differs from the RDF's"); return YAMC_EPARAMETER; }
+    if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
+    CUDA_TRY(cudaSetDevice(h->device));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    k_mol_centres<<<(h->M + 255) / 256, 256, 0, h->stream>>>(c->hsys, h->cx, h->cy, h->cz);
+    CUDA_TRY(cudaGetLastError());
+    return rdf_frame(h, c->H.p.BoxLength);
+}
+
+int yamc_rdf_result(yamc_rdf *h, double *g, double *counts, int32_t *n_frames) {
+    if (!h) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(h->device));
+    const int nt = h->ntypes, nb = h->nbin, npair = nt * nt;
+    std::vector<unsigned long long> hc((size_t)npair * nb + npair);
+    CUDA_TRY(cudaMemcpyAsync(hc.data(), h->hist, sizeof(unsigned long long) * hc.size(), cudaMemcpyDeviceToHost, h->stream));
+    CUDA_TRY(cudaStreamSynchronize(h->stream));
+    if (n_frames) *n_frames = h->n_frame;
+    if (counts)
+        for (size_t k = 0; k < (size_t)npair * nb; ++k) counts[k] = (double)hc[k];
+    if (g) {
+        // save_rdfs (mcrdf2.f90:371-440): g = cnt4 / N_frame / <1/V> / N_i / N_j / dV / factor
+        const double dr = h->dr, four_pi_dr = kFourPi * dr, small_ball = 4.0 / 3.0 * kPi * dr * dr * dr;
+        const double avg_inv_vol = h->n_frame ? h->sum_inv_vol / h->n_frame : 0.0;
+        for (int i = 0; i < nt; ++i)
+            for (int j = 0; j < nt; ++j) {
+                const int off = i * nt + j;
+                double r = 0.0;
+                for (int k = 0; k < nb; ++k) {
+                    double v = 0.0;
+                    if (j >= i && hc[(size_t)npair * nb + off] > 0) {
+                        const double dV = four_pi_dr * (r * r + r * dr) + small_ball;
+                        const double factor = i == j ? 1.0 : 2.0;
+                        v = (double)hc[(size_t)off * nb + k] / h->n_frame / avg_inv_vol / h->mol_numbers[i] /
+                            h->mol_numbers[j] / dV / factor;
+                    }
+                    g[(size_t)off * nb + k] = v;
+                    r = r + dr;
+                }
+            }
+    }
+    return YAMC_OK;
 }
 
 int yamc_volume_eval(yamc_ctx *c, double new_box_length, double *du, int32_t *overlap) {

@@ -173,3 +173,20 @@ def read_freq_file(path: str, nmol: int):
     if np.any(mv < 0):
         raise ValueError(f"read_freq_file: not all frequences defined ({path} is inconsistent with composition?)")
     return mv, xc
+
+
+def write_rdf(prefix: str, r, g, labels=None) -> list:
+    """save_rdfs' files (mcrdf2.f90:371-440): one per species pair t1 <= t2, named
+    prefix + "NN_MM.dat" (two-digit 1-based species numbers) or prefix + "label1_label2.dat",
+    each line "r g(r)" at the bin centres.  Returns the paths written."""
+    nt = g.shape[0]
+    paths = []
+    for i in range(nt):
+        for j in range(i, nt):
+            name = f"{labels[i]}_{labels[j]}" if labels else f"{i + 1:02d}_{j + 1:02d}"
+            path = f"{prefix}{name}.dat"
+            with open(path, "w") as f:
+                for rk, gk in zip(r, g[i, j]):
+                    f.write(f" {rk:24.16E} {gk:24.16E}\n")
+            paths.append(path)
+    return paths
