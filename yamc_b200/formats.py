@@ -190,3 +190,130 @@ def write_rdf(prefix: str, r, g, labels=None) -> list:
                     f.write(f" {rk:24.16E} {gk:24.16E}\n")
             paths.append(path)
     return paths
+
+
+# ---------------------------------------------------------------- trajectory writers
+# store_traj_frame (runmc.f90:373-417): MoleculeTable_calcPositionsOrientations (MoleculeTable.f90:707-769)
+# turns atom positions into molecule centres and ZYZ angles, MoleculeTable_save_binary writes them;
+# frames.dat and boxlength.dat get one row per frame / accepted volume step.
+
+def read_mol_template(path: str):
+    """Molecule_read_from_file + Molecule_centrate (Molecule.f90:142-209): the atom coordinates
+    of a .mol file (Angstrom) relative to its centre of mass, and the masses."""
+    rows = [ln.split() for ln in open(path) if ln.strip()]
+    x = np.array([float(r[1]) for r in rows]); y = np.array([float(r[2]) for r in rows])
+    z = np.array([float(r[3]) for r in rows]); m = np.array([float(r[7]) for r in rows])
+    cx, cy, cz = _center_of_mass(x, y, z, m)
+    return x - cx, y - cy, z - cz, m
+
+
+def _center_of_mass(x, y, z, m):
+    """center_of_mass (geometry.f90:170-201), summed in atom order."""
+    sx = sy = sz = tm = 0.0
+    for i in range(len(m)):
+        sx = sx + m[i] * x[i]; sy = sy + m[i] * y[i]; sz = sz + m[i] * z[i]; tm = tm + m[i]
+    return sx / tm, sy / tm, sz / tm
+
+
+def _atan2_two_pi(y, x):
+    """atan2_two_pi (geometry.f90:204-215)"""
+    r = math.atan2(y, x)
+    return r + TWO_PI if r < 0 else r
+
+
+def _prod_vect(x1, y1, z1, x2, y2, z2):
+    return y1 * z2 - z1 * y2, z1 * x2 - x1 * z2, x1 * y2 - y1 * x2
+
+
+def _inv3(A):
+    """matrix3x3_inv (matrix3x3.f90): adjugate over determinant"""
+    d = (A[0][0] * A[1][1] * A[2][2] + A[0][1] * A[1][2] * A[2][0] + A[0][2] * A[1][0] * A[2][1]
+         - A[0][0] * A[1][2] * A[2][1] - A[0][1] * A[1][0] * A[2][2] - A[0][2] * A[1][1] * A[2][0])
+    B = [[A[1][1] * A[2][2] - A[1][2] * A[2][1], -A[0][1] * A[2][2] + A[0][2] * A[2][1], A[0][1] * A[1][2] - A[0][2] * A[1][1]],
+         [-A[1][0] * A[2][2] + A[1][2] * A[2][0], A[0][0] * A[2][2] - A[0][2] * A[2][0], -A[0][0] * A[1][2] + A[0][2] * A[1][0]],
+         [A[1][0] * A[2][1] - A[1][1] * A[2][0], -A[0][0] * A[2][1] + A[0][1] * A[2][0], A[0][0] * A[1][1] - A[0][1] * A[1][0]]]
+    return [[B[i][j] / d for j in range(3)] for i in range(3)]
+
+
+def xyz_to_angles(tx, ty, tz, xn, yn, zn):
+    """xyz_to_angles (geometry.f90:352-451): the ZYZ angles (theta, phi, psi) of the rotation that
+    takes the template coordinates (tx, ty, tz) to (xn, yn, zn), both relative to the centre and in
+    Angstrom: R = X_new X^-1 from two non-collinear atoms and their cross product
+    (rotation_matrix, :334-350), then ZYZRotation_matrix_to_angles (:221-250); one atom on the
+    centre gives zeros, two atoms or a linear molecule xyz_to_angles_two_atoms (:461-520)."""
+    n = len(tx)
+    i1 = next((i for i in range(n) if abs(tx[i]) + abs(ty[i]) + abs(tz[i]) > 1e-8), -1)
+    if i1 < 0:
+        return 0.0, 0.0, 0.0
+    i2, prod = -1, None
+    for i in range(i1 + 1, n):
+        if abs(tx[i]) + abs(ty[i]) + abs(tz[i]) < 1e-8:
+            continue
+        p = _prod_vect(tx[i1], ty[i1], tz[i1], tx[i], ty[i], tz[i])
+        if abs(p[0]) + abs(p[1]) + abs(p[2]) > 1e-8:
+            i2, prod = i, p
+            break
+    if i2 < 0:
+        x, y, z = tx[i1], ty[i1], tz[i1]
+        dxz = math.sqrt(x ** 2 + z ** 2)
+        alpha = math.atan2(z, -x)
+        v = (math.asin(zn[i1] / dxz) - alpha) / PI_
+        theta = (v - math.floor(v)) * PI_
+        a = x * math.cos(theta) + z * math.sin(theta)
+        beta = math.atan2(y, a)
+        w = (math.atan2(yn[i1], xn[i1]) - beta) / TWO_PI
+        return theta, (w - math.floor(w)) * TWO_PI, 0.0
+    X = [[tx[i1], tx[i2], prod[0]], [ty[i1], ty[i2], prod[1]], [tz[i1], tz[i2], prod[2]]]
+    pn = _prod_vect(xn[i1], yn[i1], zn[i1], xn[i2], yn[i2], zn[i2])
+    Xn = [[xn[i1], xn[i2], pn[0]], [yn[i1], yn[i2], pn[1]], [zn[i1], zn[i2], pn[2]]]
+    Xi = _inv3(X)
+    R = [[sum(Xn[i][k] * Xi[k][j] for k in range(3)) for j in range(3)] for i in range(3)]
+    cos_theta = R[2][2]
+    if abs(cos_theta - 1.0) < 1e-8:
+        return 0.0, _atan2_two_pi(-R[0][1], R[0][0]), 0.0
+    return math.acos(cos_theta), _atan2_two_pi(R[1][2], R[0][2]), _atan2_two_pi(R[2][1], -R[2][0])
+
+
+PI_ = 3.14159265358979323846
+
+
+def traj_frame(x, y, z, first_atom, last_atom, species, templates, box_length):
+    """MoleculeTable_calcPositionsOrientations (MoleculeTable.f90:707-769): per molecule the centre
+    of mass (box units) and the ZYZ angles of its atoms (box units, 1-based inclusive atom ranges)
+    against its species' centred template.  Returns (cx, cy, cz, theta, phi, psi)."""
+    M = len(first_atom)
+    out = [np.zeros(M) for _ in range(6)]
+    for m in range(M):
+        a, b = int(first_atom[m]) - 1, int(last_atom[m])
+        tx, ty, tz, mass = templates[int(species[m])]
+        cx, cy, cz = _center_of_mass(x[a:b], y[a:b], z[a:b], mass)
+        xn = [(v - cx) * box_length for v in x[a:b]]
+        yn = [(v - cy) * box_length for v in y[a:b]]
+        zn = [(v - cz) * box_length for v in z[a:b]]
+        th, ph, ps = xyz_to_angles(tx, ty, tz, xn, yn, zn)
+        for k, v in enumerate((cx, cy, cz, th, ph, ps)):
+            out[k][m] = v
+    return tuple(out)
+
+
+def append_moltab(path: str, x, y, z, theta, phi, psi, nbytes_xyz: int = 3, nbytes_ang: int = 3) -> None:
+    """MoleculeTable_save_binary appended to a trajectory (store_traj_frame seeks to the end)."""
+    tmp = path + ".frame"
+    write_moltab(tmp, x, y, z, theta, phi, psi, nbytes_xyz, nbytes_ang)
+    with open(tmp, "rb") as f, open(path, "ab") as g:
+        g.write(f.read())
+    os.remove(tmp)
+
+
+def format_frames_row(frame: int, box_length: float, n_mv_steps: float, n_mv_accepted: float, n_vol_steps: float,
+                      n_vol_accepted: float, n_xchg_steps: float, n_xchg_accepted: float, wall_time: int) -> str:
+    """frames.dat row, format (I12,F15.10,F12.0,F12.0,F12.0,F12.0,F12.0,F12.0,I12) (runmc.f90:413-414)."""
+    def f0(v):  # F12.0 of a whole count: 11 digits and the point
+        return f"{int(math.floor(float(v) + 0.5)):11d}."
+    return (f"{int(frame):12d}{float(box_length):15.10f}" + "".join(f0(v) for v in (
+        n_mv_steps, n_mv_accepted, n_vol_steps, n_vol_accepted, n_xchg_steps, n_xchg_accepted)) + f"{int(wall_time):12d}")
+
+
+def format_boxlength_row(frame: int, box_length: float) -> str:
+    """boxlength.dat row (store_boxlength, runmc.f90:356-371): the frame and BoxLength."""
+    return f" {int(frame):11d} {float(box_length)!r}"
