@@ -60,3 +60,40 @@ def test_frames_and_boxlength_rows():
     assert vals[0] == "7" and vals[-1] == "1700000000"
     b = formats.format_boxlength_row(3, 39.6)
     assert b.split() == ["3", "39.6"]
+
+
+def test_force_dump_float_format(tmp_path):
+    """write_float / read_float (FloatingPoint.f90): known encodings and the round-trip precision
+    of a 23-bit mantissa; a frame written with append_forces reads back."""
+    assert formats.float_bits(1.0) == (0, 128)            # m = 1, n = 0 (exponent sign bit set for n <= 0)
+    assert formats.float_bits(-2.0) == (2 ** 23, 1)       # negative mantissa, n = 1
+    assert formats.float_bits(0.0) == (0, 255)            # below 1e-14: the underflow code, read back as 0
+    assert formats.float_value(*formats.float_bits(0.0)) == 0.0
+    r = np.random.default_rng(1)
+    for v in np.concatenate([r.normal(size=200) * 10.0 ** r.integers(-8, 8, 200), [1.0, -1.0, 0.5, 3.0]]):
+        back = formats.float_value(*formats.float_bits(float(v)))
+        assert abs(back - v) <= 2.0 ** -22 * abs(v), (v, back)
+    f = r.normal(size=(5, 3)) * 100
+    path = str(tmp_path / "forces.ftraj")
+    formats.append_forces(path, f[:, 0], f[:, 1], f[:, 2], 20.0)
+    formats.append_forces(path, f[:, 0], f[:, 1], f[:, 2], 20.0)
+    back = formats.read_forces(path, 5)
+    assert back.shape == (2, 5, 3)
+    assert np.all(np.abs(back[1] - f / 20.0) <= 2.0 ** -22 * np.abs(f / 20.0))
+
+
+import pytest  # noqa: E402
+
+
+@pytest.mark.gpu
+def test_force_dump_of_adjoint_forces(tmp_path, nacl_files):
+    """mc_calc_forces' dump, fixed: the adjoint forces of yamc_forces (every pair once, no r = 0
+    self pair) written frame by frame with store_forces' format and read back."""
+    eng = api.Engine.from_files(nacl_files)
+    path = str(tmp_path / "forces.ftraj")
+    L = eng.inputs.params.BoxLength
+    f, _, _ = eng.forces()
+    formats.append_forces(path, f[:, 0], f[:, 1], f[:, 2], L)
+    back = formats.read_forces(path, eng.natom)[0]
+    assert np.all(np.isfinite(f))
+    assert np.all(np.abs(back - f / L) <= 2.0 ** -22 * np.abs(f / L) + 1e-300)

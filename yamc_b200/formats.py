@@ -317,3 +317,64 @@ def format_frames_row(frame: int, box_length: float, n_mv_steps: float, n_mv_acc
 def format_boxlength_row(frame: int, box_length: float) -> str:
     """boxlength.dat row (store_boxlength, runmc.f90:356-371): the frame and BoxLength."""
     return f" {int(frame):11d} {float(box_length)!r}"
+
+
+# ---------------------------------------------------------------- force dump (mc_calc_forces)
+# store_forces (mc_calc_forces.f90:350-368) writes per atom fx/L, fy/L, fz/L with write_float
+# (FloatingPoint.f90): a 24-bit mantissa (sign bit + 23 bits) and an 8-bit exponent (sign bit +
+# 7 bits), little-endian, 4 bytes per number.
+LN2 = 0.6931471805599453
+
+
+def _myint(x: float) -> int:
+    """myint (FloatingPoint.f90): truncation toward zero above 0, else toward -inf (with 1e-14)"""
+    return int(x) if x > 0 else int(x - 1.0 + 1e-14)
+
+
+def float_bits(a: float, mantisse_width: int = 24, exp_width: int = 8):
+    """mantisse_exponent_real + mantisse_exponent_bits (FloatingPoint.f90): (mm, nn)."""
+    if abs(a) < float(np.float32(1e-14)):
+        m, n = math.copysign(1.0, a), -1000
+    elif abs(a) > float(np.float32(1e14)):
+        m, n = math.copysign(1.0, a), 1000
+    else:
+        n = _myint(math.log(abs(a)) / LN2)
+        m = a / 2.0 ** n
+    m_scale, n_scale = 2 ** (mantisse_width - 1), 2 ** (exp_width - 1)
+    sgn_m = 0 if m > 0 else 1
+    sgn_n = 0 if n > 0 else 1
+    if abs(n) >= n_scale:
+        return sgn_m * m_scale, sgn_n * n_scale + n_scale - 1
+    return sgn_m * m_scale + int((abs(m) - 1.0) * (m_scale - 1)), sgn_n * n_scale + abs(n)
+
+
+def float_value(mm: int, nn: int, mantisse_width: int = 24, exp_width: int = 8) -> float:
+    """construct_float (FloatingPoint.f90)."""
+    m_scale, n_scale = 2 ** (mantisse_width - 1), 2 ** (exp_width - 1)
+    mm1, sign_m = (mm - m_scale, -1) if mm >= m_scale else (mm, 1)
+    nn1, sign_n = (nn - n_scale, -1) if nn >= n_scale else (nn, 1)
+    if nn1 == n_scale - 1:
+        return 0.0 if sign_n == -1 else 1e14
+    m = mm1 / (m_scale - 1.0) + 1.0
+    return sign_m * m * 2.0 ** (sign_n * nn1)
+
+
+def append_forces(path: str, fx, fy, fz, box_length: float) -> None:
+    """store_forces: one frame of per-atom forces (kT per box length, as yamc_forces gives them)
+    divided by BoxLength, x, y, z per atom, each as write_float's 3 + 1 little-endian bytes."""
+    out = bytearray()
+    for i in range(len(fx)):
+        for v in (fx[i], fy[i], fz[i]):
+            mm, nn = float_bits(float(v) / box_length)
+            out += int(mm).to_bytes(3, "little") + int(nn).to_bytes(1, "little")
+    with open(path, "ab") as f:
+        f.write(bytes(out))
+
+
+def read_forces(path: str, natom: int):
+    """read_float over a force dump: frames x natom x 3."""
+    raw = np.fromfile(path, dtype=np.uint8).reshape(-1, 4)
+    mm = raw[:, 0].astype(np.int64) | (raw[:, 1].astype(np.int64) << 8) | (raw[:, 2].astype(np.int64) << 16)
+    nn = raw[:, 3].astype(np.int64)
+    vals = np.array([float_value(int(a), int(b)) for a, b in zip(mm, nn)])
+    return vals.reshape(-1, natom, 3)
