@@ -183,3 +183,12 @@ def test_npt_resume_and_nvt_entry_refuses(tiny_files):
     assert np.array_equal(a.energies(), b.energies())
     with pytest.raises(_lib.YamcError):
         a.run_chain(buf, 10)
+
+
+@pytest.mark.gpu
+def test_batch_refuses_npt(tiny_files):
+    """Batched replicas run NVT: a replica with volume cycles is refused at creation."""
+    from yamc_b200 import _lib, api
+    inp = api.load_inputs(tiny_files["parameters"], tiny_files["composition"], tiny_files["moltab"], NPT)
+    with pytest.raises(_lib.YamcError):
+        api.Batch([inp])
