@@ -387,7 +387,8 @@ __device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Cand
 // per-warp reduction into red[worker warp][value].  Worker-only barriers (bar 1).
 template <int NT, int EPT, int KIND, bool FORCES, bool MX>
 __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
-                                            const double4 *atom_s, const double *dhs_s, const int2 *meta_s, int *queue,
+                                            const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
+                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
                                             int *nearbuf,
                                             double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
                                             long long *prof) {
@@ -557,7 +558,9 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
                 const int jl = nb[k];
                 const double4 pj = atom_s[jl];
                 const int tj = meta_s[jl].y;
-                const double dj = dhs_s[jl];
+                // hard-core diameter: by LJ type when every atom of a type has the same one
+                // (a shared-memory table), else the atom's own (global memory: atom rank + G jl)
+                const double dj = dhs_typed ? dhs_ts[tj] : dhs_g[grank + gsize * jl];
                 unsigned msk = 0;
                 for (int s = s_lo; s < s_hi; ++s) {
                     const Slot &sl = m.slot[s];
@@ -933,8 +936,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     // shared memory carve-up (chain_smem_bytes on the host computes the same sizes)
     double2 *tab = reinterpret_cast<double2 *>(smem_raw);                     // [2 kMaxA][3][KM]
     double4 *atom_s = reinterpret_cast<double4 *>(tab + 2 * kMaxA * 3 * KM);  // [nown_max]
-    double *dhs_s = reinterpret_cast<double *>(atom_s + A.nown_max);          // [nown_max]
-    int2 *meta_s = reinterpret_cast<int2 *>(dhs_s + A.nown_max);              // [nown_max]
+    int2 *meta_s = reinterpret_cast<int2 *>(atom_s + A.nown_max);             // [nown_max]
     int *queue = reinterpret_cast<int *>(meta_s + A.nown_max);                // [qcap]
     int *nearbuf = queue + ((A.qcap + 1) & ~1);                               // [B/32][32 kCPT]
     double *red = reinterpret_cast<double *>(nearbuf + B * kCPT);             // [B/32][kNV]
@@ -944,14 +946,16 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                                 (long)(sizeof(double2) * 3 * KM + sizeof(double) + sizeof(int)));
     double *xch = red + (B / 32) * kNV;                                       // [2][G][kNV]
     double *lj_s = xch + 2 * G * kNV;                                         // [2][nt*nt]
+    double *dhs_ts = lj_s + 2 * nt * nt;                                      // [nt+1] hard core by LJ type
 
     // atoms of this CTA: j = rank + G * local (interleaved, so every CTA holds a spatial mix)
     const int nown = (D.N - rank + G - 1) / G;
     for (int i = tid; i < nown; i += B) {
         const int j = rank + G * i;
-        atom_s[i] = D.atom[j]; dhs_s[i] = D.dhs[j]; meta_s[i] = D.meta[j];
+        atom_s[i] = D.atom[j]; meta_s[i] = D.meta[j];
     }
     for (int i = tid; i < nt * nt; i += B) { lj_s[i] = D.lj_sig6[i]; lj_s[nt * nt + i] = D.lj_feps[i]; }
+    for (int i = tid; i <= nt; i += B) dhs_ts[i] = D.dhs_t[i];
 
     // the workers' k-vector entries; rho stays in registers for the whole launch
     using Rt = typename Prec<MX>::R;
@@ -1062,7 +1066,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             const int na0 = sh.cand[sh.icur].na;
             // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
             if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
-                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
                 __syncthreads();
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
                 xpar ^= 1;
@@ -1124,8 +1128,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
 
         // ------------------------------------------------ the pass over the new positions
         if (!ctl) {
-            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
-            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_s, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
         } else if (speculate && it + 1 < n_moves) {
             // prepare the next move's candidates while the workers run: lanes 1-2 after the
             // acceptance draw, lane 2 with the molecule in flight at its proposed positions (used

@@ -12,12 +12,15 @@
 namespace yamc {
 
 constexpr int kMaxA = 4;  // atoms per molecule handled on the device
+constexpr int kMaxDevTypes = 8;  // LJ types the device tables hold (the kernels take 1..4)
 
 // ------------------------------------------------------------------ system view
 struct DevSys {
     int N, M, S, nt, kmax, npair, freq_monotone, n_species;
     double rmax2, alpha, xclb, taosp, kext, m2k, dr, d_angle, xlf, xlc, psm, n_store_energy_interval;
     double rpre;           // max(cutoff, largest hard-core diameter), box units: the pair filter's reach
+    double dhs_t[kMaxDevTypes + 1];  // hard-core diameter / L by LJ type (dhs_typed: one value per type)
+    int dhs_typed;
     long long refresh_every;  // mixed form: FP64 recomputation of rho(k) every this many accepted moves (0 = never)
     double4 *atom;         // x, y, z (box units), q
     const int2 *meta;      // 0-based molecule, LJ type (0 = none)

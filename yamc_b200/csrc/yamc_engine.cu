@@ -618,12 +618,12 @@ int upload(T *d, const T *h, size_t n, cudaStream_t s) {
 size_t chain_smem_bytes(int G, int B, int kmax, int nt, int nown_max, int qcap) {
     const int KM = kmax + 1;
     size_t b = sizeof(double2) * 2 * kMaxA * 3 * KM;
-    b += (sizeof(double4) + sizeof(double) + sizeof(int2)) * (size_t)nown_max;
+    b += (sizeof(double4) + sizeof(int2)) * (size_t)nown_max;
     b += sizeof(int) * (size_t)((qcap + 1) & ~1);
     b += sizeof(int) * (size_t)B * kCPT;
     b += sizeof(double) * (size_t)(B / 32) * kNV;
     b += sizeof(double) * (size_t)2 * G * kNV;
-    b += sizeof(double) * (size_t)2 * nt * nt;
+    b += sizeof(double) * ((size_t)2 * nt * nt + nt + 1);
     return b;
 }
 
@@ -901,6 +901,22 @@ int launch_forces_kspace(yamc_ctx *c) {
                                                                                                       c->d_gy, c->d_gz);
     CUDA_TRY(cudaGetLastError());
     return YAMC_OK;
+}
+
+// hard-core diameter / L by LJ type, when every LJ atom of a type has the same one (the chain
+// kernel then keeps the table in shared memory instead of a per-atom array)
+void fill_dhs_types(const HostSystem &H, DevSys &D) {
+    D.dhs_typed = 1;
+    for (int t = 0; t <= kMaxDevTypes; ++t) D.dhs_t[t] = -1.0;
+    for (int i = 0; i < H.N; ++i) {
+        const int t = H.type_by_index[i];
+        if (t <= 0) continue;
+        if (t > kMaxDevTypes) { D.dhs_typed = 0; continue; }
+        if (D.dhs_t[t] < 0) D.dhs_t[t] = H.dhs[i];
+        else if (D.dhs_t[t] != H.dhs[i]) D.dhs_typed = 0;
+    }
+    D.dhs_t[0] = 0.0;
+    for (int t = 1; t <= kMaxDevTypes; ++t) if (D.dhs_t[t] < 0) D.dhs_t[t] = 0.0;
 }
 
 ChainArgs base_args(yamc_ctx *c, int mode) {
@@ -1194,6 +1210,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.refresh_every = P.precision == YAMC_MIXED ? c->refresh_every : 0;
     D.rpre = std::sqrt(P.rmax2);
     for (int i = 0; i < N; ++i) D.rpre = std::max(D.rpre, H.dhs[i]);
+    fill_dhs_types(H, D);
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
@@ -1447,6 +1464,7 @@ static int upload_box(yamc_ctx *c) {
     D.m2k = P.minus_two_kext; D.dr = P.dr; D.d_angle = P.d_angle;
     D.rpre = std::sqrt(P.rmax2);
     for (int i = 0; i < N; ++i) D.rpre = std::max(D.rpre, H.dhs[i]);
+    fill_dhs_types(H, D);
     if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
     c->pos_valid = true;
     return YAMC_OK;
