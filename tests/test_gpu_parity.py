@@ -254,3 +254,28 @@ def test_weighted_molecule_choice(tiny_files, tmp_path, zero):
     assert counts[-4:].mean() > 3 * counts[: n - 4].mean()
     if zero:
         assert counts[3] == 0
+
+
+@pytest.mark.parametrize("layout", ["registers", "streamed"])
+def test_chain_hard_core_per_atom(tmp_path, layout):
+    """Two species sharing one LJ type (same sigma, epsilon) with different hard-core diameters:
+    the chain kernel takes each atom's own diameter (its per-type table does not apply), and
+    overlaps, decisions and dE stay those of the oracle."""
+    from yamc_b200 import formats, systems
+    spec = systems.small_spec(name="hc", n_water=20, n_na=3, n_cl=3, box=10.0)
+    files = systems.write_system(spec, str(tmp_path / "hc"), seed=7)
+    d = files["dir"]
+    na = systems.na_atoms()[0]
+    # Cl becomes Na's LJ twin with the opposite charge and a larger hard core
+    formats.write_mol(f"{d}/Cl_Dang.mol", [formats.MolAtom("Cl", 0.0, 0.0, 0.0, na.sigma, na.epsilon, -1.0, 1.0, 2.8)])
+    o = pyoracle.Oracle(files)
+    assert o.ntype == 2  # O and the shared ion type
+    glog, olog = None, None
+    eng = api.Engine.from_files(files)
+    eng.set_kspace_layout(LAYOUTS[layout])
+    buf = grng.gfortran_stream(71, 400000)
+    glog, _, gcur, done, st = eng.run_chain(buf, 4000)
+    olog, _, ocur = o.run_mc(buf, 4000)
+    assert st == 0 and done == 4000 and gcur == ocur
+    compare_logs(glog, olog)
+    assert ((olog["flags"] & 2) != 0).any()  # the hard core is exercised
