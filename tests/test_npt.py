@@ -192,3 +192,30 @@ def test_batch_refuses_npt(tiny_files):
     inp = api.load_inputs(tiny_files["parameters"], tiny_files["composition"], tiny_files["moltab"], NPT)
     with pytest.raises(_lib.YamcError):
         api.Batch([inp])
+
+
+@pytest.mark.gpu
+def test_npt_mixed_precision(tiny_files):
+    """The mixed form with volume and exchange steps: the volume steps' full sums are FP64, the
+    chain's moves mixed; the running energies stay on an FP64 recomputation of the configuration
+    and the cycle structure follows the FP64 run up to the first decision the dE error flips."""
+    from yamc_b200 import _lib, api
+    buf = grng.gfortran_stream(61, 400000)
+    runs = {}
+    for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
+        eng = api.Engine.from_files(tiny_files, extra=NPT, precision=prec)
+        eng.set_xchange_weights(np.full(eng.nmol, 0.2))
+        log, vlog, rows, cur, done, st = eng.run_mc(buf, 20)
+        assert st == 0 and done == 20
+        runs[prec] = (log, vlog, eng)
+    lf, vf, ef = runs[_lib.YAMC_FP64]
+    lm, vm, em = runs[_lib.YAMC_MIXED]
+    n = min(len(lf), len(lm))
+    same = (lf["imol"][:n] == lm["imol"][:n]) & (lf["flags"][:n] == lm["flags"][:n])
+    k = n if same.all() else int(np.argmin(same))
+    assert k > 50
+    du_f = sum(lf[c][:k] for c in DU)
+    du_m = sum(lm[c][:k] for c in DU)
+    assert np.abs(du_f - du_m).max() <= 1e-4
+    e_inc, e_full = em.energies(), em.full_sums()
+    assert abs(e_inc[0] - e_full[0]) <= 1e-3 * max(1.0, abs(e_full[0]))
