@@ -224,10 +224,11 @@ int yamc_get_params(yamc_ctx *ctx, yamc_params *p);
    init_freq with the exchange column of a frequencies file (runmc.f90:25-173): weights[nmol]
    give xchange_freq (BiasedRandom_init) and the probability Sxch / (Smv + Sxch) that a move
    step of run_mc is an exchange step (Smv: the move weights' sum).  With a positive
-   probability yamc_run_mc reads each move's exchange draw on the host and runs exchange steps
-   there (two molecules from xchange_freq, different, swap their centres of mass; acceptance by
-   MonteCarloMove_accept_or_decline_simple) and movemc steps as one-move chain launches; their
-   records have flags bit2 set, imol = the first molecule and the second in flags bits 8..31.
+   probability the chain kernel stops before each exchange step (its exchange draw below the
+   probability) and yamc_run_mc runs the step on the host (two molecules from xchange_freq,
+   different, swap their centres of mass; acceptance by MonteCarloMove_accept_or_decline_simple)
+   before relaunching the chain; exchange records have flags bit2 set, imol = the first
+   molecule and the second in flags bits 8..31.
    yamc_run_chain refuses a context with exchange steps on. */
 int yamc_set_xchange_weights(yamc_ctx *ctx, const double *weights);
 /* The exchange step as a drop-in for the body of mc_xchange, for a host that draws its own

@@ -21,6 +21,7 @@ struct DevSys {
     double rpre;           // max(cutoff, largest hard-core diameter), box units: the pair filter's reach
     double dhs_t[kMaxDevTypes + 1];  // hard-core diameter / L by LJ type (dhs_typed: one value per type)
     int dhs_typed;
+    double xprob;          // probability of an exchange step (the chain stops before one; 0 = none)
     long long refresh_every;  // mixed form: FP64 recomputation of rho(k) every this many accepted moves (0 = never)
     double4 *atom;         // x, y, z (box units), q
     const int2 *meta;      // 0-based molecule, LJ type (0 = none)

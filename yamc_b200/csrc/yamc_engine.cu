@@ -1211,6 +1211,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.rpre = std::sqrt(P.rmax2);
     for (int i = 0; i < N; ++i) D.rpre = std::max(D.rpre, H.dhs[i]);
     fill_dhs_types(H, D);
+    D.xprob = 0.0;
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
@@ -1806,6 +1807,11 @@ int yamc_set_xchange_weights(yamc_ctx *c, const double *w) {
     for (int i = 0; i < M; ++i) nz += w[i] > 0;
     if (S > 0 && nz < 2) { set_error("exchange steps need at least two molecules with a positive weight"); return YAMC_EPARAMETER; }
     H.xchange_probability = S / (H.smv + S);
+    CUDA_TRY(cudaSetDevice(c->device));
+    c->hsys.xprob = H.xchange_probability;
+    int r = upload(c->d_sys, &c->hsys, 1, c->stream);
+    if (r) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
     return YAMC_OK;
 }
 
@@ -2051,86 +2057,85 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
             *cursor = c0;  // a move cycle: the chain kernel takes the cycle's draw itself
         }
         if (H.xchange_probability > 0) {
-            // exchange steps on: the host reads each move's draws (the cycle's pressure draw at
-            // its start, the exchange draw); an exchange step runs here, a movemc step as a
-            // one-move chain launch that takes those draws itself (runmc.f90:228-272)
+            // exchange steps on: the chain kernel runs the cycle's movemc steps and stops before an
+            // exchange step (its exchange draw below the probability) as it stops at the end of
+            // the stream; the host then reads that step's draws (the cycle's pressure draw at its
+            // start, the exchange draw, the two molecules) and runs it (runmc.f90:228-272)
             bool cycle_done = false;
             while (!cycle_done && st == YAMC_OK) {
+                const int64_t n = H.M - c->cnt_h[CN_MOVE_IN_CYCLE];
+                const bool keep = log && nlog + n <= max_log;
+                const bool want_row = rows && nrow < max_rows;
+                int64_t mdone = 0;
+                int32_t kr = 0;
+                int ks = run_chain_impl(c, c->d_rng, base, n_rng, cursor, n, &mdone, keep ? c->d_log : nullptr,
+                                        want_row ? c->d_rows : nullptr, want_row ? 1 : 0, &kr);
+                if (ks != YAMC_OK && ks != YAMC_ERNG_EXHAUSTED) return ks;
+                if (keep && mdone)
+                    CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record) * mdone, cudaMemcpyDeviceToHost));
+                if (keep) nlog += mdone;
+                if (want_row && kr) {
+                    CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9, cudaMemcpyDeviceToHost));
+                    ++nrow;
+                }
+                if ((r = pull_state(c))) return r;
+                if (ks == YAMC_OK) { cycle_done = true; break; }
+                // stopped: the end of the stream, or an exchange step next
                 const int64_t c0 = *cursor;
                 const bool at_start = c->cnt_h[CN_MOVE_IN_CYCLE] == 0;
                 double u = 0, xd = 0;
-                if ((at_start && !host_rand(rng, n_rng, cursor, &u)) || !host_rand(rng, n_rng, cursor, &xd)) {
+                if ((at_start && !host_rand(rng, n_rng, cursor, &u)) || !host_rand(rng, n_rng, cursor, &xd) ||
+                    !(xd < H.xchange_probability)) {
                     *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
                 }
-                if (xd < H.xchange_probability) {
-                    double r1 = 0, r2 = 0;
-                    bool out = !host_rand(rng, n_rng, cursor, &r1);
-                    const int imol1 = out ? 1 : host_choose(H.xfreq_beg, H.xfreq_end, r1);
-                    int imol2 = imol1;
-                    while (!out && imol2 == imol1) {
-                        out = !host_rand(rng, n_rng, cursor, &r2);
-                        if (!out) imol2 = host_choose(H.xfreq_beg, H.xfreq_end, r2);
+                double r1 = 0, r2 = 0;
+                bool out = !host_rand(rng, n_rng, cursor, &r1);
+                const int imol1 = out ? 1 : host_choose(H.xfreq_beg, H.xfreq_end, r1);
+                int imol2 = imol1;
+                while (!out && imol2 == imol1) {
+                    out = !host_rand(rng, n_rng, cursor, &r2);
+                    if (!out) imol2 = host_choose(H.xfreq_beg, H.xfreq_end, r2);
+                }
+                if (out) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
+                double du[4];
+                int ov = 0;
+                if ((r = xchange_eval(c, imol1, imol2, du, &ov))) return r;
+                bool acc = false;
+                if (!ov) {  // MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597)
+                    const double factor = std::exp(-(du[0] + (du[1] + du[2]) + du[3]));
+                    double xk = 0;
+                    if (!host_rand(rng, n_rng, cursor, &xk)) {
+                        xchange_commit(c, false);
+                        *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
                     }
-                    if (out) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
-                    double du[4];
-                    int ov = 0;
-                    if ((r = xchange_eval(c, imol1, imol2, du, &ov))) return r;
-                    bool acc = false;
-                    if (!ov) {  // MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597)
-                        const double factor = std::exp(-(du[0] + (du[1] + du[2]) + du[3]));
-                        double xk = 0;
-                        if (!host_rand(rng, n_rng, cursor, &xk)) {
-                            xchange_commit(c, false);
-                            *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
-                        }
-                        acc = !(xk > factor);
-                    }
-                    if ((r = xchange_commit(c, acc))) return r;
-                    if (log && nlog < max_log) {
-                        yamc_move_record &rec = log[nlog++];
-                        rec.imol = imol1; rec.flags = (acc ? 1 : 0) | (ov ? 2 : 0) | 4 | (imol2 << 8); rec.cursor = *cursor;
-                        rec.du_real = du[0]; rec.du_k_coul = du[1]; rec.du_k_lj = du[2]; rec.du_ext = du[3];
-                    }
-                    c->sc[SC_N_MV_STEPS] += 1;
-                    if (acc) c->sc[SC_N_MV_ACC] += 1;
-                    long long mic = c->cnt_h[CN_MOVE_IN_CYCLE] + 1;
-                    if (mic == H.M) {
-                        mic = 0;
-                        const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
-                        if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && nrow < max_rows) {
-                            double e[8];
-                            energies_from(c->sc, H.p.kext, e);
-                            double *row = rows + 9 * (size_t)nrow;
-                            row[0] = (double)c->cnt_h[CN_ICYCLE];
-                            for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
-                            ++nrow;
-                        }
-                        c->cnt_h[CN_ICYCLE] += 1;
-                        cycle_done = true;
-                    }
-                    c->cnt_h[CN_MOVE_IN_CYCLE] = mic;
-                    if ((r = push_state(c))) return r;
-                    CUDA_TRY(cudaStreamSynchronize(c->stream));
-                } else {
-                    *cursor = c0;
-                    const bool keep = log && nlog < max_log;
-                    const bool want_row = rows && nrow < max_rows;
-                    int64_t mdone = 0;
-                    int32_t kr = 0;
-                    st = run_chain_impl(c, c->d_rng, base, n_rng, cursor, 1, &mdone, keep ? c->d_log : nullptr,
-                                        want_row ? c->d_rows : nullptr, want_row ? 1 : 0, &kr);
-                    if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
-                    if (keep && mdone) {
-                        CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record), cudaMemcpyDeviceToHost));
-                        ++nlog;
-                    }
-                    if (want_row && kr) {
-                        CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9, cudaMemcpyDeviceToHost));
+                    acc = !(xk > factor);
+                }
+                if ((r = xchange_commit(c, acc))) return r;
+                if (log && nlog < max_log) {
+                    yamc_move_record &rec = log[nlog++];
+                    rec.imol = imol1; rec.flags = (acc ? 1 : 0) | (ov ? 2 : 0) | 4 | (imol2 << 8); rec.cursor = *cursor;
+                    rec.du_real = du[0]; rec.du_k_coul = du[1]; rec.du_k_lj = du[2]; rec.du_ext = du[3];
+                }
+                c->sc[SC_N_MV_STEPS] += 1;
+                if (acc) c->sc[SC_N_MV_ACC] += 1;
+                long long mic = c->cnt_h[CN_MOVE_IN_CYCLE] + 1;
+                if (mic == H.M) {
+                    mic = 0;
+                    const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
+                    if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && nrow < max_rows) {
+                        double e[8];
+                        energies_from(c->sc, H.p.kext, e);
+                        double *row = rows + 9 * (size_t)nrow;
+                        row[0] = (double)c->cnt_h[CN_ICYCLE];
+                        for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
                         ++nrow;
                     }
-                    if ((r = pull_state(c))) return r;
-                    cycle_done = mdone == 1 && c->cnt_h[CN_MOVE_IN_CYCLE] == 0;
+                    c->cnt_h[CN_ICYCLE] += 1;
+                    cycle_done = true;
                 }
+                c->cnt_h[CN_MOVE_IN_CYCLE] = mic;
+                if ((r = push_state(c))) return r;
+                CUDA_TRY(cudaStreamSynchronize(c->stream));
             }
             if (st == YAMC_ERNG_EXHAUSTED) break;
             ++done;
