@@ -36,8 +36,8 @@ METRIC = "MC trial moves/s (SPC/E+NaCl Ewald); mixed vs FP64 GPU at |ΔE err|≤
 
 # DRAM bytes per move of the chain kernel in the timed shape (mixed, streamed, cluster of 2 x 384
 # threads) from the ncu capture of one 1,000-move launch on nacl1m (dram__bytes_read.sum +
-# dram__bytes_write.sum = 1.145 MB), used for roofline.traffic
-TRAFFIC_PER_MOVE = 1145.0
+# dram__bytes_write.sum = 1.094 MB), used for roofline.traffic
+TRAFFIC_PER_MOVE = 1094.0
 
 
 def dist_env():
