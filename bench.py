@@ -201,7 +201,8 @@ def run_reference(args, files, spec_name):
 
 def target_block(local, rank, moves=2000, steps=3, warmup=2):
     """The north-star comparison on 4096 SPC/E + 76 Na + 76 Cl (12,440 atoms, L = 50 A,
-    alpha = 0.28/A, rc = 12 A, kmax = 15): one plain FP64 chain (unbiased moves, the drop-in)
+    alpha = 0.28/A, rc = 12 A, kmax = 15, the configuration of force-biased moves): one plain FP64
+    chain (the drop-in) with the configuration's force-biased moves, and one with unbiased moves,
     against a batch of mixed-precision force-biased chains (lambda = 0.1), all resident at once,
     with the mixed chains' dE against FP64 chains on the same random stream."""
     import torch
@@ -228,6 +229,20 @@ def target_block(local, rank, moves=2000, steps=3, warmup=2):
     del s0
     # dE of mixed vs FP64 force-biased chains on the same stream
     fb = systems.write_system(spec_b, base + "_b0", seed=5)
+    # one plain FP64 chain with the configuration's own move set (force-biased, lambda = 0.1)
+    eng = api.Engine.from_files(fb, device=local)
+    s1 = torch.from_numpy(grng.gfortran_stream(98, 60 * moves * (steps + warmup) + 10000)).to(dev)
+    cur = 0
+    ms = []
+    for w in range(warmup + steps):
+        cur, done, st = eng.run_chain_device(s1.data_ptr(), s1.numel(), moves, cursor=cur)
+        assert st == 0 and done == moves
+        if w >= warmup:
+            ms.append(eng.last_kernel_ms)
+    plain_fb = moves * steps / (sum(ms) / 1e3)
+    plain_fb_launch = eng.launch
+    eng.close()
+    del s1
     n_chk = 1500
     chk = grng.gfortran_stream(4243, 60 * n_chk + 10000)
     logs = {}
@@ -268,10 +283,15 @@ def target_block(local, rank, moves=2000, steps=3, warmup=2):
             ms.append(b.last_kernel_ms)
     batched = R * moves * steps / (sum(ms) / 1e3)
     out = {"workload": "nacl4k: 4096 SPC/E + 76 Na + 76 Cl, 12440 atoms, L=50 A, alpha=0.28/A, rc=12 A, kmax=15",
-           "plain_fp64_one_chain": {"value": plain, "unit": "moves/s", "launch": plain_launch},
+           "plain_fp64_one_chain": {"value": plain, "unit": "moves/s", "launch": plain_launch,
+                                    "moves": "unbiased"},
+           "plain_fp64_one_chain_force_biased": {"value": plain_fb, "unit": "moves/s", "launch": plain_fb_launch,
+                                                 "moves": "force-biased, lambda = 0.1 (the configuration's move set)"},
            "mixed_batched_force_biased": {"value": batched, "unit": "moves/s", "chains": R, "launch": b.launch,
                                           "lambda": 0.1},
-           "ratio": batched / plain,
+           # the target's ratio, the same move set on both sides; and against the unbiased plain chain
+           "ratio": batched / plain_fb,
+           "ratio_vs_unbiased_plain": batched / plain,
            "de_error_mixed_vs_fp64_force_biased": {"max_kT": float(de.max()), "moves_compared": k},
            "moves_per_step_per_chain": moves, "steps": steps}
     b.close()
