@@ -193,7 +193,9 @@ int yamc_run_chain_device(yamc_ctx *ctx, const float *d_rng, int64_t n_rng, int6
 /* ---- NPT: volume moves (mcvol, MC.f90:701-825) ----
    yamc_run_mc is run_mc (runmc.f90:178-334) by cycles, with the volume cycles of an NPT run
    (pressure_step_multiplier > 0): each cycle draws rnd = rand()*(psm+1); when psm > 0 and
-   rnd > psm the cycle is one volume step, otherwise nmol movemc calls on the device.  A volume
+   rnd > psm the cycle is one volume step, otherwise nmol movemc calls on the device (the chain
+   kernel runs the move steps and stops before a volume cycle or an exchange step, which the
+   host runs).  A volume
    step draws lambda, scales the box (scale_box, scale_box.f90:6-62), recomputes the parameters,
    the LJ tables and beta_LJ for the new length, scales beta by xclb_new/xclb_old, redoes the
    full sums on the device and takes the Metropolis test

@@ -766,13 +766,14 @@ __device__ inline void stage_molecule(const ChooseCtx &X, ChainShared &sh, Cand 
 
 // run_mc's draws before movemc: the per-cycle pressure draw, the exchange draw, the molecule
 // draw (runmc.f90:206, 232, 258).  Returns the 1-based molecule, or 0 when the stream ran out or
-// the exchange draw makes this step an exchange step (the chain then stops before it, like at
-// the end of the stream, and the host runs the exchange).
+// the draws make this step an exchange step or the cycle a volume cycle (the chain then stops
+// before it, like at the end of the stream, and the host runs it).
 __device__ inline int draw_molecule(const DevSys &D, RngReader &rng, bool cycle_start) {
-    if (cycle_start) (void)rng.next();
+    const double pd = cycle_start ? rng.next() : 0.0;
     const double xd = rng.next();
     const double r = rng.next();
     if (rng.out || xd < D.xprob) return 0;
+    if (cycle_start && D.psm > 0 && pd * (D.psm + 1) > D.psm) return 0;  // a volume cycle: the host runs it
     return choose_molecule_guess(r, D.freq_beg, D.freq_end, D.M, D.freq_monotone);
 }
 

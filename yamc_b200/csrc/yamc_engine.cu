@@ -1990,6 +1990,21 @@ int yamc_get_params(yamc_ctx *c, yamc_params *p) {
     return YAMC_OK;
 }
 
+// energy.dat row at the end of a cycle the host ran (runmc.f90:276-279), then the next cycle
+static void host_cycle_end(yamc_ctx *c, double *rows, int32_t max_rows, int32_t *nrow) {
+    const HostSystem &H = c->H;
+    const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
+    if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && *nrow < max_rows) {
+        double e[8];
+        energies_from(c->sc, H.p.kext, e);
+        double *row = rows + 9 * (size_t)*nrow;
+        row[0] = (double)c->cnt_h[CN_ICYCLE];
+        for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
+        ++*nrow;
+    }
+    c->cnt_h[CN_ICYCLE] += 1;
+}
+
 int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_cycles, int64_t *cycles_done,
                 yamc_move_record *log, int64_t max_log, int64_t *n_log, yamc_volume_record *vlog, int64_t max_vlog,
                 int64_t *n_vlog, double *rows, int32_t max_rows, int32_t *n_rows) {
@@ -2008,157 +2023,115 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
         c->rng_cap = nr;
     }
     if (nr) CUDA_TRY(cudaMemcpyAsync(c->d_rng, rng + base, nr * sizeof(float), cudaMemcpyHostToDevice, c->stream));
-    if (log && (size_t)H.M > c->log_cap) {
+    // device buffers for a launch's records and rows (a launch runs at most log_cap moves when logging)
+    const size_t want_log = (size_t)std::max<int64_t>(H.M, std::min<int64_t>(n_cycles * (int64_t)H.M, 1 << 20));
+    if (log && want_log > c->log_cap) {
         if (c->d_log) cudaFree(c->d_log);
         c->d_log = nullptr;
         c->log_cap = 0;
-        if ((r = dalloc(&c->d_log, (size_t)H.M))) return r;
-        c->log_cap = (size_t)H.M;
+        if ((r = dalloc(&c->d_log, want_log))) return r;
+        c->log_cap = want_log;
     }
-    if (rows && c->rows_cap < 1) {
-        if ((r = dalloc(&c->d_rows, 9))) return r;
-        c->rows_cap = 1;
+    if (rows && max_rows > c->rows_cap) {
+        if (c->d_rows) cudaFree(c->d_rows);
+        c->d_rows = nullptr;
+        c->rows_cap = 0;
+        if ((r = dalloc(&c->d_rows, (size_t)9 * max_rows))) return r;
+        c->rows_cap = max_rows;
     }
     int64_t done = 0, nlog = 0, nvlog = 0;
     int32_t nrow = 0;
     int st = YAMC_OK;
     if ((r = pull_state(c))) return r;
-    const double psm = H.p.pressure_step_multiplier;
-    for (int64_t cyc = 0; cyc < n_cycles; ++cyc) {
-        if (c->cnt_h[CN_MOVE_IN_CYCLE] == 0) {
-            // the cycle's draw (runmc.f90:206-207): above pressure_step_multiplier, a volume step
-            const int64_t c0 = *cursor;
-            double u;
-            if (!host_rand(rng, n_rng, cursor, &u)) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
-            if (psm > 0 && u * (psm + 1) > psm) {
-                yamc_volume_record vr{};
-                vr.cycle = c->cnt_h[CN_ICYCLE];
-                r = volume_step(c, rng, n_rng, cursor, &vr);
-                if (r == YAMC_ERNG_EXHAUSTED) { *cursor = c0; st = r; break; }
-                if (r) return r;
-                if (vr.flags & 1) c->n_vol_accepted += 1;
-                c->sc[SC_N_VOL_STEPS] += 1;
-                if (vlog && nvlog < max_vlog) vlog[nvlog++] = vr;
-                // energy.dat row at the cycle's end (runmc.f90:276-279)
-                const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
-                if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && nrow < max_rows) {
-                    double e[8];
-                    energies_from(c->sc, H.p.kext, e);
-                    double *row = rows + 9 * (size_t)nrow;
-                    row[0] = (double)c->cnt_h[CN_ICYCLE];
-                    for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
-                    ++nrow;
-                }
-                c->cnt_h[CN_ICYCLE] += 1;
-                if ((r = push_state(c))) return r;
-                ++done;
-                continue;
-            }
-            *cursor = c0;  // a move cycle: the chain kernel takes the cycle's draw itself
-        }
-        if (H.xchange_probability > 0) {
-            // exchange steps on: the chain kernel runs the cycle's movemc steps and stops before an
-            // exchange step (its exchange draw below the probability) as it stops at the end of
-            // the stream; the host then reads that step's draws (the cycle's pressure draw at its
-            // start, the exchange draw, the two molecules) and runs it (runmc.f90:228-272)
-            bool cycle_done = false;
-            while (!cycle_done && st == YAMC_OK) {
-                const int64_t n = H.M - c->cnt_h[CN_MOVE_IN_CYCLE];
-                const bool keep = log && nlog + n <= max_log;
-                const bool want_row = rows && nrow < max_rows;
-                int64_t mdone = 0;
-                int32_t kr = 0;
-                int ks = run_chain_impl(c, c->d_rng, base, n_rng, cursor, n, &mdone, keep ? c->d_log : nullptr,
-                                        want_row ? c->d_rows : nullptr, want_row ? 1 : 0, &kr);
-                if (ks != YAMC_OK && ks != YAMC_ERNG_EXHAUSTED) return ks;
-                if (keep && mdone)
-                    CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record) * mdone, cudaMemcpyDeviceToHost));
-                if (keep) nlog += mdone;
-                if (want_row && kr) {
-                    CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9, cudaMemcpyDeviceToHost));
-                    ++nrow;
-                }
-                if ((r = pull_state(c))) return r;
-                if (ks == YAMC_OK) { cycle_done = true; break; }
-                // stopped: the end of the stream, or an exchange step next
-                const int64_t c0 = *cursor;
-                const bool at_start = c->cnt_h[CN_MOVE_IN_CYCLE] == 0;
-                double u = 0, xd = 0;
-                if ((at_start && !host_rand(rng, n_rng, cursor, &u)) || !host_rand(rng, n_rng, cursor, &xd) ||
-                    !(xd < H.xchange_probability)) {
-                    *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
-                }
-                double r1 = 0, r2 = 0;
-                bool out = !host_rand(rng, n_rng, cursor, &r1);
-                const int imol1 = out ? 1 : host_choose(H.xfreq_beg, H.xfreq_end, r1);
-                int imol2 = imol1;
-                while (!out && imol2 == imol1) {
-                    out = !host_rand(rng, n_rng, cursor, &r2);
-                    if (!out) imol2 = host_choose(H.xfreq_beg, H.xfreq_end, r2);
-                }
-                if (out) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
-                double du[4];
-                int ov = 0;
-                if ((r = xchange_eval(c, imol1, imol2, du, &ov))) return r;
-                bool acc = false;
-                if (!ov) {  // MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597)
-                    const double factor = std::exp(-(du[0] + (du[1] + du[2]) + du[3]));
-                    double xk = 0;
-                    if (!host_rand(rng, n_rng, cursor, &xk)) {
-                        xchange_commit(c, false);
-                        *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
-                    }
-                    acc = !(xk > factor);
-                }
-                if ((r = xchange_commit(c, acc))) return r;
-                if (log && nlog < max_log) {
-                    yamc_move_record &rec = log[nlog++];
-                    rec.imol = imol1; rec.flags = (acc ? 1 : 0) | (ov ? 2 : 0) | 4 | (imol2 << 8); rec.cursor = *cursor;
-                    rec.du_real = du[0]; rec.du_k_coul = du[1]; rec.du_k_lj = du[2]; rec.du_ext = du[3];
-                }
-                c->sc[SC_N_MV_STEPS] += 1;
-                if (acc) c->sc[SC_N_MV_ACC] += 1;
-                long long mic = c->cnt_h[CN_MOVE_IN_CYCLE] + 1;
-                if (mic == H.M) {
-                    mic = 0;
-                    const double fr = c->sc[SC_N_MV_STEPS] / H.M + c->sc[SC_N_VOL_STEPS];
-                    if (std::fmod(fr, H.p.n_store_energy_interval) < 1e-10 && rows && nrow < max_rows) {
-                        double e[8];
-                        energies_from(c->sc, H.p.kext, e);
-                        double *row = rows + 9 * (size_t)nrow;
-                        row[0] = (double)c->cnt_h[CN_ICYCLE];
-                        for (int k = 0; k < 8; ++k) row[1 + k] = e[k];
-                        ++nrow;
-                    }
-                    c->cnt_h[CN_ICYCLE] += 1;
-                    cycle_done = true;
-                }
-                c->cnt_h[CN_MOVE_IN_CYCLE] = mic;
-                if ((r = push_state(c))) return r;
-                CUDA_TRY(cudaStreamSynchronize(c->stream));
-            }
-            if (st == YAMC_ERNG_EXHAUSTED) break;
+    const double psm = H.p.pressure_step_multiplier, xprob = H.xchange_probability;
+    // The chain kernel runs stretches of movemc steps and stops before a volume cycle or an
+    // exchange step (and at the end of the stream); the host reads the draws that decide what
+    // comes next (runmc.f90:206-259) and runs volume and exchange steps itself.
+    while (done < n_cycles) {
+        const int64_t c0 = *cursor;
+        const bool at_start = c->cnt_h[CN_MOVE_IN_CYCLE] == 0;
+        double u = 0, xd = 1.0;
+        bool out = at_start && !host_rand(rng, n_rng, cursor, &u);
+        if (!out && at_start && psm > 0 && u * (psm + 1) > psm) {
+            // a volume cycle (mcvol, MC.f90:701-825)
+            yamc_volume_record vr{};
+            vr.cycle = c->cnt_h[CN_ICYCLE];
+            r = volume_step(c, rng, n_rng, cursor, &vr);
+            if (r == YAMC_ERNG_EXHAUSTED) { *cursor = c0; st = r; break; }
+            if (r) return r;
+            if (vr.flags & 1) c->n_vol_accepted += 1;
+            c->sc[SC_N_VOL_STEPS] += 1;
+            if (vlog && nvlog < max_vlog) vlog[nvlog++] = vr;
+            host_cycle_end(c, rows, max_rows, &nrow);
+            if ((r = push_state(c))) return r;
             ++done;
             continue;
         }
-        const int64_t n = H.M - c->cnt_h[CN_MOVE_IN_CYCLE];
-        const bool keep_log = log && nlog + n <= max_log;
-        const bool want_row = rows && nrow < max_rows;
+        if (!out && xprob > 0) out = !host_rand(rng, n_rng, cursor, &xd);
+        if (out) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
+        if (xprob > 0 && xd < xprob) {
+            // an exchange step (mc_xchange, MC.f90:1325-1954): two different molecules from xchange_freq
+            double r1 = 0, r2 = 0;
+            out = !host_rand(rng, n_rng, cursor, &r1);
+            const int imol1 = out ? 1 : host_choose(H.xfreq_beg, H.xfreq_end, r1);
+            int imol2 = imol1;
+            while (!out && imol2 == imol1) {
+                out = !host_rand(rng, n_rng, cursor, &r2);
+                if (!out) imol2 = host_choose(H.xfreq_beg, H.xfreq_end, r2);
+            }
+            if (out) { *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break; }
+            double du[4];
+            int ov = 0;
+            if ((r = xchange_eval(c, imol1, imol2, du, &ov))) return r;
+            bool acc = false;
+            if (!ov) {  // MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597)
+                const double factor = std::exp(-(du[0] + (du[1] + du[2]) + du[3]));
+                double xk = 0;
+                if (!host_rand(rng, n_rng, cursor, &xk)) {
+                    xchange_commit(c, false);
+                    *cursor = c0; st = YAMC_ERNG_EXHAUSTED; break;
+                }
+                acc = !(xk > factor);
+            }
+            if ((r = xchange_commit(c, acc))) return r;
+            if (log && nlog < max_log) {
+                yamc_move_record &rec = log[nlog++];
+                rec.imol = imol1; rec.flags = (acc ? 1 : 0) | (ov ? 2 : 0) | 4 | (imol2 << 8); rec.cursor = *cursor;
+                rec.du_real = du[0]; rec.du_k_coul = du[1]; rec.du_k_lj = du[2]; rec.du_ext = du[3];
+            }
+            c->sc[SC_N_MV_STEPS] += 1;
+            if (acc) c->sc[SC_N_MV_ACC] += 1;
+            const long long mic = c->cnt_h[CN_MOVE_IN_CYCLE] + 1;
+            c->cnt_h[CN_MOVE_IN_CYCLE] = mic == H.M ? 0 : mic;
+            if (mic == H.M) { host_cycle_end(c, rows, max_rows, &nrow); ++done; }
+            if ((r = push_state(c))) return r;
+            CUDA_TRY(cudaStreamSynchronize(c->stream));
+            continue;
+        }
+        // a stretch of movemc steps: every move of the cycles still to run, or fewer when logging
+        *cursor = c0;
+        int64_t n = (n_cycles - done) * (int64_t)H.M - c->cnt_h[CN_MOVE_IN_CYCLE];
+        const bool keep = log && nlog < max_log;
+        if (keep) n = std::min<int64_t>(n, std::min<int64_t>((int64_t)c->log_cap, max_log - nlog));
+        const bool want_rows = rows && nrow < max_rows;
+        const long long icycle0 = c->cnt_h[CN_ICYCLE];
         int64_t mdone = 0;
         int32_t kr = 0;
-        st = run_chain_impl(c, c->d_rng, base, n_rng, cursor, n, &mdone, keep_log ? c->d_log : nullptr,
-                            want_row ? c->d_rows : nullptr, want_row ? 1 : 0, &kr);
-        if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
-        if (keep_log && mdone)
+        const int ks = run_chain_impl(c, c->d_rng, base, n_rng, cursor, n, &mdone, keep ? c->d_log : nullptr,
+                                      want_rows ? c->d_rows : nullptr, want_rows ? max_rows - nrow : 0, &kr);
+        if (ks != YAMC_OK && ks != YAMC_ERNG_EXHAUSTED) return ks;
+        if (keep && mdone)
             CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record) * mdone, cudaMemcpyDeviceToHost));
-        if (keep_log) nlog += mdone;
-        if (want_row && kr) {
-            CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9, cudaMemcpyDeviceToHost));
-            ++nrow;
+        if (keep) nlog += mdone;
+        if (want_rows && kr) {
+            CUDA_TRY(cudaMemcpy(rows + 9 * (size_t)nrow, c->d_rows, sizeof(double) * 9 * kr, cudaMemcpyDeviceToHost));
+            nrow += kr;
         }
         if ((r = pull_state(c))) return r;
-        if (st == YAMC_ERNG_EXHAUSTED) break;
-        ++done;
+        done += c->cnt_h[CN_ICYCLE] - icycle0;
+        // stopped with no move done although the next step is neither a volume cycle nor an
+        // exchange step (both were read above): the stream ran out inside that move
+        if (ks == YAMC_ERNG_EXHAUSTED && mdone == 0) { st = YAMC_ERNG_EXHAUSTED; break; }
     }
     if (cycles_done) *cycles_done = done;
     if (n_log) *n_log = nlog;
