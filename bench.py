@@ -2,16 +2,22 @@
 
 Workload (default): 2048 SPC/E + 38 Na+ + 38 Cl- (6,220 atoms), L = 39.6 A,
 alpha = 0.30/A, rc = 12 A, kmax = 12 (1,068 half-space / 3,796 signed k),
-dispersion-Ewald LJ, plain FP64 method, unbiased moves (0.15 A ball, 0.15 rad),
-synthetic jittered-lattice start, gfortran random stream.  One step = one
-device-resident run_mc segment of --moves moves on one independent chain per GPU
-(replicas only: the Markov chain does not shard).
+dispersion-Ewald LJ, unbiased moves (0.15 A ball, 0.15 rad), synthetic
+jittered-lattice starts, gfortran random streams.  One step = one batch graph
+launch that advances every chain of a GPU by --moves moves: as many independent
+chains as the launch shapes keep resident (replicas only: a Markov chain does not
+shard), the launch shape picked by the batch autotuner.
 
-  value  moves/s with the random stream already in HBM, CUDA events around each
-         persistent-kernel launch, L2 flushed (256 MB write) between steps
-  e2e    the same through yamc_run_chain with the stream in pinned host memory,
-         host->device copy of each step's stream window and device->host read of
-         the step result inside the timed region
+  value  moves/s of the mixed-precision form with the random streams already in
+         HBM, CUDA events around each launch, L2 flushed (256 MB write) between
+         steps; config.fp64 the plain FP64 form on the same batch, and the mixed
+         form's dE, force and total-energy error against FP64
+  e2e    the same through yamc_batch_run with the streams in pinned host memory,
+         host->device copy of each step's stream windows and device->host read of
+         every chain's energies inside the timed region
+  blocks north_star_target (4096 SPC/E + NaCl, mixed batched force-biased against
+         the plain FP64 chain), batch_ragged_96 (96 ragged replicas), npt_run_mc
+         (NPT run_mc with volume steps), cpu_baseline (the oracle on one core)
   --impl reference  the CPU restatement of the reference (oracle/, -O3) timed on
          the host cores: independent chains, one per core
 """

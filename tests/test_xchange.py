@@ -152,3 +152,20 @@ def test_xchange_per_step_api(spce_files):
     from yamc_b200 import _lib
     with pytest.raises(_lib.YamcError):
         eng.xchange_commit(True)  # nothing pending
+
+
+@pytest.mark.gpu
+def test_batch_replica_refuses_exchange_and_volume_steps(tiny_files):
+    """A batch replica is run by the batch's graph (NVT moves): exchange weights, exchange and
+    volume steps and run_mc are refused on it."""
+    from yamc_b200 import _lib, api
+    inp = api.load_inputs(tiny_files["parameters"], tiny_files["composition"], tiny_files["moltab"])
+    b = api.Batch([inp, inp])
+    rep = b.replica(0)
+    with pytest.raises(_lib.YamcError):
+        rep.set_xchange_weights(np.full(rep.nmol, 0.3))
+    with pytest.raises(_lib.YamcError):
+        rep.xchange_eval(1, 2)
+    with pytest.raises(_lib.YamcError):
+        rep.volume_eval(10.5)
+    b.close()

@@ -680,6 +680,7 @@ struct yamc_ctx {
     // NPT volume move: rho(k) as it was before the step, accepted volume steps
     double2 *rho_save = nullptr;
     double n_vol_accepted = 0;
+    bool in_batch = false;  // a batch replica: the batch's graph runs it (NVT, no exchange steps)
     int vol_stage = 0;  // 1 between yamc_volume_eval and yamc_volume_commit
     // exchange step between yamc_xchange_eval and yamc_xchange_commit (1 evaluated, 2 overlap)
     int xch_stage = 0;
@@ -1788,6 +1789,7 @@ static int host_choose(const std::vector<double> &beg, const std::vector<double>
 
 int yamc_set_xchange_weights(yamc_ctx *c, const double *w) {
     if (!c || !w) return YAMC_EPARAMETER;
+    if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
     HostSystem &H = c->H;
     const int M = H.M;
     double S = 0;
@@ -1818,6 +1820,7 @@ int yamc_set_xchange_weights(yamc_ctx *c, const double *w) {
 int yamc_xchange_eval(yamc_ctx *c, int32_t imol1, int32_t imol2, double du[4], int32_t *overlap) {
     if (!c || !du || !overlap || imol1 < 1 || imol2 < 1 || imol1 > c->H.M || imol2 > c->H.M || imol1 == imol2)
         return YAMC_EPARAMETER;
+    if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
     if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
     int ov = 0;
@@ -1953,7 +1956,7 @@ int yamc_rdf_result(yamc_rdf *h, double *g, double *counts, int32_t *n_frames) {
                 double r = 0.0;
                 for (int k = 0; k < nb; ++k) {
                     double v = 0.0;
-                    if (j >= i && hc[(size_t)npair * nb + off] > 0) {
+                    if (j >= i && h->n_frame > 0 && hc[(size_t)npair * nb + off] > 0) {
                         const double dV = four_pi_dr * (r * r + r * dr) + small_ball;
                         const double factor = i == j ? 1.0 : 2.0;
                         v = (double)hc[(size_t)off * nb + k] / h->n_frame / avg_inv_vol / h->mol_numbers[i] /
@@ -1969,6 +1972,7 @@ int yamc_rdf_result(yamc_rdf *h, double *g, double *counts, int32_t *n_frames) {
 
 int yamc_volume_eval(yamc_ctx *c, double new_box_length, double *du, int32_t *overlap) {
     if (!c || !du || !overlap || !(new_box_length > 0)) return YAMC_EPARAMETER;
+    if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
     if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
     int ov = 0;
@@ -2009,6 +2013,7 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
                 yamc_move_record *log, int64_t max_log, int64_t *n_log, yamc_volume_record *vlog, int64_t max_vlog,
                 int64_t *n_vlog, double *rows, int32_t max_rows, int32_t *n_rows) {
     if (!c || !rng || !cursor || n_cycles < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
+    if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
     if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
     HostSystem &H = c->H;
@@ -2293,6 +2298,7 @@ static int batch_create_impl(yamc_batch *b, int32_t n, const yamc_system *system
             set_error("replica " + std::to_string(i) + ": " + last_error());
             return r;
         }
+        c->in_batch = true;
         b->reps.push_back(c);
     }
     for (int i = 0; i < n; ++i) {
