@@ -143,6 +143,13 @@ def test_npt_run_mc_matches_oracle_spce256(spce_files):
 
 
 @pytest.mark.gpu
+def test_npt_run_mc_matches_oracle_spce256_tutorial_setting(spce_files):
+    """The reference tutorial's pressure_step_multiplier (5) over 120 cycles (~28,000 moves)."""
+    _npt_compare(spce_files, 120, 34, extra="pressure_step_multiplier=5,max_volume_scaling=1.01,"
+                                             "n_store_energy_interval=5")
+
+
+@pytest.mark.gpu
 def test_npt_force_biased(tiny_biased_files):
     _npt_compare(tiny_biased_files, 30, 33)
 
