@@ -169,3 +169,23 @@ def test_batch_replica_refuses_exchange_and_volume_steps(tiny_files):
     with pytest.raises(_lib.YamcError):
         rep.volume_eval(10.5)
     b.close()
+
+
+@pytest.mark.gpu
+def test_run_mc_without_log_is_the_same_run(tiny_files):
+    """run_mc with and without records (without, the chain runs every remaining move of the
+    requested cycles in one stretch): the same cursor, rows and energies."""
+    from yamc_b200 import api
+    buf = grng.gfortran_stream(88, 400000)
+    out = []
+    for log in (True, False):
+        eng = api.Engine.from_files(tiny_files, extra="pressure_step_multiplier=3,max_volume_scaling=1.02,"
+                                                      "n_store_energy_interval=1")
+        eng.set_xchange_weights(np.full(eng.nmol, 0.2))
+        _, vlog, rows, cur, done, st = eng.run_mc(buf, 40, log=log, max_rows=40)
+        assert st == 0 and done == 40
+        out.append((cur, vlog, rows, eng.energies()))
+    assert out[0][0] == out[1][0]
+    assert np.array_equal(out[0][1], out[1][1])
+    assert np.array_equal(out[0][2], out[1][2])
+    assert np.array_equal(out[0][3], out[1][3])
