@@ -189,3 +189,9 @@ def test_run_mc_without_log_is_the_same_run(tiny_files):
     assert np.array_equal(out[0][1], out[1][1])
     assert np.array_equal(out[0][2], out[1][2])
     assert np.array_equal(out[0][3], out[1][3])
+
+
+@pytest.mark.gpu
+def test_xchange_ions_nacl1m(nacl_files):
+    """Ion exchanges in the 6,220-atom system (the realistic use: swapping Na+ and Cl- positions)."""
+    _compare(nacl_files, _ion_weights, 3, 54)
