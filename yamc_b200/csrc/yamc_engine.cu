@@ -2476,6 +2476,8 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     const int Ls[] = {YAMC_KSPACE_REGISTERS, YAMC_KSPACE_STREAMED};
     std::vector<int64_t> cur(R), done(R), off(R, 0);
     double total = 0.0;
+    struct Shape { double eff; int G, B, L; };
+    std::vector<std::vector<Shape>> shapes(b->groups.size());  // every shape that fits, per group
     // every group on its own (the others run no moves): the shape with its highest moves/s
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         BatchGroup &g = b->groups[gi];
@@ -2503,6 +2505,7 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
                     const int nrep = (int)g.idx.size();
                     const double sms = (double)std::min(nrep, g.max_clusters) * G;
                     const double eff = rate / sms;
+                    shapes[gi].push_back({eff, G, B, L});
                     if (eff > best) { best = eff; bG = G; bB = B; bL = L; brate = rate; }
                 }
         if (best < 0) {
@@ -2514,9 +2517,48 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
         g.fG = bG; g.fB = bB; g.fL = bL;
         total += brate;
     }
+    // then the groups together: the whole batch's moves/s (its slowest group sets the time) with
+    // each group's next shapes by moves/s per SM in turn, a change kept when the batch gains 2 %
+    auto whole = [&](double *rate) -> int {
+        for (size_t i = 0; i < R; ++i) cur[i] = cursors[i];
+        int s2 = batch_step(b, d_rng, off.data(), n_rng, cur.data(), n_moves, done.data(), nullptr, nullptr, -1);
+        const int rr = batch_copy_state(b, keep, false);
+        if (rr) return rr;
+        if (s2 != YAMC_OK && s2 != YAMC_ERNG_EXHAUSTED) return s2;
+        double moves = 0;
+        for (size_t i = 0; i < R; ++i) moves += (double)done[i];
+        *rate = b->last_ms > 0 ? moves / (1e-3 * b->last_ms) : 0.0;
+        return YAMC_OK;
+    };
+    if ((r = batch_configure(b))) return r;
+    double best_total = 0;
+    if ((r = whole(&best_total))) return r;
+    constexpr int kAlternatives = 3;
+    for (size_t gi = 0; gi < b->groups.size(); ++gi) {
+        BatchGroup &g = b->groups[gi];
+        std::vector<Shape> &cand = shapes[gi];
+        std::sort(cand.begin(), cand.end(), [](const Shape &a, const Shape &c) { return a.eff > c.eff; });
+        int tried = 0;
+        for (const Shape &sh : cand) {
+            if (tried >= kAlternatives) break;
+            if (sh.G == g.fG && sh.B == g.fB && sh.L == g.fL) continue;
+            const int k0 = g.fG, k1 = g.fB, k2 = g.fL;
+            g.fG = sh.G; g.fB = sh.B; g.fL = sh.L;
+            ++tried;
+            double t = 0;
+            if (batch_configure(b) == YAMC_OK && g.cfg.G == sh.G && g.cfg.B == sh.B && (r = whole(&t)) == YAMC_OK &&
+                t > 1.02 * best_total) {
+                best_total = t;
+                continue;
+            }
+            if (r != YAMC_OK) return r;
+            g.fG = k0; g.fB = k1; g.fL = k2;
+            if ((r = batch_configure(b))) return r;
+        }
+    }
     r = batch_configure(b);
     for (yamc_ctx *c : b->reps) c->pos_valid = false;
-    if (best_moves_per_s) *best_moves_per_s = total;
+    if (best_moves_per_s) *best_moves_per_s = best_total > 0 ? best_total : total;
     return r;
 }
 
