@@ -333,8 +333,8 @@ int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng,
    cluster size x threads per block) that fits its replicas on n_moves moves of
    each and keeps the one with the most moves/s per SM it occupies (the groups
    share the GPU); then, with all groups running together, tries each group's next
-   three shapes in turn and keeps a change when the whole batch's moves/s rises by
-   2 %.  The replicas' state is put back after every trial, so the chains do not
+   three shapes by that measure and its three fastest shapes alone, keeping a change
+   when the whole batch's moves/s rises by 2 %.  The replicas' state is put back after every trial, so the chains do not
    advance.  best_moves_per_s: the whole batch's moves/s with the chosen shapes. */
 int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng,
                     const int64_t *cursors, int64_t n_moves, double *best_moves_per_s);

@@ -2476,7 +2476,7 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     const int Ls[] = {YAMC_KSPACE_REGISTERS, YAMC_KSPACE_STREAMED};
     std::vector<int64_t> cur(R), done(R), off(R, 0);
     double total = 0.0;
-    struct Shape { double eff; int G, B, L; };
+    struct Shape { double eff, rate; int G, B, L; };
     std::vector<std::vector<Shape>> shapes(b->groups.size());  // every shape that fits, per group
     // every group on its own (the others run no moves): the shape with its highest moves/s
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
@@ -2505,7 +2505,7 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
                     const int nrep = (int)g.idx.size();
                     const double sms = (double)std::min(nrep, g.max_clusters) * G;
                     const double eff = rate / sms;
-                    shapes[gi].push_back({eff, G, B, L});
+                    shapes[gi].push_back({eff, rate, G, B, L});
                     if (eff > best) { best = eff; bG = G; bB = B; bL = L; brate = rate; }
                 }
         if (best < 0) {
@@ -2518,7 +2518,8 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
         total += brate;
     }
     // then the groups together: the whole batch's moves/s (its slowest group sets the time) with
-    // each group's next shapes by moves/s per SM in turn, a change kept when the batch gains 2 %
+    // each group's next shapes by moves/s per SM, then its fastest shapes alone (a group that
+    // sets the batch's time gains from more SMs per chain), a change kept when the batch gains 2 %
     auto whole = [&](double *rate) -> int {
         for (size_t i = 0; i < R; ++i) cur[i] = cursors[i];
         int s2 = batch_step(b, d_rng, off.data(), n_rng, cur.data(), n_moves, done.data(), nullptr, nullptr, -1);
@@ -2536,11 +2537,20 @@ int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_r
     constexpr int kAlternatives = 3;
     for (size_t gi = 0; gi < b->groups.size(); ++gi) {
         BatchGroup &g = b->groups[gi];
-        std::vector<Shape> &cand = shapes[gi];
-        std::sort(cand.begin(), cand.end(), [](const Shape &a, const Shape &c) { return a.eff > c.eff; });
+        std::vector<Shape> by_eff = shapes[gi], by_rate = shapes[gi];
+        std::sort(by_eff.begin(), by_eff.end(), [](const Shape &a, const Shape &c) { return a.eff > c.eff; });
+        std::sort(by_rate.begin(), by_rate.end(), [](const Shape &a, const Shape &c) { return a.rate > c.rate; });
+        std::vector<Shape> cand;
+        auto add = [&](const Shape &x) {
+            for (const Shape &y : cand)
+                if (y.G == x.G && y.B == x.B && y.L == x.L) return;
+            cand.push_back(x);
+        };
+        for (size_t k = 0; k < by_eff.size() && (int)k < kAlternatives + 1; ++k) add(by_eff[k]);
+        for (size_t k = 0; k < by_rate.size() && (int)k < kAlternatives; ++k) add(by_rate[k]);
         int tried = 0;
         for (const Shape &sh : cand) {
-            if (tried >= kAlternatives) break;
+            if (tried >= 2 * kAlternatives) break;
             if (sh.G == g.fG && sh.B == g.fB && sh.L == g.fL) continue;
             const int k0 = g.fG, k1 = g.fB, k2 = g.fL;
             g.fG = sh.G; g.fB = sh.B; g.fL = sh.L;
