@@ -106,6 +106,16 @@ def test_chain_matches_oracle_nacl(nacl_files):
     assert rel_close(eng.energies(), o.energies(), 1e-9)
 
 
+def test_chain_matches_oracle_nacl1m_1e5(nacl_files):
+    """The benchmark's system (2048 SPC/E + 38 Na + 38 Cl): the identical accept/reject sequence
+    over 1e5 moves (about a minute of the oracle)."""
+    o, olog, ocur, eng, glog, gcur = _run_pair(nacl_files, 100000, seed=2026)
+    compare_logs(glog, olog)
+    assert gcur == ocur
+    assert rel_close(eng.energies(), o.energies(), 1e-9)
+    assert rel_close(eng.full_sums(), o.full_sums(), 1e-9)
+
+
 def compare_biased(glog, olog):
     assert np.array_equal(glog["imol"], olog["imol"]) and np.array_equal(glog["flags"], olog["flags"])
     assert np.array_equal(glog["cursor"], olog["cursor"])
