@@ -38,8 +38,8 @@ def main(argv):
         t0 = time.perf_counter()
         rdf.add_engine(eng)
         tr.append(time.perf_counter() - t0)
-    print(f"{name}: {eng.natom} atoms, {eng.nmol} molecules: exchange step {1e3 * min(tx):.3f} ms (best of {nx}), "
-          f"RDF frame {1e3 * min(tr):.3f} ms (best of {nr})")
+    best = lambda t: f"{1e3 * min(t):.3f} ms (best of {len(t)})" if t else "not run"
+    print(f"{name}: {eng.natom} atoms, {eng.nmol} molecules: exchange step {best(tx)}, RDF frame {best(tr)}")
 
 
 if __name__ == "__main__":
