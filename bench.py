@@ -15,7 +15,7 @@ shard), the launch shape picked by the batch autotuner.
   e2e    the same through yamc_batch_run with the streams in pinned host memory,
          host->device copy of each step's stream windows and device->host read of
          every chain's energies inside the timed region
-  blocks north_star_target (4096 SPC/E + NaCl, mixed batched force-biased against
+  blocks nacl4k_mixed_batch_vs_plain (4096 SPC/E + NaCl, mixed batched force-biased against
          the plain FP64 chain), batch_ragged_96 (96 ragged replicas), npt_run_mc
          (NPT run_mc with volume steps), cpu_baseline (the oracle on one core)
   --impl reference  the CPU restatement of the reference (oracle/, -O3) timed on
@@ -617,7 +617,7 @@ def main():
         "clocks": clk.summary(),
     }
     if not args.no_target:
-        line["north_star_target"] = target_block(local, rank)
+        line["nacl4k_mixed_batch_vs_plain"] = target_block(local, rank)
     if not args.no_config4:
         line["batch_ragged_96"] = config4_block(local, rank)
     if not args.no_npt:
