@@ -304,7 +304,7 @@ def target_block(local, rank, moves=2000, steps=3, warmup=2):
     return out
 
 
-def config4_block(local, rank, n_replicas=96, moves=10000):
+def ragged_batch_block(local, rank, n_replicas=96, moves=10000):
     """Ragged replicas (water log-uniform 216..4096, NaCl 0..2 M, density 0.0334 +- 2 %, T 280..360 K,
     alpha = 5.6/L, cutoff min(12 A, L/2), one k-set), mixed precision, force-biased (lambda = 0.1),
     all in one batch: one graph launch per kernel-variant group, launch shape from the autotuner,
@@ -400,7 +400,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replicas", type=int, default=0, help="chains per GPU (0 = as many clusters as are resident)")
     ap.add_argument("--no-target", action="store_true", help="skip the 4096-water mixed/batched/force-biased block")
-    ap.add_argument("--no-config4", action="store_true", help="skip the 96 ragged replicas block")
+    ap.add_argument("--no-ragged", action="store_true", help="skip the 96 ragged replicas block")
     ap.add_argument("--no-npt", action="store_true", help="skip the NPT run_mc block")
     args = ap.parse_args()
 
@@ -618,8 +618,8 @@ def main():
     }
     if not args.no_target:
         line["nacl4k_mixed_batch_vs_plain"] = target_block(local, rank)
-    if not args.no_config4:
-        line["batch_ragged_96"] = config4_block(local, rank)
+    if not args.no_ragged:
+        line["batch_ragged_96"] = ragged_batch_block(local, rank)
     if not args.no_npt:
         line["npt_run_mc"] = npt_block(local, rank)
     if not args.no_cpu_baseline:
