@@ -655,6 +655,9 @@ struct yamc_ctx {
     DevSys *d_sys = nullptr;
     RunSlot *d_run = nullptr;
     double *api_in = nullptr, *api_out = nullptr;
+    // pinned staging of the per-move calls: api_out, then scal, then cnt, read back in one
+    // round trip per call
+    double *h_pin = nullptr;
     float *d_rng = nullptr;
     size_t rng_cap = 0;
     yamc_move_record *d_log = nullptr;
@@ -1157,6 +1160,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->api_in, 1 + 3 * kMaxA)) ||
         (r = dalloc(&c->api_out, kNV)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
+    CUDA_TRY(cudaMallocHost(&c->h_pin, sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT));
     // full-sum work split: atom-tile pairs of the real-space sum; atom slices of rho(k) so that
     // entry blocks x slices cover the SMs about twice
     int nsm = 148;
@@ -1244,6 +1248,7 @@ int yamc_destroy(yamc_ctx *c) {
                     c->tpairs, c->rho_part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
                     c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save};
     for (void *p : ptrs) if (p) cudaFree(p);
+    if (c->h_pin) cudaFreeHost(c->h_pin);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -2152,16 +2157,23 @@ int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
     CUDA_TRY(cudaSetDevice(c->device));
     int r = ensure_cfg(c);
     if (r) return r;
-    if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
+    if ((r = sync_positions(c))) return r;
     double in[1 + 3 * kMaxA] = {};
     in[0] = imol;
     if ((r = upload(c->api_in, in, 1 + 3 * kMaxA, c->stream))) return r;
     RunSlot rs{};
     if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
     if ((r = launch_chain(c, base_args(c, MODE_OLD)))) return r;
-    double out[kNV];
-    CUDA_TRY(cudaMemcpyAsync(out, c->api_out, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    // the kernel reads the scalars and counters without changing them: one read-back of its
+    // outputs and of the state the next calls use
+    double *pin = c->h_pin;
+    CUDA_TRY(cudaMemcpyAsync(pin, c->api_out, sizeof(double) * kNV, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(pin + kNV, c->scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(pin + kNV + SC_COUNT, c->cnt, sizeof(long long) * CN_COUNT, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const double *out = pin;
+    std::memcpy(c->sc, pin + kNV, sizeof(double) * SC_COUNT);
+    std::memcpy(c->cnt_h, pin + kNV + SC_COUNT, sizeof(long long) * CN_COUNT);
     const HostSystem &H = c->H;
     const int f0 = H.first[imol - 1], na = H.natoms[imol - 1];
     for (int k = 0; k < 3; ++k) c->api_eold[k] = out[k];
@@ -2190,9 +2202,9 @@ int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn
     int r = upload(c->api_in, in, 1 + 3 * kMaxA, c->stream);
     if (r) return r;
     if ((r = launch_chain(c, base_args(c, MODE_EVAL)))) return r;
-    double out[kNV];
-    CUDA_TRY(cudaMemcpyAsync(out, c->api_out, sizeof(out), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->h_pin, c->api_out, sizeof(double) * kNV, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    const double *out = c->h_pin;
     for (int v = 0; v < kNV; ++v) c->api_new[v] = out[v];
     for (int a = 0; a < na; ++a) { c->api_xn[a] = xn[a]; c->api_yn[a] = yn[a]; c->api_zn[a] = zn[a]; }
     const int ovl = out[RV_OVL] > 0.0;
@@ -2249,8 +2261,9 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     c->sc[SC_EK_C] += c->api_new[RV_DUC];
     c->sc[SC_EK_LJ] += c->api_new[RV_DUL];
     c->sc[SC_MU_X] += c->api_dmu[0]; c->sc[SC_MU_Y] += c->api_dmu[1]; c->sc[SC_MU_Z] += c->api_dmu[2];
+    // the copies come from pageable memory, staged before they return: nothing to wait for here,
+    // the next call on the stream is ordered after them
     if ((r = push_state(c))) return r;
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
     c->api_stage = 0;
     return YAMC_OK;
 }
