@@ -94,6 +94,15 @@ def algorithmic_bytes_per_move(spec, nk, nsigned, ntype, p_acc):
     return real + rho + beta + kidx + commit
 
 
+def algorithmic_flops_per_move(spec, nsigned, ntype):
+    """Floating-point work of an unbiased move at least: real-space pairs at the old and the
+    new positions (2 n_m N_nb pairs at 60 flop each, sqrt/exp/divide counted as one) and the
+    k-space energy, S (2 n_m 14 + 6 (1 + T^2)) flop; n_m = mean atoms of a chosen molecule."""
+    nnb = spec.natom / spec.box ** 3 * 4.0 / 3.0 * math.pi * spec.rc ** 3
+    n_m = spec.natom / spec.nmol
+    return 2 * n_m * nnb * 60 + nsigned * (2 * n_m * 14 + 6 * (1 + ntype * ntype))
+
+
 class Clocks:
     """nvidia-smi sampling of SM clock and throttle reasons during the timed region."""
 
@@ -592,6 +601,9 @@ def main():
     moves_launch = R * args.moves
     achieved = bpm * moves_launch / (ms_launch / 1e3) / 1e9
     peak, which = peaks()
+    fpm = algorithmic_flops_per_move(spec, v0.nsigned, v0.ntype)
+    fp_achieved = fpm * moves_launch / (ms_launch / 1e3) / 1e12
+    p64, p32 = api.fma_peak(local, True), api.fma_peak(local, False)
     launch = b.launch
     line = {
         "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
@@ -611,7 +623,11 @@ def main():
                    "single_chain": single, "resident_clusters_by_cluster_size": resident},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": TRAFFIC_PER_MOVE * moves_launch, "peak_source": which,
-                     "algorithmic_bytes_per_move": bpm},
+                     "algorithmic_bytes_per_move": bpm,
+                     "fp_pipe": {"algorithmic_flops_per_move": fpm, "achieved_tflops": fp_achieved,
+                                 "fp64_fma_peak_tflops": p64, "fp32_fma_peak_tflops": p32,
+                                 "frac_of_fp64": fp_achieved / p64, "frac_of_fp32": fp_achieved / p32,
+                                 "peak_source": "measured live (yamc_fma_peak)"}},
         "e2e": {"value": e2e, "unit": "moves/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": int(sum(launch_counts)),
         "clocks": clk.summary(),

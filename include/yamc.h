@@ -384,6 +384,15 @@ int yamc_realspace_sums_static(const yamc_params *p, int32_t natom, const double
                                const double *sigma6_tab, const double *four_eps_tab, double *uu,
                                double *fx, double *fy, double *fz, double *sums, void *stream);
 
+/* ---- measurement ----
+   No counterpart in the reference.  The FP64 (fp64 != 0) or FP32 fused-multiply-add
+   throughput of GPU `device` in TFLOP/s (2 flops per FMA), measured: independent FMA
+   recurrences on every SM, the median of 5 timed launches of about 10-20 ms after one
+   warm-up.  The trial move is not a contraction, so this -- not the tensor-core peak --
+   is the compute roofline of the chain kernel.  Allocates and frees a few MB of device
+   memory and its own stream; synchronous. */
+int yamc_fma_peak(int32_t device, int32_t fp64, double *tflops);
+
 #ifdef __cplusplus
 }
 #endif

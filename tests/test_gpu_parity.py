@@ -289,3 +289,12 @@ def test_chain_hard_core_per_atom(tmp_path, layout):
     assert st == 0 and done == 4000 and gcur == ocur
     compare_logs(glog, olog)
     assert ((olog["flags"] & 2) != 0).any()  # the hard core is exercised
+
+
+def test_fma_peak_measures_the_pipes():
+    """yamc_fma_peak: both pipes give a finite positive rate, FP32 at least that of FP64."""
+    p64, p32 = api.fma_peak(0, True), api.fma_peak(0, False)
+    assert 0.5 < p64 < 500.0 and 0.5 < p32 < 500.0, (p64, p32)
+    assert p32 >= p64, (p64, p32)
+    with pytest.raises(_lib.YamcError):
+        api.fma_peak(-1, True)

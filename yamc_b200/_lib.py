@@ -140,6 +140,7 @@ SIGNATURES = {
     "yamc_batch_last_launches": (ctypes.c_int, [_VP, _ip]),
     "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +
                                    [ctypes.c_int32] + [_VP] * 8),
+    "yamc_fma_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _dp]),
     "yamc_error_string": (ctypes.c_char_p, [ctypes.c_int]),
     "yamc_last_error_detail": (ctypes.c_char_p, []),
 }

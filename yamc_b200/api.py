@@ -100,6 +100,13 @@ def load_inputs(parameters: str, composition: str, moltab: str, extra: str = "")
         lib.yamc_inputs_free(h)
 
 
+def fma_peak(device: int = 0, fp64: bool = True) -> float:
+    """Measured FP64 (or FP32) FMA throughput of ``device`` in TFLOP/s (yamc_fma_peak)."""
+    t = ctypes.c_double()
+    check(_lib.load().yamc_fma_peak(int(device), 1 if fp64 else 0, ctypes.byref(t)), "yamc_fma_peak")
+    return t.value
+
+
 class Engine:
     """initmc + movemc + run_mc of one system on one GPU."""
 

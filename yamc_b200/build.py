@@ -14,7 +14,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libyamc_b200.so")
 SOURCES = ["yamc_chain_t1.cu", "yamc_chain_t2.cu", "yamc_chain_t3.cu", "yamc_chain_t4.cu", "yamc_engine.cu",
-           "yamc_static.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
+           "yamc_static.cu", "yamc_peaks.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
 HEADERS = ["yamc_chain.cuh", "yamc_device.cuh", "yamc_internal.h", os.path.join("..", "..", "include", "yamc.h")]
 
 NVCC_FLAGS = [
