@@ -4,8 +4,9 @@
  * The engine replaces the body of the reference's MC module (MC.f90): initmc,
  * movemc and mc_total_energy, and the run_mc loop that calls movemc
  * (runmc.f90:178-334).  A Fortran host binds these entry points through
- * ISO_C_BINDING (the interface module is given in INTEGRATION.md); the
- * Python package yamc_b200 binds them through ctypes.
+ * ISO_C_BINDING (an interface module of BIND(C) declarations, one per entry
+ * point, with the structs below as BIND(C) derived types); the Python package
+ * yamc_b200 binds them through ctypes.
  *
  * Conventions (as in the reference): coordinates in box units (-0.5..0.5),
  * energies in kT, molecule numbers 1-based, atoms stored molecule by molecule.
@@ -373,10 +374,12 @@ int yamc_batch_last_launches(yamc_batch *b, int32_t *n);
    and bad_type (1 when some lj_type is outside 0..n_types; those atoms get no LJ).
    Asynchronous on `stream` (a cudaStream_t, NULL = default stream): read the
    outputs after that stream has finished.  natom above YAMC_STATIC_MAX_ATOMS is
-   rejected with YAMC_ELIMITS.  The first call on a device looks up the static
-   array's device address (cudaGetSymbolAddress) and should come before any stream
-   capture.  Every call on a device shares the one scratch array: calls that
-   overlap on the GPU (other streams, other host threads) race on it. */
+   rejected with YAMC_ELIMITS.  Every call looks up the static array's device
+   address in the current context (cudaGetSymbolAddress, which allocates nothing),
+   so a device reset between calls is followed; the first call on a device loads
+   the library's device code and should come before any stream capture.  Every
+   call on a device shares the one scratch array: calls that overlap on the GPU
+   (other streams, other host threads) race on it. */
 #define YAMC_STATIC_MAX_ATOMS 262144
 int yamc_realspace_sums_static(const yamc_params *p, int32_t natom, const double *x, const double *y,
                                const double *z, const double *charge, const int32_t *mol,

@@ -1,0 +1,106 @@
+"""The oracle and the GPU engine against the reference's own tutorial run (statistical pin).
+
+The reference ships the outputs of its tutorial's NPT run of 100 SPC/E + 5 Na + 5 Cl at 300 K
+and 1 bar (energy.dat, boxlength.dat, RDF_*.dat; fixture golden/tutorial_npt.json).  Its
+initial configuration and seed are not shipped, so the pin is statistical: the same inputs are
+run here from seeded lattice starts, and every compared quantity of the reference must lie
+within 4 run-to-run standard deviations of the runs' mean (tutorial.z_score).  Exchange steps
+play no part: the shipped parameters.prm names no frequencies file (freq_file = 'none').
+
+* CPU: the oracle, 6 runs of 3,000 cycles in parallel processes, compared with the reference
+  over cycles 500-3,000: U_total, U_total_ew, U_total_lj, uu_ew, E_k_coulomb (energy.dat rows)
+  and the time-averaged box length (the compression from 15.42 A toward 14.8 A happens here).
+* GPU: yamc_run_mc, 5 runs of the full 10,000 cycles, compared over cycles 2,000-10,000, plus
+  mcrdf2's g(r) over the run's 100 frames (every 100 cycles, from the device positions through
+  yamc_rdf_add_ctx): the first peak of water-water, water-Na, water-Cl and Na-Cl within one
+  bin (0.1 A) of the reference's and its height within 4 standard deviations.
+"""
+import multiprocessing as mp
+from concurrent.futures import ProcessPoolExecutor
+
+import numpy as np
+import pytest
+
+import tutorial as T
+
+NSIG = 4.0
+
+
+def _compare(ref: dict, runs: list, where: str):
+    report = []
+    for k, v in ref.items():
+        ours = [r[k] for r in runs]
+        z = T.z_score(v, ours)
+        report.append((k, v, float(np.mean(ours)), float(np.std(ours, ddof=1)), z))
+    text = "\n".join(f"{where} {k}: reference {v:.4f}, ours {m:.4f} +- {s:.4f} (sd), z = {z:.2f}"
+                     for k, v, m, s, z in report)
+    print(text)
+    assert all(z < NSIG for *_, z in report), text
+    return report
+
+
+def test_fixture_is_the_reference_run():
+    g = T.GOLD
+    rows = np.asarray(g["energy"])
+    assert rows.shape == (100, 9) and rows[0, 0] == 100 and rows[-1, 0] == 10000
+    # energy.dat's totals are the sums of its parts (store_energy: mc_total_energy, U_total_ew,
+    # U_total_lj): U_total = U_total_ew + U_total_lj to the printed digits
+    assert np.allclose(rows[:, 1], rows[:, 2] + rows[:, 3], rtol=0, atol=1e-9 * np.abs(rows[:, 1]).max())
+    b = np.asarray(g["boxlength"])
+    assert len(b) == 517 and np.all(np.diff(b[:, 0]) > 0) and b[-1, 0] <= g["n_cycles"]
+    assert abs(T.initial_box_length() - 15.4202166972758) < 1e-9
+    assert T.prm_value("pressure_step_multiplier") == 5 and T.prm_value("temp") == 300
+    for name in T.RDF_PAIRS:
+        assert len(g["rdf"][name]) == len(g["rdf_r"]) == 121
+
+
+def test_oracle_reproduces_reference_tutorial_averages():
+    n_cycles, seeds = 3000, [101, 102, 103, 104, 105, 106]
+    with ProcessPoolExecutor(max_workers=len(seeds), mp_context=mp.get_context("spawn")) as ex:
+        results = list(ex.map(T.oracle_run, seeds, [n_cycles] * len(seeds)))
+    runs = []
+    for rows, cyc, box, L0 in results:
+        assert abs(L0 - T.initial_box_length()) < 1e-9
+        runs.append(T.window_means(rows, T.box_per_cycle(cyc, box, n_cycles, L0), 500, n_cycles))
+    _compare(T.reference_window_means(500, n_cycles), runs, "oracle")
+
+
+@pytest.mark.gpu
+def test_gpu_reproduces_reference_tutorial_averages_and_rdf(tmp_path):
+    from yamc_b200 import api, rng
+    n_cycles, chunk, seeds = T.GOLD["n_cycles"], 100, [301, 302, 303, 304, 305]
+    runs, peaks = [], {name: [] for name in T.RDF_PAIRS}
+    for seed in seeds:
+        files = T.write_inputs(str(tmp_path / f"s{seed}"), seed)
+        eng = api.Engine.from_files(files, extra=f"random_seed={seed}", device=0)
+        L0 = eng.current_params().BoxLength
+        rdf = api.RDF.for_engine(eng, dr=T.GOLD["rdf_dr"], rmax=T.GOLD["rdf_rmax"])
+        buf = rng.gfortran_stream(seed, n_cycles * T.NMOL * 20)
+        cur, rows, cyc, box = 0, [], [], []
+        for c0 in range(0, n_cycles, chunk):
+            _, vrec, r, cur, done, st = eng.run_mc(buf, chunk, cursor=cur, log=False, max_rows=chunk)
+            assert st == 0 and done == chunk, (seed, c0, st, done)
+            rows.append(r)
+            acc = vrec[(vrec["flags"] & 1) == 1]
+            cyc += [int(v) for v in acc["cycle"]]
+            box += [float(v) for v in acc["box_new"]]
+            rdf.add_engine(eng)  # the trajectory frame of this cycle (store_traj_frame)
+        rows = np.concatenate(rows)
+        assert rows.shape[0] == n_cycles // 100 and rows[-1, 0] == n_cycles
+        runs.append(T.window_means(rows, T.box_per_cycle(cyc, box, n_cycles, L0), 2000, n_cycles))
+        _, g, _, nf = rdf.result()
+        assert nf == n_cycles // chunk
+        for name, (a, b) in T.RDF_PAIRS.items():
+            peaks[name].append(T.rdf_peak(g[a, b]))
+        rdf.close()
+        eng.close()
+    _compare(T.reference_window_means(2000, n_cycles), runs, "gpu")
+    for name in T.RDF_PAIRS:
+        ref_bin, ref_h = T.rdf_peak(np.asarray(T.GOLD["rdf"][name]))
+        bins = np.array([p[0] for p in peaks[name]])
+        hs = np.array([p[1] for p in peaks[name]])
+        z = T.z_score(ref_h, hs)
+        print(f"gpu g_{name}: reference peak {ref_h:.3f} at bin {ref_bin}, ours {hs.mean():.3f} +- {hs.std(ddof=1):.3f} "
+              f"at bins {bins.tolist()}, z = {z:.2f}")
+        assert abs(int(np.round(np.median(bins))) - ref_bin) <= 1, (name, ref_bin, bins)
+        assert z < NSIG, (name, ref_h, hs)

@@ -13,8 +13,11 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libyamc_b200.so")
-SOURCES = ["yamc_chain_t1.cu", "yamc_chain_t2.cu", "yamc_chain_t3.cu", "yamc_chain_t4.cu", "yamc_engine.cu",
-           "yamc_static.cu", "yamc_peaks.cu", "yamc_host.cpp", "yamc_inputs.cpp"]
+# (source, object, extra flags): the chain kernel's variants are compiled once per LJ type count
+UNITS = [("yamc_chain_inst.cu", f"yamc_chain_nt{n}.o", [f"-DYAMC_NT={n}"]) for n in (1, 2, 3, 4)] + [
+    (src, src.rsplit(".", 1)[0] + ".o", []) for src in
+    ("yamc_engine.cu", "yamc_static.cu", "yamc_peaks.cu", "yamc_host.cpp", "yamc_inputs.cpp")]
+SOURCES = sorted({u[0] for u in UNITS})
 HEADERS = ["yamc_chain.cuh", "yamc_device.cuh", "yamc_internal.h", os.path.join("..", "..", "include", "yamc.h")]
 
 NVCC_FLAGS = [
@@ -42,22 +45,23 @@ def stale() -> bool:
 
 
 def build(force: bool = False, verbose: bool = False) -> str:
-    """Compile every source to an object in parallel (the chain kernel's variants sit in one
-    file per LJ type count), then link the shared library."""
+    """Compile every unit to an object in parallel (the chain kernel's variants once per LJ type
+    count), then link the shared library."""
     if not force and not stale():
         return LIB
     from concurrent.futures import ThreadPoolExecutor
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
 
-    def compile_one(src):
-        obj = os.path.join(objdir, os.path.splitext(src)[0] + ".o")
-        cmd = [nvcc(), *NVCC_FLAGS, "-c", "-o", obj, os.path.join(CSRC, src)]
+    def compile_one(unit):
+        src, objname, extra = unit
+        obj = os.path.join(objdir, objname)
+        cmd = [nvcc(), *NVCC_FLAGS, *extra, "-c", "-o", obj, os.path.join(CSRC, src)]
         res = subprocess.run(cmd, cwd=CSRC, capture_output=True, text=True)
         return obj, cmd, res
 
-    with ThreadPoolExecutor(max_workers=max(1, min(len(SOURCES), os.cpu_count() or 1))) as ex:
-        results = list(ex.map(compile_one, SOURCES))
+    with ThreadPoolExecutor(max_workers=max(1, min(len(UNITS), os.cpu_count() or 1))) as ex:
+        results = list(ex.map(compile_one, UNITS))
     log = ""
     failed = False
     for obj, cmd, res in results:

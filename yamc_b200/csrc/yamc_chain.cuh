@@ -1,6 +1,6 @@
 // The persistent chain kernel (run_mc + movemc on the device) and its launch helpers.
 // Included by the engine (types and declarations) and by one instantiation file per LJ type
-// count (yamc_chain_t1.cu .. yamc_chain_t4.cu), so the kernel variants compile in parallel.
+// count (yamc_chain_inst.cu, compiled once per count), so the kernel variants compile in parallel.
 #pragma once
 
 #include <cooperative_groups.h>
@@ -1430,14 +1430,17 @@ int max_clusters_t(const LaunchCfg &L, int *out) {
 }
 
 
-// one instantiation file per LJ type count: every (entries per thread, split, mixed) variant
-int launch_chain_t1(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
-int launch_chain_t2(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
-int launch_chain_t3(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
-int launch_chain_t4(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
-int max_clusters_t1(const LaunchCfg &L, bool split, bool mx, int *out);
-int max_clusters_t2(const LaunchCfg &L, bool split, bool mx, int *out);
-int max_clusters_t3(const LaunchCfg &L, bool split, bool mx, int *out);
-int max_clusters_t4(const LaunchCfg &L, bool split, bool mx, int *out);
+// the launch entry points of each LJ type count, defined in yamc_chain_inst.cu (compiled once per
+// count): every (entries per thread, split, mixed) variant of that count
+template <int NT> int launch_chain_nt(const LaunchCfg &L, bool split, bool mx, cudaStream_t s, int nrep, const ChainArgs &a);
+template <int NT> int max_clusters_nt(const LaunchCfg &L, bool split, bool mx, int *out);
+#define YAMC_DECLARE_NT(N)                                                                                       \
+    template <> int launch_chain_nt<N>(const LaunchCfg &, bool, bool, cudaStream_t, int, const ChainArgs &);     \
+    template <> int max_clusters_nt<N>(const LaunchCfg &, bool, bool, int *);
+YAMC_DECLARE_NT(1)
+YAMC_DECLARE_NT(2)
+YAMC_DECLARE_NT(3)
+YAMC_DECLARE_NT(4)
+#undef YAMC_DECLARE_NT
 
 }  // namespace yamc

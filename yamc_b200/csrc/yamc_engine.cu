@@ -629,6 +629,9 @@ size_t chain_smem_bytes(int G, int B, int kmax, int nt, int nown_max, int qcap) 
 
 }  // namespace
 
+// byte offset of the per-move commit's staging inside yamc_ctx::h_pin (after the read-back block)
+constexpr size_t kPinCommit = ((sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT + 255) / 256) * 256;
+
 struct yamc_ctx {
     HostSystem H;
     int device = 0;
@@ -656,7 +659,8 @@ struct yamc_ctx {
     RunSlot *d_run = nullptr;
     double *api_in = nullptr, *api_out = nullptr;
     // pinned staging of the per-move calls: api_out, then scal, then cnt, read back in one
-    // round trip per call
+    // round trip per call; after them (kPinCommit) the commit's uploads: the moved atoms'
+    // records, scal and cnt
     double *h_pin = nullptr;
     float *d_rng = nullptr;
     size_t rng_cap = 0;
@@ -759,10 +763,10 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
 int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, bool mx, cudaStream_t stream, int nrep,
                      const ChainArgs &args) {
     switch (nt) {
-        case 1: return launch_chain_t1(L, split, mx, stream, nrep, args);
-        case 2: return launch_chain_t2(L, split, mx, stream, nrep, args);
-        case 3: return launch_chain_t3(L, split, mx, stream, nrep, args);
-        case 4: return launch_chain_t4(L, split, mx, stream, nrep, args);
+        case 1: return launch_chain_nt<1>(L, split, mx, stream, nrep, args);
+        case 2: return launch_chain_nt<2>(L, split, mx, stream, nrep, args);
+        case 3: return launch_chain_nt<3>(L, split, mx, stream, nrep, args);
+        case 4: return launch_chain_nt<4>(L, split, mx, stream, nrep, args);
     }
     set_error("LJ type count outside 1..4");
     return YAMC_ELIMITS;
@@ -770,10 +774,10 @@ int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, bool mx, cudaStream
 
 int max_clusters_cfg(const LaunchCfg &L, int nt, bool split, bool mx, int *out) {
     switch (nt) {
-        case 1: return max_clusters_t1(L, split, mx, out);
-        case 2: return max_clusters_t2(L, split, mx, out);
-        case 3: return max_clusters_t3(L, split, mx, out);
-        case 4: return max_clusters_t4(L, split, mx, out);
+        case 1: return max_clusters_nt<1>(L, split, mx, out);
+        case 2: return max_clusters_nt<2>(L, split, mx, out);
+        case 3: return max_clusters_nt<3>(L, split, mx, out);
+        case 4: return max_clusters_nt<4>(L, split, mx, out);
     }
     set_error("LJ type count outside 1..4");
     return YAMC_ELIMITS;
@@ -1160,7 +1164,8 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->api_in, 1 + 3 * kMaxA)) ||
         (r = dalloc(&c->api_out, kNV)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
-    CUDA_TRY(cudaMallocHost(&c->h_pin, sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT));
+    CUDA_TRY(cudaMallocHost(&c->h_pin, kPinCommit + sizeof(double4) * kMaxA + sizeof(double) * SC_COUNT +
+                                           sizeof(long long) * CN_COUNT));
     // full-sum work split: atom-tile pairs of the real-space sum; atom slices of rho(k) so that
     // entry blocks x slices cover the SMs about twice
     int nsm = 148;
@@ -2248,22 +2253,27 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     const int n = (1 + H.nt) * H.S;
     k_commit_rho<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, c->scratch + n, n);
     CUDA_TRY(cudaGetLastError());
-    std::vector<double4> a(na);
+    // the uploads come from the pinned commit block: every per-move call that follows ends with
+    // a stream synchronisation before the host writes that block again
+    unsigned char *stage = reinterpret_cast<unsigned char *>(c->h_pin) + kPinCommit;
+    double4 *a = reinterpret_cast<double4 *>(stage);
+    double *sc = reinterpret_cast<double *>(a + kMaxA);
+    long long *cn = reinterpret_cast<long long *>(sc + SC_COUNT);
     for (int i = 0; i < na; ++i) {
         H.x[f0 + i] = c->api_xn[i]; H.y[f0 + i] = c->api_yn[i]; H.z[f0 + i] = c->api_zn[i];
         a[i] = make_double4(H.x[f0 + i], H.y[f0 + i], H.z[f0 + i], H.q[f0 + i]);
     }
-    int r = upload(c->atom + f0, a.data(), na, c->stream);
-    if (r) return r;
     c->sc[SC_UU_EW] += c->api_new[RV_EW] - c->api_eold[0];
     c->sc[SC_UU_LJ6] += c->api_new[RV_LJ6] - c->api_eold[1];
     c->sc[SC_UU_LJ12] += c->api_new[RV_LJ12] - c->api_eold[2];
     c->sc[SC_EK_C] += c->api_new[RV_DUC];
     c->sc[SC_EK_LJ] += c->api_new[RV_DUL];
     c->sc[SC_MU_X] += c->api_dmu[0]; c->sc[SC_MU_Y] += c->api_dmu[1]; c->sc[SC_MU_Z] += c->api_dmu[2];
-    // the copies come from pageable memory, staged before they return: nothing to wait for here,
-    // the next call on the stream is ordered after them
-    if ((r = push_state(c))) return r;
+    std::memcpy(sc, c->sc, sizeof(double) * SC_COUNT);
+    std::memcpy(cn, c->cnt_h, sizeof(long long) * CN_COUNT);
+    CUDA_TRY(cudaMemcpyAsync(c->atom + f0, a, sizeof(double4) * na, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->scal, sc, sizeof(double) * SC_COUNT, cudaMemcpyHostToDevice, c->stream));
+    CUDA_TRY(cudaMemcpyAsync(c->cnt, cn, sizeof(long long) * CN_COUNT, cudaMemcpyHostToDevice, c->stream));
     c->api_stage = 0;
     return YAMC_OK;
 }

@@ -85,7 +85,12 @@ done:
 
 extern "C" int yamc_fma_peak(int32_t device, int32_t fp64, double *tflops) {
     if (!tflops || device < 0) return YAMC_EPARAMETER;
-    cudaError_t e = cudaSetDevice(device);
+    // the caller's current device is put back before returning
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
     if (e != cudaSuccess) { yamc::set_error(cudaGetErrorString(e)); return YAMC_ECUDA; }
-    return fp64 ? yamc::measure<double>(device, tflops) : yamc::measure<float>(device, tflops);
+    if ((e = cudaSetDevice(device)) != cudaSuccess) { yamc::set_error(cudaGetErrorString(e)); return YAMC_ECUDA; }
+    const int rc = fp64 ? yamc::measure<double>(device, tflops) : yamc::measure<float>(device, tflops);
+    if ((e = cudaSetDevice(prev)) != cudaSuccess) { yamc::set_error(cudaGetErrorString(e)); return YAMC_ECUDA; }
+    return rc;
 }

@@ -20,7 +20,6 @@
 #include <cuda_runtime.h>
 
 #include <cstdint>
-#include <mutex>
 #include <string>
 
 #include "../../include/yamc.h"
@@ -33,7 +32,6 @@ namespace {
 constexpr int kStaticTile = 256;  // threads per block = atoms per block
 constexpr int kStaticParts = 8;   // ew, lj6, lj12, ew_intra, lj6_intra, lj12_intra, overlap, bad type
 constexpr int kStaticMaxBlocks = (YAMC_STATIC_MAX_ATOMS + kStaticTile - 1) / kStaticTile;
-constexpr int kStaticMaxDevices = 64;
 
 // The scratch: kStaticParts doubles per block of kStaticTile atoms, for at most
 // YAMC_STATIC_MAX_ATOMS atoms (64 KiB).  Every GPU that loads the library holds one copy
@@ -42,14 +40,6 @@ constexpr int kStaticMaxDevices = 64;
 // nothing has to be cleared between calls.  In host code this name is only a handle for
 // cudaGetSymbolAddress, never a device address.
 static __device__ __align__(256) double g_static_parts[kStaticMaxBlocks * kStaticParts];
-
-// device address of g_static_parts, looked up once per device
-struct StaticSlot {
-    bool ready = false;
-    double *parts = nullptr;
-};
-std::mutex g_static_mu;
-StaticSlot g_static_slot[kStaticMaxDevices];
 
 struct StaticIn {
     int N, nt;
@@ -174,18 +164,15 @@ int cuda_fail(cudaError_t e, const char *what) {
     return YAMC_ECUDA;
 }
 
-// the device address of g_static_parts on the current device (set-up on first use)
-int static_parts_address(int dev, double **out) {
-    std::lock_guard<std::mutex> lock(g_static_mu);
-    StaticSlot &s = g_static_slot[dev];
-    if (!s.ready) {
-        void *ptr = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_parts);
-        if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_parts)");
-        s.parts = static_cast<double *>(ptr);
-        s.ready = true;
-    }
-    *out = s.parts;
+// The device address of g_static_parts in the current context, looked up on every call: a
+// host-side lookup that allocates nothing.  Not cached, because a host that resets the device
+// (cudaDeviceReset) or re-creates its primary context gets the module loaded again, possibly
+// at another address, and a cached pointer would then point at memory that is no longer mapped.
+int static_parts_address(double **out) {
+    void *ptr = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&ptr, g_static_parts);
+    if (e != cudaSuccess) return cuda_fail(e, "cudaGetSymbolAddress(g_static_parts)");
+    *out = static_cast<double *>(ptr);
     return YAMC_OK;
 }
 
@@ -227,7 +214,6 @@ extern "C" int yamc_realspace_sums_static(const yamc_params *p, int32_t natom, c
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return cuda_fail(e, "cudaGetDevice");
-    if (dev < 0 || dev >= kStaticMaxDevices) { set_error("device ordinal above 63"); return YAMC_ELIMITS; }
     int r;
     if ((r = check_device_array(x, 8, dev, "x")) || (r = check_device_array(y, 8, dev, "y")) ||
         (r = check_device_array(z, 8, dev, "z")) || (r = check_device_array(charge, 8, dev, "charge")) ||
@@ -242,7 +228,7 @@ extern "C" int yamc_realspace_sums_static(const yamc_params *p, int32_t natom, c
         (fy && (r = check_device_array(fy, 8, dev, "fy"))) || (fz && (r = check_device_array(fz, 8, dev, "fz"))))
         return r;
     double *parts = nullptr;
-    if ((r = static_parts_address(dev, &parts))) return r;
+    if ((r = static_parts_address(&parts))) return r;
 
     StaticIn in;
     in.N = natom; in.nt = n_types;

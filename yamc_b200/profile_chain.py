@@ -5,7 +5,9 @@
 builds the named workload (systems.WORKLOADS) on cuda:0 with PRECISION (0 FP64, 1 mixed),
 k-space LAYOUT (1 registers, 2 streamed) and a cluster of G CTAs of THREADS threads, runs a
 300-move warm-up launch and then one launch of MOVES moves (default 1000), and prints its
-CUDA-event time.  Capture the second launch with ``ncu -k regex:k_chain -s 1 -c 1``.
+CUDA-event time.  Capture the second launch with
+``ncu --clock-control none -k regex:k_chain -s 1 -c 1`` (``--clock-control none`` leaves the
+GPU's clocks as they are), on a workload that fits a short capture.
 """
 from __future__ import annotations
 

@@ -6,8 +6,9 @@ builds the named workload (systems.WORKLOADS) on cuda:0, runs yamc_full_sums onc
 warm-up and then REPEATS more times (default 3), timing each call on the host (the call
 synchronises), then VOLUME_STEPS volume steps through yamc_volume_eval/_commit (default 0)
 and FORCES calls of the adjoint yamc_forces (default 0).
-Capture the kernels of the second call with
-``ncu -k regex:"k_realspace_full|k_rho_full|k_rho_reduce|k_kspace_energy" -s 4 -c 4``.
+Capture one kernel of the second call at a time, e.g.
+``ncu --clock-control none -k regex:k_realspace_full -s 1 -c 1`` (``--clock-control none`` leaves
+the GPU's clocks as they are).
 """
 from __future__ import annotations
 

@@ -5,7 +5,9 @@
 builds the named workload (systems.WORKLOADS) on cuda:0, evaluates XCHG_STEPS exchange steps of
 random molecule pairs through yamc_xchange_eval / _commit (rejected, so the state stays; default
 4) and adds RDF_FRAMES frames of the engine's configuration to a GPU RDF (default 2), timing
-each on the host.  Capture with ``ncu -k "regex:k_xchg|k_rdf_count|k_mol_centres" -s ... -c ...``.
+each on the host.  Capture one kernel at a time, e.g.
+``ncu --clock-control none -k regex:k_rdf_count -s 1 -c 1`` (``--clock-control none`` leaves the
+GPU's clocks as they are).
 """
 from __future__ import annotations
 
