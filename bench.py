@@ -1,25 +1,30 @@
 """Benchmark: MC trial moves/s of YAMC's movemc path on B200.
 
-Workload (default): 2048 SPC/E + 38 Na+ + 38 Cl- (6,220 atoms), L = 39.6 A,
-alpha = 0.30/A, rc = 12 A, kmax = 12 (1,068 half-space / 3,796 signed k),
-dispersion-Ewald LJ, unbiased moves (0.15 A ball, 0.15 rad), synthetic
-jittered-lattice starts, gfortran random streams.  One step = one batch graph
-launch that advances every chain of a GPU by --moves moves: as many independent
-chains as the launch shapes keep resident (replicas only: a Markov chain does not
+Workload (default, the force-biased configuration the metric's target is stated on): 4096
+SPC/E + 76 Na+ + 76 Cl- (12,440 atoms), L = 50 A, alpha = 0.28/A, rc = 12 A, kmax = 15 (2,045
+half-space / 7,427 signed k), dispersion-Ewald LJ, force-biased moves (lambda = 0.1 for force
+and torque, 0.15 A / 0.15 rad), synthetic jittered-lattice starts, gfortran random streams.
+One step = one batch graph launch that advances every chain of a GPU by --moves moves: as many
+independent chains as the launch shapes keep resident (replicas only: a Markov chain does not
 shard), the launch shape picked by the batch autotuner.
 
-  value  moves/s of the mixed-precision form with the random streams already in
-         HBM, CUDA events around each launch, L2 flushed (256 MB write) between
-         steps; config.fp64 the plain FP64 form on the same batch, and the mixed
-         form's dE, force and total-energy error against FP64
-  e2e    the same through yamc_batch_run with the streams in pinned host memory,
-         host->device copy of each step's stream windows and device->host read of
-         every chain's energies inside the timed region
-  blocks nacl4k_mixed_batch_vs_plain (4096 SPC/E + NaCl, mixed batched force-biased against
-         the plain FP64 chain), batch_ragged_96 (96 ragged replicas), npt_run_mc
-         (NPT run_mc with volume steps), cpu_baseline (the oracle on one core)
-  --impl reference  the CPU restatement of the reference (oracle/, -O3) timed on
-         the host cores: independent chains, one per core
+  value   moves/s of the mixed-precision form with the random streams already in HBM, CUDA
+          events around each launch, L2 flushed (256 MB write) between steps
+  config  fp64_batched: the same chains and shape search in FP64 (mixed_over_fp64_batched);
+          plain_fp64_one_chain: the FP64 drop-in, one chain alone, the same move set
+          (target_ratio = value over it, target 5); the mixed form's dE, force and
+          total-energy error against FP64 (precision_errors_vs_fp64)
+  e2e     the same through yamc_batch_run with the streams in pinned host memory, host->device
+          copy of each step's stream windows and device->host read of every chain's energies
+          inside the timed region
+  configs the other configurations of the metric, each with its plain FP64 chain, mixed and
+          FP64 batches and precision errors: spce256 (256 SPC/E), nacl1m (2048 SPC/E + NaCl,
+          unbiased), nacl16k (16384 SPC/E + NaCl, force-biased), batch_ragged_96 (96 ragged
+          replicas in one batch), npt_run_mc (NPT run_mc with volume steps)
+  cpu_baseline  the oracle (-O3 C restatement of the reference) on one host core, a bounded
+          sample of the same workload
+  --impl reference  the CPU restatement of the reference (oracle/, -O3) timed on the host
+          cores: independent chains, one per core
 """
 from __future__ import annotations
 
@@ -40,10 +45,11 @@ sys.path.insert(0, ROOT)
 METRIC = "MC trial moves/s (SPC/E+NaCl Ewald); mixed vs FP64 GPU at |ΔE err|≤1e-4 kT"
 
 
-# DRAM bytes per move of the chain kernel in the timed shape (mixed, streamed, cluster of 2 x 384
-# threads) from the ncu capture of one 1,000-move launch on nacl1m (dram__bytes_read.sum +
-# dram__bytes_write.sum = 1.094 MB), used for roofline.traffic
-TRAFFIC_PER_MOVE = 1094.0
+# DRAM bytes per move of the chain kernel in the timed shape, by workload, from one ncu capture
+# (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its moves; profiles/), used for
+# roofline.traffic: nacl1m mixed streamed 2 x 384 threads, 1,000 moves: 1.094 MB; nacl4k mixed
+# force-biased streamed 3 x 384 threads, 500 moves: 2.57 MB
+TRAFFIC_PER_MOVE = {"nacl1m": 1094.0, "nacl4k": 5142.0}
 
 
 def dist_env():
@@ -94,13 +100,17 @@ def algorithmic_bytes_per_move(spec, nk, nsigned, ntype, p_acc):
     return real + rho + beta + kidx + commit
 
 
-def algorithmic_flops_per_move(spec, nsigned, ntype):
-    """Floating-point work of an unbiased move at least: real-space pairs at the old and the
-    new positions (2 n_m N_nb pairs at 60 flop each, sqrt/exp/divide counted as one) and the
-    k-space energy, S (2 n_m 14 + 6 (1 + T^2)) flop; n_m = mean atoms of a chosen molecule."""
+def algorithmic_flops_per_move(spec, nsigned, ntype, forces=False):
+    """Floating-point work of a move at least: real-space pairs at the old and the new positions
+    (2 n_m N_nb pairs at 60 flop each, sqrt/exp/divide counted as one) and the k-space energy,
+    S (2 n_m 14 + 6 (1 + T^2)) flop; a force-biased move adds the k-space forces at both
+    positions, S 2 n_m (6 + 6 T).  n_m = mean atoms of a chosen molecule."""
     nnb = spec.natom / spec.box ** 3 * 4.0 / 3.0 * math.pi * spec.rc ** 3
     n_m = spec.natom / spec.nmol
-    return 2 * n_m * nnb * 60 + nsigned * (2 * n_m * 14 + 6 * (1 + ntype * ntype))
+    f = 2 * n_m * nnb * 60 + nsigned * (2 * n_m * 14 + 6 * (1 + ntype * ntype))
+    if forces:
+        f += nsigned * 2 * n_m * (6 + 6 * ntype)
+    return f
 
 
 class Clocks:
@@ -180,7 +190,7 @@ def _ref_worker(args):
     import pyoracle
     from yamc_b200 import rng as grng
     o = pyoracle.Oracle(files, fast=True)
-    buf = grng.gfortran_stream(seed, 40 * moves + 10000)
+    buf = grng.gfortran_stream(seed, 60 * moves + 10000)
     t0 = time.perf_counter()
     o.run_mc(buf, moves)
     return moves, time.perf_counter() - t0
@@ -214,110 +224,128 @@ def run_reference(args, files, spec_name):
     print(json.dumps(line), flush=True)
 
 
-def target_block(local, rank, moves=2000, steps=3, warmup=2):
-    """The north-star comparison on 4096 SPC/E + 76 Na + 76 Cl (12,440 atoms, L = 50 A,
-    alpha = 0.28/A, rc = 12 A, kmax = 15, the configuration of force-biased moves): one plain FP64
-    chain (the drop-in) with the configuration's force-biased moves, and one with unbiased moves,
-    against a batch of mixed-precision force-biased chains (lambda = 0.1), all resident at once,
-    with the mixed chains' dE against FP64 chains on the same random stream."""
-    import torch
-    from yamc_b200 import _lib, api, rng as grng, systems
-    dev = f"cuda:{local}"
-    spec_b = systems.WORKLOADS["nacl4k"]                      # force-biased, lambda = 0.1
-    spec_p = systems.SystemSpec(**{**spec_b.__dict__, "name": "nacl4k_plain", "xlambda": 0.0})
-    base = f"/tmp/yamc_bench_target_r{rank}_{os.getpid()}"
-    fp = systems.write_system(spec_p, base + "_plain", seed=5)
-    per_move = 40
-    # one plain FP64 chain
-    eng = api.Engine.from_files(fp, device=local)
-    s0 = torch.from_numpy(grng.gfortran_stream(99, per_move * moves * (steps + warmup) + 10000)).to(dev)
-    cur = 0
-    ms = []
-    for w in range(warmup + steps):
-        cur, done, st = eng.run_chain_device(s0.data_ptr(), s0.numel(), moves, cursor=cur)
-        assert st == 0 and done == moves
-        if w >= warmup:
-            ms.append(eng.last_kernel_ms)
-    plain = moves * steps / (sum(ms) / 1e3)
-    plain_launch = eng.launch
-    eng.close()
-    del s0
-    # dE of mixed vs FP64 force-biased chains on the same stream
-    fb = systems.write_system(spec_b, base + "_b0", seed=5)
-    # one plain FP64 chain with the configuration's own move set (force-biased, lambda = 0.1)
-    eng = api.Engine.from_files(fb, device=local)
-    s1 = torch.from_numpy(grng.gfortran_stream(98, 60 * moves * (steps + warmup) + 10000)).to(dev)
-    cur = 0
-    ms = []
-    for w in range(warmup + steps):
-        cur, done, st = eng.run_chain_device(s1.data_ptr(), s1.numel(), moves, cursor=cur)
-        assert st == 0 and done == moves
-        if w >= warmup:
-            ms.append(eng.last_kernel_ms)
-    plain_fb = moves * steps / (sum(ms) / 1e3)
-    plain_fb_launch = eng.launch
-    eng.close()
-    del s1
-    n_chk = 1500
-    chk = grng.gfortran_stream(4243, 60 * n_chk + 10000)
-    logs = {}
-    for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
-        e = api.Engine.from_files(fb, device=local, precision=prec)
-        logs[prec] = e.run_chain(chk, n_chk)[0]
-        e.close()
-    lf, lm = logs[_lib.YAMC_FP64], logs[_lib.YAMC_MIXED]
-    same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
-    k = n_chk if same.all() else int(np.argmin(same))
-    cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
-    de = np.abs(sum(lm[c][:k] for c in cols) - sum(lf[c][:k] for c in cols)) if k else np.zeros(1)
-    # the mixed force-biased batch: as many chains as one shape keeps resident
-    inp0 = api.load_inputs(fb["parameters"], fb["composition"], fb["moltab"])
-    probe = api.Batch([inp0], device=local, precision=_lib.YAMC_MIXED)
-    R = 1
+def _files_for(spec, tag, rank, r):
+    """Input files of chain r of a workload (distinct seeds for every rank and chain)."""
+    from yamc_b200 import systems
+    seed, rng_seed = replica_seeds(rank, r)
+    return systems.write_system(spec, f"/tmp/yamc_bench_{tag}_r{rank}_{os.getpid()}_{r}", seed=seed, rng_seed=rng_seed)
+
+
+def _resident_chains(inp, local, precision):
+    """The most chains of this system any launch shape keeps resident at once."""
+    from yamc_b200 import api
+    probe = api.Batch([inp], device=local, precision=precision)
+    resident = {}
     for G in range(1, 17):
         try:
             probe.set_launch(G, 0)
         except Exception:
             continue
-        R = max(R, probe.launch["resident_clusters"])
+        resident[G] = probe.launch["resident_clusters"]
     probe.close()
-    R = min(R, 148)
-    files = [fb] + [systems.write_system(spec_b, f"{base}_b{r}", seed=5 + 13 * r, rng_seed=777 + r) for r in range(1, R)]
-    b = api.Batch([api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in files], device=local,
-                  precision=_lib.YAMC_MIXED)
-    ds = [torch.from_numpy(grng.gfortran_stream(1000 + r, per_move * moves * (steps + warmup + 1) + 10000)).to(dev)
-          for r in range(R)]
-    ptrs, nr = [t.data_ptr() for t in ds], [t.numel() for t in ds]
-    curs = np.zeros(R, dtype=np.int64)
-    b.tune(ptrs, nr, curs, 200)
+    return min(148, max(resident.values(), default=1)), resident
+
+
+def single_chain_rate(files, local, precision, moves, per_move, reps=2, extra=""):
+    """One chain alone (the plain drop-in: no batching), device-resident stream, CUDA-event time."""
+    import torch
+    from yamc_b200 import api, rng as grng
+    eng = api.Engine.from_files(files, extra=extra, device=local, precision=precision)
+    s0 = torch.from_numpy(grng.gfortran_stream(99, per_move * moves * (reps + 1) + 10000)).to(f"cuda:{local}")
+    cur, done, st = eng.run_chain_device(s0.data_ptr(), s0.numel(), moves)
+    assert st == 0 and done == moves, (st, done)
     ms = []
-    for w in range(warmup + steps):
-        done, st, s_all = b.run_device(ptrs, nr, curs, moves)
-        assert s_all == 0 and (done == moves).all(), (s_all, done)
-        if w >= warmup:
-            ms.append(b.last_kernel_ms)
-    batched = R * moves * steps / (sum(ms) / 1e3)
-    out = {"workload": "nacl4k: 4096 SPC/E + 76 Na + 76 Cl, 12440 atoms, L=50 A, alpha=0.28/A, rc=12 A, kmax=15",
-           "plain_fp64_one_chain": {"value": plain, "unit": "moves/s", "launch": plain_launch,
-                                    "moves": "unbiased"},
-           "plain_fp64_one_chain_force_biased": {"value": plain_fb, "unit": "moves/s", "launch": plain_fb_launch,
-                                                 "moves": "force-biased, lambda = 0.1 (the configuration's move set)"},
-           "mixed_batched_force_biased": {"value": batched, "unit": "moves/s", "chains": R, "launch": b.launch,
-                                          "lambda": 0.1},
-           # the target's ratio, the same move set on both sides; and against the unbiased plain chain
-           "ratio": batched / plain_fb,
-           "ratio_vs_unbiased_plain": batched / plain,
-           "de_error_mixed_vs_fp64_force_biased": {"max_kT": float(de.max()), "moves_compared": k},
-           "moves_per_step_per_chain": moves, "steps": steps}
-    b.close()
+    for _ in range(reps):
+        cur, done, st = eng.run_chain_device(s0.data_ptr(), s0.numel(), moves, cursor=cur)
+        assert st == 0 and done == moves, (st, done)
+        ms.append(eng.last_kernel_ms)
+    out = {"value": moves / (np.mean(ms) / 1e3), "unit": "moves/s", "launch": eng.launch}
+    eng.close()
     return out
+
+
+def precision_errors(files, local, n_chk=1500, n_force=200, seed=4242):
+    """The mixed form against FP64 on one system (north_star (2): dE, force and total-energy
+    error for every result): a mixed and an FP64 chain on the same random stream, compared move
+    by move up to their first different decision; the molecular forces of the force-bias path
+    (yamc_move_old, movemc Steps 3-4) of both forms on the same configuration; the mixed chain's
+    running total energy against an FP64 recomputation of its own configuration."""
+    from yamc_b200 import _lib, api, rng as grng
+    chk = grng.gfortran_stream(seed, 60 * n_chk + 10000)
+    logs, e_tot = {}, {}
+    for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
+        eng = api.Engine.from_files(files, device=local, precision=prec)
+        logs[prec] = eng.run_chain(chk, n_chk)[0]
+        if prec == _lib.YAMC_MIXED:
+            e_tot = {"incremental": float(eng.energies()[0]), "fp64_full": float(eng.full_sums()[0])}
+        eng.close()
+    lf, lm = logs[_lib.YAMC_FP64], logs[_lib.YAMC_MIXED]
+    same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
+    k = n_chk if same.all() else int(np.argmin(same))
+    cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
+    de = np.abs(sum(lm[c][:k] for c in cols) - sum(lf[c][:k] for c in cols)) if k else np.zeros(1)
+    ef = api.Engine.from_files(files, device=local, precision=_lib.YAMC_FP64)
+    em = api.Engine.from_files(files, device=local, precision=_lib.YAMC_MIXED)
+    ferr, fscale, nf = 0.0, 0.0, 0
+    for imol in range(1, ef.nmol + 1, max(1, ef.nmol // n_force)):
+        f1, _ = ef.move_old(imol)
+        ef.move_commit(False)
+        f2, _ = em.move_old(imol)
+        em.move_commit(False)
+        fscale = max(fscale, float(np.abs(f1).max()))
+        ferr = max(ferr, float(np.abs(f2 - f1).max()))
+        nf += 1
+    ef.close()
+    em.close()
+    return {"de_max_kT": float(de.max()), "de_rms_kT": float(np.sqrt((de ** 2).mean())), "moves_compared": k,
+            "bar_kT": 1e-4, "force_max_abs_err": ferr, "force_scale": fscale,
+            "force_rel_err": ferr / max(fscale, 1e-300), "molecules_compared": nf,
+            "total_energy_err_kT": abs(e_tot["incremental"] - e_tot["fp64_full"]),
+            "total_energy_kT": e_tot["fp64_full"], "mixed_chain_moves": n_chk}
+
+
+def batch_rates(spec, tag, local, rank, moves, steps, warmup, per_move, precisions, chains=0, tune_moves=200):
+    """As many independent chains of a workload as one launch shape keeps resident, run as one
+    batch (one graph launch per step), for each precision: moves/s over `steps` timed steps
+    (CUDA events on the batch stream, L2 flushed between steps)."""
+    import torch
+    from yamc_b200 import _lib, api, rng as grng
+    dev = f"cuda:{local}"
+    f0 = _files_for(spec, tag, rank, 0)
+    inp0 = api.load_inputs(f0["parameters"], f0["composition"], f0["moltab"])
+    R = chains or _resident_chains(inp0, local, _lib.YAMC_MIXED)[0]
+    files = [f0] + [_files_for(spec, tag, rank, r) for r in range(1, R)]
+    inputs = [inp0] + [api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in files[1:]]
+    ds = [torch.from_numpy(grng.gfortran_stream(replica_seeds(rank, r)[1], per_move * moves * (steps + warmup + 1)
+                                                + 10000)).to(dev) for r in range(R)]
+    ptrs, nr = [t.data_ptr() for t in ds], [t.numel() for t in ds]
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
+    out = {"chains": R}
+    for prec in precisions:
+        b = api.Batch(inputs, device=local, precision=prec)
+        cur = np.zeros(R, dtype=np.int64)
+        b.tune(ptrs, nr, cur, tune_moves)
+        ms = []
+        for w in range(warmup + steps):
+            done, st, s_all = b.run_device(ptrs, nr, cur, moves)
+            assert s_all == 0 and (done == moves).all(), (s_all, done)
+            if w >= warmup:
+                ms.append(b.last_kernel_ms)
+            flush.fill_(1.0)
+        torch.cuda.synchronize()
+        name = "mixed" if prec == _lib.YAMC_MIXED else "fp64"
+        out[name] = {"value": R * moves * steps / (sum(ms) / 1e3), "unit": "moves/s", "launch": b.groups}
+        b.close()
+    del ds
+    return out, files[0]
 
 
 def ragged_batch_block(local, rank, n_replicas=96, moves=10000):
     """Ragged replicas (water log-uniform 216..4096, NaCl 0..2 M, density 0.0334 +- 2 %, T 280..360 K,
     alpha = 5.6/L, cutoff min(12 A, L/2), one k-set), mixed precision, force-biased (lambda = 0.1),
     all in one batch: one graph launch per kernel-variant group, launch shape from the autotuner,
-    `moves` trial moves per replica.  dE of the mixed form against FP64 on two replicas."""
+    `moves` trial moves per replica.  The mixed form's dE, force and total-energy error against
+    FP64 on the smallest and the largest replica."""
     import torch
     from yamc_b200 import _lib, api, rng as grng, systems
     dev = f"cuda:{local}"
@@ -338,27 +366,17 @@ def ragged_batch_block(local, rank, n_replicas=96, moves=10000):
     ms = b.last_kernel_ms
     launch = b.groups
     b.close()
-    # mixed against FP64 on the smallest and the largest replica, same random stream
-    de = []
+    # the mixed form against FP64 on the smallest and the largest replica: dE on the same random
+    # stream, forces and the running total energy
     natoms = [inp.natom for inp in inputs]
-    for i in (int(np.argmin(natoms)), int(np.argmax(natoms))):
-        chk = grng.gfortran_stream(6000 + i, 60 * 1000 + 10000)
-        logs = []
-        for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
-            e = api.Engine(inputs[i], device=local, precision=prec)
-            logs.append(e.run_chain(chk, 1000)[0])
-            e.close()
-        lf, lm = logs
-        same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
-        k = 1000 if same.all() else int(np.argmin(same))
-        cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
-        if k:
-            de.append(float(np.abs(sum(lm[c][:k] for c in cols) - sum(lf[c][:k] for c in cols)).max()))
+    errs = {}
+    for tag, i in (("smallest", int(np.argmin(natoms))), ("largest", int(np.argmax(natoms)))):
+        errs[tag] = {"atoms": natoms[i], **precision_errors(files[i], local, n_chk=1000, n_force=100, seed=6000 + i)}
     return {"workload": f"{n_replicas} ragged replicas: water 216..4096 (log-uniform), NaCl 0..2 M, T 280..360 K, "
                         f"alpha = 5.6/L, kmax {specs[0].kmax}; {min(natoms)}..{max(natoms)} atoms",
             "method": "mixed precision, force-biased (lambda = 0.1), one batch", "moves_per_replica": moves,
             "value": n_replicas * moves / (ms / 1e3), "unit": "moves/s", "ms": ms, "launch": launch,
-            "de_error_vs_fp64_max_kT": max(de) if de else None}
+            "precision_errors_vs_fp64": errs}
 
 
 def npt_block(local, rank, cycles=12):
@@ -402,15 +420,14 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--moves", type=int, default=20000, help="moves per step")
-    ap.add_argument("--workload", default="nacl1m")
+    ap.add_argument("--moves", type=int, default=4000, help="moves per chain per step")
+    ap.add_argument("--workload", default="nacl4k")
     ap.add_argument("--impl", default="engine", choices=["engine", "reference"])
-    ap.add_argument("--ref-moves", type=int, default=1500)
+    ap.add_argument("--ref-moves", type=int, default=300)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--replicas", type=int, default=0, help="chains per GPU (0 = as many clusters as are resident)")
-    ap.add_argument("--no-target", action="store_true", help="skip the 4096-water mixed/batched/force-biased block")
-    ap.add_argument("--no-ragged", action="store_true", help="skip the 96 ragged replicas block")
-    ap.add_argument("--no-npt", action="store_true", help="skip the NPT run_mc block")
+    ap.add_argument("--no-blocks", action="store_true",
+                    help="skip the other configurations (spce256, nacl1m, nacl16k, 96 ragged replicas, NPT)")
     args = ap.parse_args()
 
     from yamc_b200 import systems
@@ -438,88 +455,36 @@ def main():
     from yamc_b200 import _lib, api, rng as grng
 
     dev = f"cuda:{local}"
-    n_steps = args.warmup + args.steps
-    per_move = 16  # upper bound of random numbers per unbiased move (about 11 on average)
-    n_stream = per_move * args.moves * (2 * n_steps + 2) + 100000
+    biased = spec.xlambda > 0
+    # random numbers per move, an upper bound (about 11 for an unbiased move, 20 for a force-biased one)
+    per_move = 40 if biased else 16
+    n_stream = per_move * args.moves * (2 * (args.warmup + args.steps) + 2) + 100000
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)
 
     def l2_flush():
         flush.fill_(1.0)
         torch.cuda.synchronize()
 
-    # ---------------- one chain alone: the latency of the move, FP64 and mixed (beside the batch)
-    def single_chain(precision):
-        eng = api.Engine.from_files(files, device=local, precision=precision)
-        s0 = grng.gfortran_stream(replica_seeds(rank, 0)[1], per_move * args.moves * 3 + 100000)
-        d_s0 = torch.from_numpy(s0).to(dev)
-        c0, _, _ = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves)
-        ms = []
-        for _ in range(2):
-            l2_flush()
-            c0, done, st = eng.run_chain_device(d_s0.data_ptr(), d_s0.numel(), args.moves, cursor=c0)
-            assert st == 0 and done == args.moves
-            ms.append(eng.last_kernel_ms)
-        out = {"moves_per_s": args.moves / (np.mean(ms) / 1e3), "launch": eng.launch}
-        eng.close()
-        return out
+    # ---------------- the plain drop-in: one FP64 chain alone, with the workload's own move set and
+    # (force-biased workloads) with unbiased moves; one mixed chain
+    single = {"fp64": single_chain_rate(files, local, _lib.YAMC_FP64, max(500, args.moves // 4), per_move),
+              "mixed": single_chain_rate(files, local, _lib.YAMC_MIXED, max(500, args.moves // 4), per_move)}
+    if biased:
+        single["fp64_unbiased_moves"] = single_chain_rate(files, local, _lib.YAMC_FP64, max(500, args.moves // 4), 16,
+                                                          extra="xlambda_f=0,xlambda_c=0")
 
-    single = {"fp64": single_chain(_lib.YAMC_FP64), "mixed": single_chain(_lib.YAMC_MIXED)}
-
-    # ---------------- dE of the mixed form against the FP64 form, move by move on the same stream
-    # (both chains take the same decisions until a draw falls within the dE error of its
-    # threshold; the comparison runs up to there)
-    n_chk = 4000
-    chk = grng.gfortran_stream(4242 + rank, 40 * n_chk + 10000)
-    logs = {}
-    e_tot = {}
-    for prec in (_lib.YAMC_FP64, _lib.YAMC_MIXED):
-        eng = api.Engine.from_files(files, device=local, precision=prec)
-        logs[prec] = eng.run_chain(chk, n_chk)[0]
-        if prec == _lib.YAMC_MIXED:
-            # the mixed chain's running total energy against an FP64 recomputation of its own configuration
-            e_tot = {"incremental": float(eng.energies()[0]), "fp64_full": float(eng.full_sums()[0])}
-        eng.close()
-    lf, lm = logs[_lib.YAMC_FP64], logs[_lib.YAMC_MIXED]
-    same = (lf["imol"] == lm["imol"]) & (lf["flags"] == lm["flags"]) & (lf["cursor"] == lm["cursor"])
-    k_same = n_chk if same.all() else int(np.argmin(same))
-    cols = ("du_real", "du_k_coul", "du_k_lj", "du_ext")
-    de = np.abs(sum(lm[c][:k_same] for c in cols) - sum(lf[c][:k_same] for c in cols))
-    # molecular forces of the force-bias path (movemc Steps 3-4) in both forms, same configuration
-    ef = api.Engine.from_files(files, device=local, precision=_lib.YAMC_FP64)
-    em = api.Engine.from_files(files, device=local, precision=_lib.YAMC_MIXED)
-    ferr, fscale, nf = 0.0, 0.0, 0
-    for imol in range(1, ef.nmol + 1, max(1, ef.nmol // 200)):
-        f1, t1 = ef.move_old(imol)
-        f2, t2 = em.move_old(imol)
-        fscale = max(fscale, float(np.abs(f1).max()))
-        ferr = max(ferr, float(np.abs(f2 - f1).max()))
-        nf += 1
-    ef.close()
-    em.close()
-    de_err = {"max_kT": float(de.max()) if k_same else None, "rms_kT": float(np.sqrt((de ** 2).mean())) if k_same else None,
-              "moves_compared": k_same, "bar_kT": 1e-4,
-              "force_max_abs_err": ferr, "force_scale": fscale, "molecules_compared": nf,
-              "total_energy_err_kT": abs(e_tot["incremental"] - e_tot["fp64_full"]),
-              "total_energy_kT": e_tot["fp64_full"]}
+    # ---------------- the mixed form's errors against FP64 (dE, force, total energy)
+    de_err = precision_errors(files, local, n_chk=1500 if biased else 4000, seed=4242 + rank)
 
     # ---------------- the batch: R independent chains of the workload, one graph launch per step
     # R = the most chains any launch shape keeps resident at once (the tuner then picks the shape)
-    probe = api.Batch([api.load_inputs(files["parameters"], files["composition"], files["moltab"])], device=local)
-    R = args.replicas
-    resident = {}
-    for G in range(1, 17):
-        try:
-            probe.set_launch(G, 0)
-        except Exception:
-            continue
-        resident[G] = probe.launch["resident_clusters"]
-    if not R:
-        R = min(148, max(resident.values(), default=1))
-    probe.close()
-    R = max(R, 1)
+    inp0 = api.load_inputs(files["parameters"], files["composition"], files["moltab"])
+    R, resident = _resident_chains(inp0, local, _lib.YAMC_MIXED)
+    if args.replicas:
+        R = args.replicas
     rep_files = [files] + [systems.write_system(spec, f"{wdir}_{r}", seed=replica_seeds(rank, r)[0],
                                                 rng_seed=replica_seeds(rank, r)[1]) for r in range(1, R)]
-    rep_inputs = [api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files]
+    rep_inputs = [inp0] + [api.load_inputs(f["parameters"], f["composition"], f["moltab"]) for f in rep_files[1:]]
     streams = [grng.gfortran_stream(replica_seeds(rank, r)[1], n_stream) for r in range(R)]
     d_streams = [torch.from_numpy(x).to(dev) for x in streams]
     d_ptrs = [t.data_ptr() for t in d_streams]
@@ -550,7 +515,7 @@ def main():
 
     b64, _, ms64, t64, _ = timed_batch(_lib.YAMC_FP64)
     value_fp64 = ws * R * args.steps * args.moves / t64
-    launch_fp64 = b64.launch
+    launch_fp64 = b64.groups
     b64.close()
     clk = Clocks(local)
     b, cur, kernel_ms, t_dev, launch_counts = timed_batch(_lib.YAMC_MIXED, clk)
@@ -593,7 +558,7 @@ def main():
         return
 
     # ---------------- roofline of the chain kernel
-    log, _, _, _, _ = b.run(host, 2000, cursors=ecur, log=True)
+    log, _, _, _, _ = b.run(host, 1000, cursors=ecur, log=True)
     p_acc = float(np.mean(log["flags"] & 1))
     v0 = views[0]
     bpm = algorithmic_bytes_per_move(spec, v0.nk, v0.nsigned, v0.ntype, p_acc)
@@ -601,28 +566,39 @@ def main():
     moves_launch = R * args.moves
     achieved = bpm * moves_launch / (ms_launch / 1e3) / 1e9
     peak, which = peaks()
-    fpm = algorithmic_flops_per_move(spec, v0.nsigned, v0.ntype)
+    fpm = algorithmic_flops_per_move(spec, v0.nsigned, v0.ntype, biased)
     fp_achieved = fpm * moves_launch / (ms_launch / 1e3) / 1e12
     p64, p32 = api.fma_peak(local, True), api.fma_peak(local, False)
-    launch = b.launch
+    launch = b.groups
+    b.close()
+    del d_streams
+    torch.cuda.empty_cache()
+    move_set = "force-biased moves (lambda = 0.1)" if biased else "unbiased moves"
     line = {
         "metric": METRIC, "value": value, "unit": "moves/s", "n_gpus": ws, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": 1e3 * t_dev / args.steps, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32+f64 (mixed)", "data": "synthetic",
         "config": {"workload": f"{args.workload}: {spec.n_water} SPC/E + {spec.n_na} Na + {spec.n_cl} Cl, "
                                f"{spec.natom} atoms, L={spec.box} A, alpha={spec.alpha}/A, rc={spec.rc} A, "
-                               f"kmax={spec.kmax}",
+                               f"kmax={spec.kmax}, {move_set}",
                    "method": "mixed precision (FP32 phases, k-space terms and pair exp; FP64 rho, sums, "
-                             "Metropolis; FP64 rho refresh every 1e4 accepted moves), unbiased moves",
-                   "fp64": {"value": value_fp64, "unit": "moves/s", "launch": launch_fp64},
-                   "mixed_over_fp64": value / value_fp64,
-                   "de_error_vs_fp64": de_err,
+                             f"Metropolis; FP64 rho refresh every 1e4 accepted moves), {move_set}, "
+                             "independent chains batched in one graph launch per step",
+                   "fp64_batched": {"value": value_fp64, "unit": "moves/s", "launch": launch_fp64,
+                                    "note": "the same chains, workload and shape search in FP64"},
+                   "mixed_over_fp64_batched": value / value_fp64,
+                   "plain_fp64_one_chain": single["fp64"],
+                   "target_ratio": {"value": value / single["fp64"]["value"], "target": 5.0,
+                                    "what": "mixed batched moves/s over the plain FP64 drop-in (one chain, the same "
+                                            "move set)"},
+                   "single_chain": single,
+                   "precision_errors_vs_fp64": de_err,
                    "moves_per_step_per_chain": args.moves, "chains_per_gpu": R,
                    "parallelism": "independent replicas (one cluster per chain)",
                    "launch": launch, "l2": "256 MB write between steps", "accept_fraction": p_acc,
-                   "single_chain": single, "resident_clusters_by_cluster_size": resident},
+                   "resident_clusters_by_cluster_size": resident},
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": TRAFFIC_PER_MOVE * moves_launch, "peak_source": which,
+                     "traffic": None, "peak_source": which,
                      "algorithmic_bytes_per_move": bpm,
                      "fp_pipe": {"algorithmic_flops_per_move": fpm, "achieved_tflops": fp_achieved,
                                  "fp64_fma_peak_tflops": p64, "fp32_fma_peak_tflops": p32,
@@ -632,15 +608,41 @@ def main():
         "gpu_launches": int(sum(launch_counts)),
         "clocks": clk.summary(),
     }
-    if not args.no_target:
-        line["nacl4k_mixed_batch_vs_plain"] = target_block(local, rank)
-    if not args.no_ragged:
-        line["batch_ragged_96"] = ragged_batch_block(local, rank)
-    if not args.no_npt:
-        line["npt_run_mc"] = npt_block(local, rank)
+    tpm = TRAFFIC_PER_MOVE.get(args.workload)
+    if tpm is not None:
+        line["roofline"]["traffic"] = tpm * moves_launch
+        line["roofline"]["traffic_note"] = "ncu DRAM bytes per move of the timed kernel shape x moves of one launch"
+    blocks = {}
+    if not args.no_blocks:
+        blocks["spce256"] = config_block("spce256", local, rank, moves=10000, steps=3, warmup=2)
+        blocks["nacl1m"] = config_block("nacl1m", local, rank, moves=10000, steps=3, warmup=2)
+        blocks["nacl16k"] = config_block("nacl16k", local, rank, moves=300, steps=3, warmup=1)
+        blocks["batch_ragged_96"] = ragged_batch_block(local, rank, moves=4000)
+        blocks["npt_run_mc"] = npt_block(local, rank)
+    line["configs"] = blocks
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(files)
     print(json.dumps(line), flush=True)
+
+
+def config_block(name, local, rank, moves, steps, warmup):
+    """One more configuration of the metric: its plain FP64 chain, the mixed and FP64 batches
+    (as many chains as are resident at once) and the mixed form's errors against FP64."""
+    from yamc_b200 import _lib, systems
+    spec = systems.WORKLOADS[name]
+    per_move = 40 if spec.xlambda > 0 else 16
+    rates, f0 = batch_rates(spec, name, local, rank, moves, steps, warmup, per_move, (_lib.YAMC_FP64, _lib.YAMC_MIXED))
+    one = single_chain_rate(f0, local, _lib.YAMC_FP64, max(200, moves // 4), per_move)
+    out = {"workload": f"{name}: {spec.n_water} SPC/E + {spec.n_na} Na + {spec.n_cl} Cl, {spec.natom} atoms, "
+                       f"L={spec.box} A, alpha={spec.alpha}/A, rc={spec.rc} A, kmax={spec.kmax}, "
+                       + ("force-biased moves (lambda = 0.1)" if spec.xlambda > 0 else "unbiased moves"),
+           "plain_fp64_one_chain": one, **rates,
+           "mixed_over_fp64_batched": rates["mixed"]["value"] / rates["fp64"]["value"],
+           "batched_mixed_over_plain_fp64": rates["mixed"]["value"] / one["value"],
+           "moves_per_step_per_chain": moves, "steps": steps,
+           "precision_errors_vs_fp64": precision_errors(f0, local, n_chk=400 if spec.natom > 20000 else 1500,
+                                                        n_force=60 if spec.natom > 20000 else 200)}
+    return out
 
 
 if __name__ == "__main__":

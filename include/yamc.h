@@ -36,6 +36,14 @@ extern "C" {
 #define YAMC_ECUDA (-10)
 #define YAMC_ETIMEOUT (-11)
 #define YAMC_ERNG_EXHAUSTED (-12)
+/* YAMC_ENAN: a non-finite value where the arithmetic cannot go on.  Refused inputs (a
+   non-finite coordinate, charge or LJ parameter at yamc_create or yamc_set_positions) leave the
+   context unchanged.  A chain (yamc_run_chain, yamc_run_mc, a batch replica) whose move gives a
+   non-finite energy change or bias force stops before deciding that move, with the state, the
+   records and *cursor as they were after the last completed move.  yamc_move_old/_eval return
+   it for a non-finite energy or force (the move cannot be committed), yamc_forces when a force
+   is non-finite (the outputs hold the values), and a full sum (yamc_full_sums, a volume step)
+   when an energy is non-finite (the context then holds those sums: load finite positions). */
 #define YAMC_ENAN (-13)
 #define YAMC_EOVERLAP_INIT (-14)
 
@@ -147,6 +155,22 @@ int yamc_sizes(yamc_ctx *ctx, int32_t out[5]);
    e (optional) receives the 8 energy.dat numbers.  The counterpart of loading a
    new frame into atomic_data before a full recompute. */
 int yamc_set_positions(yamc_ctx *ctx, const double *x, const double *y, const double *z, double e[8]);
+
+/* ---- exact checkpoint ----
+   The reference restarts a run from the last trajectory frame and a new seed (mccont.f90:121-171),
+   which continues the ensemble but not the chain.  These calls save and restore a context's whole
+   state bit for bit -- positions, rho(k), the engine scalars (energies, dipole, tails, step
+   counts), the run_mc counters, the parameters and box-dependent tables as they stand after NPT
+   steps -- together with the caller's random-stream cursor, so a chain continued from a loaded
+   state in a fresh context is identical, move for move and bit for bit, to the uninterrupted one.
+   yamc_state_size gives the blob's size for this context; yamc_save_state writes it (host
+   buffer, host byte order); yamc_load_state reads it into a context created from the same system
+   (same atom, molecule, LJ type and k counts, else YAMC_EPARAMETER), keeping that context's
+   precision, and returns the saved cursor.  Neither may come between an eval and its commit
+   (YAMC_EWRONG_FUNCTION); a batch replica can be saved but not loaded into. */
+int yamc_state_size(yamc_ctx *ctx, int64_t *bytes);
+int yamc_save_state(yamc_ctx *ctx, int64_t cursor, void *buf, int64_t bytes);
+int yamc_load_state(yamc_ctx *ctx, const void *buf, int64_t bytes, int64_t *cursor);
 
 /* ---- adjoint forces ----
    Forces = -gradient of the total energy as implemented, for every atom (kT per

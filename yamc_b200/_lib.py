@@ -16,7 +16,10 @@ LIB_PATH = os.path.join(HERE, "libyamc_b200.so")
 
 YAMC_OK = 0
 YAMC_ELIMITS = -2
+YAMC_EPARAMETER = -3
+YAMC_EWRONG_FUNCTION = -5
 YAMC_ERNG_EXHAUSTED = -12
+YAMC_ENAN = -13
 YAMC_KSPACE_AUTO = 0
 YAMC_KSPACE_REGISTERS = 1
 YAMC_KSPACE_STREAMED = 2
@@ -141,6 +144,9 @@ SIGNATURES = {
     "yamc_realspace_sums_static": (ctypes.c_int, [ctypes.POINTER(YamcParams), ctypes.c_int32] + [_VP] * 7 +
                                    [ctypes.c_int32] + [_VP] * 8),
     "yamc_fma_peak": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int32, _dp]),
+    "yamc_state_size": (ctypes.c_int, [_VP, ctypes.POINTER(ctypes.c_int64)]),
+    "yamc_save_state": (ctypes.c_int, [_VP, ctypes.c_int64, ctypes.c_void_p, ctypes.c_int64]),
+    "yamc_load_state": (ctypes.c_int, [_VP, ctypes.c_void_p, ctypes.c_int64, ctypes.POINTER(ctypes.c_int64)]),
     "yamc_error_string": (ctypes.c_char_p, [ctypes.c_int]),
     "yamc_last_error_detail": (ctypes.c_char_p, []),
 }

@@ -199,7 +199,7 @@ class Engine:
         st = self.lib.yamc_run_chain(self.h, rng.ctypes.data, rng.size, ctypes.byref(cur), int(n_moves), ctypes.byref(done),
                                      rec.ctypes.data if log else None, rows.ctypes.data if max_rows else None,
                                      int(max_rows), ctypes.byref(nrow))
-        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED, _lib.YAMC_ENAN):
             check(st, "yamc_run_chain")
         return rec[: done.value], rows[: nrow.value], cur.value, done.value, st
 
@@ -218,7 +218,7 @@ class Engine:
                                   rec.ctypes.data if log else None, max_log, ctypes.byref(nlog), vrec.ctypes.data,
                                   int(n_cycles), ctypes.byref(nvlog), rows.ctypes.data if max_rows else None,
                                   int(max_rows), ctypes.byref(nrow))
-        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED):
+        if st not in (_lib.YAMC_OK, _lib.YAMC_ERNG_EXHAUSTED, _lib.YAMC_ENAN):
             check(st, "yamc_run_mc")
         return rec[: nlog.value], vrec[: nvlog.value], rows[: nrow.value], cur.value, done.value, st
 
@@ -250,6 +250,21 @@ class Engine:
 
     def xchange_commit(self, accepted: bool) -> None:
         check(self.lib.yamc_xchange_commit(self.h, int(bool(accepted))), "yamc_xchange_commit")
+
+    def save_state(self, cursor: int = 0) -> bytes:
+        """The context's exact state and the caller's stream cursor (yamc_save_state)."""
+        n = ctypes.c_int64(0)
+        check(self.lib.yamc_state_size(self.h, ctypes.byref(n)), "yamc_state_size")
+        buf = ctypes.create_string_buffer(n.value)
+        check(self.lib.yamc_save_state(self.h, int(cursor), buf, n.value), "yamc_save_state")
+        return buf.raw
+
+    def load_state(self, state: bytes) -> int:
+        """Puts a saved state into this context (same system); returns the saved cursor."""
+        cur = ctypes.c_int64(0)
+        buf = ctypes.create_string_buffer(bytes(state), len(state))
+        check(self.lib.yamc_load_state(self.h, buf, len(state), ctypes.byref(cur)), "yamc_load_state")
+        return cur.value
 
     def current_params(self) -> "_lib.YamcParams":
         """The parameters as they stand now (BoxLength follows accepted volume steps)."""

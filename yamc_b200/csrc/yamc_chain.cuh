@@ -136,6 +136,10 @@ struct ChainShared {
     int wnext;
 };
 
+// why a chain stops before its last move (ChainShared::abort)
+constexpr int kAbortStream = 1;     // the random stream ran out (YAMC_ERNG_EXHAUSTED, resumable)
+constexpr int kAbortNonFinite = 2;  // a non-finite energy change or bias force (YAMC_ENAN)
+
 __device__ __forceinline__ void worker_sync(int nwork) {
     asm volatile("bar.sync 1, %0;" ::"r"(nwork) : "memory");
 }
@@ -1237,6 +1241,13 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     mol_force_torque(na, x, y, z, M.mass, fx, fy, fz, F, T);
                 }
                 const double du_total = du_real + (du_kc + du_kl) + du_ext;
+                // a non-finite energy change or bias force (an input the arithmetic cannot take:
+                // NaN positions or random numbers, coincident charges) stops the chain before
+                // the move is decided, with the state as it was after the last completed move
+                bool finite = isfinite(du_total);
+                if (biased)
+                    for (int c = 0; c < 3; ++c) finite = finite && isfinite(F[c]) && isfinite(T[c]);
+                if (!finite) { sh.abort = kAbortNonFinite; sh.accepted = 0; goto decided; }
                 if (biased || SPLIT) {
                     MoveState mv = M.mv;
                     mcm_init_new(mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
@@ -1253,7 +1264,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             }
             sh.accepted = 0;
             if (out) {
-                sh.abort = 1;  // the interrupted move restarts from its first draw (sh.cursor unchanged)
+                sh.abort = kAbortStream;  // the interrupted move restarts from its first draw (sh.cursor unchanged)
             } else {
                 sh.accepted = acc;
                 if (acc) {
@@ -1320,6 +1331,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     }
                 }
             }
+        decided:;
         }
         __syncthreads();
         YAMC_PH(PH_DECIDE);
@@ -1377,7 +1389,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             run->moves_done = moves_done;
             run->n_rows = rows;
             run->accepted = n_acc;
-            run->status = sh.abort ? YAMC_ERNG_EXHAUSTED : YAMC_OK;
+            run->status = sh.abort == kAbortNonFinite ? YAMC_ENAN : (sh.abort ? YAMC_ERNG_EXHAUSTED : YAMC_OK);
         }
     } else if (tid == 0 && rank == 0) {
         run->moves_done = moves_done;

@@ -850,6 +850,8 @@ int full_sums(yamc_ctx *c, int *overlap = nullptr) {
     double tot[kFullParts] = {};
     CUDA_TRY(cudaMemcpyAsync(tot, c->sums, sizeof(tot), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
+    for (int v = 0; v < 6; ++v)
+        if (!std::isfinite(tot[v])) { set_error("non-finite real-space sum"); return YAMC_ENAN; }
     if (overlap) *overlap = tot[6] > 0;
     else if (tot[6] > 0) { set_error("hard-core overlap in the configuration"); return YAMC_EOVERLAP_INIT; }
     switch (H.nt) {
@@ -874,6 +876,7 @@ int full_sums(yamc_ctx *c, int *overlap = nullptr) {
     CUDA_TRY(cudaMemcpyAsync(ek, c->sums + kFullParts, sizeof(ek), cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     const double ekc = ek[0], ekl = ek[1];
+    if (!std::isfinite(ekc) || !std::isfinite(ekl)) { set_error("non-finite k-space sum"); return YAMC_ENAN; }
     // EwaldSumExternal_calc_mu over all atoms, in atom order (EwaldSumExternal.f90:34-52)
     double mx = 0, my = 0, mz = 0;
     for (int i = 0; i < H.N; ++i) { mx = mx + H.q[i] * H.x[i]; my = my + H.q[i] * H.y[i]; mz = mz + H.q[i] * H.z[i]; }
@@ -1433,7 +1436,8 @@ int yamc_run_chain(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor
     int32_t nrow = 0;
     const int st = run_chain_impl(c, c->d_rng, *cursor, n_rng, cursor, n_moves, &done, log ? c->d_log : nullptr,
                                   rows ? c->d_rows : nullptr, rows ? max_rows : 0, &nrow);
-    if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED) return st;
+    if (st != YAMC_OK && st != YAMC_ERNG_EXHAUSTED && st != YAMC_ENAN) return st;
+    if (st == YAMC_ENAN) set_error("non-finite energy change or bias force: the chain stopped before that move");
     if (log && done) CUDA_TRY(cudaMemcpy(log, c->d_log, sizeof(yamc_move_record) * done, cudaMemcpyDeviceToHost));
     if (rows && nrow) CUDA_TRY(cudaMemcpy(rows, c->d_rows, sizeof(double) * 9 * nrow, cudaMemcpyDeviceToHost));
     if (moves_done) *moves_done = done;
@@ -2098,6 +2102,11 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
             double du[4];
             int ov = 0;
             if ((r = xchange_eval(c, imol1, imol2, du, &ov))) return r;
+            if (!ov && !(std::isfinite(du[0]) && std::isfinite(du[1]) && std::isfinite(du[2]) && std::isfinite(du[3]))) {
+                xchange_commit(c, false);
+                set_error("non-finite energy change of an exchange step");
+                *cursor = c0; st = YAMC_ENAN; break;
+            }
             bool acc = false;
             if (!ov) {  // MonteCarloMove_accept_or_decline_simple (MonteCarloMove.f90:572-597)
                 const double factor = std::exp(-(du[0] + (du[1] + du[2]) + du[3]));
@@ -2134,7 +2143,7 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
         int32_t kr = 0;
         const int ks = run_chain_impl(c, c->d_rng, base, n_rng, cursor, n, &mdone, keep ? c->d_log : nullptr,
                                       want_rows ? c->d_rows : nullptr, want_rows ? max_rows - nrow : 0, &kr);
-        if (ks != YAMC_OK && ks != YAMC_ERNG_EXHAUSTED) return ks;
+        if (ks != YAMC_OK && ks != YAMC_ERNG_EXHAUSTED && ks != YAMC_ENAN) return ks;
         if (keep && mdone)
             CUDA_TRY(cudaMemcpy(log + nlog, c->d_log, sizeof(yamc_move_record) * mdone, cudaMemcpyDeviceToHost));
         if (keep) nlog += mdone;
@@ -2144,6 +2153,8 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
         }
         if ((r = pull_state(c))) return r;
         done += c->cnt_h[CN_ICYCLE] - icycle0;
+        // a non-finite energy change: the chain stopped before deciding that move
+        if (ks == YAMC_ENAN) { st = YAMC_ENAN; break; }
         // stopped with no move done although the next step is neither a volume cycle nor an
         // exchange step (both were read above): the stream ran out inside that move
         if (ks == YAMC_ERNG_EXHAUSTED && mdone == 0) { st = YAMC_ERNG_EXHAUSTED; break; }
@@ -2181,6 +2192,12 @@ int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
     std::memcpy(c->cnt_h, pin + kNV + SC_COUNT, sizeof(long long) * CN_COUNT);
     const HostSystem &H = c->H;
     const int f0 = H.first[imol - 1], na = H.natoms[imol - 1];
+    for (int k = 0; k < RV_F + 3 * na; ++k)
+        if (k != RV_DUC && k != RV_DUL && k != RV_OVL && !std::isfinite(out[k])) {
+            set_error("non-finite old-position energy or force");
+            c->api_stage = 0;
+            return YAMC_ENAN;
+        }
     for (int k = 0; k < 3; ++k) c->api_eold[k] = out[k];
     for (int k = 0; k < 3 * na; ++k) c->api_fold[k] = out[RV_F + k];
     double fx[kMaxA], fy[kMaxA], fz[kMaxA];
@@ -2239,6 +2256,16 @@ int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn
     mol_force_torque(na, xn, yn, zn, &H.mass[f0], fx, fy, fz, F, T);
     if (f) { f[0] = F[0]; f[1] = F[1]; f[2] = F[2]; }
     if (tau) { tau[0] = T[0]; tau[1] = T[1]; tau[2] = T[2]; }
+    if (!ovl) {
+        bool finite = std::isfinite(enew - eold) && std::isfinite(out[RV_DUC]) && std::isfinite(out[RV_DUL]) &&
+                      std::isfinite(du_ext);
+        for (int k = 0; k < 3; ++k) finite = finite && std::isfinite(F[k]) && std::isfinite(T[k]);
+        if (!finite) {
+            set_error("non-finite energy change or force at the proposed positions (the move cannot be committed)");
+            c->api_stage = 0;
+            return YAMC_ENAN;
+        }
+    }
     c->api_stage = ovl ? 0 : 2;
     return YAMC_OK;
 }
@@ -2643,8 +2670,10 @@ int yamc_forces(yamc_ctx *c, double *fx, double *fy, double *fz, double *mol_f, 
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     // external term: F = -2 kext q mu (EwaldSumExternal.f90:84-102)
     const double mx = c->sc[SC_MU_X], my = c->sc[SC_MU_Y], mz = c->sc[SC_MU_Z], m2k = H.p.minus_two_kext;
+    bool finite = true;
     for (int i = 0; i < N; ++i) {
         gx[i] = gx[i] + m2k * H.q[i] * mx; gy[i] = gy[i] + m2k * H.q[i] * my; gz[i] = gz[i] + m2k * H.q[i] * mz;
+        finite = finite && std::isfinite(gx[i]) && std::isfinite(gy[i]) && std::isfinite(gz[i]);
         if (fx) fx[i] = gx[i];
         if (fy) fy[i] = gy[i];
         if (fz) fz[i] = gz[i];
@@ -2665,6 +2694,139 @@ int yamc_forces(yamc_ctx *c, double *fx, double *fy, double *fz, double *mol_f, 
             }
         }
     }
+    if (!finite) { set_error("non-finite force (the outputs hold it)"); return YAMC_ENAN; }
+    return YAMC_OK;
+}
+
+// ---------------------------------------------------------------- exact checkpoint
+
+namespace {
+
+// The state blob: a fixed header (sizes that must match the context it is loaded into), the
+// parameters as they stand, the engine scalars and counters, the host-side tables that depend
+// on the box length (NPT steps rescale them with rounding, so they are stored, not rebuilt),
+// the positions and rho(k).  Host byte order; every field 8-byte aligned.
+constexpr char kStateMagic[8] = {'Y', 'A', 'M', 'C', 'S', 'T', '0', '1'};
+struct StateHeader {
+    char magic[8];
+    int32_t natom, nmol, ntype, nk, nsigned, npair;
+    int64_t cursor;
+    int64_t bytes;
+};
+
+struct StateWriter {
+    unsigned char *p;
+    void put(const void *v, size_t bytes) { std::memcpy(p, v, bytes); p += bytes; }
+    void putv(const std::vector<double> &v) { put(v.data(), sizeof(double) * v.size()); }
+};
+struct StateReader {
+    const unsigned char *p;
+    void get(void *v, size_t bytes) { std::memcpy(v, p, bytes); p += bytes; }
+    void getv(std::vector<double> &v) { get(v.data(), sizeof(double) * v.size()); }
+};
+
+size_t state_bytes(const HostSystem &H) {
+    const size_t N = H.N, nt = H.nt;
+    size_t b = sizeof(StateHeader) + sizeof(yamc_params) + sizeof(double) * SC_COUNT + sizeof(long long) * CN_COUNT;
+    b += sizeof(double) * 4;                                   // n_vol_accepted, the three tails
+    b += sizeof(double) * 5 * N;                               // x, y, z, sigma, dhs
+    b += sizeof(double) * nt;                                  // type_sigma
+    b += sizeof(double) * H.nk;                                // beta
+    b += sizeof(double) * (size_t)H.npair * H.S;               // beta_LJ per entry
+    b += sizeof(double) * 5 * nt * nt;                         // lj6, lj12, four_eps, sigma6, sigma2
+    b += sizeof(double2) * (1 + nt) * (size_t)H.S;             // rho(k)
+    return (b + 7) & ~size_t(7);
+}
+
+bool state_idle(const yamc_ctx *c) {
+    if (c->api_stage || c->vol_stage || c->xch_stage) {
+        set_error("a per-move, volume or exchange step is between its eval and commit");
+        return false;
+    }
+    return true;
+}
+
+}  // namespace
+
+int yamc_state_size(yamc_ctx *c, int64_t *bytes) {
+    if (!c || !bytes) return YAMC_EPARAMETER;
+    *bytes = (int64_t)state_bytes(c->H);
+    return YAMC_OK;
+}
+
+int yamc_save_state(yamc_ctx *c, int64_t cursor, void *buf, int64_t bytes) {
+    if (!c || !buf) return YAMC_EPARAMETER;
+    HostSystem &H = c->H;
+    const size_t need = state_bytes(H);
+    if (bytes < (int64_t)need) { set_error("state buffer smaller than yamc_state_size"); return YAMC_ELIMITS; }
+    if (!state_idle(c)) return YAMC_EWRONG_FUNCTION;
+    CUDA_TRY(cudaSetDevice(c->device));
+    int r;
+    if ((r = sync_positions(c)) || (r = pull_state(c))) return r;
+    const size_t nrho = (size_t)(1 + H.nt) * H.S;
+    std::vector<double2> rho(nrho);
+    CUDA_TRY(cudaMemcpyAsync(rho.data(), c->rho, sizeof(double2) * nrho, cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    StateHeader h{};
+    std::memcpy(h.magic, kStateMagic, 8);
+    h.natom = H.N; h.nmol = H.M; h.ntype = H.nt; h.nk = H.nk; h.nsigned = H.S; h.npair = H.npair;
+    h.cursor = cursor;
+    h.bytes = (int64_t)need;
+    std::memset(buf, 0, need);
+    StateWriter w{static_cast<unsigned char *>(buf)};
+    w.put(&h, sizeof h);
+    w.put(&H.p, sizeof H.p);
+    w.put(c->sc, sizeof(double) * SC_COUNT);
+    w.put(c->cnt_h, sizeof(long long) * CN_COUNT);
+    const double extra[4] = {c->n_vol_accepted, H.U_tail_coul, H.U_tail_lj6, H.U_tail_lj12};
+    w.put(extra, sizeof extra);
+    w.putv(H.x); w.putv(H.y); w.putv(H.z); w.putv(H.sigma); w.putv(H.dhs);
+    w.putv(H.type_sigma); w.putv(H.beta); w.putv(H.ebetalj);
+    w.putv(H.lj6); w.putv(H.lj12); w.putv(H.four_eps); w.putv(H.sigma6); w.putv(H.sigma2);
+    w.put(rho.data(), sizeof(double2) * nrho);
+    return YAMC_OK;
+}
+
+int yamc_load_state(yamc_ctx *c, const void *buf, int64_t bytes, int64_t *cursor) {
+    if (!c || !buf) return YAMC_EPARAMETER;
+    HostSystem &H = c->H;
+    const size_t need = state_bytes(H);
+    if (bytes < (int64_t)sizeof(StateHeader)) { set_error("state buffer too short"); return YAMC_EPARAMETER; }
+    StateReader rd{static_cast<const unsigned char *>(buf)};
+    StateHeader h{};
+    rd.get(&h, sizeof h);
+    if (std::memcmp(h.magic, kStateMagic, 8) != 0) { set_error("not a yamc state (bad magic or version)"); return YAMC_EPARAMETER; }
+    if (h.natom != H.N || h.nmol != H.M || h.ntype != H.nt || h.nk != H.nk || h.nsigned != H.S ||
+        h.npair != H.npair || h.bytes != (int64_t)need || bytes < (int64_t)need) {
+        set_error("the state was saved from a context of another system (atom, molecule, LJ type or k counts differ)");
+        return YAMC_EPARAMETER;
+    }
+    if (c->in_batch) {
+        set_error("a batch replica: its batch's graph holds a copy of the replica's tables; load into a context of its own");
+        return YAMC_EWRONG_FUNCTION;
+    }
+    if (!state_idle(c)) return YAMC_EWRONG_FUNCTION;
+    CUDA_TRY(cudaSetDevice(c->device));
+    const int precision = H.p.precision;  // the context's own precision stays
+    rd.get(&H.p, sizeof H.p);
+    H.p.precision = precision;
+    rd.get(c->sc, sizeof(double) * SC_COUNT);
+    rd.get(c->cnt_h, sizeof(long long) * CN_COUNT);
+    double extra[4];
+    rd.get(extra, sizeof extra);
+    c->n_vol_accepted = extra[0];
+    H.U_tail_coul = extra[1]; H.U_tail_lj6 = extra[2]; H.U_tail_lj12 = extra[3];
+    rd.getv(H.x); rd.getv(H.y); rd.getv(H.z); rd.getv(H.sigma); rd.getv(H.dhs);
+    rd.getv(H.type_sigma); rd.getv(H.beta); rd.getv(H.ebetalj);
+    rd.getv(H.lj6); rd.getv(H.lj12); rd.getv(H.four_eps); rd.getv(H.sigma6); rd.getv(H.sigma2);
+    const size_t nrho = (size_t)(1 + H.nt) * H.S;
+    std::vector<double2> rho(nrho);
+    rd.get(rho.data(), sizeof(double2) * nrho);
+    int r;
+    if ((r = upload_box(c)) || (r = upload(c->rho, rho.data(), nrho, c->stream)) || (r = push_state(c))) return r;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    c->api_stage = 0;
+    if (cursor) *cursor = h.cursor;
     return YAMC_OK;
 }
 
@@ -2672,6 +2834,11 @@ int yamc_set_positions(yamc_ctx *c, const double *x, const double *y, const doub
     if (!c || !x || !y || !z) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(c->device));
     HostSystem &H = c->H;
+    for (int i = 0; i < H.N; ++i)
+        if (!(std::isfinite(x[i]) && std::isfinite(y[i]) && std::isfinite(z[i]))) {
+            set_error("non-finite coordinate of atom " + std::to_string(i + 1) + " (the configuration is unchanged)");
+            return YAMC_ENAN;
+        }
     std::vector<double4> a(H.N);
     for (int i = 0; i < H.N; ++i) {
         H.x[i] = x[i]; H.y[i] = y[i]; H.z[i] = z[i];

@@ -340,6 +340,15 @@ int prepare_host_system(const yamc_system *sys, const yamc_params *pin, HostSyst
         set_error("incomplete yamc_system");
         return YAMC_EPARAMETER;
     }
+    for (int i = 0; i < N; ++i) {
+        const double v[8] = {sys->x[i], sys->y[i], sys->z[i], sys->charge[i], sys->sigma[i], sys->epsilon[i],
+                             sys->hard_core_angstr[i], sys->mass[i]};
+        for (double x : v)
+            if (!std::isfinite(x)) {
+                set_error("non-finite input of atom " + std::to_string(i + 1));
+                return YAMC_ENAN;
+            }
+    }
     H.N = N; H.M = M;
     H.x.assign(sys->x, sys->x + N); H.y.assign(sys->y, sys->y + N); H.z.assign(sys->z, sys->z + N);
     H.q.assign(sys->charge, sys->charge + N); H.sigma.assign(sys->sigma, sys->sigma + N);
