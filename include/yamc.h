@@ -317,8 +317,9 @@ int yamc_get_launch(yamc_ctx *ctx, int32_t out[4]);
 int yamc_last_kernel_ms(yamc_ctx *ctx, double *ms);
 /* Per-phase clock64 cycles of the chain kernel, summed over moves by block 0
    (control warp: choose, speculation of the next move, proposal, reduction, Metropolis,
-   commit; worker warps: phase tables, k-space, pair filter, pairs).  mode 1 = reset and enable, 0 = disable,
-   2 = read only; out receives min(n, 11) counters. */
+   commit; worker warps: phase tables, k-space, pair filter, pairs, and -- force-biased moves --
+   the k-space sweep of the next molecule).  mode 1 = reset and enable, 0 = disable,
+   2 = read only; out receives min(n, 12) counters in that order. */
 int yamc_phase_cycles(yamc_ctx *ctx, int32_t mode, int64_t *out, int32_t n);
 const char *yamc_error_string(int status);
 const char *yamc_last_error_detail(void);

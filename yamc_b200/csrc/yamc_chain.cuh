@@ -76,17 +76,19 @@ struct ChainArgs {
     // per-move API (R == 1): imol (1-based) and proposed positions in, results out
     const double *api_in;  // [0] imol, [1 + 3a + c] coordinate c of atom a
     double *api_out;       // the reduction vector of the pass (RV_* layout)
-    double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas
+    double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas (scratch_buf: FP32 pairs in the mixed form)
     long long *prof;       // optional per-phase cycle counters (PH_* layout), CTA 0
 };
 
 // phases timed when ChainArgs::prof is set (control lane 0 or worker thread 32 of CTA 0)
 enum Phase { PH_CHOOSE = 0, PH_SPECULATE, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE,
-             PH_CLUSTER, PH_DECIDE, PH_COMMIT, PH_COUNT };
+             PH_CLUSTER, PH_DECIDE, PH_COMMIT, PH_KSPACE_NEXT, PH_COUNT };
 
-// reduction vector of one pass
+// reduction vector of one pass: the moved molecule's energies, k-space energy change, overlap
+// flag and per-atom forces
 constexpr int RV_EW = 0, RV_LJ6 = 1, RV_LJ12 = 2, RV_DUC = 3, RV_DUL = 4, RV_OVL = 5, RV_F = 6;
 constexpr int kNV = 6 + 3 * kMaxA;
+constexpr int kNVP = kNV;
 
 enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
 
@@ -118,6 +120,10 @@ struct ChainShared {
     long long cursor;     // stream position after the last completed move
     long long icycle, mic;
     double eold[3], fold[3 * kMaxA];
+    // the biased proposal on two warps: the rotation thread's result and stream positions
+    MoveState mrot;
+    long long disp_end, rot_start, rot_end;
+    int disp_out, rot_out;
     double sc[SC_COUNT];
     double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (staged copies may lag in other CTAs)
     int qcount;
@@ -179,27 +185,36 @@ template <> __device__ __forceinline__ float2 cvt2<float2>(double2 v) { return m
 __device__ __forceinline__ double2 to_d2(double2 v) { return v; }
 __device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
 
+// Buffer i of a chain's scratch (0: the moved molecule's old phase sums, 1: the rho deltas of the
+// pass), in the pass's arithmetic type: FP64 pairs in the plain form, FP32 pairs in the mixed
+// form (half the bytes, and loads that need no conversion).
+template <bool MX>
+__host__ __device__ __forceinline__ typename Prec<MX>::R2 *scratch_buf(double2 *base, int i, int nstruct, int S) {
+    return reinterpret_cast<typename Prec<MX>::R2 *>(base) + (size_t)i * nstruct * S;
+}
+
 // Per-thread partial sums of a pass: FP64; in the mixed form FP64 for the pair terms (which
 // reach tens of kT) and FP32 with two-sum compensation (the running sum and its rounding
 // error, added in FP64 when the warp reduces) for the FP32 k-space terms.
-template <bool MX>
+template <bool MX, int N = kNVP>
 struct Acc {
-    double v[kNV];
+    double v[N];
     __device__ __forceinline__ void zero() {
 #pragma unroll
-        for (int i = 0; i < kNV; ++i) v[i] = 0.0;
+        for (int i = 0; i < N; ++i) v[i] = 0.0;
     }
     __device__ __forceinline__ void add(int i, double x) { v[i] += x; }
+    __device__ __forceinline__ void add_plain(int i, double x) { v[i] += x; }
     __device__ __forceinline__ void flag(int i) { v[i] = 1.0; }
     __device__ __forceinline__ double get(int i) const { return v[i]; }
 };
-template <>
-struct Acc<true> {
-    double d[kNV];
-    float s[kNV], c[kNV];
+template <int N>
+struct Acc<true, N> {
+    double d[N];
+    float s[N], c[N];
     __device__ __forceinline__ void zero() {
 #pragma unroll
-        for (int i = 0; i < kNV; ++i) { d[i] = 0.0; s[i] = 0.f; c[i] = 0.f; }
+        for (int i = 0; i < N; ++i) { d[i] = 0.0; s[i] = 0.f; c[i] = 0.f; }
     }
     __device__ __forceinline__ void add(int i, double x) { d[i] += x; }
     __device__ __forceinline__ void add(int i, float x) {  // TwoSum (Knuth)
@@ -208,6 +223,9 @@ struct Acc<true> {
         c[i] += (s[i] - (t - bp)) + (x - bp);
         s[i] = t;
     }
+    // plain FP32 sum, for the k-space forces: they only bias the proposal (their error is
+    // reported beside the dE error), and a few entries per thread keep it near FP32 rounding
+    __device__ __forceinline__ void add_plain(int i, float x) { s[i] += x; }
     __device__ __forceinline__ void flag(int i) { d[i] = 1.0; }
     __device__ __forceinline__ double get(int i) const { return d[i] + ((double)s[i] + (double)c[i]); }
 };
@@ -244,13 +262,13 @@ struct PhaseTabs {
 // Phase tables of slots [s0, s1) of move m, by the workers.  The FP32 form reduces 2 k u
 // modulo 2 in FP64 before the FP32 sincospi.
 template <bool MX>
-__device__ __forceinline__ void build_tables(typename Prec<MX>::R2 *tab, const Cand &m, int s0, int s1, int KM, int wtid,
-                                             int nwork) {
+__device__ __forceinline__ void build_tables(typename Prec<MX>::R2 *tab, const Slot *slots, int s0, int s1, int KM,
+                                             int wtid, int nwork) {
     using R = typename Prec<MX>::R;
     const int n = (s1 - s0) * 3 * KM;
     for (int idx = wtid; idx < n; idx += nwork) {
         const int sl = s0 + idx / (3 * KM), r = idx % (3 * KM), d = r / KM, k = r % KM;
-        const double u = d == 0 ? m.slot[sl].x : (d == 1 ? m.slot[sl].y : m.slot[sl].z);
+        const double u = d == 0 ? slots[sl].x : (d == 1 ? slots[sl].y : slots[sl].z);
         R s, c;
         if constexpr (MX) {
             double t = 2.0 * (double)k * u;
@@ -268,7 +286,7 @@ __device__ __forceinline__ void build_tables(typename Prec<MX>::R2 *tab, const C
 // Coulomb phase q (cos, sin), LJ phase = Coulomb phase * (1/q) (the unit phase when q == 0),
 // accumulated per LJ type in atom order.  ph/phl keep the per-atom phases for the forces.
 template <int NT, bool MX>
-__device__ __forceinline__ void mol_phase_sum(const PhaseTabs<MX> &pt, const Cand &m, int s0, int na, int kx, int ky,
+__device__ __forceinline__ void mol_phase_sum(const PhaseTabs<MX> &pt, const Slot *slots, int s0, int na, int kx, int ky,
                                               int kz, typename Prec<MX>::R2 (&out)[1 + NT],
                                               typename Prec<MX>::R2 (&ph)[kMaxA], typename Prec<MX>::R2 (&phl)[kMaxA]) {
     using R = typename Prec<MX>::R;
@@ -281,7 +299,7 @@ __device__ __forceinline__ void mol_phase_sum(const PhaseTabs<MX> &pt, const Can
         ph[a] = mk2(R(0), R(0));
         phl[a] = mk2(R(0), R(0));
         if (a < na) {
-            const Slot &sl = m.slot[s0 + a];
+            const Slot &sl = slots[s0 + a];
             const R2 *T = pt.T + (size_t)(s0 + a) * 3 * KM;
             const R q = (R)sl.q;
             R c = 0, s = 0;
@@ -306,19 +324,19 @@ __device__ __forceinline__ void mol_phase_sum(const PhaseTabs<MX> &pt, const Can
 // k-space force on the molecule's atoms from one entry: 4 pi beta (C sin - S cos) k per atom,
 // Coulomb with the q-weighted phase, plus the dispersion terms of the atom's LJ type against
 // every type's structure factor (ForceKSpace.f90:59-302).
-template <int NT, bool MX>
-__device__ __forceinline__ void entry_forces(const Cand &m, int s0, int na, int kx, int ky, int kz,
+template <int NT, bool MX, class AccT>
+__device__ __forceinline__ void entry_forces(const Slot *slots, int s0, int na, int kx, int ky, int kz,
                                              typename Prec<MX>::R beta,
                                              const typename Prec<MX>::R (&bl)[NPair<NT>::value],
                                              const typename Prec<MX>::R2 (&C)[1 + NT],
                                              const typename Prec<MX>::R2 (&ph)[kMaxA],
-                                             const typename Prec<MX>::R2 (&phl)[kMaxA], Acc<MX> &acc) {
+                                             const typename Prec<MX>::R2 (&phl)[kMaxA], AccT &acc, int f0 = RV_F) {
     using R = typename Prec<MX>::R;
     const R fourpi = (R)kFourPi;
 #pragma unroll
     for (int a = 0; a < kMaxA; ++a) {
         if (a < na) {
-            const int ta = m.slot[s0 + a].type;
+            const int ta = slots[s0 + a].type;
             R w = fourpi * ((C[0].x * ph[a].y - C[0].y * ph[a].x) * beta);
             if (ta > 0) {
 #pragma unroll
@@ -330,33 +348,33 @@ __device__ __forceinline__ void entry_forces(const Cand &m, int s0, int na, int 
                     w += fourpi * ((C[1 + t].x * phl[a].y - C[1 + t].y * phl[a].x) * b);
                 }
             }
-            acc.add(RV_F + 3 * a, w * (R)kx);
-            acc.add(RV_F + 3 * a + 1, w * (R)ky);
-            acc.add(RV_F + 3 * a + 2, w * (R)kz);
+            acc.add_plain(f0 + 3 * a, w * (R)kx);
+            acc.add_plain(f0 + 3 * a + 1, w * (R)ky);
+            acc.add_plain(f0 + 3 * a + 2, w * (R)kz);
         }
     }
 }
 
 // One signed entry of a pass: the molecule's phase sums at the old positions (into mold) and/or
 // the new ones, the delta (into dl), dU_k Coulomb + LJ against rho, and the k-space forces.
-template <int NT, int KIND, bool FORCES, bool MX>
-__device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Cand &m, int na, int kx,
+template <int NT, int KIND, bool FORCES, bool MX, class AccT>
+__device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Slot *slots, int na, int kx,
                                              int ky, int kz, typename Prec<MX>::R beta,
                                              const typename Prec<MX>::R (&bl)[NPair<NT>::value],
                                              const double2 (&rho)[1 + NT], typename Prec<MX>::R2 (&mold)[1 + NT],
-                                             typename Prec<MX>::R2 (&dl)[1 + NT], Acc<MX> &acc) {
+                                             typename Prec<MX>::R2 (&dl)[1 + NT], AccT &acc) {
     using R = typename Prec<MX>::R;
     using R2 = typename Prec<MX>::R2;
     R2 ph[kMaxA], phl[kMaxA];
     R2 C[1 + NT];
 #pragma unroll
     for (int t = 0; t <= NT; ++t) C[t] = cvt2<R2>(rho[t]);
-    if constexpr (KIND != PASS_NEW) mol_phase_sum<NT, MX>(pt, m, na, na, kx, ky, kz, mold, ph, phl);
+    if constexpr (KIND != PASS_NEW) mol_phase_sum<NT, MX>(pt, slots, na, na, kx, ky, kz, mold, ph, phl);
     if constexpr (KIND == PASS_OLD) {
-        if constexpr (FORCES) entry_forces<NT, MX>(m, na, na, kx, ky, kz, beta, bl, C, ph, phl, acc);
+        if constexpr (FORCES) entry_forces<NT, MX>(slots, na, na, kx, ky, kz, beta, bl, C, ph, phl, acc);
     } else {
         R2 mnew[1 + NT];
-        mol_phase_sum<NT, MX>(pt, m, 0, na, kx, ky, kz, mnew, ph, phl);
+        mol_phase_sum<NT, MX>(pt, slots, 0, na, kx, ky, kz, mnew, ph, phl);
 #pragma unroll
         for (int t = 0; t <= NT; ++t) dl[t] = mk2(mnew[t].x - mold[t].x, mnew[t].y - mold[t].y);
         {   // EwaldSumKSpace_calc_dU_coulomb (EwaldSumKSpace.f90:528-620)
@@ -365,6 +383,8 @@ __device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Cand
         }
         // EwaldSumKSpace_calc_dU_LJ (EwaldSumKSpace.f90:623-753): t1 over all types, t2 over the
         // molecule's types (a type absent from the molecule has a zero delta and adds nothing)
+        // (the entry's terms summed in order first, then added to the compensated running sum)
+        R dul = R(0);
 #pragma unroll
         for (int t1 = 0; t1 < NT; ++t1) {
             const R2 C1 = C[1 + t1], D1 = dl[1 + t1];
@@ -373,88 +393,74 @@ __device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Cand
             for (int t2 = 0; t2 < NT; ++t2) {
                 if (!((pt.tmask >> t2) & 1)) continue;
                 const R2 D2 = dl[1 + t2];
-                acc.add(RV_DUL, (tc * D2.x + ts * D2.y) * bl[pair_idx<NT>(t1, t2)]);
+                dul += (tc * D2.x + ts * D2.y) * bl[pair_idx<NT>(t1, t2)];
             }
         }
+        acc.add(RV_DUL, dul);
         if constexpr (KIND == PASS_NEW && FORCES) {  // against total_new = rho + delta (MC.f90:1136-1163)
             R2 Cn[1 + NT];
 #pragma unroll
             for (int t = 0; t <= NT; ++t) Cn[t] = mk2(C[t].x + dl[t].x, C[t].y + dl[t].y);
-            entry_forces<NT, MX>(m, 0, na, kx, ky, kz, beta, bl, Cn, ph, phl, acc);
+            entry_forces<NT, MX>(slots, 0, na, kx, ky, kz, beta, bl, Cn, ph, phl, acc);
         }
     }
 }
 
-// The workers' part of one pass over the molecule's slots: k-space over their entries, real
-// space over the CTA's atoms (pairs inside the cutoff laid out in the queue by a prefix sum
-// over threads -- a deterministic order -- then evaluated item i by worker i % nwork), and a
-// per-warp reduction into red[worker warp][value].  Worker-only barriers (bar 1).
-template <int NT, int EPT, int KIND, bool FORCES, bool MX>
-__device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
-                                            const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
-                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
-                                            int *nearbuf,
-                                            double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
-                                            long long *prof) {
-    constexpr int NVMAX = FORCES ? kNV : RV_F;
-    const Cand &m = sh.cand[sh.icur];
-    const int na = m.na;
-    const int KM = D.kmax + 1;
-    const int nt = D.nt;
-    const int imol0 = m.imol - 1;
-    const int nwork = blockDim.x - kCtl;
-    const int wtid = threadIdx.x - kCtl;
-    const int lane = threadIdx.x & 31;
-    const int wwarp = wtid >> 5, nww = nwork >> 5;
-    const int s_lo = (KIND == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
-    const int s_hi = (KIND == PASS_NEW) ? na : 2 * na;
+// The k-space sweep of one pass over the worker's entries (kspace_entry per entry).
+// Registers layout: k, beta, beta_LJ and rho stay in registers (R); the old phase sums are R.mold
+// (or read from mold_in when given), the delta R.dl.  Streamed layout: every entry is read from
+// memory (L2-resident), the next entry's loads in flight while the current one computes; the old
+// sums come from mold_in (PASS_NEW, PASS_BOTH's are computed), the delta goes to the chain's
+// scratch.  PASS_OLD stores its phase sums to mold_out (registers layout: when mold_store).
+template <int NT, int EPT, int KIND, bool FORCES, bool MX, class AccT>
+__device__ __forceinline__ void kspace_sweep(const DevSys &D, RegsOf<NT, EPT, MX> &R, const PhaseTabs<MX> &pt,
+                                             const Slot *slots, int na, int e0, int estep,
+                                             const typename Prec<MX>::R2 *mold_in, typename Prec<MX>::R2 *mold_out,
+                                             bool mold_store, AccT &acc) {
     using Rt = typename Prec<MX>::R;
     using R2 = typename Prec<MX>::R2;
-    R2 *tab = reinterpret_cast<R2 *>(tab_raw);
-    const bool pf = prof && wtid == 0;
-    long long t_mark = pf ? clock64() : 0;
-#define YAMC_WPH(ph) do { if (pf) { const long long t_now = clock64(); prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
-
-    build_tables<MX>(tab, m, s_lo, s_hi, KM, wtid, nwork);
-    worker_sync(nwork);
-    YAMC_WPH(PH_TABLES);
-    int tmask = 0;
-    for (int a = 0; a < na; ++a)
-        if (m.slot[a].type > 0) tmask |= 1 << (m.slot[a].type - 1);
-    const PhaseTabs<MX> pt{tab, KM, tmask};
-
-    Acc<MX> acc;
-    acc.zero();
-
+    const int S = D.S;
+    R2 *dl_g = scratch_buf<MX>(D.scratch, 1, 1 + NT, S);
     if constexpr (EPT > 0) {
         static_for<0, EPT>([&](auto kc) {
             constexpr int k = decltype(kc)::value;
             if (R.e[k] < 0) return;
-            kspace_entry<NT, KIND, FORCES, MX>(pt, m, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k], R.rho[k],
-                                               R.mold[k], R.dl[k], acc);
+            if (KIND == PASS_NEW && mold_in) {
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) R.mold[k][t] = mold_in[(size_t)t * S + R.e[k]];
+            }
+            kspace_entry<NT, KIND, FORCES, MX>(pt, slots, na, R.kx[k], R.ky[k], R.kz[k], R.beta[k], R.bl[k],
+                                               R.rho[k], R.mold[k], R.dl[k], acc);
+            if (KIND == PASS_OLD && mold_store) {
+#pragma unroll
+                for (int t = 0; t <= NT; ++t) mold_out[(size_t)t * S + R.e[k]] = R.mold[k][t];
+            }
         });
     } else {
-        // streamed layout: entries e0, e0 + estep, ... read from memory, the next entry's loads in
-        // flight while the current one computes; the old sums and the deltas go to the chain's
-        // scratch for the next pass and the commit
-        const int S = D.S;
-        double2 *mold_g = D.scratch;
-        double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
         // U entries per iteration: their independent dependency chains interleave
         constexpr int U = YAMC_KSPACE_UNROLL;
+        constexpr bool IN_MOLD = KIND == PASS_NEW;   // read the old sums
         int4 kv_n[U];
         Rt beta_n[U], bl_n[U][NPair<NT>::value];
         double2 rho_n[U][1 + NT];
         R2 mold_n[U][1 + NT];
+        // the loads of the next entry stay in flight until the entry is taken up: no value is
+        // converted here (the mixed form reads FP32 copies of the beta tables and FP32 scratch)
         auto fetch = [&](int j, int e) {
             kv_n[j] = D.kvec[e];
-            beta_n[j] = (Rt)D.ebeta[e];
+            if constexpr (MX) {
+                beta_n[j] = D.ebeta_f[e];
 #pragma unroll
-            for (int p = 0; p < NPair<NT>::value; ++p) bl_n[j][p] = (Rt)D.ebetalj[(size_t)p * S + e];
+                for (int p = 0; p < NPair<NT>::value; ++p) bl_n[j][p] = D.ebetalj_f[(size_t)p * S + e];
+            } else {
+                beta_n[j] = D.ebeta[e];
+#pragma unroll
+                for (int p = 0; p < NPair<NT>::value; ++p) bl_n[j][p] = D.ebetalj[(size_t)p * S + e];
+            }
 #pragma unroll
             for (int t = 0; t <= NT; ++t) {
                 rho_n[j][t] = D.rho[(size_t)t * S + e];
-                mold_n[j][t] = (KIND == PASS_NEW) ? cvt2<R2>(mold_g[(size_t)t * S + e]) : mk2(Rt(0), Rt(0));
+                mold_n[j][t] = IN_MOLD ? mold_in[(size_t)t * S + e] : mk2(Rt(0), Rt(0));
             }
         };
         const int step = U * estep;
@@ -481,20 +487,64 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
 #pragma unroll
             for (int j = 0; j < U; ++j)
                 if (e + j * estep < S)
-                    kspace_entry<NT, KIND, FORCES, MX>(pt, m, na, kx[j], ky[j], kz[j], beta[j], bl[j], rho[j], mold[j],
-                                                       dl[j], acc);
+                    kspace_entry<NT, KIND, FORCES, MX>(pt, slots, na, kx[j], ky[j], kz[j], beta[j], bl[j], rho[j],
+                                                       mold[j], dl[j], acc);
 #pragma unroll
             for (int j = 0; j < U; ++j) {
                 const int ej = e + j * estep;
                 if (ej >= S) continue;
 #pragma unroll
                 for (int t = 0; t <= NT; ++t) {
-                    if (KIND == PASS_OLD) mold_g[(size_t)t * S + ej] = to_d2(mold[j][t]);
-                    else dl_g[(size_t)t * S + ej] = to_d2(dl[j][t]);
+                    if (KIND == PASS_OLD) mold_out[(size_t)t * S + ej] = mold[j][t];
+                    else dl_g[(size_t)t * S + ej] = dl[j][t];
                 }
             }
         }
     }
+}
+
+// The workers' part of one pass over the molecule's slots: k-space over their entries, real
+// space over the CTA's atoms (pairs inside the cutoff laid out in the queue by a prefix sum
+// over threads -- a deterministic order -- then evaluated item i by worker i % nwork), and a
+// per-warp reduction into red[worker warp][value].  Worker-only barriers (bar 1).
+template <int NT, int EPT, int KIND, bool FORCES, bool MX>
+__device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
+                                            const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
+                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
+                                            int *nearbuf,
+                                            double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
+                                            long long *prof, typename Prec<MX>::R2 *mold_buf, bool mold_out) {
+    constexpr int NVMAX = FORCES ? kNVP : RV_F;
+    const Cand &m = sh.cand[sh.icur];
+    const int na = m.na;
+    const int KM = D.kmax + 1;
+    const int nt = D.nt;
+    const int imol0 = m.imol - 1;
+    const int nwork = blockDim.x - kCtl;
+    const int wtid = threadIdx.x - kCtl;
+    const int lane = threadIdx.x & 31;
+    const int wwarp = wtid >> 5, nww = nwork >> 5;
+    const int s_lo = (KIND == PASS_OLD) ? na : 0;  // active slots [s_lo, s_hi)
+    const int s_hi = (KIND == PASS_NEW) ? na : 2 * na;
+    using Rt = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+    R2 *tab = reinterpret_cast<R2 *>(tab_raw);
+    const bool pf = prof && wtid == 0;
+    long long t_mark = pf ? clock64() : 0;
+#define YAMC_WPH(ph) do { if (pf) { const long long t_now = clock64(); prof[ph] += t_now - t_mark; t_mark = t_now; } } while (0)
+
+    build_tables<MX>(tab, m.slot, s_lo, s_hi, KM, wtid, nwork);
+    worker_sync(nwork);
+    YAMC_WPH(PH_TABLES);
+    int tmask = 0;
+    for (int a = 0; a < na; ++a)
+        if (m.slot[a].type > 0) tmask |= 1 << (m.slot[a].type - 1);
+    const PhaseTabs<MX> pt{tab, KM, tmask};
+
+    Acc<MX> acc;
+    acc.zero();
+    kspace_sweep<NT, EPT, KIND, FORCES, MX>(D, R, pt, m.slot, na, e0, estep, EPT > 0 ? nullptr : mold_buf, mold_buf,
+                                            mold_out, acc);
     YAMC_WPH(PH_KSPACE);
 
     // bounding spheres of the molecule at its new (slot 0) and old (slot na) positions: an atom
@@ -672,47 +722,89 @@ __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, Re
 #undef YAMC_WPH
 }
 
+// The passes are called, not inlined, when the k entries are streamed (EPT <= 0): each pass then
+// gets the kernel's whole register budget for its own loops instead of sharing it with the
+// control code and the other passes (fewer spills); with entries in registers (EPT > 0) they
+// are inlined, since the entry registers R must stay registers across the passes.
+template <int NT, int EPT, int KIND, bool FORCES, bool MX>
+__device__ __noinline__ void worker_pass_call(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
+                                              const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
+                                              int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
+                                              int *nearbuf, double *red, const double *lj_s, int nown, int qcap, int e0,
+                                              int estep, long long *prof, typename Prec<MX>::R2 *mold_buf, bool mold_out) {
+    worker_pass_body<NT, EPT, KIND, FORCES, MX>(D, sh, R, tab_raw, atom_s, dhs_ts, dhs_g, dhs_typed, grank, gsize, meta_s,
+                                                queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof, mold_buf, mold_out);
+}
+
+template <int NT, int EPT, int KIND, bool FORCES, bool MX>
+__device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
+                                            const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
+                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
+                                            int *nearbuf, double *red, const double *lj_s, int nown, int qcap, int e0,
+                                            int estep, long long *prof, typename Prec<MX>::R2 *mold_buf, bool mold_out) {
+    if constexpr (EPT > 0)
+        worker_pass_body<NT, EPT, KIND, FORCES, MX>(D, sh, R, tab_raw, atom_s, dhs_ts, dhs_g, dhs_typed, grank, gsize,
+                                                    meta_s, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof,
+                                                    mold_buf, mold_out);
+    else
+        worker_pass_call<NT, EPT, KIND, FORCES, MX>(D, sh, R, tab_raw, atom_s, dhs_ts, dhs_g, dhs_typed, grank, gsize,
+                                                    meta_s, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof,
+                                                    mold_buf, mold_out);
+}
+
 // Control warp, after the workers' per-warp partials: trees over the worker warps, then over the
 // cluster's CTAs in a fixed order, so every CTA holds bit-identical totals in sh.tot.  Called by
-// all threads (the cluster barrier needs everyone).
+// all threads (the cluster barrier needs everyone).  Lane l of the control warp owns values l and
+// l + 32 (nv <= 64).
 __device__ __forceinline__ void reduce_pass(ChainShared &sh, const double *red, double *xch, int nv, int G, int rank,
                                             int xpar, cg::cluster_group &cluster) {
-    // lane v of the control warp owns value v: the worker warps' partials in warp order, then
-    // (cluster) every CTA's sum in rank order -- the same order in every CTA
+    // the worker warps' partials in warp order, then (cluster) every CTA's sum in rank order --
+    // the same order in every CTA
     const int lane = threadIdx.x & 31;
     const int nww = (blockDim.x - kCtl) >> 5;
     if (threadIdx.x < kCtl) {
-        double x = 0.0;
-        if (lane < nv) {
-            for (int w = 0; w < nww; ++w) {
-                const double y = red[w * kNV + lane];
-                x = (lane == RV_OVL) ? fmax(x, y) : x + y;
-            }
+        double x[2] = {0.0, 0.0};
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int v = lane + 32 * h;
+            if (v < nv)
+                for (int w = 0; w < nww; ++w) {
+                    const double y = red[w * kNV + v];
+                    x[h] = (v == RV_OVL) ? fmax(x[h], y) : x[h] + y;
+                }
         }
         if (G > 1) {
             // value v of this CTA to every rank's exchange row; lanes cover (v, r) pairs
             for (int idx = 0; idx < nv * G; idx += 32) {
                 const int my = idx + lane;
                 const int v = my % nv, r = my / nv;
-                const double xv = __shfl_sync(0xffffffffu, x, v < 32 ? v : 0);
+                const double x0 = __shfl_sync(0xffffffffu, x[0], v & 31);
+                const double x1 = __shfl_sync(0xffffffffu, x[1], v & 31);
                 if (my < nv * G) {
                     double *dst = cluster.map_shared_rank(xch, r);
-                    dst[(xpar * G + rank) * kNV + v] = xv;
+                    dst[(xpar * G + rank) * kNV + v] = v < 32 ? x0 : x1;
                 }
             }
-        } else if (lane < nv) {
-            sh.tot[lane] = x;
+        } else {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+                if (lane + 32 * h < nv) sh.tot[lane + 32 * h] = x[h];
         }
     }
     if (G > 1) {
         cluster.sync();
-        if (threadIdx.x < kCtl && lane < nv) {
-            double x = 0.0;
-            for (int r = 0; r < G; ++r) {
-                const double y = xch[(xpar * G + r) * kNV + lane];
-                x = (lane == RV_OVL) ? fmax(x, y) : x + y;
+        if (threadIdx.x < kCtl) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int v = lane + 32 * h;
+                if (v >= nv) continue;
+                double x = 0.0;
+                for (int r = 0; r < G; ++r) {
+                    const double y = xch[(xpar * G + r) * kNV + v];
+                    x = (v == RV_OVL) ? fmax(x, y) : x + y;
+                }
+                sh.tot[v] = x;
             }
-            sh.tot[lane] = x;
         }
     }
 }
@@ -986,7 +1078,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
 #pragma unroll
         for (int t = 0; t <= NT; ++t) {
             R.rho[k][t] = e < S ? D.rho[(size_t)t * S + e] : make_double2(0, 0);
-            R.mold[k][t] = (A.mode == MODE_EVAL && e < S) ? cvt2<R2>(A.scratch[(size_t)t * S + e]) : mk2(Rt(0), Rt(0));
+            R.mold[k][t] = (A.mode == MODE_EVAL && e < S) ? scratch_buf<MX>(A.scratch, 0, 1 + NT, S)[(size_t)t * S + e]
+                                                          : mk2(Rt(0), Rt(0));
             R.dl[k][t] = mk2(Rt(0), Rt(0));
         }
     }
@@ -1028,7 +1121,10 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     }
     __syncthreads();
     const bool biased = SPLIT && (D.xlf > 0.0 || D.xlc > 0.0);
-    const bool speculate = !SPLIT;
+    // the next move is prepared while the workers run the current pass: chosen and proposed for
+    // unbiased moves, only chosen for force-biased ones (their proposal needs the old forces)
+    const bool choose_only = biased && A.mode == MODE_RUN;
+    const bool speculate = !SPLIT || choose_only;
     const ChooseCtx X{&D, run, rwin[0], rwin[1], atom_s, G};
 
     long long moves_done = 0;
@@ -1047,6 +1143,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     bool have_next = false;  // sh.cur already prepared by the previous iteration's speculation
     for (long long it = 0; it < n_moves; ++it) {
         if (pc) t_mark = clock64();
+        R2 *mold_g = scratch_buf<MX>(D.scratch, 0, 1 + NT, S);  // the moved molecule's old phase sums
         if (!have_next) {
             // choose the molecule and stage its atoms (no move in flight)
             if (tid == 0) {
@@ -1065,15 +1162,17 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     C.cur_prop = sh.cursor;
                 }
                 stage_molecule(X, sh, C, imol, -1, nullptr, cluster);
-                sh.abort = C.valid ? 0 : 1;
+                sh.abort = C.valid ? 0 : kAbortStream;
             }
             __syncthreads();
             if (sh.abort) break;
             YAMC_PH(PH_CHOOSE);
+        }
+        if (!have_next || choose_only) {
             const int na0 = sh.cand[sh.icur].na;
             // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
             if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
-                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
                 __syncthreads();
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
                 xpar ^= 1;
@@ -1092,7 +1191,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     for (int k = 0; k < EPT; ++k)
                         if (R.e[k] >= 0) {
 #pragma unroll
-                            for (int t = 0; t <= NT; ++t) A.scratch[(size_t)t * S + R.e[k]] = to_d2(R.mold[k][t]);
+                            for (int t = 0; t <= NT; ++t) mold_g[(size_t)t * S + R.e[k]] = R.mold[k][t];
                         }
                     __syncthreads();
                     if (tid == 0 && rank == 0) {
@@ -1104,22 +1203,85 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 }
             }
             // the proposal (movemc Step 5)
-            if (tid == 0) {
-                Cand &C = sh.cand[sh.icur];
-                if (A.mode == MODE_RUN) {
-                    RngReader rng = make_reader(X, sh, C.cur_prop);
-                    double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
-                    if (biased) {
+            if (biased && A.mode == MODE_RUN) {
+                // on two warps: thread 0 draws the displacement (its Newton iteration is the long
+                // serial part) while thread 32 skips the displacement's draws and draws the rotation;
+                // both read the old forces thread 0 has just written
+                __syncthreads();
+                if (tid == 0 || tid == 32) {
+                    const Cand &C = sh.cand[sh.icur];
+                    double F[3], T[3];
+                    {
                         double xo[kMaxA], yo[kMaxA], zo[kMaxA], fx[kMaxA], fy[kMaxA], fz[kMaxA];
-                        for (int a = 0; a < na0; ++a) {
-                            xo[a] = C.slot[na0 + a].x; yo[a] = C.slot[na0 + a].y; zo[a] = C.slot[na0 + a].z;
+#pragma unroll
+                        for (int a = 0; a < kMaxA; ++a) {
+                            const int s0 = a < na0 ? na0 + a : na0;
+                            xo[a] = C.slot[s0].x; yo[a] = C.slot[s0].y; zo[a] = C.slot[s0].z;
                             fx[a] = sh.fold[3 * a]; fy[a] = sh.fold[3 * a + 1]; fz[a] = sh.fold[3 * a + 2];
                         }
                         mol_force_torque(na0, xo, yo, zo, C.mass, fx, fy, fz, F, T);
                     }
-                    propose(D, C, rng, F, T);
+                    RngReader rng = make_reader(X, sh, C.cur_prop);
+                    if (tid == 0) {
+                        MoveState &m = sh.cand[sh.icur].mv;
+                        mcm_init_old(m, F, T);
+                        mcm_choose_displacement(m, rng, D.xlf, D.dr);
+                        sh.disp_end = rng.cur;
+                        sh.disp_out = rng.out;
+                    } else {
+                        MoveState mr;
+                        mcm_init_old(mr, F, T);
+                        mcm_skip_displacement(mr, rng, D.xlf, D.dr);
+                        sh.rot_start = rng.cur;
+                        if (!rng.out) mcm_choose_rotation(mr, rng, D.xlc, D.d_angle);
+                        sh.mrot = mr;
+                        sh.rot_end = rng.cur;
+                        sh.rot_out = rng.out;
+                    }
+                }
+                __syncthreads();
+                if (tid == 0) {
+                    Cand &C = sh.cand[sh.icur];
+                    MoveState &m = C.mv;
+                    bool out = sh.disp_out != 0;
+                    long long cur = sh.disp_end;
+                    if (!out) {
+                        if (sh.rot_start == sh.disp_end) {
+                            copy_rotation(m, sh.mrot);
+                            cur = sh.rot_end;
+                            out = sh.rot_out != 0;
+                        } else {  // (the skip always draws what the displacement draws; kept as a guard)
+                            RngReader rng = make_reader(X, sh, sh.disp_end);
+                            mcm_choose_rotation(m, rng, D.xlc, D.d_angle);
+                            cur = rng.cur;
+                            out = rng.out != 0;
+                        }
+                    }
+                    if (out) {
+                        C.valid = 0;
+                        sh.abort = kAbortStream;
+                    } else {
+                        double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
+#pragma unroll
+                        for (int a = 0; a < kMaxA; ++a) {
+                            const Slot &o = C.slot[a < na0 ? na0 + a : na0];
+                            xo[a] = o.x; yo[a] = o.y; zo[a] = o.z;
+                        }
+                        place_molecule(m, na0, xo, yo, zo, C.mass, xn, yn, zn);
+#pragma unroll
+                        for (int a = 0; a < kMaxA; ++a)
+                            if (a < na0) { C.slot[a].x = xn[a]; C.slot[a].y = yn[a]; C.slot[a].z = zn[a]; }
+                        C.cur_prop = cur;
+                    }
+                }
+            } else if (tid == 0) {
+                Cand &C = sh.cand[sh.icur];
+                if (A.mode == MODE_RUN) {
+                    RngReader rng = make_reader(X, sh, C.cur_prop);
+                    const double Z[3] = {0, 0, 0};
+                    propose(D, C, rng, Z, Z);
                     C.cur_prop = rng.cur;
-                    if (rng.out) { C.valid = 0; sh.abort = 1; }
+                    if (rng.out) { C.valid = 0; sh.abort = kAbortStream; }
                 } else {  // MODE_EVAL: positions from the host
                     for (int a = 0; a < na0; ++a) {
                         C.slot[a].x = A.api_in[1 + 3 * a]; C.slot[a].y = A.api_in[2 + 3 * a]; C.slot[a].z = A.api_in[3 + 3 * a];
@@ -1135,8 +1297,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
 
         // ------------------------------------------------ the pass over the new positions
         if (!ctl) {
-            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
-            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof);
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
+            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
         } else if (speculate && it + 1 < n_moves) {
             // prepare the next move's candidates while the workers run: lanes 1-2 after the
             // acceptance draw, lane 2 with the molecule in flight at its proposed positions (used
@@ -1176,7 +1338,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 const Slot *moving = (lane == 2) ? &M.slot[0] : &M.slot[M.na];
                 stage_molecule(X, sh, C, imol > 0 ? imol : 1, M.imol - 1, moving, cluster);
                 const double Z[3] = {0, 0, 0};
-                if (C.valid) propose(D, C, rng, Z, Z);
+                if (C.valid && !choose_only) propose(D, C, rng, Z, Z);
                 C.cur_prop = rng.cur;
                 if (rng.out) C.valid = 0;
             }
@@ -1192,7 +1354,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             for (int k = 0; k < EPT; ++k)
                 if (R.e[k] >= 0) {
 #pragma unroll
-                    for (int t = 0; t <= NT; ++t) A.scratch[(size_t)(1 + nt + t) * S + R.e[k]] = to_d2(R.dl[k][t]);
+                    for (int t = 0; t <= NT; ++t) scratch_buf<MX>(A.scratch, 1, 1 + NT, S)[(size_t)t * S + R.e[k]] = R.dl[k][t];
                 }
             __syncthreads();
             if (tid == 0 && rank == 0)
@@ -1344,12 +1506,12 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 for (int t = 0; t <= NT; ++t) { R.rho[k][t].x += R.dl[k][t].x; R.rho[k][t].y += R.dl[k][t].y; }
             if constexpr (EPT <= 0) {
                 if (!ctl) {
-                    const double2 *dl_g = D.scratch + (size_t)(1 + NT) * S;
+                    const R2 *dl_g = scratch_buf<MX>(D.scratch, 1, 1 + NT, S);
                     for (int e = e0; e < S; e += gwork)
 #pragma unroll
                         for (int t = 0; t <= NT; ++t) {
                             double2 r = D.rho[(size_t)t * S + e];
-                            const double2 d = dl_g[(size_t)t * S + e];
+                            const double2 d = to_d2(dl_g[(size_t)t * S + e]);
                             r.x += d.x; r.y += d.y;
                             D.rho[(size_t)t * S + e] = r;
                         }

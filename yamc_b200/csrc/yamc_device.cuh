@@ -31,10 +31,11 @@ struct DevSys {
     const int4 *kvec;      // kx, signed ky, signed kz, half-space index
     const double *ebeta;   // Coulomb beta per signed entry (2x for kx>0 folded in)
     const double *ebetalj; // npair x S
+    const float *ebeta_f, *ebetalj_f;  // FP32 copies of ebeta and ebetalj (the mixed form's k-space reads)
     const int *pair_index; // nt*nt -> pair row
     const double *lj_sig6, *lj_feps;  // nt*nt tables (offset (t1-1)*nt + t2-1)
     double2 *rho;          // (1+nt) x S: Coulomb then one row per LJ type
-    double2 *scratch;      // 2 x (1+nt) x S: the moved molecule's old phase sums, then the rho deltas
+    double2 *scratch;      // 2 x (1+nt) x S: the moved molecule's old phase sums, then the rho deltas (FP32 pairs in the mixed form)
     const double *freq_beg, *freq_end;
     double *scal;          // engine scalars, see Scal
     long long *cnt;        // run_mc counters, see Cnt
@@ -406,7 +407,10 @@ __host__ __device__ inline void mcm_choose_displacement(MoveState &m, RngReader 
         double u;
         if (z <= log(4.0)) { const double s = exp(z); u = pow(3.0 * s, 1.0 / 3.0) - s / 10.0; }
         else u = z - log(z / 2.0);
-        for (int k = 1; k <= 10; ++k) {   // Newton on h(u) = u + ln(u ch u - sh u) = z
+        // Newton on h(u) = u + ln(u ch u - sh u) = z, 10 iterations, the last one only for e at the
+        // final u.  Once an update leaves u unchanged every later iteration repeats the same
+        // arithmetic on the same u, so the loop stops there with the same u and e bit for bit.
+        for (int k = 1; k <= 10; ++k) {
             e = exp(-2.0 * u);
             const double ch = (1.0 + e) / 2.0;
             double sh = (1.0 - e) / 2.0;
@@ -415,7 +419,11 @@ __host__ __device__ inline void mcm_choose_displacement(MoveState &m, RngReader 
             if (u < 1e-3) g = u * u * u / 3.0;
             const double h = u + log(g);
             const double h1 = u * sh / g;
-            if (k < 10) u = u + (z - h) / h1;
+            if (k < 10) {
+                const double un = u + (z - h) / h1;
+                if (un == u) break;
+                u = un;
+            }
         }
         const double deltar = u / (xlf * m.fo);
         xksi = 1.0;
@@ -450,6 +458,45 @@ __host__ __device__ inline void mcm_choose_displacement(MoveState &m, RngReader 
         umax = 0.0; m.cold = 1.0;
     }
     m.umaxold = umax;
+}
+
+// The random numbers MonteCarloMove_chooseDisplacement draws, without its arithmetic: its
+// rejection loops alone (the force direction decides the w test), so the rotation, which draws
+// next, can start on another thread while the displacement itself is computed.  Draws exactly
+// what mcm_choose_displacement draws, in the same order.
+__host__ __device__ inline void mcm_skip_displacement(const MoveState &m, RngReader &rng, double xlf, double dr) {
+    const double umax = xlf * m.fo * dr;
+    double v2, vx, vy, vz;
+    if (umax > 1e-2) {
+        double xksi = 0.0;
+        while (xksi < 1e-10) { xksi = rng.next(); if (rng.out) return; }
+        xksi = 1.0;
+        while (xksi > (1.0 - 1e-10) || xksi < 1e-10) { xksi = rng.next(); if (rng.out) return; }
+        double w = -1.0, wx, wy, wz;
+        while (w <= 1e-10) {
+            v2 = 2.0;
+            while (v2 > 1.0) {
+                vx = 2.0 * rng.next() - 1.0; vy = 2.0 * rng.next() - 1.0; vz = 2.0 * rng.next() - 1.0;
+                if (rng.out) return;
+                v2 = vx * vx + vy * vy + vz * vz;
+            }
+            cross(vx, vy, vz, m.fxo, m.fyo, m.fzo, wx, wy, wz);
+            w = sqrt(wx * wx + wy * wy + wz * wz);
+        }
+    } else {
+        v2 = 2.0;
+        while (v2 > 1.0) {
+            vx = 2.0 * rng.next() - 1.0; vy = 2.0 * rng.next() - 1.0; vz = 2.0 * rng.next() - 1.0;
+            if (rng.out) return;
+            v2 = vx * vx + vy * vy + vz * vz;
+        }
+    }
+}
+
+// the fields MonteCarloMove_chooseRotation sets
+__host__ __device__ inline void copy_rotation(MoveState &d, const MoveState &s) {
+    d.qold = s.qold; d.vx = s.vx; d.vy = s.vy; d.vz = s.vz; d.angle = s.angle; d.vmaxold = s.vmaxold;
+    d.ca = s.ca; d.sa = s.sa; d.ct = s.ct; d.st = s.st; d.cphi = s.cphi; d.sphi = s.sphi;
 }
 
 // MonteCarloMove_chooseRotation (MonteCarloMove.f90:269-444)

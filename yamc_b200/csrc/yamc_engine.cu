@@ -591,6 +591,11 @@ __global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { double2 r = rho[i]; const double2 d = delta[i]; r.x += d.x; r.y += d.y; rho[i] = r; }
 }
+// the same with the FP32 deltas of the mixed form's pass (rho itself stays FP64)
+__global__ void k_commit_rho_f(double2 *rho, const float2 *delta, int n) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) { double2 r = rho[i]; const float2 d = delta[i]; r.x += (double)d.x; r.y += (double)d.y; rho[i] = r; }
+}
 
 }  // namespace yamc
 
@@ -642,6 +647,8 @@ struct yamc_ctx {
     double4 *atom = nullptr;
     int2 *meta = nullptr, *mol = nullptr;
     double *dhs = nullptr, *mass = nullptr, *ebeta = nullptr, *ebetalj = nullptr, *lj_sig6 = nullptr, *lj_feps = nullptr;
+    float *ebeta_f = nullptr, *ebetalj_f = nullptr;  // FP32 copies of ebeta / ebetalj for the mixed form
+    std::vector<float> h_ebeta_f, h_ebetalj_f;       // their host sources (kept: the uploads are asynchronous)
     int4 *kvec = nullptr;
     int *pair_index = nullptr;
     double2 *rho = nullptr, *scratch = nullptr;
@@ -1147,6 +1154,8 @@ const char *yamc_error_string(int s) {
 
 int yamc_destroy(yamc_ctx *c);
 
+static int upload_beta_f(yamc_ctx *c);
+
 static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p, int32_t device) {
     int r = prepare_host_system(sys, p, &c->H);
     if (r) return r;
@@ -1160,6 +1169,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     const int N = H.N, M = H.M, S = H.S, nt = H.nt;
     if ((r = dalloc(&c->atom, N)) || (r = dalloc(&c->meta, N)) || (r = dalloc(&c->dhs, N)) || (r = dalloc(&c->mass, N)) ||
         (r = dalloc(&c->mol, M)) || (r = dalloc(&c->kvec, S)) || (r = dalloc(&c->ebeta, S)) ||
+        (r = dalloc(&c->ebeta_f, S)) || (r = dalloc(&c->ebetalj_f, (size_t)H.npair * S)) ||
         (r = dalloc(&c->ebetalj, (size_t)H.npair * S)) || (r = dalloc(&c->pair_index, nt * nt)) ||
         (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
         (r = dalloc(&c->scratch, (size_t)2 * (1 + nt) * S)) || (r = dalloc(&c->freq_beg, M)) || (r = dalloc(&c->freq_end, M)) ||
@@ -1208,7 +1218,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = upload(c->dhs, H.dhs.data(), N, c->stream)) || (r = upload(c->mass, H.mass.data(), N, c->stream)) ||
         (r = upload(c->mol, mo.data(), M, c->stream)) || (r = upload(c->kvec, kv.data(), S, c->stream)) ||
         (r = upload(c->ebeta, H.ebeta.data(), S, c->stream)) || (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) ||
-        (r = upload(c->pair_index, pidx.data(), nt * nt, c->stream)) || (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
+        (r = upload_beta_f(c)) || (r = upload(c->pair_index, pidx.data(), nt * nt, c->stream)) || (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
         (r = upload(c->lj_feps, H.four_eps.data(), nt * nt, c->stream)) || (r = upload(c->freq_beg, H.freq_beg.data(), M, c->stream)) ||
         (r = upload(c->freq_end, H.freq_end.data(), M, c->stream)) ||
         (r = upload(c->spec, reinterpret_cast<const int4 *>(H.spec.data()), H.spec.size() / 4, c->stream)))
@@ -1227,6 +1237,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.xprob = 0.0;
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
+    D.ebeta_f = c->ebeta_f; D.ebetalj_f = c->ebetalj_f;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
     D.nspec = (int)(H.spec.size() / 4); D.spec = c->spec;
     if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
@@ -1251,7 +1262,8 @@ int yamc_destroy(yamc_ctx *c) {
     if (!c) return YAMC_OK;
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
-    void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->lj_sig6, c->lj_feps, c->kvec,
+    void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->ebeta_f, c->ebetalj_f,
+                    c->lj_sig6, c->lj_feps, c->kvec,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
                     c->tpairs, c->rho_part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
                     c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save};
@@ -1461,6 +1473,18 @@ static bool host_rand(const float *rng, int64_t n_rng, int64_t *cursor, double *
 
 // the device data that depend on the box length, from the host copy: positions, hard-core
 // diameters / L, beta and beta_LJ per signed entry, the LJ tables and the scalar parameters
+// the mixed form's FP32 copies of the beta tables, from H.ebeta / H.ebetalj as they stand
+static int upload_beta_f(yamc_ctx *c) {
+    const HostSystem &H = c->H;
+    c->h_ebeta_f.assign(H.ebeta.begin(), H.ebeta.end());
+    c->h_ebetalj_f.assign(H.ebetalj.begin(), H.ebetalj.end());
+    int r;
+    if ((r = upload(c->ebeta_f, c->h_ebeta_f.data(), c->h_ebeta_f.size(), c->stream)) ||
+        (r = upload(c->ebetalj_f, c->h_ebetalj_f.data(), c->h_ebetalj_f.size(), c->stream)))
+        return r;
+    return YAMC_OK;
+}
+
 static int upload_box(yamc_ctx *c) {
     HostSystem &H = c->H;
     const int N = H.N, S = H.S, nt = H.nt;
@@ -1470,7 +1494,7 @@ static int upload_box(yamc_ctx *c) {
     int r;
     if ((r = upload(c->atom, a.data(), N, c->stream)) || (r = upload(c->dhs, H.dhs.data(), N, c->stream)) ||
         (r = upload(c->ebeta, H.ebeta.data(), S, c->stream)) ||
-        (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) ||
+        (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) || (r = upload_beta_f(c)) ||
         (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
         (r = upload(c->lj_feps, H.four_eps.data(), nt * nt, c->stream)))
         return r;
@@ -2278,7 +2302,10 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     HostSystem &H = c->H;
     const int imol = c->api_imol, f0 = H.first[imol - 1], na = H.natoms[imol - 1];
     const int n = (1 + H.nt) * H.S;
-    k_commit_rho<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, c->scratch + n, n);
+    if (is_mixed(c))  // the chain kernel's deltas: scratch buffer 1 in the pass's arithmetic type
+        k_commit_rho_f<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, scratch_buf<true>(c->scratch, 1, 1 + H.nt, H.S), n);
+    else
+        k_commit_rho<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, scratch_buf<false>(c->scratch, 1, 1 + H.nt, H.S), n);
     CUDA_TRY(cudaGetLastError());
     // the uploads come from the pinned commit block: every per-move call that follows ends with
     // a stream synchronisation before the host writes that block again
