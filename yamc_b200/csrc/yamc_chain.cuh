@@ -50,7 +50,6 @@ struct LaunchCfg {
 // current one ends after a hard-core overlap (no acceptance draw) or one draw later, and when
 // the next molecule is the one being moved its old positions depend on the decision, so lanes
 // 0-2 prepare the (at most) three candidates and the decision picks one.
-enum ChainMode { MODE_RUN = 0, MODE_OLD = 1, MODE_EVAL = 2 };
 
 // per-replica run control, in device memory
 struct RunSlot {
@@ -70,12 +69,8 @@ struct ChainArgs {
     const DevSys *sys;  // [R]
     RunSlot *run;       // [R]
     int G;              // CTAs per chain (cluster size)
-    int mode;
     int nown_max;       // atoms staged per CTA (interleaved ownership: atom j lives in CTA j % G)
     int qcap;           // pair queue capacity per CTA
-    // per-move API (R == 1): imol (1-based) and proposed positions in, results out
-    const double *api_in;  // [0] imol, [1 + 3a + c] coordinate c of atom a
-    double *api_out;       // the reduction vector of the pass (RV_* layout)
     double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas (scratch_buf: FP32 pairs in the mixed form)
     long long *prof;       // optional per-phase cycle counters (PH_* layout), CTA 0
 };
@@ -1009,7 +1004,7 @@ __device__ __noinline__ void refresh_in_chain(const DevSys &D, Regs &R, double2 
 }
 
 // SPLIT = false: unbiased device-resident chain only (one fused pass per move, speculation);
-// SPLIT = true: force-biased moves and the per-move API (old pass + new pass with forces).
+// SPLIT = true: force-biased moves (old pass + new pass with forces).
 template <int NT, int EPT, bool SPLIT, bool MX>
 __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThreads, 1) k_chain(ChainArgs A) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1078,8 +1073,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
 #pragma unroll
         for (int t = 0; t <= NT; ++t) {
             R.rho[k][t] = e < S ? D.rho[(size_t)t * S + e] : make_double2(0, 0);
-            R.mold[k][t] = (A.mode == MODE_EVAL && e < S) ? scratch_buf<MX>(A.scratch, 0, 1 + NT, S)[(size_t)t * S + e]
-                                                          : mk2(Rt(0), Rt(0));
+            R.mold[k][t] = mk2(Rt(0), Rt(0));
             R.dl[k][t] = mk2(Rt(0), Rt(0));
         }
     }
@@ -1112,7 +1106,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
         }
     }
     // first random window at the start cursor
-    if (ctl && A.mode == MODE_RUN) {
+    if (ctl) {
         const long long base = run->cursor;
         const long long avail = n_rng - base;
         const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
@@ -1123,7 +1117,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     const bool biased = SPLIT && (D.xlf > 0.0 || D.xlc > 0.0);
     // the next move is prepared while the workers run the current pass: chosen and proposed for
     // unbiased moves, only chosen for force-biased ones (their proposal needs the old forces)
-    const bool choose_only = biased && A.mode == MODE_RUN;
+    const bool choose_only = biased;
     const bool speculate = !SPLIT || choose_only;
     const ChooseCtx X{&D, run, rwin[0], rwin[1], atom_s, G};
 
@@ -1131,9 +1125,9 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     int n_acc = 0, rows = 0;
     // mixed form: accepted moves since the last FP64 recomputation of rho(k), known to every thread
     long long acc_since = D.cnt[CN_ACC_SINCE_REFRESH], refreshes = 0;
-    const long long refresh_every = (MX && A.mode == MODE_RUN) ? D.refresh_every : 0;
+    const long long refresh_every = MX ? D.refresh_every : 0;
     int xpar = 0;  // parity of the cluster exchange buffer, flipped after every pass
-    const long long n_moves = (A.mode == MODE_RUN) ? run->n_moves : 1;
+    const long long n_moves = run->n_moves;
     long long *prof = (A.prof && rank == 0) ? A.prof : nullptr;
     const bool pc = prof && tid == 0;
     long long t_mark = 0;
@@ -1149,18 +1143,11 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             if (tid == 0) {
                 Cand &C = sh.cand[sh.icur];
                 C.cur_start = sh.cursor;
-                int imol;
-                if (A.mode == MODE_RUN) {
-                    RngReader rng = make_reader(X, sh, sh.cursor);
-                    imol = draw_molecule(D, rng, sh.mic == 0);
-                    C.valid = imol > 0;
-                    C.cur_prop = rng.cur;
-                    if (!imol) imol = 1;
-                } else {
-                    imol = (int)A.api_in[0];
-                    C.valid = 1;
-                    C.cur_prop = sh.cursor;
-                }
+                RngReader rng = make_reader(X, sh, sh.cursor);
+                int imol = draw_molecule(D, rng, sh.mic == 0);
+                C.valid = imol > 0;
+                C.cur_prop = rng.cur;
+                if (!imol) imol = 1;
                 stage_molecule(X, sh, C, imol, -1, nullptr, cluster);
                 sh.abort = C.valid ? 0 : kAbortStream;
             }
@@ -1170,8 +1157,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
         }
         if (!have_next || choose_only) {
             const int na0 = sh.cand[sh.icur].na;
-            // old forces for force-biased moves and the per-move API (movemc Steps 3-4)
-            if constexpr (SPLIT) if ((biased && A.mode == MODE_RUN) || A.mode == MODE_OLD) {
+            // old forces for force-biased moves (movemc Steps 3-4)
+            if constexpr (SPLIT) if (biased) {
                 if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
                 __syncthreads();
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
@@ -1186,24 +1173,9 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                         sh.fold[3 * a + 2] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * sh.sc[SC_MU_Z];
                     }
                 }
-                if (A.mode == MODE_OLD) {
-#pragma unroll
-                    for (int k = 0; k < EPT; ++k)
-                        if (R.e[k] >= 0) {
-#pragma unroll
-                            for (int t = 0; t <= NT; ++t) mold_g[(size_t)t * S + R.e[k]] = R.mold[k][t];
-                        }
-                    __syncthreads();
-                    if (tid == 0 && rank == 0) {
-                        for (int c = 0; c < 3; ++c) A.api_out[c] = sh.eold[c];
-                        for (int c = 0; c < 3 * na0; ++c) A.api_out[RV_F + c] = sh.fold[c];
-                    }
-                    moves_done = 1;
-                    break;
-                }
             }
             // the proposal (movemc Step 5)
-            if (biased && A.mode == MODE_RUN) {
+            if (biased) {
                 // on two warps: thread 0 draws the displacement (its Newton iteration is the long
                 // serial part) while thread 32 skips the displacement's draws and draws the rotation;
                 // both read the old forces thread 0 has just written
@@ -1276,17 +1248,11 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 }
             } else if (tid == 0) {
                 Cand &C = sh.cand[sh.icur];
-                if (A.mode == MODE_RUN) {
-                    RngReader rng = make_reader(X, sh, C.cur_prop);
-                    const double Z[3] = {0, 0, 0};
-                    propose(D, C, rng, Z, Z);
-                    C.cur_prop = rng.cur;
-                    if (rng.out) { C.valid = 0; sh.abort = kAbortStream; }
-                } else {  // MODE_EVAL: positions from the host
-                    for (int a = 0; a < na0; ++a) {
-                        C.slot[a].x = A.api_in[1 + 3 * a]; C.slot[a].y = A.api_in[2 + 3 * a]; C.slot[a].z = A.api_in[3 + 3 * a];
-                    }
-                }
+                RngReader rng = make_reader(X, sh, C.cur_prop);
+                const double Z[3] = {0, 0, 0};
+                propose(D, C, rng, Z, Z);
+                C.cur_prop = rng.cur;
+                if (rng.out) { C.valid = 0; sh.abort = kAbortStream; }
             }
             __syncthreads();
             if (sh.abort) break;
@@ -1348,20 +1314,6 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
         reduce_pass(sh, red, xch, split ? RV_F + 3 * na : RV_F, G, rank, xpar, cluster);
         xpar ^= 1;
         YAMC_PH(PH_REDUCE);
-
-        if (A.mode == MODE_EVAL) {
-#pragma unroll
-            for (int k = 0; k < EPT; ++k)
-                if (R.e[k] >= 0) {
-#pragma unroll
-                    for (int t = 0; t <= NT; ++t) scratch_buf<MX>(A.scratch, 1, 1 + NT, S)[(size_t)t * S + R.e[k]] = R.dl[k][t];
-                }
-            __syncthreads();
-            if (tid == 0 && rank == 0)
-                for (int v = 0; v < RV_F + 3 * na; ++v) A.api_out[v] = sh.tot[v];
-            moves_done = 1;
-            break;
-        }
 
         // ------------------------------------------------ Metropolis (Steps 7-13) and commit (Step 14)
         if (tid == 0) {
@@ -1534,7 +1486,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     }
 #undef YAMC_PH
 
-    if (A.mode == MODE_RUN) {  // write back the register and shared state
+    {  // write back the register and shared state
 #pragma unroll
         for (int k = 0; k < EPT; ++k)
             if (R.e[k] >= 0) {
@@ -1553,9 +1505,6 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             run->accepted = n_acc;
             run->status = sh.abort == kAbortNonFinite ? YAMC_ENAN : (sh.abort ? YAMC_ERNG_EXHAUSTED : YAMC_OK);
         }
-    } else if (tid == 0 && rank == 0) {
-        run->moves_done = moves_done;
-        run->status = YAMC_OK;
     }
     if (G > 1) cluster.sync();  // no CTA leaves while another may still address its shared memory
 }

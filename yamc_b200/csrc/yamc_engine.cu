@@ -586,15 +586,185 @@ __global__ void __launch_bounds__(256) k_rdf_count(const double *cx, const doubl
         if (hs[k]) atomicAdd(&hist[k], (unsigned long long)hs[k]);
 }
 
-// per-move API commit: rho += delta (Step 14, MC.f90:1245)
+// the exchange step's commit: rho += delta (MC.f90:1245 for the two molecules)
 __global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) { double2 r = rho[i]; const double2 d = delta[i]; r.x += d.x; r.y += d.y; rho[i] = r; }
 }
-// the same with the FP32 deltas of the mixed form's pass (rho itself stays FP64)
-__global__ void k_commit_rho_f(double2 *rho, const float2 *delta, int n) {
+
+// ------------------------------------------------------------------------------------------
+// the per-move drop-in (yamc_move_old / yamc_move_eval): one grid-wide pass per call
+// ------------------------------------------------------------------------------------------
+// The molecule (1-based) and, for an evaluation, its proposed atom positions (box units).
+struct MoveIn {
+    int imol;
+    double x[kMaxA], y[kMaxA], z[kMaxA];
+};
+
+constexpr int kMoveThreads = 256;
+
+// One pass of a single move over the whole system, spread over the GPU (the persistent chain
+// kernel stages every atom and k entry of the system in one cluster first, which a single move
+// does not repay).  Every block stages the molecule's slots -- the proposed positions (EVAL) at
+// [0, na), the current ones at [na, 2 na), as the chain's candidates -- and builds their phase
+// tables, then each thread takes one slice of the signed k entries (kspace_entry, the chain
+// pass's arithmetic: the old phase sums to scratch buffer 0 (OLD), or the deltas against them to
+// buffer 1, dU_k and the k-space forces (EVAL)) and one slice of the atoms (the molecule's pairs
+// inside the cutoff with their forces; EVAL: the hard-core overlap test).  Block sums in a fixed
+// tree; the last block to finish adds the blocks in block order and writes the reduction vector
+// (RV_* layout; OLD: the old energies and forces with the external field -2 kext q mu added, as
+// the chain's old pass hands them on).  Deterministic run to run.
+template <int NT, bool MX, bool EVAL>
+__global__ void __launch_bounds__(kMoveThreads) k_move_pass(DevSys D, MoveIn in, double *part, unsigned *counter,
+                                                            double *out) {
+    using R = typename Prec<MX>::R;
+    using R2 = typename Prec<MX>::R2;
+    constexpr int KIND = EVAL ? PASS_NEW : PASS_OLD;
+    extern __shared__ __align__(16) unsigned char move_smem[];
+    __shared__ Slot sl[2 * kMaxA];
+    __shared__ double red[(kMoveThreads / 32 + 1) * kNV];
+    __shared__ int na_s, last;
+    const int tid = threadIdx.x;
+    const int KM = D.kmax + 1, S = D.S, nt = D.nt;
+    const int imol0 = in.imol - 1;
+    if (tid == 0) {
+        const int2 mr = D.mol[imol0];
+        na_s = mr.y;
+        for (int a = 0; a < mr.y; ++a) {
+            const int j = mr.x + a;
+            const double4 p = D.atom[j];
+            Slot o;
+            o.x = p.x; o.y = p.y; o.z = p.z; o.q = p.w; o.iq = p.w != 0.0 ? 1.0 / p.w : 0.0;
+            o.dhs = D.dhs[j]; o.type = D.meta[j].y; o.pad = 0;
+            sl[mr.y + a] = o;
+            if (EVAL) { o.x = in.x[a]; o.y = in.y[a]; o.z = in.z[a]; }
+            sl[a] = o;
+        }
+    }
+    __syncthreads();
+    const int na = na_s;
+    const int s_lo = EVAL ? 0 : na, s_hi = EVAL ? na : 2 * na;
+    R2 *tab = reinterpret_cast<R2 *>(move_smem);
+    build_tables<MX>(tab, sl, s_lo, s_hi, KM, tid, kMoveThreads);
+    int tmask = 0;
+    for (int a = 0; a < na; ++a)
+        if (sl[a].type > 0) tmask |= 1 << (sl[a].type - 1);
+    __syncthreads();
+    const PhaseTabs<MX> pt{tab, KM, tmask};
+    Acc<MX> acc;
+    acc.zero();
+    const int gt = blockIdx.x * kMoveThreads + tid, gs = gridDim.x * kMoveThreads;
+    // k space: the chain pass's arithmetic, one entry at a time
+    R2 *mold_g = scratch_buf<MX>(D.scratch, 0, 1 + NT, S), *dl_g = scratch_buf<MX>(D.scratch, 1, 1 + NT, S);
+    for (int e = gt; e < S; e += gs) {
+        const int4 kv = D.kvec[e];
+        R beta, bl[NPair<NT>::value];
+        if constexpr (MX) {
+            beta = D.ebeta_f[e];
+#pragma unroll
+            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = D.ebetalj_f[(size_t)p * S + e];
+        } else {
+            beta = D.ebeta[e];
+#pragma unroll
+            for (int p = 0; p < NPair<NT>::value; ++p) bl[p] = D.ebetalj[(size_t)p * S + e];
+        }
+        double2 rho[1 + NT];
+        R2 mold[1 + NT], dl[1 + NT];
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) {
+            rho[t] = D.rho[(size_t)t * S + e];
+            mold[t] = EVAL ? mold_g[(size_t)t * S + e] : mk2(R(0), R(0));
+        }
+        kspace_entry<NT, KIND, true, MX>(pt, sl, na, kv.x, kv.y, kv.z, beta, bl, rho, mold, dl, acc);
+#pragma unroll
+        for (int t = 0; t <= NT; ++t) {
+            if (EVAL) dl_g[(size_t)t * S + e] = dl[t];
+            else mold_g[(size_t)t * S + e] = mold[t];
+        }
+    }
+    // real space: the molecule's pairs with every other atom
+    for (int j = gt; j < D.N; j += gs) {
+        const int2 mt = D.meta[j];
+        if (mt.x == imol0) continue;
+        const double4 pj = D.atom[j];
+        const double dj = D.dhs[j];
+        const int tj = mt.y;
+#pragma unroll
+        for (int a = 0; a < kMaxA; ++a) {
+            if (a >= na) continue;
+            const Slot &ss = sl[s_lo + a];
+            const double dx = min_image(ss.x - pj.x), dy = min_image(ss.y - pj.y), dz = min_image(ss.z - pj.z);
+            const double r2 = dx * dx + dy * dy + dz * dz;
+            const bool lj = ss.type > 0 && tj > 0;
+            if (EVAL && lj) {  // hard core (EwaldSumRealSpace.f90:409)
+                const double d12 = (ss.dhs + dj) / 2;
+                if (r2 < d12 * d12) acc.flag(RV_OVL);
+            }
+            if (r2 >= D.rmax2) continue;
+            const int off = lj ? (ss.type - 1) * nt + (tj - 1) : 0;
+            const double qq = D.xclb * ss.q * pj.w;
+            const double s6 = lj ? D.lj_sig6[off] : 0.0, fe = lj ? D.lj_feps[off] : 0.0;
+            const PairTerm<double> t = MX ? pair_term_mx<true>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false)
+                                          : pair_term<double, true>(r2, qq, lj, s6, fe, D.alpha, D.taosp, false);
+            acc.add(RV_EW, t.ew); acc.add(RV_LJ6, t.lj6); acc.add(RV_LJ12, t.lj12);
+            acc.add(RV_F + 3 * a, dx * t.FR); acc.add(RV_F + 3 * a + 1, dy * t.FR); acc.add(RV_F + 3 * a + 2, dz * t.FR);
+        }
+    }
+    double v[kNV];
+#pragma unroll
+    for (int i = 0; i < kNV; ++i) v[i] = acc.get(i);
+    block_sum<kMoveThreads>(v, kNV, red);  // (the overlap flags add up: a positive total is an overlap)
+    if (tid < kNV) part[(size_t)blockIdx.x * kNV + tid] = v[tid];
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) last = atomicAdd(counter, 1u) == gridDim.x - 1;
+    __syncthreads();
+    if (!last) return;
+    if (tid < kNV) {
+        const volatile double *pv = part;
+        double x = 0.0;
+        for (int b = 0; b < (int)gridDim.x; ++b) x += pv[(size_t)b * kNV + tid];
+        if (tid == RV_OVL) x = x > 0.0 ? 1.0 : 0.0;
+        if (!EVAL && tid >= RV_F && tid < RV_F + 3 * na) {  // the external field at the old dipole (MC.f90:988-997)
+            const int a = (tid - RV_F) / 3, c = (tid - RV_F) % 3;
+            x = x + D.m2k * sl[na + a].q * D.scal[SC_MU_X + c];
+        }
+        out[tid] = x;
+    }
+    // the engine scalars and counters beside them (the host's copies of the state the next calls use)
+    if (tid >= 64 && tid < 64 + SC_COUNT) out[kNV + tid - 64] = D.scal[tid - 64];
+    if (tid >= 96 && tid < 96 + CN_COUNT) reinterpret_cast<long long *>(out + kNV + SC_COUNT)[tid - 96] = D.cnt[tid - 96];
+    if (tid == 0) *counter = 0u;
+}
+
+// The step-14 commit of an accepted per-move step in one launch: rho += the pass's deltas
+// (FP32 deltas in the mixed form), the moved atoms' positions and the engine scalars and
+// counters from the host (kernel arguments, nothing staged in host memory).
+struct MoveCommit {
+    int first, na;
+    double x[kMaxA], y[kMaxA], z[kMaxA];
+    double sc[SC_COUNT];
+    long long cnt[CN_COUNT];
+};
+template <class D2>
+__global__ void k_commit_move(double2 *rho, const D2 *delta, int n, DevSys D, MoveCommit mc) {
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < n) { double2 r = rho[i]; const float2 d = delta[i]; r.x += (double)d.x; r.y += (double)d.y; rho[i] = r; }
+    if (i < n) {
+        double2 r = rho[i];
+        const D2 d = delta[i];
+        r.x += (double)d.x;
+        r.y += (double)d.y;
+        rho[i] = r;
+    }
+    if (blockIdx.x == 0) {
+        const int t = threadIdx.x;
+        if (t < mc.na) {  // x, y, z of the double4 (q unchanged)
+            double *pa = reinterpret_cast<double *>(D.atom + mc.first + t);
+            pa[0] = mc.x[t]; pa[1] = mc.y[t]; pa[2] = mc.z[t];
+        }
+        if (t >= 32 && t < 32 + SC_COUNT) D.scal[t - 32] = mc.sc[t - 32];
+        if (t >= 64 && t < 64 + CN_COUNT) D.cnt[t - 64] = mc.cnt[t - 64];
+    }
 }
 
 }  // namespace yamc
@@ -634,9 +804,6 @@ size_t chain_smem_bytes(int G, int B, int kmax, int nt, int nown_max, int qcap) 
 
 }  // namespace
 
-// byte offset of the per-move commit's staging inside yamc_ctx::h_pin (after the read-back block)
-constexpr size_t kPinCommit = ((sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT + 255) / 256) * 256;
-
 struct yamc_ctx {
     HostSystem H;
     int device = 0;
@@ -664,11 +831,13 @@ struct yamc_ctx {
     DevSys hsys{};
     DevSys *d_sys = nullptr;
     RunSlot *d_run = nullptr;
-    double *api_in = nullptr, *api_out = nullptr;
-    // pinned staging of the per-move calls: api_out, then scal, then cnt, read back in one
-    // round trip per call; after them (kPinCommit) the commit's uploads: the moved atoms'
-    // records, scal and cnt
-    double *h_pin = nullptr;
+    // the per-move pass's outputs: its reduction vector, then the engine scalars and counters, in
+    // mapped pinned host memory the kernel writes directly (h_out on the host, d_hout on the device)
+    double *h_out = nullptr, *d_hout = nullptr;
+    // the per-move pass (k_move_pass): block partials and the finished-block counter
+    double *d_mpart = nullptr;
+    unsigned *d_mcount = nullptr;
+    int mblocks = 0;
     float *d_rng = nullptr;
     size_t rng_cap = 0;
     yamc_move_record *d_log = nullptr;
@@ -763,6 +932,39 @@ int pick_launch_for(const std::vector<const HostSystem *> &hosts, int device, in
 
 bool is_mixed(const yamc_ctx *c) { return c->H.p.precision == YAMC_MIXED; }
 
+// one k_move_pass launch (OLD: the molecule's current positions; EVAL: in's proposed ones) into
+// c->api_out on the context's stream
+template <int NT, bool MX>
+int launch_move_pass_t(yamc_ctx *c, const MoveIn &in, bool eval, size_t smem) {
+    auto kfn = eval ? k_move_pass<NT, MX, true> : k_move_pass<NT, MX, false>;
+    if (smem > 48 * 1024) CUDA_TRY(cudaFuncSetAttribute(kfn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    kfn<<<c->mblocks, kMoveThreads, smem, c->stream>>>(c->hsys, in, c->d_mpart, c->d_mcount, c->d_hout);
+    CUDA_TRY(cudaGetLastError());
+    return YAMC_OK;
+}
+
+int launch_move_pass(yamc_ctx *c, const MoveIn &in, bool eval) {
+    const HostSystem &H = c->H;
+    if (!c->d_mpart) {
+        // one thread per atom and per signed entry, at most two blocks per SM
+        const int need = std::max((H.N + kMoveThreads - 1) / kMoveThreads, (H.S + kMoveThreads - 1) / kMoveThreads);
+        c->mblocks = std::max(1, std::min(need, 2 * c->nsm));
+        int r;
+        if ((r = dalloc(&c->d_mpart, (size_t)c->mblocks * kNV)) || (r = dalloc(&c->d_mcount, 1))) return r;
+        CUDA_TRY(cudaMemsetAsync(c->d_mcount, 0, sizeof(unsigned), c->stream));
+    }
+    const size_t smem = sizeof(double2) * 2 * kMaxA * 3 * (size_t)(H.kmax + 1);
+    const bool mx = is_mixed(c);
+    switch (H.nt) {
+        case 1: return mx ? launch_move_pass_t<1, true>(c, in, eval, smem) : launch_move_pass_t<1, false>(c, in, eval, smem);
+        case 2: return mx ? launch_move_pass_t<2, true>(c, in, eval, smem) : launch_move_pass_t<2, false>(c, in, eval, smem);
+        case 3: return mx ? launch_move_pass_t<3, true>(c, in, eval, smem) : launch_move_pass_t<3, false>(c, in, eval, smem);
+        case 4: return launch_move_pass_t<4, false>(c, in, eval, smem);
+        default: set_error("LJ type count outside 1..4"); return YAMC_ELIMITS;
+    }
+}
+
+
 int pick_launch(yamc_ctx *c, LaunchCfg *out) {
     return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, c->force_layout, is_mixed(c), out);
 }
@@ -790,12 +992,11 @@ int max_clusters_cfg(const LaunchCfg &L, int nt, bool split, bool mx, int *out) 
     return YAMC_ELIMITS;
 }
 
-bool split_variant(const HostSystem &H, int mode) {
-    return mode != MODE_RUN || H.p.xlambda_f > 0.0 || H.p.xlambda_c > 0.0;
-}
+// the chain kernel with separate old and new passes: force-biased moves
+bool split_variant(const HostSystem &H) { return H.p.xlambda_f > 0.0 || H.p.xlambda_c > 0.0; }
 
 int launch_chain(yamc_ctx *c, const ChainArgs &args) {
-    return launch_chain_cfg(c->cfg, c->H.nt, split_variant(c->H, args.mode), c->H.p.precision == YAMC_MIXED, c->stream, 1,
+    return launch_chain_cfg(c->cfg, c->H.nt, split_variant(c->H), c->H.p.precision == YAMC_MIXED, c->stream, 1,
                             args);
 }
 
@@ -937,11 +1138,11 @@ void fill_dhs_types(const HostSystem &H, DevSys &D) {
     for (int t = 1; t <= kMaxDevTypes; ++t) if (D.dhs_t[t] < 0) D.dhs_t[t] = 0.0;
 }
 
-ChainArgs base_args(yamc_ctx *c, int mode) {
+ChainArgs base_args(yamc_ctx *c) {
     ChainArgs a{};
-    a.sys = c->d_sys; a.run = c->d_run; a.G = c->cfg.G; a.mode = mode;
+    a.sys = c->d_sys; a.run = c->d_run; a.G = c->cfg.G;
     a.nown_max = c->cfg.nown_max; a.qcap = c->cfg.qcap;
-    a.api_in = c->api_in; a.api_out = c->api_out; a.scratch = c->scratch;
+    a.scratch = c->scratch;
     a.prof = c->prof_on ? c->d_prof : nullptr;
     return a;
 }
@@ -1024,7 +1225,7 @@ int batch_build_graph(yamc_batch *b) {
         BatchGroup &g = b->groups[k];
         if (cudaStreamWaitEvent(g.stream, b->fork, 0) != cudaSuccess) { r = YAMC_ECUDA; break; }
         ChainArgs a{};
-        a.sys = g.d_sys; a.run = g.d_run; a.G = g.cfg.G; a.mode = MODE_RUN;
+        a.sys = g.d_sys; a.run = g.d_run; a.G = g.cfg.G;
         a.nown_max = g.cfg.nown_max; a.qcap = g.cfg.qcap;
         if ((r = launch_chain_cfg(g.cfg, g.nt, g.split, g.mx, g.stream, (int)g.idx.size(), a))) break;
         if (cudaEventRecord(g.done, g.stream) != cudaSuccess || cudaStreamWaitEvent(b->stream, g.done, 0) != cudaSuccess)
@@ -1174,11 +1375,11 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
         (r = dalloc(&c->scratch, (size_t)2 * (1 + nt) * S)) || (r = dalloc(&c->freq_beg, M)) || (r = dalloc(&c->freq_end, M)) ||
         (r = dalloc(&c->scal, SC_COUNT)) || (r = dalloc(&c->cnt, CN_COUNT)) ||
-        (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->api_in, 1 + 3 * kMaxA)) ||
-        (r = dalloc(&c->api_out, kNV)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
+        (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = 0) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
-    CUDA_TRY(cudaMallocHost(&c->h_pin, kPinCommit + sizeof(double4) * kMaxA + sizeof(double) * SC_COUNT +
-                                           sizeof(long long) * CN_COUNT));
+    CUDA_TRY(cudaHostAlloc(&c->h_out, sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT,
+                           cudaHostAllocMapped));
+    CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->d_hout), c->h_out, 0));
     // full-sum work split: atom-tile pairs of the real-space sum; atom slices of rho(k) so that
     // entry blocks x slices cover the SMs about twice
     int nsm = 148;
@@ -1265,10 +1466,11 @@ int yamc_destroy(yamc_ctx *c) {
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->ebeta_f, c->ebetalj_f,
                     c->lj_sig6, c->lj_feps, c->kvec,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
-                    c->tpairs, c->rho_part, c->d_sys, c->d_run, c->api_in, c->api_out, c->d_rng, c->d_log, c->d_rows,
-                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save};
+                    c->tpairs, c->rho_part, c->d_sys, c->d_run, c->d_rng, c->d_log, c->d_rows,
+                    c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save, c->d_mpart,
+                    c->d_mcount};
     for (void *p : ptrs) if (p) cudaFree(p);
-    if (c->h_pin) cudaFreeHost(c->h_pin);
+    if (c->h_out) cudaFreeHost(c->h_out);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -1364,7 +1566,7 @@ static int run_chain_impl(yamc_ctx *c, const float *d_rng, long long rng_off, lo
     rs.rng = d_rng; rs.rng_off = rng_off; rs.n_rng = n_rng; rs.cursor = *cursor; rs.n_moves = n_moves;
     rs.log = d_log; rs.rows = d_rows; rs.max_rows = max_rows;
     if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
-    ChainArgs a = base_args(c, MODE_RUN);
+    ChainArgs a = base_args(c);
     CUDA_TRY(cudaEventRecord(c->ev0, c->stream));
     if ((r = launch_chain(c, a))) return r;
     CUDA_TRY(cudaEventRecord(c->ev1, c->stream));
@@ -2195,25 +2397,17 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
 int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
     if (!c || imol < 1 || imol > c->H.M) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(c->device));
-    int r = ensure_cfg(c);
+    if (c->H.nt == 4 && is_mixed(c)) { set_error("the mixed form takes up to 3 LJ types"); return YAMC_ELIMITS; }
+    int r = sync_positions(c);
     if (r) return r;
-    if ((r = sync_positions(c))) return r;
-    double in[1 + 3 * kMaxA] = {};
-    in[0] = imol;
-    if ((r = upload(c->api_in, in, 1 + 3 * kMaxA, c->stream))) return r;
-    RunSlot rs{};
-    if ((r = upload(c->d_run, &rs, 1, c->stream))) return r;
-    if ((r = launch_chain(c, base_args(c, MODE_OLD)))) return r;
-    // the kernel reads the scalars and counters without changing them: one read-back of its
-    // outputs and of the state the next calls use
-    double *pin = c->h_pin;
-    CUDA_TRY(cudaMemcpyAsync(pin, c->api_out, sizeof(double) * kNV, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(pin + kNV, c->scal, sizeof(double) * SC_COUNT, cudaMemcpyDeviceToHost, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(pin + kNV + SC_COUNT, c->cnt, sizeof(long long) * CN_COUNT, cudaMemcpyDeviceToHost, c->stream));
+    MoveIn in{};
+    in.imol = imol;
+    if ((r = launch_move_pass(c, in, false))) return r;
+    // the kernel writes its outputs, the scalars and the counters straight into mapped host memory
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    const double *out = pin;
-    std::memcpy(c->sc, pin + kNV, sizeof(double) * SC_COUNT);
-    std::memcpy(c->cnt_h, pin + kNV + SC_COUNT, sizeof(long long) * CN_COUNT);
+    const double *out = c->h_out;
+    std::memcpy(c->sc, out + kNV, sizeof(double) * SC_COUNT);
+    std::memcpy(c->cnt_h, out + kNV + SC_COUNT, sizeof(long long) * CN_COUNT);
     const HostSystem &H = c->H;
     const int f0 = H.first[imol - 1], na = H.natoms[imol - 1];
     for (int k = 0; k < RV_F + 3 * na; ++k)
@@ -2242,15 +2436,13 @@ int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn
     CUDA_TRY(cudaSetDevice(c->device));
     const HostSystem &H = c->H;
     const int f0 = H.first[imol - 1], na = H.natoms[imol - 1];
-    double in[1 + 3 * kMaxA] = {};
-    in[0] = imol;
-    for (int a = 0; a < na; ++a) { in[1 + 3 * a] = xn[a]; in[2 + 3 * a] = yn[a]; in[3 + 3 * a] = zn[a]; }
-    int r = upload(c->api_in, in, 1 + 3 * kMaxA, c->stream);
+    MoveIn in{};
+    in.imol = imol;
+    for (int a = 0; a < na; ++a) { in.x[a] = xn[a]; in.y[a] = yn[a]; in.z[a] = zn[a]; }
+    int r = launch_move_pass(c, in, true);
     if (r) return r;
-    if ((r = launch_chain(c, base_args(c, MODE_EVAL)))) return r;
-    CUDA_TRY(cudaMemcpyAsync(c->h_pin, c->api_out, sizeof(double) * kNV, cudaMemcpyDeviceToHost, c->stream));
     CUDA_TRY(cudaStreamSynchronize(c->stream));
-    const double *out = c->h_pin;
+    const double *out = c->h_out;
     for (int v = 0; v < kNV; ++v) c->api_new[v] = out[v];
     for (int a = 0; a < na; ++a) { c->api_xn[a] = xn[a]; c->api_yn[a] = yn[a]; c->api_zn[a] = zn[a]; }
     const int ovl = out[RV_OVL] > 0.0;
@@ -2302,20 +2494,11 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     HostSystem &H = c->H;
     const int imol = c->api_imol, f0 = H.first[imol - 1], na = H.natoms[imol - 1];
     const int n = (1 + H.nt) * H.S;
-    if (is_mixed(c))  // the chain kernel's deltas: scratch buffer 1 in the pass's arithmetic type
-        k_commit_rho_f<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, scratch_buf<true>(c->scratch, 1, 1 + H.nt, H.S), n);
-    else
-        k_commit_rho<<<(n + 255) / 256, 256, 0, c->stream>>>(c->rho, scratch_buf<false>(c->scratch, 1, 1 + H.nt, H.S), n);
-    CUDA_TRY(cudaGetLastError());
-    // the uploads come from the pinned commit block: every per-move call that follows ends with
-    // a stream synchronisation before the host writes that block again
-    unsigned char *stage = reinterpret_cast<unsigned char *>(c->h_pin) + kPinCommit;
-    double4 *a = reinterpret_cast<double4 *>(stage);
-    double *sc = reinterpret_cast<double *>(a + kMaxA);
-    long long *cn = reinterpret_cast<long long *>(sc + SC_COUNT);
+    MoveCommit mc{};
+    mc.first = f0; mc.na = na;
     for (int i = 0; i < na; ++i) {
         H.x[f0 + i] = c->api_xn[i]; H.y[f0 + i] = c->api_yn[i]; H.z[f0 + i] = c->api_zn[i];
-        a[i] = make_double4(H.x[f0 + i], H.y[f0 + i], H.z[f0 + i], H.q[f0 + i]);
+        mc.x[i] = H.x[f0 + i]; mc.y[i] = H.y[f0 + i]; mc.z[i] = H.z[f0 + i];
     }
     c->sc[SC_UU_EW] += c->api_new[RV_EW] - c->api_eold[0];
     c->sc[SC_UU_LJ6] += c->api_new[RV_LJ6] - c->api_eold[1];
@@ -2323,11 +2506,16 @@ int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
     c->sc[SC_EK_C] += c->api_new[RV_DUC];
     c->sc[SC_EK_LJ] += c->api_new[RV_DUL];
     c->sc[SC_MU_X] += c->api_dmu[0]; c->sc[SC_MU_Y] += c->api_dmu[1]; c->sc[SC_MU_Z] += c->api_dmu[2];
-    std::memcpy(sc, c->sc, sizeof(double) * SC_COUNT);
-    std::memcpy(cn, c->cnt_h, sizeof(long long) * CN_COUNT);
-    CUDA_TRY(cudaMemcpyAsync(c->atom + f0, a, sizeof(double4) * na, cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(c->scal, sc, sizeof(double) * SC_COUNT, cudaMemcpyHostToDevice, c->stream));
-    CUDA_TRY(cudaMemcpyAsync(c->cnt, cn, sizeof(long long) * CN_COUNT, cudaMemcpyHostToDevice, c->stream));
+    std::memcpy(mc.sc, c->sc, sizeof(double) * SC_COUNT);
+    std::memcpy(mc.cnt, c->cnt_h, sizeof(long long) * CN_COUNT);
+    // rho += the pass's deltas (scratch buffer 1, in the pass's arithmetic type), the moved atoms,
+    // the scalars and the counters: one launch, the host values passed as kernel arguments
+    const int nb = std::max(1, (n + 255) / 256);
+    if (is_mixed(c))
+        k_commit_move<<<nb, 256, 0, c->stream>>>(c->rho, scratch_buf<true>(c->scratch, 1, 1 + H.nt, H.S), n, c->hsys, mc);
+    else
+        k_commit_move<<<nb, 256, 0, c->stream>>>(c->rho, scratch_buf<false>(c->scratch, 1, 1 + H.nt, H.S), n, c->hsys, mc);
+    CUDA_TRY(cudaGetLastError());
     c->api_stage = 0;
     return YAMC_OK;
 }
@@ -2380,7 +2568,7 @@ static int batch_create_impl(yamc_batch *b, int32_t n, const yamc_system *system
     }
     for (int i = 0; i < n; ++i) {
         const HostSystem &H = b->reps[i]->H;
-        const bool split = split_variant(H, MODE_RUN);
+        const bool split = split_variant(H);
         const bool mx = H.p.precision == YAMC_MIXED;
         const int cls = H.N <= 1024 ? 0 : H.N <= 2048 ? 1 : H.N <= 4096 ? 2 : H.N <= 8192 ? 3 : 4;
         size_t k = 0;
