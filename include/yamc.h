@@ -374,7 +374,7 @@ int yamc_batch_get_launch(yamc_batch *b, int32_t out[5]);
 int yamc_batch_groups(yamc_batch *b, int32_t *n);
 int yamc_batch_group_launch(yamc_batch *b, int32_t group, int32_t out[7]);
 /* device time (ms, CUDA events on the batch stream) of the last run, and the kernels it
-   launched (one chain launch per variant group) */
+   launched (per variant group: the staging-order kernel and the chain kernel) */
 int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms);
 int yamc_batch_last_launches(yamc_batch *b, int32_t *n);
 

@@ -69,7 +69,7 @@ struct ChainArgs {
     const DevSys *sys;  // [R]
     RunSlot *run;       // [R]
     int G;              // CTAs per chain (cluster size)
-    int nown_max;       // atoms staged per CTA (interleaved ownership: atom j lives in CTA j % G)
+    int nown_max;       // atoms staged per CTA (interleaved ownership: atom j lives in CTA j % G, in slot D.slot[j])
     int qcap;           // pair queue capacity per CTA
     double2 *scratch;      // [2][(1+nt) S]: molecule old sums, rho deltas (scratch_buf: FP32 pairs in the mixed form)
     long long *prof;       // optional per-phase cycle counters (PH_* layout), CTA 0
@@ -90,11 +90,140 @@ enum PassKind { PASS_OLD = 0, PASS_NEW = 1, PASS_BOTH = 2 };
 struct Slot { double x, y, z, q, iq, dhs; int type, pad; };
 constexpr int kMaxSpecies = 8;
 constexpr int kCPT = 8;   // atoms each worker thread tests per filter round
+constexpr int kBlk = 32;  // atoms per bounding box of the pair filter (one warp's candidates per round and c)
 constexpr int kQueueMax = 4096;  // pair-queue chunk (items); a round's pairs are consumed in chunks
 constexpr int kWin = 256; // random-stream window held in shared memory
 constexpr int kCtl = 32;  // threads of the control warp
 constexpr int kChainMaxThreads = 256;  // one CTA per SM, up to 255 registers per thread
 constexpr int kChainMaxThreadsWide = YAMC_WIDE_THREADS;  // streamed k entries, more warps, fewer registers
+
+// ------------------------------------------------------------------ spatial staging
+// Each CTA stages its atoms in spatial order (k_stage_order), so kBlk consecutive slots hold
+// atoms of a compact region; per block a bounding box (centre and half extent per axis, box
+// units, float) lets the pair filter skip blocks that lie outside the query sphere.  The box
+// holds every staged position p of the block as p = centre + t + n (n integer, |t| <= half);
+// kBoxPad widens the half extents beyond the rounding of centre and extent to float.
+constexpr double kBoxPad = 1e-6;
+
+__device__ __forceinline__ double wrap_half(double d) { return d - rint(d); }  // into [-1/2, 1/2]
+
+// the block's box from its staged positions, relative to its first atom
+__device__ inline void block_box(const double4 *atom_s, int b, int nown, float4 *box_s) {
+    const int s0 = b * kBlk, s1 = min(s0 + kBlk, nown);
+    const double4 r = atom_s[s0];
+    double lx = 0, ly = 0, lz = 0, hx = 0, hy = 0, hz = 0;
+    for (int s = s0 + 1; s < s1; ++s) {
+        const double4 p = atom_s[s];
+        const double tx = wrap_half(p.x - r.x), ty = wrap_half(p.y - r.y), tz = wrap_half(p.z - r.z);
+        lx = fmin(lx, tx); ly = fmin(ly, ty); lz = fmin(lz, tz);
+        hx = fmax(hx, tx); hy = fmax(hy, ty); hz = fmax(hz, tz);
+    }
+    box_s[2 * b] = make_float4((float)(r.x + 0.5 * (lx + hx)), (float)(r.y + 0.5 * (ly + hy)),
+                               (float)(r.z + 0.5 * (lz + hz)), 0.f);
+    box_s[2 * b + 1] = make_float4(__double2float_ru(0.5 * (hx - lx) + kBoxPad), __double2float_ru(0.5 * (hy - ly) + kBoxPad),
+                                   __double2float_ru(0.5 * (hz - lz) + kBoxPad), 0.f);
+}
+
+// the block's box grown to hold position (x, y, z) as well (an accepted move's new position)
+__device__ inline void box_expand(float4 *box_s, int b, double x, double y, double z) {
+    float4 c = box_s[2 * b], h = box_s[2 * b + 1];
+    const double p[3] = {x, y, z};
+    float *cc[3] = {&c.x, &c.y, &c.z}, *hh[3] = {&h.x, &h.y, &h.z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const double t = wrap_half(p[d] - (double)*cc[d]), e = (double)*hh[d];
+        if (t > e || t < -e) {
+            const double lo = fmin(-e, t), hi = fmax(e, t);
+            *cc[d] = (float)((double)*cc[d] + 0.5 * (lo + hi));
+            *hh[d] = __double2float_ru(0.5 * (hi - lo) + kBoxPad);
+        }
+    }
+    box_s[2 * b] = c;
+    box_s[2 * b + 1] = h;
+}
+
+// false only if no position the box holds is within sqrt(r2) of (qx, qy, qz) under any periodic
+// image: per axis the nearest image of the box is |wrap(q - centre)| - half away (or 0)
+__device__ __forceinline__ bool box_near(const float4 *box_s, int b, double qx, double qy, double qz, double r2) {
+    const float4 c = box_s[2 * b], h = box_s[2 * b + 1];
+    const double ex = fmax(fabs(wrap_half(qx - (double)c.x)) - (double)h.x, 0.0);
+    const double ey = fmax(fabs(wrap_half(qy - (double)c.y)) - (double)h.y, 0.0);
+    const double ez = fmax(fabs(wrap_half(qz - (double)c.z)) - (double)h.z, 0.0);
+    return ex * ex + ey * ey + ez * ez < r2;
+}
+
+// Order of the staged atoms (one block per chain and CTA, before each chain launch): CTA r of a
+// chain of G CTAs owns atoms j = r + G i; they are ordered by the Morton index of their cell on
+// an nc^3 grid (nc a power of two <= 16, about four owned atoms per cell), stably (by i) within a
+// cell.  Writes D.slot[j] (the slot of atom j in its CTA) and D.atom_of[s G + r] (the atom in
+// slot s of CTA r).  Shared memory: kStageMaxCells + atoms-per-CTA ints.
+constexpr int kStageThreads = 256;
+constexpr int kStageMaxCells = 4096;
+
+__device__ __forceinline__ unsigned spread3(unsigned v) {  // bits b of v (b < 4) to bits 3 b
+    return (v & 1u) | ((v & 2u) << 2) | ((v & 4u) << 4) | ((v & 8u) << 6);
+}
+
+__device__ __forceinline__ int cell_axis(double u, int nc) {
+    const double w = u - floor(u);
+    return min((int)(w * nc), nc - 1);
+}
+
+static __global__ void __launch_bounds__(kStageThreads) k_stage_order(const DevSys *sys, int G) {
+    extern __shared__ int st_smem[];
+    const int rank = blockIdx.x % G;
+    const DevSys &D = sys[blockIdx.x / G];
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int nown = (D.N - rank + G - 1) / G;
+    int nc = 1;
+    while (nc < 16 && 4 * (2 * nc) * (2 * nc) * (2 * nc) <= nown) nc *= 2;
+    const int ncell = nc * nc * nc;
+    int *hist = st_smem, *key = st_smem + kStageMaxCells;
+    for (int c = tid; c < ncell; c += kStageThreads) hist[c] = 0;
+    __syncthreads();
+    for (int i = tid; i < nown; i += kStageThreads) {
+        const double4 p = D.atom[rank + G * i];
+        const int k = (int)(spread3(cell_axis(p.x, nc)) | (spread3(cell_axis(p.y, nc)) << 1) |
+                            (spread3(cell_axis(p.z, nc)) << 2));
+        key[i] = k;
+        atomicAdd(&hist[k], 1);
+    }
+    __syncthreads();
+    if (tid < 32) {
+        // exclusive prefix of the cell counts: each lane a contiguous run of cells
+        const int per = (ncell + 31) / 32;
+        const int lo = min(lane * per, ncell), hi = min(lo + per, ncell);
+        int sum = 0;
+        for (int c = lo; c < hi; ++c) sum += hist[c];
+        int x = sum;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const int y = __shfl_up_sync(0xffffffffu, x, o);
+            if (lane >= o) x += y;
+        }
+        int run = x - sum;
+        for (int c = lo; c < hi; ++c) { const int h = hist[c]; hist[c] = run; run += h; }
+        __syncwarp();
+        // stable placement, 32 atoms at a time: atoms of one cell take consecutive slots in i order
+        for (int i0 = 0; i0 < nown; i0 += 32) {
+            const int i = i0 + lane;
+            const int k = i < nown ? key[i] : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, k);
+            const int before = __popc(peers & ((1u << lane) - 1u));
+            const int pos = i < nown ? hist[k] + before : 0;
+            __syncwarp();
+            if (i < nown && before == __popc(peers) - 1) hist[k] = pos + 1;
+            if (i < nown) key[i] = pos;
+            __syncwarp();
+        }
+    }
+    __syncthreads();
+    for (int i = tid; i < nown; i += kStageThreads) {
+        const int j = rank + G * i, s = key[i];
+        D.slot[j] = s;
+        D.atom_of[s * G + rank] = j;
+    }
+}
 
 // a prepared move: the molecule, its atoms at the old and proposed positions, the proposal
 struct Cand {
@@ -123,6 +252,8 @@ struct ChainShared {
     double lx[kMaxA], ly[kMaxA], lz[kMaxA];  // last accepted move (staged copies may lag in other CTAs)
     int qcount;
     int wcount[64];       // per-warp pair counts and their exclusive prefix
+    int wmore[32];        // per worker warp: near blocks left after this filter round
+    int qmore;            // some worker warp has near blocks left
     double tot[kNV];
     double du[4];
     int flags;
@@ -505,7 +636,8 @@ __device__ __forceinline__ void kspace_sweep(const DevSys &D, RegsOf<NT, EPT, MX
 template <int NT, int EPT, int KIND, bool FORCES, bool MX>
 __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
                                             const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
-                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
+                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, const float4 *box_s,
+                                            int *blist, int *queue,
                                             int *nearbuf,
                                             double *red, const double *lj_s, int nown, int qcap, int e0, int estep,
                                             long long *prof, typename Prec<MX>::R2 *mold_buf, bool mold_out) {
@@ -570,14 +702,34 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
         rb2 = rb * rb;
     }
 
-    const int round_atoms = nwork * kCPT;
+    // this warp's near blocks: of the blocks wwarp + nww k (kBlk consecutive slots each; the
+    // staged atoms are in spatial order), those whose bounding box comes within the query sphere.
+    // A block outside it holds no atom that the per-atom test below keeps.
+    const int nblk = (nown + kBlk - 1) / kBlk;
+    const int wcap = (nblk + nww - 1) / nww;
+    int *wl = blist + wwarp * wcap;
+    int nnb = 0;
+    {
+        const double qx = KIND == PASS_BOTH ? cbx : (KIND == PASS_NEW ? cnx : cox);
+        const double qy = KIND == PASS_BOTH ? cby : (KIND == PASS_NEW ? cny : coy);
+        const double qz = KIND == PASS_BOTH ? cbz : (KIND == PASS_NEW ? cnz : coz);
+        const double qr2 = KIND == PASS_BOTH ? rb2 : rp2;
+        for (int k0 = 0; k0 < wcap; k0 += 32) {
+            const int k = k0 + lane, b = wwarp + nww * k;
+            const bool near = k < wcap && b < nblk && box_near(box_s, b, qx, qy, qz, qr2);
+            const unsigned bal = __ballot_sync(0xffffffffu, near);
+            if (near) wl[nnb + __popc(bal & ((1u << lane) - 1u))] = b;
+            nnb += __popc(bal);
+        }
+        __syncwarp();
+    }
     int *nb = nearbuf + wwarp * 32 * kCPT;  // this warp's near atoms of the round
-    for (int c0 = 0; c0 < nown; c0 += round_atoms) {
-        // near atoms of the warp's 32 x kCPT candidates, compacted in (c, lane) order
+    for (int r0 = 0;; r0 += kCPT) {
+        // near atoms of the warp's next kCPT near blocks, compacted in (block, lane) order
         int nnear = 0;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            const int jl = c0 + c * nwork + wtid;
+            const int jl = r0 + c < nnb ? wl[r0 + c] * kBlk + lane : nown;
             bool near = false;
             if (jl < nown && meta_s[jl].x != imol0) {
                 const double4 pj = atom_s[jl];
@@ -608,8 +760,8 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
                 const double4 pj = atom_s[jl];
                 const int tj = meta_s[jl].y;
                 // hard-core diameter: by LJ type when every atom of a type has the same one
-                // (a shared-memory table), else the atom's own (global memory: atom rank + G jl)
-                const double dj = dhs_typed ? dhs_ts[tj] : dhs_g[grank + gsize * jl];
+                // (a shared-memory table), else the atom's own (global memory, by the atom in slot jl)
+                const double dj = dhs_typed ? dhs_ts[tj] : dhs_g[D.atom_of[jl * gsize + grank]];
                 unsigned msk = 0;
                 for (int s = s_lo; s < s_hi; ++s) {
                     const Slot &sl = m.slot[s];
@@ -631,7 +783,7 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
             const int y = __shfl_up_sync(0xffffffffu, incl, o);
             if (lane >= o) incl += y;
         }
-        if (lane == 31) sh.wcount[wwarp] = incl;
+        if (lane == 31) { sh.wcount[wwarp] = incl; sh.wmore[wwarp] = nnb > r0 + kCPT; }
         worker_sync(nwork);
         if (wwarp == 0) {
             const int v = lane < nww ? sh.wcount[lane] : 0;
@@ -643,8 +795,13 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
             }
             if (lane < nww) sh.wcount[32 + lane] = x - v;
             if (lane == 31) sh.qcount = x;
+            const bool more = __any_sync(0xffffffffu, lane < nww && sh.wmore[lane] != 0);
+            if (lane == 0) sh.qmore = more;
         }
         worker_sync(nwork);
+        // another round while some warp has near blocks left (read here: the next round's
+        // writes come after its first barrier)
+        const bool more_rounds = sh.qmore != 0;
         // the round's pairs in queue order (thread order by the prefix sums), consumed in chunks of
         // qcap: each thread writes its items that fall in the chunk, the workers evaluate them
         const int base = sh.wcount[32 + wwarp] + incl - count;
@@ -698,6 +855,7 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
             worker_sync(nwork);
         }
         YAMC_WPH(PH_PAIRS);
+        if (!more_rounds) break;
     }
 
     // per-warp reduction (xor tree) into red[worker warp][value]
@@ -724,26 +882,28 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
 template <int NT, int EPT, int KIND, bool FORCES, bool MX>
 __device__ __noinline__ void worker_pass_call(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
                                               const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
-                                              int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
+                                              int dhs_typed, int grank, int gsize, const int2 *meta_s, const float4 *box_s,
+                                            int *blist, int *queue,
                                               int *nearbuf, double *red, const double *lj_s, int nown, int qcap, int e0,
                                               int estep, long long *prof, typename Prec<MX>::R2 *mold_buf, bool mold_out) {
     worker_pass_body<NT, EPT, KIND, FORCES, MX>(D, sh, R, tab_raw, atom_s, dhs_ts, dhs_g, dhs_typed, grank, gsize, meta_s,
-                                                queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof, mold_buf, mold_out);
+                                                box_s, blist, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof, mold_buf, mold_out);
 }
 
 template <int NT, int EPT, int KIND, bool FORCES, bool MX>
 __device__ __forceinline__ void worker_pass(const DevSys &D, ChainShared &sh, RegsOf<NT, EPT, MX> &R, double2 *tab_raw,
                                             const double4 *atom_s, const double *dhs_ts, const double *dhs_g,
-                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, int *queue,
+                                            int dhs_typed, int grank, int gsize, const int2 *meta_s, const float4 *box_s,
+                                            int *blist, int *queue,
                                             int *nearbuf, double *red, const double *lj_s, int nown, int qcap, int e0,
                                             int estep, long long *prof, typename Prec<MX>::R2 *mold_buf, bool mold_out) {
     if constexpr (EPT > 0)
         worker_pass_body<NT, EPT, KIND, FORCES, MX>(D, sh, R, tab_raw, atom_s, dhs_ts, dhs_g, dhs_typed, grank, gsize,
-                                                    meta_s, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof,
+                                                    meta_s, box_s, blist, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof,
                                                     mold_buf, mold_out);
     else
         worker_pass_call<NT, EPT, KIND, FORCES, MX>(D, sh, R, tab_raw, atom_s, dhs_ts, dhs_g, dhs_typed, grank, gsize,
-                                                    meta_s, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof,
+                                                    meta_s, box_s, blist, queue, nearbuf, red, lj_s, nown, qcap, e0, estep, prof,
                                                     mold_buf, mold_out);
 }
 
@@ -831,20 +991,26 @@ __device__ inline void stage_molecule(const ChooseCtx &X, ChainShared &sh, Cand 
     else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
     C.imol = imol; C.first = first; C.na = nam;
     double mx = 0, my = 0, mz = 0;
-    for (int a = 0; a < nam; ++a) {
+    int slots[kMaxA];  // staging slots of the molecule's atoms (loaded together)
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) slots[a] = a < nam ? D.slot[first + a] : 0;
+#pragma unroll
+    for (int a = 0; a < kMaxA; ++a) {
+        if (a >= nam) break;
         const int j = first + a;
         Slot s;
         if (sp >= 0) { s = sh.sp_atom[sp][a]; C.mass[a] = sh.sp_mass[sp][a]; }
         else {
             const double q = D.atom[j].w;
-            s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y; s.pad = 0;
+            s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y;
             C.mass[a] = D.mass[j];
         }
+        s.pad = slots[a];  // the commit updates the staged copy in this slot of CTA j % G
         if (imol - 1 == moving) { s.x = moving_pos[a].x; s.y = moving_pos[a].y; s.z = moving_pos[a].z; }
         else if (imol - 1 == sh.last_mol) { s.x = sh.lx[a]; s.y = sh.ly[a]; s.z = sh.lz[a]; }
         else {
             const double4 *src = (X.G > 1) ? cluster.map_shared_rank(X.atom_s, j % X.G) : X.atom_s;
-            const double4 p = src[j / X.G];
+            const double4 p = src[slots[a]];
             s.x = p.x; s.y = p.y; s.z = p.z;
         }
         C.slot[nam + a] = s;  // old positions
@@ -1028,8 +1194,10 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     const int lane = tid & 31;
 
     // shared memory carve-up (chain_smem_bytes on the host computes the same sizes)
+    const int nblk_max = (A.nown_max + kBlk - 1) / kBlk;
     double2 *tab = reinterpret_cast<double2 *>(smem_raw);                     // [2 kMaxA][3][KM]
-    double4 *atom_s = reinterpret_cast<double4 *>(tab + 2 * kMaxA * 3 * KM);  // [nown_max]
+    float4 *box_s = reinterpret_cast<float4 *>(tab + 2 * kMaxA * 3 * KM);     // [nblk_max][2]
+    double4 *atom_s = reinterpret_cast<double4 *>(box_s + 2 * nblk_max);      // [nown_max]
     int2 *meta_s = reinterpret_cast<int2 *>(atom_s + A.nown_max);             // [nown_max]
     int *queue = reinterpret_cast<int *>(meta_s + A.nown_max);                // [qcap]
     int *nearbuf = queue + ((A.qcap + 1) & ~1);                               // [B/32][32 kCPT]
@@ -1041,13 +1209,17 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     double *xch = red + (B / 32) * kNV;                                       // [2][G][kNV]
     double *lj_s = xch + 2 * G * kNV;                                         // [2][nt*nt]
     double *dhs_ts = lj_s + 2 * nt * nt;                                      // [nt+1] hard core by LJ type
+    int *blist = reinterpret_cast<int *>(dhs_ts + nt + 1);                    // [nblk_max + 32] near blocks
 
-    // atoms of this CTA: j = rank + G * local (interleaved, so every CTA holds a spatial mix)
+    // atoms of this CTA: j = rank + G * i (interleaved, so every CTA holds a spatial mix), in
+    // the spatial order of k_stage_order (slot D.slot[j]), with the bounding box of every kBlk slots
     const int nown = (D.N - rank + G - 1) / G;
     for (int i = tid; i < nown; i += B) {
-        const int j = rank + G * i;
-        atom_s[i] = D.atom[j]; meta_s[i] = D.meta[j];
+        const int j = rank + G * i, sl = D.slot[j];
+        atom_s[sl] = D.atom[j]; meta_s[sl] = D.meta[j];
     }
+    __syncthreads();
+    for (int b = tid; b < (nown + kBlk - 1) / kBlk; b += B) block_box(atom_s, b, nown, box_s);
     for (int i = tid; i < nt * nt; i += B) { lj_s[i] = D.lj_sig6[i]; lj_s[nt * nt + i] = D.lj_feps[i]; }
     for (int i = tid; i <= nt; i += B) dhs_ts[i] = D.dhs_t[i];
 
@@ -1159,7 +1331,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
             const int na0 = sh.cand[sh.icur].na;
             // old forces for force-biased moves (movemc Steps 3-4)
             if constexpr (SPLIT) if (biased) {
-                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
+                if (!ctl) worker_pass<NT, EPT, PASS_OLD, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, box_s, blist, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
                 __syncthreads();
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
                 xpar ^= 1;
@@ -1263,8 +1435,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
 
         // ------------------------------------------------ the pass over the new positions
         if (!ctl) {
-            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
-            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
+            if constexpr (SPLIT) worker_pass<NT, EPT, PASS_NEW, true, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, box_s, blist, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
+            else worker_pass<NT, EPT, PASS_BOTH, false, MX>(D, sh, R, tab, atom_s, dhs_ts, D.dhs, D.dhs_typed, rank, G, meta_s, box_s, blist, queue, nearbuf, red, lj_s, nown, A.qcap, e0, gwork, prof, mold_g, false);
         } else if (speculate && it + 1 < n_moves) {
             // prepare the next move's candidates while the workers run: lanes 1-2 after the
             // acceptance draw, lane 2 with the molecule in flight at its proposed positions (used
@@ -1393,9 +1565,11 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     for (int a = 0; a < na; ++a) {
                         const int j = M.first + a;
                         if (j % G == rank) {
-                            double4 p = atom_s[j / G];
+                            const int sl = M.slot[a].pad;  // the atom's staging slot
+                            double4 p = atom_s[sl];
                             p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
-                            atom_s[j / G] = p;
+                            atom_s[sl] = p;
+                            box_expand(box_s, sl / kBlk, p.x, p.y, p.z);
                         }
                     }
                     ++n_acc;

@@ -41,6 +41,9 @@ struct DevSys {
     long long *cnt;        // run_mc counters, see Cnt
     int nspec;             // runs of identical consecutive molecules (molecule species)
     const int4 *spec;      // first molecule, count, atoms per molecule, first atom (0-based)
+    // the chain kernel's spatial staging: slot[j] = the shared-memory slot of atom j in its CTA
+    // (j % G), atom_of[r * nown_max + s] = the atom in slot s of CTA r (written at launch start)
+    int *slot, *atom_of;
 };
 
 // engine scalars (double)

@@ -792,13 +792,16 @@ int upload(T *d, const T *h, size_t n, cudaStream_t s) {
 
 size_t chain_smem_bytes(int G, int B, int kmax, int nt, int nown_max, int qcap) {
     const int KM = kmax + 1;
+    const size_t nblk_max = (size_t)(nown_max + kBlk - 1) / kBlk;
     size_t b = sizeof(double2) * 2 * kMaxA * 3 * KM;
+    b += sizeof(float4) * 2 * nblk_max;
     b += (sizeof(double4) + sizeof(int2)) * (size_t)nown_max;
     b += sizeof(int) * (size_t)((qcap + 1) & ~1);
     b += sizeof(int) * (size_t)B * kCPT;
     b += sizeof(double) * (size_t)(B / 32) * kNV;
     b += sizeof(double) * (size_t)2 * G * kNV;
     b += sizeof(double) * ((size_t)2 * nt * nt + nt + 1);
+    b += sizeof(int) * (nblk_max + 32);
     return b;
 }
 
@@ -822,6 +825,7 @@ struct yamc_ctx {
     double *freq_beg = nullptr, *freq_end = nullptr, *scal = nullptr;
     long long *cnt = nullptr;
     int4 *spec = nullptr;
+    int *slot = nullptr, *atom_of = nullptr;  // the chain kernel's staging order (k_stage_order)
     double *part = nullptr, *sums = nullptr;  // block partials of the full sums, their totals
     int2 *tpairs = nullptr;                    // atom-tile pairs of the real-space full sum
     int ntpairs = 0;
@@ -969,8 +973,20 @@ int pick_launch(yamc_ctx *c, LaunchCfg *out) {
     return pick_launch_for({&c->H}, c->device, c->force_G, c->force_B, c->force_layout, is_mixed(c), out);
 }
 
+// the spatial staging order of every CTA of nrep chains (k_stage_order), ahead of their launch
+int launch_stage_order(const LaunchCfg &L, cudaStream_t stream, int nrep, const DevSys *d_sys) {
+    const size_t smem = sizeof(int) * ((size_t)kStageMaxCells + L.nown_max);
+    if (smem > 48 * 1024)
+        CUDA_TRY(cudaFuncSetAttribute(k_stage_order, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k_stage_order<<<L.G * nrep, kStageThreads, smem, stream>>>(d_sys, L.G);
+    CUDA_TRY(cudaGetLastError());
+    return YAMC_OK;
+}
+
+// nrep chains: the staging order, then the chain kernel (two launches)
 int launch_chain_cfg(const LaunchCfg &L, int nt, bool split, bool mx, cudaStream_t stream, int nrep,
                      const ChainArgs &args) {
+    if (const int r = launch_stage_order(L, stream, nrep, args.sys)) return r;
     switch (nt) {
         case 1: return launch_chain_nt<1>(L, split, mx, stream, nrep, args);
         case 2: return launch_chain_nt<2>(L, split, mx, stream, nrep, args);
@@ -1178,7 +1194,7 @@ struct yamc_batch {
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, fork = nullptr;
     cudaGraphExec_t graph = nullptr;
     float last_ms = 0.f;
-    int last_launches = 0;  // kernels launched by the last run (chain launches + refresh kernels)
+    int last_launches = 0;  // kernels launched by the last run (staging order + chain, per group)
     int force_G = 0, force_B = 0, force_layout = YAMC_KSPACE_AUTO;
     float *d_rng = nullptr;
     size_t rng_cap = 0;
@@ -1276,7 +1292,7 @@ int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, c
     CUDA_TRY(cudaEventRecord(b->ev1, b->stream));
     CUDA_TRY(cudaStreamSynchronize(b->stream));
     cudaEventElapsedTime(&b->last_ms, b->ev0, b->ev1);
-    b->last_launches = (int)b->groups.size();
+    b->last_launches = 2 * (int)b->groups.size();
     int worst = YAMC_OK;
     for (BatchGroup &g : b->groups)
         for (size_t k = 0; k < g.idx.size(); ++k) {
@@ -1375,7 +1391,8 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
         (r = dalloc(&c->scratch, (size_t)2 * (1 + nt) * S)) || (r = dalloc(&c->freq_beg, M)) || (r = dalloc(&c->freq_end, M)) ||
         (r = dalloc(&c->scal, SC_COUNT)) || (r = dalloc(&c->cnt, CN_COUNT)) ||
-        (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = 0) || (r = dalloc(&c->spec, H.spec.size() / 4)))
+        (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->slot, N)) ||
+        (r = dalloc(&c->atom_of, (size_t)N + 16)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
     CUDA_TRY(cudaHostAlloc(&c->h_out, sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT,
                            cudaHostAllocMapped));
@@ -1441,6 +1458,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     D.ebeta_f = c->ebeta_f; D.ebetalj_f = c->ebetalj_f;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
     D.nspec = (int)(H.spec.size() / 4); D.spec = c->spec;
+    D.slot = c->slot; D.atom_of = c->atom_of;
     if ((r = upload(c->d_sys, &D, 1, c->stream))) return r;
     c->cnt_h[CN_ICYCLE] = 1;
     c->cnt_h[CN_MOVE_IN_CYCLE] = 0;
@@ -1468,7 +1486,7 @@ int yamc_destroy(yamc_ctx *c) {
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
                     c->tpairs, c->rho_part, c->d_sys, c->d_run, c->d_rng, c->d_log, c->d_rows,
                     c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save, c->d_mpart,
-                    c->d_mcount};
+                    c->d_mcount, c->slot, c->atom_of};
     for (void *p : ptrs) if (p) cudaFree(p);
     if (c->h_out) cudaFreeHost(c->h_out);
     if (c->ev0) cudaEventDestroy(c->ev0);
