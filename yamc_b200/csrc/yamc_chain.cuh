@@ -8,6 +8,7 @@
 #include <cuda_runtime.h>
 
 #include <string>
+#include <type_traits>
 
 #include "yamc_device.cuh"
 #include "yamc_internal.h"
@@ -156,7 +157,8 @@ __device__ __forceinline__ bool box_near(const float4 *box_s, int b, double qx, 
 // chain of G CTAs owns atoms j = r + G i; they are ordered by the Morton index of their cell on
 // an nc^3 grid (nc a power of two <= 16, about four owned atoms per cell), stably (by i) within a
 // cell.  Writes D.slot[j] (the slot of atom j in its CTA) and D.atom_of[s G + r] (the atom in
-// slot s of CTA r).  Shared memory: kStageMaxCells + atoms-per-CTA ints.
+// slot s of CTA r), and the FP32 copy of rho that the mixed form's streamed sweeps read (the
+// chain's blocks split its entries).  Shared memory: kStageMaxCells + atoms-per-CTA ints.
 constexpr int kStageThreads = 256;
 constexpr int kStageMaxCells = 4096;
 
@@ -175,6 +177,10 @@ static __global__ void __launch_bounds__(kStageThreads) k_stage_order(const DevS
     const DevSys &D = sys[blockIdx.x / G];
     const int tid = threadIdx.x, lane = tid & 31;
     const int nown = (D.N - rank + G - 1) / G;
+    for (int i = rank * kStageThreads + tid, n = (1 + D.nt) * D.S; i < n; i += G * kStageThreads) {
+        const double2 r = D.rho[i];
+        D.rho_f[i] = make_float2((float)r.x, (float)r.y);
+    }
     int nc = 1;
     while (nc < 16 && 4 * (2 * nc) * (2 * nc) * (2 * nc) <= nown) nc *= 2;
     const int ncell = nc * nc * nc;
@@ -308,6 +314,8 @@ __device__ __forceinline__ float2 mk2(float x, float y) { return make_float2(x, 
 template <class R2> __device__ __forceinline__ R2 cvt2(double2 v);
 template <> __device__ __forceinline__ double2 cvt2<double2>(double2 v) { return v; }
 template <> __device__ __forceinline__ float2 cvt2<float2>(double2 v) { return make_float2((float)v.x, (float)v.y); }
+template <class R2> __device__ __forceinline__ R2 cvt2(float2 v);  // (FP32 rho copies: the mixed form only)
+template <> __device__ __forceinline__ float2 cvt2<float2>(float2 v) { return v; }
 __device__ __forceinline__ double2 to_d2(double2 v) { return v; }
 __device__ __forceinline__ double2 to_d2(float2 v) { return make_double2((double)v.x, (double)v.y); }
 
@@ -354,6 +362,9 @@ struct Acc<true, N> {
     __device__ __forceinline__ void add_plain(int i, float x) { s[i] += x; }
     __device__ __forceinline__ void flag(int i) { d[i] = 1.0; }
     __device__ __forceinline__ double get(int i) const { return d[i] + ((double)s[i] + (double)c[i]); }
+    // the FP32 part alone, and its clearing (the k-space sums are reduced before the real space)
+    __device__ __forceinline__ double kpart(int i) const { return (double)s[i] + (double)c[i]; }
+    __device__ __forceinline__ void clear_kpart(int i) { s[i] = 0.f; c[i] = 0.f; }
 };
 
 template <int NT, int EPT, bool MX = false>
@@ -483,11 +494,11 @@ __device__ __forceinline__ void entry_forces(const Slot *slots, int s0, int na, 
 
 // One signed entry of a pass: the molecule's phase sums at the old positions (into mold) and/or
 // the new ones, the delta (into dl), dU_k Coulomb + LJ against rho, and the k-space forces.
-template <int NT, int KIND, bool FORCES, bool MX, class AccT>
+template <int NT, int KIND, bool FORCES, bool MX, class AccT, class RhoT>
 __device__ __forceinline__ void kspace_entry(const PhaseTabs<MX> &pt, const Slot *slots, int na, int kx,
                                              int ky, int kz, typename Prec<MX>::R beta,
                                              const typename Prec<MX>::R (&bl)[NPair<NT>::value],
-                                             const double2 (&rho)[1 + NT], typename Prec<MX>::R2 (&mold)[1 + NT],
+                                             const RhoT (&rho)[1 + NT], typename Prec<MX>::R2 (&mold)[1 + NT],
                                              typename Prec<MX>::R2 (&dl)[1 + NT], AccT &acc) {
     using R = typename Prec<MX>::R;
     using R2 = typename Prec<MX>::R2;
@@ -566,14 +577,17 @@ __device__ __forceinline__ void kspace_sweep(const DevSys &D, RegsOf<NT, EPT, MX
         // U entries per iteration: their independent dependency chains interleave
         constexpr int U = YAMC_KSPACE_UNROLL;
         constexpr bool IN_MOLD = KIND == PASS_NEW;   // read the old sums
-        int4 kv_n[U];
+        // the mixed form reads FP32 rho (D.rho_f, equal to rho rounded to FP32, which is what its
+        // arithmetic takes), FP32 beta tables and FP32 scratch; k comes packed in one word
+        using RhoT = std::conditional_t<MX, float2, double2>;
+        int kv_n[U];
         Rt beta_n[U], bl_n[U][NPair<NT>::value];
-        double2 rho_n[U][1 + NT];
+        RhoT rho_n[U][1 + NT];
         R2 mold_n[U][1 + NT];
         // the loads of the next entry stay in flight until the entry is taken up: no value is
-        // converted here (the mixed form reads FP32 copies of the beta tables and FP32 scratch)
+        // converted here
         auto fetch = [&](int j, int e) {
-            kv_n[j] = D.kvec[e];
+            kv_n[j] = D.kpack[e];
             if constexpr (MX) {
                 beta_n[j] = D.ebeta_f[e];
 #pragma unroll
@@ -585,7 +599,8 @@ __device__ __forceinline__ void kspace_sweep(const DevSys &D, RegsOf<NT, EPT, MX
             }
 #pragma unroll
             for (int t = 0; t <= NT; ++t) {
-                rho_n[j][t] = D.rho[(size_t)t * S + e];
+                if constexpr (MX) rho_n[j][t] = D.rho_f[(size_t)t * S + e];
+                else rho_n[j][t] = D.rho[(size_t)t * S + e];
                 mold_n[j][t] = IN_MOLD ? mold_in[(size_t)t * S + e] : mk2(Rt(0), Rt(0));
             }
         };
@@ -596,11 +611,11 @@ __device__ __forceinline__ void kspace_sweep(const DevSys &D, RegsOf<NT, EPT, MX
         for (int e = e0; e < S; e += step) {
             int kx[U], ky[U], kz[U];
             Rt beta[U], bl[U][NPair<NT>::value];
-            double2 rho[U][1 + NT];
+            RhoT rho[U][1 + NT];
             R2 mold[U][1 + NT], dl[U][1 + NT];
 #pragma unroll
             for (int j = 0; j < U; ++j) {
-                kx[j] = kv_n[j].x; ky[j] = kv_n[j].y; kz[j] = kv_n[j].z;
+                kx[j] = kv_n[j] & 255; ky[j] = ((kv_n[j] >> 8) & 255) - 128; kz[j] = (kv_n[j] >> 16) - 128;
                 beta[j] = beta_n[j];
 #pragma unroll
                 for (int p = 0; p < NPair<NT>::value; ++p) bl[j][p] = bl_n[j][p];
@@ -672,6 +687,22 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
     acc.zero();
     kspace_sweep<NT, EPT, KIND, FORCES, MX>(D, R, pt, m.slot, na, e0, estep, EPT > 0 ? nullptr : mold_buf, mold_buf,
                                             mold_out, acc);
+    // the mixed form's FP32 k-space sums (dU_k, k-space forces) leave the registers here: reduced
+    // over the warp into its row now, so the real-space phase holds only its own accumulators;
+    // the real-space values are added to the row at the end
+    const int nv = FORCES ? (RV_F + 3 * na) : RV_F;
+    auto kvalue = [&](int v) { return (KIND != PASS_OLD && (v == RV_DUC || v == RV_DUL)) || (FORCES && v >= RV_F && v < nv); };
+    if constexpr (MX) {
+#pragma unroll
+        for (int v = 0; v < NVMAX; ++v) {
+            if (!kvalue(v)) continue;
+            double x = acc.kpart(v);
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) x += __shfl_xor_sync(0xffffffffu, x, o);
+            if (lane == 0) red[wwarp * kNV + v] = x;
+            acc.clear_kpart(v);
+        }
+    }
     YAMC_WPH(PH_KSPACE);
 
     // bounding spheres of the molecule at its new (slot 0) and old (slot na) positions: an atom
@@ -858,8 +889,8 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
         if (!more_rounds) break;
     }
 
-    // per-warp reduction (xor tree) into red[worker warp][value]
-    const int nv = FORCES ? (RV_F + 3 * na) : RV_F;
+    // per-warp reduction (xor tree) into red[worker warp][value] (the mixed form adds its
+    // k-space part, already there)
 #pragma unroll
     for (int v = 0; v < NVMAX; ++v) {
         if (v < nv) {
@@ -869,7 +900,7 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
                 const double y = __shfl_xor_sync(0xffffffffu, x, o);
                 x = (v == RV_OVL) ? fmax(x, y) : x + y;
             }
-            if (lane == 0) red[wwarp * kNV + v] = x;
+            if (lane == 0) red[wwarp * kNV + v] = (MX && kvalue(v)) ? red[wwarp * kNV + v] + x : x;
         }
     }
 #undef YAMC_WPH
@@ -1138,7 +1169,10 @@ __device__ __noinline__ void refresh_in_chain(const DevSys &D, Regs &R, double2 
 #pragma unroll
             for (int t = 0; t <= NT; ++t) {
                 if constexpr (EPT > 0) R.rho[j][t] = acc[j][t];
-                else D.rho[(size_t)t * S + e] = acc[j][t];
+                else {
+                    D.rho[(size_t)t * S + e] = acc[j][t];
+                    D.rho_f[(size_t)t * S + e] = make_float2((float)acc[j][t].x, (float)acc[j][t].y);
+                }
             }
             ekc += D.ebeta[e] * (acc[j][0].x * acc[j][0].x + acc[j][0].y * acc[j][0].y);
 #pragma unroll
@@ -1640,6 +1674,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                             const double2 d = to_d2(dl_g[(size_t)t * S + e]);
                             r.x += d.x; r.y += d.y;
                             D.rho[(size_t)t * S + e] = r;
+                            if constexpr (MX) D.rho_f[(size_t)t * S + e] = make_float2((float)r.x, (float)r.y);
                         }
                 }
             }

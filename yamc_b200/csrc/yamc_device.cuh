@@ -29,12 +29,15 @@ struct DevSys {
     const double *mass;    // per atom
     const int2 *mol;       // first atom (0-based), atoms in molecule
     const int4 *kvec;      // kx, signed ky, signed kz, half-space index
+    const int *kpack;      // the same k in one word, kx | (ky + 128) << 8 | (kz + 128) << 16 (streamed sweeps)
     const double *ebeta;   // Coulomb beta per signed entry (2x for kx>0 folded in)
     const double *ebetalj; // npair x S
     const float *ebeta_f, *ebetalj_f;  // FP32 copies of ebeta and ebetalj (the mixed form's k-space reads)
     const int *pair_index; // nt*nt -> pair row
     const double *lj_sig6, *lj_feps;  // nt*nt tables (offset (t1-1)*nt + t2-1)
     double2 *rho;          // (1+nt) x S: Coulomb then one row per LJ type
+    float2 *rho_f;         // the mixed form's FP32 copy of rho, read by its streamed sweeps: written from rho
+                           // before every chain launch (k_stage_order), kept with rho by the chain's commits
     double2 *scratch;      // 2 x (1+nt) x S: the moved molecule's old phase sums, then the rho deltas (FP32 pairs in the mixed form)
     const double *freq_beg, *freq_end;
     double *scal;          // engine scalars, see Scal

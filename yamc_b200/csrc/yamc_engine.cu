@@ -820,6 +820,8 @@ struct yamc_ctx {
     float *ebeta_f = nullptr, *ebetalj_f = nullptr;  // FP32 copies of ebeta / ebetalj for the mixed form
     std::vector<float> h_ebeta_f, h_ebetalj_f;       // their host sources (kept: the uploads are asynchronous)
     int4 *kvec = nullptr;
+    int *kpack = nullptr;      // kvec packed in one word (the chain kernel's streamed sweeps)
+    float2 *rho_f = nullptr;   // FP32 copy of rho (the mixed form's streamed sweeps)
     int *pair_index = nullptr;
     double2 *rho = nullptr, *scratch = nullptr;
     double *freq_beg = nullptr, *freq_end = nullptr, *scal = nullptr;
@@ -1385,7 +1387,8 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     CUDA_TRY(cudaEventCreate(&c->ev1));
     const int N = H.N, M = H.M, S = H.S, nt = H.nt;
     if ((r = dalloc(&c->atom, N)) || (r = dalloc(&c->meta, N)) || (r = dalloc(&c->dhs, N)) || (r = dalloc(&c->mass, N)) ||
-        (r = dalloc(&c->mol, M)) || (r = dalloc(&c->kvec, S)) || (r = dalloc(&c->ebeta, S)) ||
+        (r = dalloc(&c->mol, M)) || (r = dalloc(&c->kvec, S)) || (r = dalloc(&c->kpack, S)) ||
+        (r = dalloc(&c->rho_f, (size_t)(1 + nt) * S)) || (r = dalloc(&c->ebeta, S)) ||
         (r = dalloc(&c->ebeta_f, S)) || (r = dalloc(&c->ebetalj_f, (size_t)H.npair * S)) ||
         (r = dalloc(&c->ebetalj, (size_t)H.npair * S)) || (r = dalloc(&c->pair_index, nt * nt)) ||
         (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
@@ -1430,11 +1433,15 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     for (int i = 0; i < M; ++i) mo[i] = make_int2(H.first[i], H.natoms[i]);
     std::vector<int4> kv(S);
     for (int e = 0; e < S; ++e) kv[e] = make_int4(H.ekx[e], H.eky[e], H.ekz[e], H.ekk[e]);
+    if (H.kmax > 127) { set_error("kmax above 127 (the packed k of the chain kernel holds 8 bits per component)"); return YAMC_ELIMITS; }
+    std::vector<int> kp(S);
+    for (int e = 0; e < S; ++e) kp[e] = H.ekx[e] | ((H.eky[e] + 128) << 8) | ((H.ekz[e] + 128) << 16);
     std::vector<int> pidx(nt * nt);
     for (int i = 0; i < nt * nt; ++i) pidx[i] = H.pair_index[i];
     if ((r = upload(c->atom, a.data(), N, c->stream)) || (r = upload(c->meta, m.data(), N, c->stream)) ||
         (r = upload(c->dhs, H.dhs.data(), N, c->stream)) || (r = upload(c->mass, H.mass.data(), N, c->stream)) ||
         (r = upload(c->mol, mo.data(), M, c->stream)) || (r = upload(c->kvec, kv.data(), S, c->stream)) ||
+        (r = upload(c->kpack, kp.data(), S, c->stream)) ||
         (r = upload(c->ebeta, H.ebeta.data(), S, c->stream)) || (r = upload(c->ebetalj, H.ebetalj.data(), (size_t)H.npair * S, c->stream)) ||
         (r = upload_beta_f(c)) || (r = upload(c->pair_index, pidx.data(), nt * nt, c->stream)) || (r = upload(c->lj_sig6, H.sigma6.data(), nt * nt, c->stream)) ||
         (r = upload(c->lj_feps, H.four_eps.data(), nt * nt, c->stream)) || (r = upload(c->freq_beg, H.freq_beg.data(), M, c->stream)) ||
@@ -1454,6 +1461,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     fill_dhs_types(H, D);
     D.xprob = 0.0;
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
+    D.kpack = c->kpack; D.rho_f = c->rho_f;
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
     D.ebeta_f = c->ebeta_f; D.ebetalj_f = c->ebetalj_f;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
@@ -1482,7 +1490,7 @@ int yamc_destroy(yamc_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->ebeta_f, c->ebetalj_f,
-                    c->lj_sig6, c->lj_feps, c->kvec,
+                    c->lj_sig6, c->lj_feps, c->kvec, c->kpack, c->rho_f,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
                     c->tpairs, c->rho_part, c->d_sys, c->d_run, c->d_rng, c->d_log, c->d_rows,
                     c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save, c->d_mpart,
