@@ -1407,12 +1407,11 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                         sh.disp_end = rng.cur;
                         sh.disp_out = rng.out;
                     } else {
-                        MoveState mr;
+                        MoveState &mr = sh.mrot;
                         mcm_init_old(mr, F, T);
                         mcm_skip_displacement(mr, rng, D.xlf, D.dr);
                         sh.rot_start = rng.cur;
                         if (!rng.out) mcm_choose_rotation(mr, rng, D.xlc, D.d_angle);
-                        sh.mrot = mr;
                         sh.rot_end = rng.cur;
                         sh.rot_out = rng.out;
                     }
@@ -1550,13 +1549,16 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 du_ext = D.kext * ((2 * mux + dmx) * dmx + (2 * muy + dmy) * dmy + (2 * muz + dmz) * dmz);
                 double F[3] = {0, 0, 0}, T[3] = {0, 0, 0};
                 if (biased) {
+                    // (loops over kMaxA with constant indices: the arrays stay in registers)
                     double fx[kMaxA], fy[kMaxA], fz[kMaxA], x[kMaxA], y[kMaxA], z[kMaxA];
-                    for (int a = 0; a < na; ++a) {
-                        const double q = M.slot[a].q;
-                        fx[a] = sh.tot[RV_F + 3 * a] + D.m2k * q * (mux + dmx);
-                        fy[a] = sh.tot[RV_F + 3 * a + 1] + D.m2k * q * (muy + dmy);
-                        fz[a] = sh.tot[RV_F + 3 * a + 2] + D.m2k * q * (muz + dmz);
-                        x[a] = M.slot[a].x; y[a] = M.slot[a].y; z[a] = M.slot[a].z;
+#pragma unroll
+                    for (int a = 0; a < kMaxA; ++a) {
+                        const int b = a < na ? a : 0;
+                        const double q = M.slot[b].q;
+                        fx[a] = sh.tot[RV_F + 3 * b] + D.m2k * q * (mux + dmx);
+                        fy[a] = sh.tot[RV_F + 3 * b + 1] + D.m2k * q * (muy + dmy);
+                        fz[a] = sh.tot[RV_F + 3 * b + 2] + D.m2k * q * (muz + dmz);
+                        x[a] = M.slot[b].x; y[a] = M.slot[b].y; z[a] = M.slot[b].z;
                     }
                     mol_force_torque(na, x, y, z, M.mass, fx, fy, fz, F, T);
                 }
@@ -1569,7 +1571,8 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     for (int c = 0; c < 3; ++c) finite = finite && isfinite(F[c]) && isfinite(T[c]);
                 if (!finite) { sh.abort = kAbortNonFinite; sh.accepted = 0; goto decided; }
                 if (biased || SPLIT) {
-                    MoveState mv = M.mv;
+                    // (the bias state in shared memory, where the proposal left it: no copy to spill)
+                    MoveState &mv = sh.cand[sh.icur].mv;
                     mcm_init_new(mv, F, T, D.xlf, D.xlc, D.dr, D.d_angle);
                     acc = mcm_accept(mv, du_total, D.xlf, D.xlc, rng);
                 } else {
