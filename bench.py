@@ -20,7 +20,8 @@ shard), the launch shape picked by the batch autotuner.
   configs the other configurations of the metric, each with its plain FP64 chain, mixed and
           FP64 batches and precision errors: spce256 (256 SPC/E), nacl1m (2048 SPC/E + NaCl,
           unbiased), nacl16k (16384 SPC/E + NaCl, force-biased), batch_ragged_96 (96 ragged
-          replicas in one batch), npt_run_mc (NPT run_mc with volume steps)
+          replicas in one batch), npt_run_mc (NPT run_mc with volume steps), per_move_drop_in
+          (host latency of the per-move C ABI: movemc split as a Fortran host calls it)
   cpu_baseline  the oracle (-O3 C restatement of the reference) on one host core, a bounded
           sample of the same workload
   --impl reference  the CPU restatement of the reference (oracle/, -O3) timed on the host
@@ -415,6 +416,50 @@ def npt_block(local, rank, cycles=12):
             "box_length_A": L}
 
 
+def per_move_block(local, rank, n=300):
+    """The per-move drop-in (yamc_move_old + yamc_move_eval + yamc_move_commit, movemc split as a
+    Fortran host calls it) on nacl1m, FP64: host-clock latency per move of n moves of random
+    waters, each displaced by 1e-3 box units and rejected, called through ctypes with every
+    argument built before the timed loop (the median and the parts' medians)."""
+    import ctypes
+    from yamc_b200 import api, systems
+    base = f"/tmp/yamc_bench_pm_r{rank}_{os.getpid()}"
+    files = systems.write_system(systems.WORKLOADS["nacl1m"], base, seed=3)
+    eng = api.Engine.from_files(files, device=local)
+    lib, h = eng.lib, eng.h
+    x, y, z = (np.ascontiguousarray(v, dtype=np.float64) for v in eng.positions())
+    rs = np.random.default_rng(0)
+    mols = rs.integers(1, 2049, size=n)
+    new = [tuple(np.ascontiguousarray(v[3 * (m - 1):3 * m] + (1e-3 if k == 0 else 0.0)) for k, v in enumerate((x, y, z)))
+           for m in mols]
+    dp = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    f, t, du = np.zeros(3), np.zeros(3), np.zeros(4)
+    pf, pt, pdu = dp(f), dp(t), dp(du)
+    ov = ctypes.c_int32(0)
+    pov = ctypes.byref(ov)
+    args = [(int(m), dp(a), dp(b), dp(c)) for m, (a, b, c) in zip(mols, new)]
+    for m, pa, pb, pc in args[:20]:  # warm-up
+        lib.yamc_move_old(h, m, pf, pt); lib.yamc_move_eval(h, m, pa, pb, pc, pdu, pov, pf, pt); lib.yamc_move_commit(h, 0)
+    to, te, tc = [], [], []
+    clk = time.perf_counter
+    for m, pa, pb, pc in args:
+        t0 = clk()
+        r0 = lib.yamc_move_old(h, m, pf, pt)
+        t1 = clk()
+        r1 = lib.yamc_move_eval(h, m, pa, pb, pc, pdu, pov, pf, pt)
+        t2 = clk()
+        r2 = lib.yamc_move_commit(h, 0)
+        t3 = clk()
+        assert r0 == r1 == r2 == 0, (r0, r1, r2)
+        to.append(t1 - t0); te.append(t2 - t1); tc.append(t3 - t2)
+    eng.close()
+    med = lambda v: 1e6 * float(np.median(v))
+    tot = [a + b + c for a, b, c in zip(to, te, tc)]
+    return {"workload": "nacl1m (6220 atoms), FP64, one water per move, rejected",
+            "calls": "yamc_move_old + yamc_move_eval + yamc_move_commit through ctypes, arguments prebuilt",
+            "moves": n, "us_per_move_median": med(tot), "old_us": med(to), "eval_us": med(te), "commit_us": med(tc)}
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -619,6 +664,7 @@ def main():
         blocks["nacl16k"] = config_block("nacl16k", local, rank, moves=300, steps=3, warmup=1)
         blocks["batch_ragged_96"] = ragged_batch_block(local, rank, moves=4000)
         blocks["npt_run_mc"] = npt_block(local, rank)
+        blocks["per_move_drop_in"] = per_move_block(local, rank)
     line["configs"] = blocks
     if not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(files)

@@ -46,6 +46,11 @@ extern "C" {
    when an energy is non-finite (the context then holds those sums: load finite positions). */
 #define YAMC_ENAN (-13)
 #define YAMC_EOVERLAP_INIT (-14)
+/* YAMC_EBOUNDS: bounds-checked builds only (libyamc_b200_checked.so, compiled with
+   -DYAMC_CHECKED): an index the chain kernel computed fell outside its array.  The kernel
+   replaced it by 0 (no fault) and the call returns this code; yamc_last_error_detail names the
+   source line.  The state of the context is then unreliable. */
+#define YAMC_EBOUNDS (-15)
 
 /* precision of the device arithmetic */
 #define YAMC_FP64 0   /* plain method: every operation in FP64 */
@@ -315,12 +320,22 @@ int yamc_set_kspace_layout(yamc_ctx *ctx, int32_t layout);
 int yamc_get_launch(yamc_ctx *ctx, int32_t out[4]);
 /* device time (ms) of the last run_chain kernel, measured with CUDA events on its stream */
 int yamc_last_kernel_ms(yamc_ctx *ctx, double *ms);
-/* Per-phase clock64 cycles of the chain kernel, summed over moves by block 0
-   (control warp: choose, speculation of the next move, proposal, reduction, Metropolis,
-   commit; worker warps: phase tables, k-space, pair filter, pairs, and -- force-biased moves --
-   the k-space sweep of the next molecule).  mode 1 = reset and enable, 0 = disable,
+/* Per-phase clock64 cycles of the chain kernel, summed over moves by block 0, in the order
+   choose, speculate, propose, tables, kspace, pair_filter, pairs, reduce, old_pass,
+   metropolis, commit, kspace_next (control warp: molecule choice, speculation of the next
+   move, proposal, reduction, the force-biased old pass with its reduction, Metropolis,
+   commit; worker warps: phase tables, k-space, pair filter, pairs; kspace_next is unused).
+   mode 1 = reset and enable, 0 = disable,
    2 = read only; out receives min(n, 12) counters in that order. */
 int yamc_phase_cycles(yamc_ctx *ctx, int32_t mode, int64_t *out, int32_t n);
+/* No counterpart in the reference (whose checked build is gfortran's -ffpe-trap=invalid debug
+   Makefile): *checked = 1 for the bounds-checked build of this library, 0 otherwise; and one
+   checked read of a 4-value device array at `index` with the array taken as `size` long (at most
+   4), on device `device`, with no context: *value = the value read (array[0] when the index is
+   out of bounds) and *line = the source line the check recorded (0 when the index was in
+   bounds) -- the index check on its own, in every build, for tests. */
+int yamc_checked_build(int32_t *checked);
+int yamc_bounds_check_selftest(int32_t device, int64_t index, int64_t size, double *value, int32_t *line);
 const char *yamc_error_string(int status);
 const char *yamc_last_error_detail(void);
 

@@ -12,7 +12,9 @@ import os
 import numpy as np
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libyamc_b200.so")
+# the engine library; YAMC_LIBRARY names another build of it (the bounds-checked
+# libyamc_b200_checked.so, for instance)
+LIB_PATH = os.environ.get("YAMC_LIBRARY") or os.path.join(HERE, "libyamc_b200.so")
 
 YAMC_OK = 0
 YAMC_ELIMITS = -2
@@ -20,6 +22,7 @@ YAMC_EPARAMETER = -3
 YAMC_EWRONG_FUNCTION = -5
 YAMC_ERNG_EXHAUSTED = -12
 YAMC_ENAN = -13
+YAMC_EBOUNDS = -15
 YAMC_KSPACE_AUTO = 0
 YAMC_KSPACE_REGISTERS = 1
 YAMC_KSPACE_STREAMED = 2
@@ -127,6 +130,8 @@ SIGNATURES = {
     "yamc_get_launch": (ctypes.c_int, [_VP, _ip]),
     "yamc_last_kernel_ms": (ctypes.c_int, [_VP, _dp]),
     "yamc_phase_cycles": (ctypes.c_int, [_VP, ctypes.c_int32, ctypes.POINTER(ctypes.c_int64), ctypes.c_int32]),
+    "yamc_checked_build": (ctypes.c_int, [_ip]),
+    "yamc_bounds_check_selftest": (ctypes.c_int, [ctypes.c_int32, ctypes.c_int64, ctypes.c_int64, _dp, _ip]),
     "yamc_batch_create": (ctypes.c_int, [ctypes.c_int32, ctypes.POINTER(YamcSystem), ctypes.POINTER(YamcParams),
                                          ctypes.c_int32, _PPP]),
     "yamc_batch_destroy": (ctypes.c_int, [_VP]),

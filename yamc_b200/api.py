@@ -309,7 +309,7 @@ class Engine:
                 "smem_bytes": int(out[3])}
 
     PHASES = ("choose", "speculate", "propose", "tables", "kspace", "pair_filter", "pairs", "reduce",
-              "cluster", "metropolis", "commit", "kspace_next")
+              "old_pass", "metropolis", "commit", "kspace_next")
 
     def phase_cycles(self, mode: int = 2) -> dict:
         out = np.zeros(len(self.PHASES), dtype=np.int64)

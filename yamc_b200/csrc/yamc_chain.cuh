@@ -78,7 +78,7 @@ struct ChainArgs {
 
 // phases timed when ChainArgs::prof is set (control lane 0 or worker thread 32 of CTA 0)
 enum Phase { PH_CHOOSE = 0, PH_SPECULATE, PH_PROPOSE, PH_TABLES, PH_KSPACE, PH_FILTER, PH_PAIRS, PH_REDUCE,
-             PH_CLUSTER, PH_DECIDE, PH_COMMIT, PH_KSPACE_NEXT, PH_COUNT };
+             PH_OLD_PASS, PH_DECIDE, PH_COMMIT, PH_KSPACE_NEXT, PH_COUNT };
 
 // reduction vector of one pass: the moved molecule's energies, k-space energy change, overlap
 // flag and per-atom forces
@@ -227,7 +227,7 @@ static __global__ void __launch_bounds__(kStageThreads) k_stage_order(const DevS
     for (int i = tid; i < nown; i += kStageThreads) {
         const int j = rank + G * i, s = key[i];
         D.slot[j] = s;
-        D.atom_of[s * G + rank] = j;
+        D.atom_of[YAMC_IX(s * G + rank, D.N + 16)] = j;
     }
 }
 
@@ -587,7 +587,7 @@ __device__ __forceinline__ void kspace_sweep(const DevSys &D, RegsOf<NT, EPT, MX
         // the loads of the next entry stay in flight until the entry is taken up: no value is
         // converted here
         auto fetch = [&](int j, int e) {
-            kv_n[j] = D.kpack[e];
+            kv_n[j] = D.kpack[YAMC_IX(e, S)];
             if constexpr (MX) {
                 beta_n[j] = D.ebeta_f[e];
 #pragma unroll
@@ -749,7 +749,7 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
             const int k = k0 + lane, b = wwarp + nww * k;
             const bool near = k < wcap && b < nblk && box_near(box_s, b, qx, qy, qz, qr2);
             const unsigned bal = __ballot_sync(0xffffffffu, near);
-            if (near) wl[nnb + __popc(bal & ((1u << lane) - 1u))] = b;
+            if (near) wl[YAMC_IX(nnb + __popc(bal & ((1u << lane) - 1u)), wcap)] = b;
             nnb += __popc(bal);
         }
         __syncwarp();
@@ -760,10 +760,10 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
         int nnear = 0;
 #pragma unroll
         for (int c = 0; c < kCPT; ++c) {
-            const int jl = r0 + c < nnb ? wl[r0 + c] * kBlk + lane : nown;
+            const int jl = r0 + c < nnb ? wl[YAMC_IX(r0 + c, wcap)] * kBlk + lane : nown;
             bool near = false;
-            if (jl < nown && meta_s[jl].x != imol0) {
-                const double4 pj = atom_s[jl];
+            if (jl < nown && meta_s[YAMC_IX(jl, nown)].x != imol0) {
+                const double4 pj = atom_s[YAMC_IX(jl, nown)];
                 if (KIND == PASS_BOTH) {
                     const double dx = min_image(cbx - pj.x), dy = min_image(cby - pj.y), dz = min_image(cbz - pj.z);
                     near = dx * dx + dy * dy + dz * dz < rb2;
@@ -776,7 +776,7 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
                 }
             }
             const unsigned bal = __ballot_sync(0xffffffffu, near);
-            if (near) nb[nnear + __popc(bal & ((1u << lane) - 1u))] = jl;
+            if (near) nb[YAMC_IX(nnear + __popc(bal & ((1u << lane) - 1u)), 32 * kCPT)] = jl;
             nnear += __popc(bal);
         }
         __syncwarp();
@@ -787,12 +787,12 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
         for (int c = 0; c < kCPT; ++c) {
             const int k = c * 32 + lane;
             if (k < nnear) {
-                const int jl = nb[k];
-                const double4 pj = atom_s[jl];
-                const int tj = meta_s[jl].y;
+                const int jl = nb[YAMC_IX(k, 32 * kCPT)];
+                const double4 pj = atom_s[YAMC_IX(jl, nown)];
+                const int tj = meta_s[YAMC_IX(jl, nown)].y;
                 // hard-core diameter: by LJ type when every atom of a type has the same one
                 // (a shared-memory table), else the atom's own (global memory, by the atom in slot jl)
-                const double dj = dhs_typed ? dhs_ts[tj] : dhs_g[D.atom_of[jl * gsize + grank]];
+                const double dj = dhs_typed ? dhs_ts[tj] : dhs_g[D.atom_of[YAMC_IX(jl * gsize + grank, D.N + 16)]];
                 unsigned msk = 0;
                 for (int s = s_lo; s < s_hi; ++s) {
                     const Slot &sl = m.slot[s];
@@ -847,7 +847,7 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
                     while (msk) {
                         const int s = __ffs(msk) - 1;
                         msk &= msk - 1;
-                        if (pos >= q0 && pos < q0 + qcap) queue[pos - q0] = (jl << 3) | s;
+                        if (pos >= q0 && pos < q0 + qcap) queue[YAMC_IX(pos - q0, qcap)] = (jl << 3) | s;
                         ++pos;
                     }
                 }
@@ -856,11 +856,11 @@ __device__ __forceinline__ void worker_pass_body(const DevSys &D, ChainShared &s
             if (q0 == 0) YAMC_WPH(PH_FILTER);
             const int nc = min(qcap, nq - q0);
             for (int qi = wtid; qi < nc; qi += nwork) {
-                const int item = queue[qi];
+                const int item = queue[YAMC_IX(qi, qcap)];
                 const int jl = item >> 3, s = item & 7;
                 const Slot &sl = m.slot[s];
-                const double4 pj = atom_s[jl];
-                const int tj = meta_s[jl].y;
+                const double4 pj = atom_s[YAMC_IX(jl, nown)];
+                const int tj = meta_s[YAMC_IX(jl, nown)].y;
                 const double dx = min_image(sl.x - pj.x), dy = min_image(sl.y - pj.y), dz = min_image(sl.z - pj.z);
                 const double r2 = dx * dx + dy * dy + dz * dz;
                 const bool lj = sl.type > 0 && tj > 0;
@@ -1019,12 +1019,12 @@ __device__ inline void stage_molecule(const ChooseCtx &X, ChainShared &sh, Cand 
         if (imol - 1 >= sh.sp_m0[q] && imol - 1 < sh.sp_m0[q] + sh.sp_cnt[q]) { sp = q; break; }
     int first, nam;
     if (sp >= 0) { nam = sh.sp_na[sp]; first = sh.sp_a0[sp] + (imol - 1 - sh.sp_m0[sp]) * nam; }
-    else { const int2 mr = D.mol[imol - 1]; first = mr.x; nam = mr.y; }
+    else { const int2 mr = D.mol[YAMC_IX(imol - 1, D.M)]; first = mr.x; nam = mr.y; }
     C.imol = imol; C.first = first; C.na = nam;
     double mx = 0, my = 0, mz = 0;
     int slots[kMaxA];  // staging slots of the molecule's atoms (loaded together)
 #pragma unroll
-    for (int a = 0; a < kMaxA; ++a) slots[a] = a < nam ? D.slot[first + a] : 0;
+    for (int a = 0; a < kMaxA; ++a) slots[a] = a < nam ? D.slot[YAMC_IX(first + a, D.N)] : 0;
 #pragma unroll
     for (int a = 0; a < kMaxA; ++a) {
         if (a >= nam) break;
@@ -1032,9 +1032,10 @@ __device__ inline void stage_molecule(const ChooseCtx &X, ChainShared &sh, Cand 
         Slot s;
         if (sp >= 0) { s = sh.sp_atom[sp][a]; C.mass[a] = sh.sp_mass[sp][a]; }
         else {
-            const double q = D.atom[j].w;
-            s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[j]; s.type = D.meta[j].y;
-            C.mass[a] = D.mass[j];
+            const int jc = (int)YAMC_IX(j, D.N);
+            const double q = D.atom[jc].w;
+            s.q = q; s.iq = q != 0.0 ? 1.0 / q : 0.0; s.dhs = D.dhs[jc]; s.type = D.meta[jc].y;
+            C.mass[a] = D.mass[jc];
         }
         s.pad = slots[a];  // the commit updates the staged copy in this slot of CTA j % G
         if (imol - 1 == moving) { s.x = moving_pos[a].x; s.y = moving_pos[a].y; s.z = moving_pos[a].z; }
@@ -1249,7 +1250,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     // the spatial order of k_stage_order (slot D.slot[j]), with the bounding box of every kBlk slots
     const int nown = (D.N - rank + G - 1) / G;
     for (int i = tid; i < nown; i += B) {
-        const int j = rank + G * i, sl = D.slot[j];
+        const int j = rank + G * i, sl = (int)YAMC_IX(D.slot[j], A.nown_max);
         atom_s[sl] = D.atom[j]; meta_s[sl] = D.meta[j];
     }
     __syncthreads();
@@ -1316,7 +1317,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
         const long long base = run->cursor;
         const long long avail = n_rng - base;
         const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
-        for (int i = lane; i < nw; i += 32) rwin[0][i] = run->rng[base + i - run->rng_off];
+        for (int i = lane; i < nw; i += 32) rwin[0][i] = run->rng[YAMC_IX(base + i - run->rng_off, n_rng - run->rng_off)];
         if (lane == 0) { sh.wbase[0] = base; sh.wn[0] = nw; sh.wbase[1] = -1; sh.wn[1] = 0; sh.wnext = 1; }
     }
     __syncthreads();
@@ -1370,6 +1371,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 reduce_pass(sh, red, xch, RV_F + 3 * na0, G, rank, xpar, cluster);
                 xpar ^= 1;
                 __syncthreads();
+                YAMC_PH(PH_OLD_PASS);  // the force-biased old pass and its reduction (the control warp's view)
                 if (tid == 0) {
                     sh.eold[0] = sh.tot[RV_EW]; sh.eold[1] = sh.tot[RV_LJ6]; sh.eold[2] = sh.tot[RV_LJ12];
                     for (int a = 0; a < na0; ++a) {  // external-field force -2 kext q mu (MC.f90:988-997)
@@ -1486,7 +1488,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     const long long avail = n_rng - c1;
                     const int nw = (int)(avail < (long long)kWin ? (avail > 0 ? avail : 0) : kWin);
                     __syncwarp();
-                    for (int i = lane; i < nw; i += 32) rwin[b][i] = run->rng[c1 + i - run->rng_off];
+                    for (int i = lane; i < nw; i += 32) rwin[b][i] = run->rng[YAMC_IX(c1 + i - run->rng_off, n_rng - run->rng_off)];
                     __syncwarp();
                     if (lane == 0) { sh.wbase[b] = c1; sh.wn[b] = nw; sh.wnext = b ^ 1; }
                     __syncwarp();
@@ -1602,7 +1604,7 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                     for (int a = 0; a < na; ++a) {
                         const int j = M.first + a;
                         if (j % G == rank) {
-                            const int sl = M.slot[a].pad;  // the atom's staging slot
+                            const int sl = (int)YAMC_IX(M.slot[a].pad, nown);  // the atom's staging slot
                             double4 p = atom_s[sl];
                             p.x = M.slot[a].x; p.y = M.slot[a].y; p.z = M.slot[a].z;
                             atom_s[sl] = p;

@@ -47,7 +47,24 @@ struct DevSys {
     // the chain kernel's spatial staging: slot[j] = the shared-memory slot of atom j in its CTA
     // (j % G), atom_of[r * nown_max + s] = the atom in slot s of CTA r (written at launch start)
     int *slot, *atom_of;
+    int *check;            // bounds-checked builds: source line of the first index found out of bounds (0 = none)
 };
+
+// Bounds-checked builds (-DYAMC_CHECKED, libyamc_b200_checked.so): YAMC_IX(i, n) checks every
+// index the chain kernel computes into its atom, staging, k-entry, scratch, pair-queue, near-atom
+// and table arrays.  An index outside [0, n) records the source line in *D.check (the first one
+// wins) and is replaced by 0, so the access stays inside the array: no trap, no fault; the host
+// returns YAMC_EBOUNDS after the launch.  In normal builds YAMC_IX(i, n) is i.
+__device__ __forceinline__ long long checked_ix(long long i, long long n, int line, int *check) {
+    if (i >= 0 && i < n) return i;
+    if (check) atomicCAS(check, 0, line);
+    return 0;
+}
+#ifdef YAMC_CHECKED
+#define YAMC_IX(i, n) ::yamc::checked_ix((long long)(i), (long long)(n), __LINE__, D.check)
+#else
+#define YAMC_IX(i, n) (i)
+#endif
 
 // engine scalars (double)
 enum Scal {

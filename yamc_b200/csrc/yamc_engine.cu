@@ -18,9 +18,11 @@
 #include <cooperative_groups.h>
 #include <cuda_pipeline.h>
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <array>
+#include <chrono>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -31,6 +33,15 @@
 #include "yamc_chain.cuh"
 #include "yamc_device.cuh"
 #include "yamc_internal.h"
+
+
+// an NVTX range around each public entry point (header-only NVTX 3: it costs nothing unless a
+// profiler that records NVTX ranges is attached)
+struct NvtxRange {
+    explicit NvtxRange(const char *name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+};
+#define YAMC_RANGE(name) NvtxRange yamc_nvtx_range_(name)
 
 namespace yamc {
 
@@ -599,6 +610,7 @@ __global__ void k_commit_rho(double2 *rho, const double2 *delta, int n) {
 struct MoveIn {
     int imol;
     double x[kMaxA], y[kMaxA], z[kMaxA];
+    long long seq;  // the call's sequence number, written as the completion word when the results are out
 };
 
 constexpr int kMoveThreads = 256;
@@ -735,6 +747,10 @@ __global__ void __launch_bounds__(kMoveThreads) k_move_pass(DevSys D, MoveIn in,
     if (tid >= 64 && tid < 64 + SC_COUNT) out[kNV + tid - 64] = D.scal[tid - 64];
     if (tid >= 96 && tid < 96 + CN_COUNT) reinterpret_cast<long long *>(out + kNV + SC_COUNT)[tid - 96] = D.cnt[tid - 96];
     if (tid == 0) *counter = 0u;
+    // then the completion word (after CN_COUNT counters): every result is visible to the host first
+    __threadfence_system();
+    __syncthreads();
+    if (tid == 0) reinterpret_cast<volatile long long *>(out + kNV + SC_COUNT)[CN_COUNT] = in.seq;
 }
 
 // The step-14 commit of an accepted per-move step in one launch: rho += the pass's deltas
@@ -821,6 +837,7 @@ struct yamc_ctx {
     std::vector<float> h_ebeta_f, h_ebetalj_f;       // their host sources (kept: the uploads are asynchronous)
     int4 *kvec = nullptr;
     int *kpack = nullptr;      // kvec packed in one word (the chain kernel's streamed sweeps)
+    int *d_check = nullptr;    // bounds-checked builds: the first out-of-bounds source line (DevSys::check)
     float2 *rho_f = nullptr;   // FP32 copy of rho (the mixed form's streamed sweeps)
     int *pair_index = nullptr;
     double2 *rho = nullptr, *scratch = nullptr;
@@ -838,8 +855,10 @@ struct yamc_ctx {
     DevSys *d_sys = nullptr;
     RunSlot *d_run = nullptr;
     // the per-move pass's outputs: its reduction vector, then the engine scalars and counters, in
-    // mapped pinned host memory the kernel writes directly (h_out on the host, d_hout on the device)
+    // mapped pinned host memory the kernel writes directly (h_out on the host, d_hout on the device):
+    // kNV pass values, SC_COUNT scalars, CN_COUNT counters, then the per-move passes' completion word
     double *h_out = nullptr, *d_hout = nullptr;
+    long long move_seq = 0;  // sequence number of the last per-move pass
     // the per-move pass (k_move_pass): block partials and the finished-block counter
     double *d_mpart = nullptr;
     unsigned *d_mcount = nullptr;
@@ -949,8 +968,29 @@ int launch_move_pass_t(yamc_ctx *c, const MoveIn &in, bool eval, size_t smem) {
     return YAMC_OK;
 }
 
-int launch_move_pass(yamc_ctx *c, const MoveIn &in, bool eval) {
+// the per-move passes' completion word in mapped host memory
+volatile long long &move_pass_done(yamc_ctx *c) {
+    return reinterpret_cast<volatile long long *>(c->h_out + kNV + SC_COUNT)[CN_COUNT];
+}
+
+// Waits for the per-move pass with sequence number seq: the kernel writes its results into mapped
+// host memory and then the completion word, so the host spins on that word (for up to 200 ms)
+// rather than synchronising the stream, which saves the synchronisation's wake-up latency.  A
+// pass that has not finished by then, or has failed, is reported by the stream synchronisation
+// that follows.  Later work goes to the same stream, so it stays ordered after the pass.
+int wait_move_pass(yamc_ctx *c, long long seq) {
+    const auto t0 = std::chrono::steady_clock::now();
+    for (long long n = 1; move_pass_done(c) != seq; ++n)
+        if (n % 1024 == 0 && std::chrono::steady_clock::now() - t0 > std::chrono::milliseconds(200)) break;
+    if (move_pass_done(c) == seq) return YAMC_OK;
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (move_pass_done(c) != seq) { set_error("a per-move pass ended without its results"); return YAMC_ECUDA; }
+    return YAMC_OK;
+}
+
+int launch_move_pass(yamc_ctx *c, MoveIn &in, bool eval) {
     const HostSystem &H = c->H;
+    in.seq = ++c->move_seq;
     if (!c->d_mpart) {
         // one thread per atom and per signed entry, at most two blocks per SM
         const int need = std::max((H.N + kMoveThreads - 1) / kMoveThreads, (H.S + kMoveThreads - 1) / kMoveThreads);
@@ -1268,6 +1308,25 @@ int batch_build_graph(yamc_batch *b) {
 }
 
 // one step of every replica: replica i's stream holds positions [rng_off[i], n_rng[i]) at rng[i]
+// Bounds-checked builds: the index check word of a context after its kernels ran (YAMC_EBOUNDS
+// with the source line when an index was out of bounds; the word is cleared).  Normal builds
+// compile the checks out and return `status`.
+static int bounds_status(yamc_ctx *c, int status) {
+#ifdef YAMC_CHECKED
+    int line = 0;
+    CUDA_TRY(cudaMemcpyAsync(&line, c->d_check, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if (line) {
+        CUDA_TRY(cudaMemsetAsync(c->d_check, 0, sizeof(int), c->stream));
+        set_error("index out of bounds in the chain kernel at yamc_chain.cuh line " + std::to_string(line));
+        return YAMC_EBOUNDS;
+    }
+#else
+    (void)c;
+#endif
+    return status;
+}
+
 int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, const int64_t *n_rng,
                int64_t *cursors, int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log,
                int only_group = -1) {
@@ -1306,6 +1365,10 @@ int batch_step(yamc_batch *b, const float *const *rng, const int64_t *rng_off, c
             b->reps[i]->pos_valid = false;
             if (rs.status != YAMC_OK && (worst == YAMC_OK || worst == YAMC_ERNG_EXHAUSTED)) worst = rs.status;
         }
+    for (yamc_ctx *c : b->reps) {
+        const int bs = bounds_status(c, YAMC_OK);
+        if (bs != YAMC_OK) return bs;
+    }
     return worst;
 }
 
@@ -1367,6 +1430,7 @@ const char *yamc_error_string(int s) {
         case YAMC_ERNG_EXHAUSTED: return "random stream exhausted";
         case YAMC_ENAN: return "non-finite value";
         case YAMC_EOVERLAP_INIT: return "hard-core overlap in the initial configuration";
+        case YAMC_EBOUNDS: return "index out of bounds (bounds-checked build)";
         default: return "unknown status";
     }
 }
@@ -1388,7 +1452,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     const int N = H.N, M = H.M, S = H.S, nt = H.nt;
     if ((r = dalloc(&c->atom, N)) || (r = dalloc(&c->meta, N)) || (r = dalloc(&c->dhs, N)) || (r = dalloc(&c->mass, N)) ||
         (r = dalloc(&c->mol, M)) || (r = dalloc(&c->kvec, S)) || (r = dalloc(&c->kpack, S)) ||
-        (r = dalloc(&c->rho_f, (size_t)(1 + nt) * S)) || (r = dalloc(&c->ebeta, S)) ||
+        (r = dalloc(&c->rho_f, (size_t)(1 + nt) * S)) || (r = dalloc(&c->d_check, 1)) || (r = dalloc(&c->ebeta, S)) ||
         (r = dalloc(&c->ebeta_f, S)) || (r = dalloc(&c->ebetalj_f, (size_t)H.npair * S)) ||
         (r = dalloc(&c->ebetalj, (size_t)H.npair * S)) || (r = dalloc(&c->pair_index, nt * nt)) ||
         (r = dalloc(&c->lj_sig6, nt * nt)) || (r = dalloc(&c->lj_feps, nt * nt)) || (r = dalloc(&c->rho, (size_t)(1 + nt) * S)) ||
@@ -1397,8 +1461,9 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
         (r = dalloc(&c->d_sys, 1)) || (r = dalloc(&c->d_run, 1)) || (r = dalloc(&c->slot, N)) ||
         (r = dalloc(&c->atom_of, (size_t)N + 16)) || (r = dalloc(&c->spec, H.spec.size() / 4)))
         return r;
-    CUDA_TRY(cudaHostAlloc(&c->h_out, sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * CN_COUNT,
+    CUDA_TRY(cudaHostAlloc(&c->h_out, sizeof(double) * (kNV + SC_COUNT) + sizeof(long long) * (CN_COUNT + 1),
                            cudaHostAllocMapped));
+    move_pass_done(c) = 0;
     CUDA_TRY(cudaHostGetDevicePointer(reinterpret_cast<void **>(&c->d_hout), c->h_out, 0));
     // full-sum work split: atom-tile pairs of the real-space sum; atom slices of rho(k) so that
     // entry blocks x slices cover the SMs about twice
@@ -1461,7 +1526,8 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
     fill_dhs_types(H, D);
     D.xprob = 0.0;
     D.atom = c->atom; D.meta = c->meta; D.dhs = c->dhs; D.mass = c->mass; D.mol = c->mol; D.kvec = c->kvec;
-    D.kpack = c->kpack; D.rho_f = c->rho_f;
+    D.kpack = c->kpack; D.rho_f = c->rho_f; D.check = c->d_check;
+    CUDA_TRY(cudaMemsetAsync(c->d_check, 0, sizeof(int), c->stream));
     D.ebeta = c->ebeta; D.ebetalj = c->ebetalj; D.pair_index = c->pair_index; D.lj_sig6 = c->lj_sig6; D.lj_feps = c->lj_feps;
     D.ebeta_f = c->ebeta_f; D.ebetalj_f = c->ebetalj_f;
     D.rho = c->rho; D.scratch = c->scratch; D.freq_beg = c->freq_beg; D.freq_end = c->freq_end; D.scal = c->scal; D.cnt = c->cnt;
@@ -1476,6 +1542,7 @@ static int create_impl(yamc_ctx *c, const yamc_system *sys, const yamc_params *p
 }
 
 int yamc_create(const yamc_system *sys, const yamc_params *p, int32_t device, yamc_ctx **out) {
+    YAMC_RANGE("yamc_create");
     if (!out) return YAMC_EPARAMETER;
     *out = nullptr;
     yamc_ctx *c = new yamc_ctx();
@@ -1490,7 +1557,7 @@ int yamc_destroy(yamc_ctx *c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     void *ptrs[] = {c->atom, c->meta, c->mol, c->dhs, c->mass, c->ebeta, c->ebetalj, c->ebeta_f, c->ebetalj_f,
-                    c->lj_sig6, c->lj_feps, c->kvec, c->kpack, c->rho_f,
+                    c->lj_sig6, c->lj_feps, c->kvec, c->kpack, c->rho_f, c->d_check,
                     c->pair_index, c->rho, c->scratch, c->freq_beg, c->freq_end, c->scal, c->cnt, c->part, c->sums,
                     c->tpairs, c->rho_part, c->d_sys, c->d_run, c->d_rng, c->d_log, c->d_rows,
                     c->d_prof, c->spec, c->d_gx, c->d_gy, c->d_gz, c->d_fpart, c->rho_save, c->d_mpart,
@@ -1520,6 +1587,7 @@ int yamc_energies(yamc_ctx *c, double e[8]) {
 }
 
 int yamc_full_sums(yamc_ctx *c, double e[8]) {
+    YAMC_RANGE("yamc_full_sums");
     if (!c) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(c->device));
     int r = pull_state(c);
@@ -1604,7 +1672,7 @@ static int run_chain_impl(yamc_ctx *c, const float *d_rng, long long rng_off, lo
     *cursor = back.cursor;
     if (moves_done) *moves_done = back.moves_done;
     if (n_rows) *n_rows = back.n_rows;
-    return back.status;
+    return bounds_status(c, back.status);
 }
 
 int yamc_set_refresh(yamc_ctx *c, int64_t accepted_moves) {
@@ -1629,6 +1697,7 @@ int yamc_refresh_count(yamc_ctx *c, int64_t *count) {
 
 int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_t *cursor, int64_t n_moves,
                           int64_t *moves_done, yamc_move_record *d_log, double *d_rows, int32_t max_rows, int32_t *n_rows) {
+    YAMC_RANGE("yamc_run_chain_device");
     if (!c || !d_rng || !cursor || n_moves < 0) return YAMC_EPARAMETER;
     if (c->H.p.pressure_step_multiplier > 0 || c->H.xchange_probability > 0) {
         set_error("NPT volume cycles or exchange steps are on: they run through yamc_run_mc");
@@ -1640,6 +1709,7 @@ int yamc_run_chain_device(yamc_ctx *c, const float *d_rng, int64_t n_rng, int64_
 
 int yamc_run_chain(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_moves, int64_t *moves_done,
                    yamc_move_record *log, double *rows, int32_t max_rows, int32_t *n_rows) {
+    YAMC_RANGE("yamc_run_chain");
     if (!c || !rng || !cursor || n_moves < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
     if (c->H.p.pressure_step_multiplier > 0 || c->H.xchange_probability > 0) {
         set_error("NPT volume cycles or exchange steps are on: they run through yamc_run_mc");
@@ -2084,6 +2154,7 @@ int yamc_set_xchange_weights(yamc_ctx *c, const double *w) {
 }
 
 int yamc_xchange_eval(yamc_ctx *c, int32_t imol1, int32_t imol2, double du[4], int32_t *overlap) {
+    YAMC_RANGE("yamc_xchange_eval");
     if (!c || !du || !overlap || imol1 < 1 || imol2 < 1 || imol1 > c->H.M || imol2 > c->H.M || imol1 == imol2)
         return YAMC_EPARAMETER;
     if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
@@ -2096,6 +2167,7 @@ int yamc_xchange_eval(yamc_ctx *c, int32_t imol1, int32_t imol2, double du[4], i
 }
 
 int yamc_xchange_commit(yamc_ctx *c, int32_t accepted) {
+    YAMC_RANGE("yamc_xchange_commit");
     if (!c) return YAMC_EPARAMETER;
     if (!c->xch_stage) { set_error("no exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
@@ -2237,6 +2309,7 @@ int yamc_rdf_result(yamc_rdf *h, double *g, double *counts, int32_t *n_frames) {
 }
 
 int yamc_volume_eval(yamc_ctx *c, double new_box_length, double *du, int32_t *overlap) {
+    YAMC_RANGE("yamc_volume_eval");
     if (!c || !du || !overlap || !(new_box_length > 0)) return YAMC_EPARAMETER;
     if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
     if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
@@ -2248,6 +2321,7 @@ int yamc_volume_eval(yamc_ctx *c, double new_box_length, double *du, int32_t *ov
 }
 
 int yamc_volume_commit(yamc_ctx *c, int32_t accepted) {
+    YAMC_RANGE("yamc_volume_commit");
     if (!c) return YAMC_EPARAMETER;
     if (!c->vol_stage) { set_error("no volume step is pending"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
@@ -2278,6 +2352,7 @@ static void host_cycle_end(yamc_ctx *c, double *rows, int32_t max_rows, int32_t 
 int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, int64_t n_cycles, int64_t *cycles_done,
                 yamc_move_record *log, int64_t max_log, int64_t *n_log, yamc_volume_record *vlog, int64_t max_vlog,
                 int64_t *n_vlog, double *rows, int32_t max_rows, int32_t *n_rows) {
+    YAMC_RANGE("yamc_run_mc");
     if (!c || !rng || !cursor || n_cycles < 0 || *cursor < 0 || *cursor > n_rng) return YAMC_EPARAMETER;
     if (c->in_batch) { set_error("a batch replica runs NVT moves only (volume and exchange steps need a context of its own)"); return YAMC_EWRONG_FUNCTION; }
     if (c->api_stage || c->vol_stage || c->xch_stage) { set_error("a move, volume or exchange step is pending"); return YAMC_EWRONG_FUNCTION; }
@@ -2421,6 +2496,7 @@ int yamc_run_mc(yamc_ctx *c, const float *rng, int64_t n_rng, int64_t *cursor, i
 // ---------------------------------------------------------------- per-move drop-in
 
 int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
+    YAMC_RANGE("yamc_move_old");
     if (!c || imol < 1 || imol > c->H.M) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(c->device));
     if (c->H.nt == 4 && is_mixed(c)) { set_error("the mixed form takes up to 3 LJ types"); return YAMC_ELIMITS; }
@@ -2430,7 +2506,7 @@ int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
     in.imol = imol;
     if ((r = launch_move_pass(c, in, false))) return r;
     // the kernel writes its outputs, the scalars and the counters straight into mapped host memory
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if ((r = wait_move_pass(c, in.seq))) return r;
     const double *out = c->h_out;
     std::memcpy(c->sc, out + kNV, sizeof(double) * SC_COUNT);
     std::memcpy(c->cnt_h, out + kNV + SC_COUNT, sizeof(long long) * CN_COUNT);
@@ -2457,6 +2533,7 @@ int yamc_move_old(yamc_ctx *c, int32_t imol, double f[3], double tau[3]) {
 
 int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn, const double *zn, double du[4],
                    int32_t *overlap, double f[3], double tau[3]) {
+    YAMC_RANGE("yamc_move_eval");
     if (!c || !xn || !yn || !zn) return YAMC_EPARAMETER;
     if (c->api_stage != 1 || imol != c->api_imol) { set_error("yamc_move_eval must follow yamc_move_old for the same molecule"); return YAMC_EWRONG_FUNCTION; }
     CUDA_TRY(cudaSetDevice(c->device));
@@ -2467,7 +2544,7 @@ int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn
     for (int a = 0; a < na; ++a) { in.x[a] = xn[a]; in.y[a] = yn[a]; in.z[a] = zn[a]; }
     int r = launch_move_pass(c, in, true);
     if (r) return r;
-    CUDA_TRY(cudaStreamSynchronize(c->stream));
+    if ((r = wait_move_pass(c, in.seq))) return r;
     const double *out = c->h_out;
     for (int v = 0; v < kNV; ++v) c->api_new[v] = out[v];
     for (int a = 0; a < na; ++a) { c->api_xn[a] = xn[a]; c->api_yn[a] = yn[a]; c->api_zn[a] = zn[a]; }
@@ -2513,6 +2590,7 @@ int yamc_move_eval(yamc_ctx *c, int32_t imol, const double *xn, const double *yn
 }
 
 int yamc_move_commit(yamc_ctx *c, int32_t accepted) {
+    YAMC_RANGE("yamc_move_commit");
     if (!c) return YAMC_EPARAMETER;
     if (!accepted) { c->api_stage = 0; return YAMC_OK; }
     if (c->api_stage != 2) { set_error("yamc_move_commit(accepted) must follow a successful yamc_move_eval"); return YAMC_EWRONG_FUNCTION; }
@@ -2644,6 +2722,7 @@ int yamc_batch_replica(yamc_batch *b, int32_t i, yamc_ctx **ctx) {
 
 int yamc_batch_run_device(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng, int64_t *cursors,
                           int64_t n_moves, int64_t *moves_done, int32_t *status, yamc_move_record *d_log) {
+    YAMC_RANGE("yamc_batch_run_device");
     if (!b || !d_rng || !n_rng || !cursors || n_moves < 0) return YAMC_EPARAMETER;
     const size_t R = b->reps.size();
     std::vector<int64_t> off(R, 0);
@@ -2658,6 +2737,7 @@ int yamc_batch_run_device(yamc_batch *b, const float *const *d_rng, const int64_
 
 int yamc_batch_run(yamc_batch *b, const float *const *rng, const int64_t *n_rng, int64_t *cursors, int64_t n_moves,
                    int64_t *moves_done, int32_t *status, yamc_move_record *log) {
+    YAMC_RANGE("yamc_batch_run");
     if (!b || !rng || !n_rng || !cursors || n_moves < 0) return YAMC_EPARAMETER;
     const size_t R = b->reps.size();
     std::vector<size_t> base(R);
@@ -2755,6 +2835,7 @@ int yamc_batch_last_kernel_ms(yamc_batch *b, double *ms) {
 
 int yamc_batch_tune(yamc_batch *b, const float *const *d_rng, const int64_t *n_rng, const int64_t *cursors,
                     int64_t n_moves, double *best_moves_per_s) {
+    YAMC_RANGE("yamc_batch_tune");
     if (!b || !d_rng || !n_rng || !cursors || n_moves < 1) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(b->device));
     const size_t R = b->reps.size();
@@ -2880,6 +2961,7 @@ int yamc_batch_group_launch(yamc_batch *b, int32_t group, int32_t out[7]) {
 // ---------------------------------------------------------------- adjoint forces
 
 int yamc_forces(yamc_ctx *c, double *fx, double *fy, double *fz, double *mol_f, double *mol_tau) {
+    YAMC_RANGE("yamc_forces");
     if (!c) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(c->device));
     HostSystem &H = c->H;
@@ -2996,6 +3078,7 @@ int yamc_state_size(yamc_ctx *c, int64_t *bytes) {
 }
 
 int yamc_save_state(yamc_ctx *c, int64_t cursor, void *buf, int64_t bytes) {
+    YAMC_RANGE("yamc_save_state");
     if (!c || !buf) return YAMC_EPARAMETER;
     HostSystem &H = c->H;
     const size_t need = state_bytes(H);
@@ -3029,6 +3112,7 @@ int yamc_save_state(yamc_ctx *c, int64_t cursor, void *buf, int64_t bytes) {
 }
 
 int yamc_load_state(yamc_ctx *c, const void *buf, int64_t bytes, int64_t *cursor) {
+    YAMC_RANGE("yamc_load_state");
     if (!c || !buf) return YAMC_EPARAMETER;
     HostSystem &H = c->H;
     const size_t need = state_bytes(H);
@@ -3072,6 +3156,7 @@ int yamc_load_state(yamc_ctx *c, const void *buf, int64_t bytes, int64_t *cursor
 }
 
 int yamc_set_positions(yamc_ctx *c, const double *x, const double *y, const double *z, double e[8]) {
+    YAMC_RANGE("yamc_set_positions");
     if (!c || !x || !y || !z) return YAMC_EPARAMETER;
     CUDA_TRY(cudaSetDevice(c->device));
     HostSystem &H = c->H;
@@ -3091,6 +3176,50 @@ int yamc_set_positions(yamc_ctx *c, const double *x, const double *y, const doub
     if ((r = pull_state(c)) || (r = full_sums(c))) return r;
     CUDA_TRY(cudaStreamSynchronize(c->stream));
     if (e) energies_from(c->sc, H.p.kext, e);
+    return YAMC_OK;
+}
+
+namespace {
+// one checked read of arr[index] (arr holds 4 values): the index check of the bounds-checked
+// builds on its own, so a test can see it record an out-of-bounds index and keep the access in bounds
+__global__ void k_bounds_selftest(long long index, long long size, const double *arr, double *out, int *check) {
+    out[0] = arr[checked_ix(index, size < 4 ? size : 4, __LINE__, check)];
+}
+}  // namespace
+
+int yamc_checked_build(int32_t *checked) {
+    if (!checked) return YAMC_EPARAMETER;
+#ifdef YAMC_CHECKED
+    *checked = 1;
+#else
+    *checked = 0;
+#endif
+    return YAMC_OK;
+}
+
+int yamc_bounds_check_selftest(int32_t device, int64_t index, int64_t size, double *value, int32_t *line) {
+    if (!value || !line) return YAMC_EPARAMETER;
+    CUDA_TRY(cudaSetDevice(device));
+    const double h[4] = {10.0, 11.0, 12.0, 13.0};
+    double *d = nullptr;
+    int *chk = nullptr;
+    CUDA_TRY(cudaMalloc(&d, sizeof(double) * 5));
+    cudaError_t e = cudaMalloc(&chk, sizeof(int));
+    if (e == cudaSuccess) e = cudaMemcpy(d, h, sizeof h, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(chk, 0, sizeof(int));
+    if (e == cudaSuccess) {
+        k_bounds_selftest<<<1, 1>>>((long long)index, (long long)size, d, d + 4, chk);
+        e = cudaGetLastError();
+    }
+    int l = 0;
+    double v = 0.0;
+    if (e == cudaSuccess) e = cudaMemcpy(&v, d + 4, sizeof(double), cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(&l, chk, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (chk) cudaFree(chk);
+    if (e != cudaSuccess) { set_error(cudaGetErrorString(e)); return YAMC_ECUDA; }
+    *value = v;
+    *line = l;
     return YAMC_OK;
 }
 
