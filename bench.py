@@ -266,8 +266,8 @@ def single_chain_rate(files, local, precision, moves, per_move, reps=2, extra=""
 
 
 def precision_errors(files, local, n_chk=1500, n_force=200, seed=4242):
-    """The mixed form against FP64 on one system (north_star (2): dE, force and total-energy
-    error for every result): a mixed and an FP64 chain on the same random stream, compared move
+    """The mixed form against FP64 on one system (its dE, force and total-energy errors, stated
+    for every result): a mixed and an FP64 chain on the same random stream, compared move
     by move up to their first different decision; the molecular forces of the force-bias path
     (yamc_move_old, movemc Steps 3-4) of both forms on the same configuration; the mixed chain's
     running total energy against an FP64 recomputation of its own configuration."""

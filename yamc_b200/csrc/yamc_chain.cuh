@@ -1216,7 +1216,16 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
     const int G = A.G;
     const int rank = G > 1 ? (int)cluster.block_rank() : 0;
     const int rep = blockIdx.x / G;
-    const DevSys D = A.sys[rep];
+    // the system's parameters and array pointers in shared memory: every thread reads them from
+    // there (a per-thread copy would live in local memory, which the staged atoms leave little L1 for)
+    __shared__ DevSys D_s;
+    {
+        const int *src = reinterpret_cast<const int *>(A.sys + rep);
+        int *dst = reinterpret_cast<int *>(&D_s);
+        for (int i = threadIdx.x; i < (int)(sizeof(DevSys) / sizeof(int)); i += blockDim.x) dst[i] = src[i];
+        __syncthreads();
+    }
+    const DevSys &D = D_s;
     RunSlot *run = A.run + rep;
     const int B = blockDim.x;
     const int tid = threadIdx.x;
