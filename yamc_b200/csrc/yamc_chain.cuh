@@ -1074,16 +1074,11 @@ __device__ inline void propose(const DevSys &D, Cand &C, RngReader &rng, const d
     mcm_init_old(m, F, T);
     mcm_choose_displacement(m, rng, D.xlf, D.dr);
     if (!rng.out) mcm_choose_rotation(m, rng, D.xlc, D.d_angle);
-    double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
-#pragma unroll
-    for (int a = 0; a < kMaxA; ++a) {
-        const Slot &o = C.slot[a < na ? na + a : na];
-        xo[a] = o.x; yo[a] = o.y; zo[a] = o.z;
-    }
-    place_molecule(m, na, xo, yo, zo, C.mass, xn, yn, zn);
-#pragma unroll
-    for (int a = 0; a < kMaxA; ++a)
-        if (a < na) { C.slot[a].x = xn[a]; C.slot[a].y = yn[a]; C.slot[a].z = zn[a]; }
+    // old positions from slots [na, 2 na), new ones into [0, na): no overlap
+    const Slot *os = C.slot + na;
+    Slot *ns = C.slot;
+    place_molecule_f(m, na, [&](int i, int d) { return d == 0 ? os[i].x : (d == 1 ? os[i].y : os[i].z); }, C.mass,
+                     [&](int i, double x, double y, double z) { ns[i].x = x; ns[i].y = y; ns[i].z = z; });
 }
 
 // The mixed form's FP64 recomputation of rho(k) (RhoSquared_addAtoms, RhoSquared.f90:188-243)
@@ -1400,16 +1395,10 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                 if (tid == 0 || tid == 32) {
                     const Cand &C = sh.cand[sh.icur];
                     double F[3], T[3];
-                    {
-                        double xo[kMaxA], yo[kMaxA], zo[kMaxA], fx[kMaxA], fy[kMaxA], fz[kMaxA];
-#pragma unroll
-                        for (int a = 0; a < kMaxA; ++a) {
-                            const int s0 = a < na0 ? na0 + a : na0;
-                            xo[a] = C.slot[s0].x; yo[a] = C.slot[s0].y; zo[a] = C.slot[s0].z;
-                            fx[a] = sh.fold[3 * a]; fy[a] = sh.fold[3 * a + 1]; fz[a] = sh.fold[3 * a + 2];
-                        }
-                        mol_force_torque(na0, xo, yo, zo, C.mass, fx, fy, fz, F, T);
-                    }
+                    // (old positions and forces read where they are, in shared memory)
+                    const Slot *os = C.slot + na0;
+                    mol_force_torque_f(na0, [&](int i, int d) { return d == 0 ? os[i].x : (d == 1 ? os[i].y : os[i].z); },
+                                       C.mass, [&](int i, int d) { return sh.fold[3 * i + d]; }, F, T);
                     RngReader rng = make_reader(X, sh, C.cur_prop);
                     if (tid == 0) {
                         MoveState &m = sh.cand[sh.icur].mv;
@@ -1449,16 +1438,11 @@ __global__ void __launch_bounds__(EPT < 0 ? kChainMaxThreadsWide : kChainMaxThre
                         C.valid = 0;
                         sh.abort = kAbortStream;
                     } else {
-                        double xo[kMaxA], yo[kMaxA], zo[kMaxA], xn[kMaxA], yn[kMaxA], zn[kMaxA];
-#pragma unroll
-                        for (int a = 0; a < kMaxA; ++a) {
-                            const Slot &o = C.slot[a < na0 ? na0 + a : na0];
-                            xo[a] = o.x; yo[a] = o.y; zo[a] = o.z;
-                        }
-                        place_molecule(m, na0, xo, yo, zo, C.mass, xn, yn, zn);
-#pragma unroll
-                        for (int a = 0; a < kMaxA; ++a)
-                            if (a < na0) { C.slot[a].x = xn[a]; C.slot[a].y = yn[a]; C.slot[a].z = zn[a]; }
+                        // old positions from slots [na0, 2 na0), new ones into [0, na0): no overlap
+                        const Slot *os = C.slot + na0;
+                        Slot *ns = C.slot;
+                        place_molecule_f(m, na0, [&](int i, int d) { return d == 0 ? os[i].x : (d == 1 ? os[i].y : os[i].z); },
+                                         C.mass, [&](int i, double x, double y, double z) { ns[i].x = x; ns[i].y = y; ns[i].z = z; });
                         C.cur_prop = cur;
                     }
                 }

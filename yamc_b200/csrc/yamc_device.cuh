@@ -602,13 +602,14 @@ __host__ __device__ inline int mcm_accept(const MoveState &m, double dutot, doub
 // movemc Step 5 (MC.f90:1031-1067): new atom positions from the proposal.
 // Centre of mass of the old atoms, wrapped new centre (ANINT), rotation of the
 // atoms about the centre with fill_rot_matrix/rotate_vect (geometry.f90:103-168).
-__host__ __device__ inline void place_molecule(const MoveState &m, int na, const double *xo, const double *yo,
-                                               const double *zo, const double *mass, double *xn, double *yn,
-                                               double *zn) {
+// (generic over where the positions come from and go to: pos(i, d) is coordinate d of old atom i,
+// put(i, x, y, z) stores new atom i; the arithmetic is the same for every caller)
+template <class Pos, class Put>
+__host__ __device__ inline void place_molecule_f(const MoveState &m, int na, Pos pos, const double *mass, Put put) {
     double sx = 0, sy = 0, sz = 0, tm = 0;
 #pragma unroll
     for (int i = 0; i < kMaxA; ++i)
-        if (i < na) { sx = sx + mass[i] * xo[i]; sy = sy + mass[i] * yo[i]; sz = sz + mass[i] * zo[i]; tm = tm + mass[i]; }
+        if (i < na) { sx = sx + mass[i] * pos(i, 0); sy = sy + mass[i] * pos(i, 1); sz = sz + mass[i] * pos(i, 2); tm = tm + mass[i]; }
     const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
     const double xcn = xc + m.deltx - round(xc + m.deltx);
     const double ycn = yc + m.delty - round(yc + m.delty);
@@ -627,36 +628,47 @@ __host__ __device__ inline void place_molecule(const MoveState &m, int na, const
 #pragma unroll
         for (int i = 0; i < kMaxA; ++i)
             if (i < na) {
-                const double xr = xo[i] - xc, yr = yo[i] - yc, zr = zo[i] - zc;
-                xn[i] = (rxx * xr + rxy * yr + rxz * zr) + xcn;
-                yn[i] = (ryx * xr + ryy * yr + ryz * zr) + ycn;
-                zn[i] = (rzx * xr + rzy * yr + rzz * zr) + zcn;
+                const double xr = pos(i, 0) - xc, yr = pos(i, 1) - yc, zr = pos(i, 2) - zc;
+                put(i, (rxx * xr + rxy * yr + rxz * zr) + xcn, (ryx * xr + ryy * yr + ryz * zr) + ycn,
+                    (rzx * xr + rzy * yr + rzz * zr) + zcn);
             }
     } else {
-        xn[0] = xcn; yn[0] = ycn; zn[0] = zcn;
+        put(0, xcn, ycn, zcn);
     }
+}
+__host__ __device__ inline void place_molecule(const MoveState &m, int na, const double *xo, const double *yo,
+                                               const double *zo, const double *mass, double *xn, double *yn,
+                                               double *zn) {
+    place_molecule_f(m, na, [&](int i, int d) { return d == 0 ? xo[i] : (d == 1 ? yo[i] : zo[i]); }, mass,
+                     [&](int i, double x, double y, double z) { xn[i] = x; yn[i] = y; zn[i] = z; });
 }
 
 // molecular force and torque about the centre of mass (MC.f90:1002-1025)
-__host__ __device__ inline void mol_force_torque(int na, const double *x, const double *y, const double *z,
-                                                 const double *mass, const double *fx, const double *fy,
-                                                 const double *fz, double F[3], double T[3]) {
+// (generic: pos(i, d) and frc(i, d) are coordinate d of atom i's position and force)
+template <class Pos, class Frc>
+__host__ __device__ inline void mol_force_torque_f(int na, Pos pos, const double *mass, Frc frc, double F[3], double T[3]) {
     double sx = 0, sy = 0, sz = 0, tm = 0;
 #pragma unroll
     for (int i = 0; i < kMaxA; ++i)
-        if (i < na) { sx = sx + mass[i] * x[i]; sy = sy + mass[i] * y[i]; sz = sz + mass[i] * z[i]; tm = tm + mass[i]; }
+        if (i < na) { sx = sx + mass[i] * pos(i, 0); sy = sy + mass[i] * pos(i, 1); sz = sz + mass[i] * pos(i, 2); tm = tm + mass[i]; }
     const double xc = sx / tm, yc = sy / tm, zc = sz / tm;
     F[0] = F[1] = F[2] = 0; T[0] = T[1] = T[2] = 0;
 #pragma unroll
     for (int i = 0; i < kMaxA; ++i)
-        if (i < na) { F[0] = F[0] + fx[i]; F[1] = F[1] + fy[i]; F[2] = F[2] + fz[i]; }
+        if (i < na) { F[0] = F[0] + frc(i, 0); F[1] = F[1] + frc(i, 1); F[2] = F[2] + frc(i, 2); }
 #pragma unroll
     for (int i = 0; i < kMaxA; ++i)
         if (i < na) {
             double tx, ty, tz;
-            cross(x[i] - xc, y[i] - yc, z[i] - zc, fx[i], fy[i], fz[i], tx, ty, tz);
+            cross(pos(i, 0) - xc, pos(i, 1) - yc, pos(i, 2) - zc, frc(i, 0), frc(i, 1), frc(i, 2), tx, ty, tz);
             T[0] = T[0] + tx; T[1] = T[1] + ty; T[2] = T[2] + tz;
         }
+}
+__host__ __device__ inline void mol_force_torque(int na, const double *x, const double *y, const double *z,
+                                                 const double *mass, const double *fx, const double *fy,
+                                                 const double *fz, double F[3], double T[3]) {
+    mol_force_torque_f(na, [&](int i, int d) { return d == 0 ? x[i] : (d == 1 ? y[i] : z[i]); }, mass,
+                       [&](int i, int d) { return d == 0 ? fx[i] : (d == 1 ? fy[i] : fz[i]); }, F, T);
 }
 
 }  // namespace yamc
