@@ -48,9 +48,9 @@ METRIC = "MC trial moves/s (SPC/E+NaCl Ewald); mixed vs FP64 GPU at |ΔE err|≤
 
 # DRAM bytes per move of the chain kernel in the timed shape, by workload, from one ncu capture
 # (dram__bytes_read.sum + dram__bytes_write.sum of one launch / its moves; profiles/), used for
-# roofline.traffic: nacl1m mixed streamed 2 x 384 threads, 1,000 moves: 1.094 MB; nacl4k mixed
+# roofline.traffic: nacl1m mixed streamed 2 x 384 threads, 1,000 moves: 1.102 MB; nacl4k mixed
 # force-biased streamed 3 x 384 threads, one chain, 400 moves: 2.088 MB
-TRAFFIC_PER_MOVE = {"nacl1m": 1094.0, "nacl4k": 5222.0}
+TRAFFIC_PER_MOVE = {"nacl1m": 1102.0, "nacl4k": 5222.0}
 
 
 def dist_env():
